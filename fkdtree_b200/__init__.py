@@ -1,0 +1,204 @@
+"""fkdtree_b200 -- the FKDTree flat kd-tree built and searched on B200 (sm_100a).
+
+Python mirror of the reference's ``FKDTree<T, dim>`` interface (FKDTree.h:6-22,
+FKDTree_cpu.h:16-327) over the C ABI of include/fkdtree_b200.h:
+
+    tree = FKDTree(coords, ids)          # FKDTree_CPU(points) -- coords (dim, n) float32
+    tree.build()                         # FKDTree_CPU::build
+    tree.search_in_the_box(lo, hi)       # ids, in the reference's emission order
+    tree.search_in_the_box_BFS(lo, hi)   # same list (the BFS variant emits the same order)
+    tree.search_in_the_box_branchless(lo, hi)
+    tree.search_in_the_box_recursive(lo, hi)   # same set; order: ascending heap index
+    tree.search_in_the_box_multiple(mins, maxs)  # per-box counts (OpenCL backend semantics)
+    tree.getDimensionVector(d), tree.getIdVector()
+
+Batch entry points (``search_boxes``, ``count_boxes``, ``digest_boxes``) take
+(dim, q) SoA boxes.  Inputs may be numpy arrays (host) or CUDA torch tensors
+(device); everything runs on the GPU and there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _capi
+from ._capi import FKDError, MEM_DEVICE, MEM_HOST, FLAG_ASYNC, check, lib
+
+__all__ = ["FKDTree", "FKDError", "lib", "version"]
+
+
+def version() -> str:
+    return lib().fkd_version().decode()
+
+
+def _is_torch(x) -> bool:
+    return type(x).__module__.startswith("torch")
+
+
+def _ptr(x):
+    if x is None:
+        return None
+    if _is_torch(x):
+        return C.c_void_p(x.data_ptr())
+    return x.ctypes.data_as(C.c_void_p)
+
+
+def _host_f32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _stream_handle(stream):
+    if stream is None:
+        return None
+    if hasattr(stream, "cuda_stream"):
+        return C.c_void_p(stream.cuda_stream)
+    return C.c_void_p(int(stream))
+
+
+class FKDTree:
+    """The B200 tree.  ``coords`` is (dim, n) float32 SoA (numpy or CUDA
+    tensor), ``ids`` (n,) uint32 (int32 tensors are reinterpreted); when ids are
+    omitted they are 0..n-1, as in the reference drivers (main.cpp:182)."""
+
+    def __init__(self, coords, ids=None, dim: int | None = None, stream=None, flags: int = 0):
+        self._lib = lib()
+        self.device = _is_torch(coords)
+        if self.device:
+            import torch
+            coords = coords.contiguous()
+            if coords.dtype != torch.float32:
+                raise TypeError("coords must be float32")
+            if ids is None:
+                ids = torch.arange(coords.shape[1], dtype=torch.int32, device=coords.device)
+            ids = ids.contiguous()
+            if ids.dtype not in (torch.int32, torch.uint32):
+                raise TypeError("ids must be a 32-bit integer tensor")
+        else:
+            coords = _host_f32(coords)
+            if coords.ndim == 1:
+                coords = coords.reshape(1, -1)
+            ids = np.arange(coords.shape[1], dtype=np.uint32) if ids is None else np.ascontiguousarray(ids, dtype=np.uint32)
+        self.dim = int(coords.shape[0]) if dim is None else int(dim)
+        self.n = int(coords.shape[1])
+        if ids.shape[0] != self.n:
+            raise ValueError("ids and coords disagree on the number of points")
+        self._coords, self._ids = coords, ids
+        h = C.c_void_p()
+        check(self._lib.fkd_create(self.dim, flags, _stream_handle(stream), C.byref(h)))
+        self._h = h
+        self._tables = None
+
+    # -- FKDTree_CPU::build (FKDTree_cpu.h:221-277)
+    def build(self) -> "FKDTree":
+        mem = MEM_DEVICE if self.device else MEM_HOST
+        check(self._lib.fkd_build(self._h, _ptr(self._coords), _ptr(self._ids), self.n, mem))
+        self._tables = None
+        return self
+
+    # -- getDimensionVector / getIdVector (FKDTree_cpu.h:209-213)
+    def tables(self) -> tuple[np.ndarray, np.ndarray]:
+        if self._tables is None:
+            tab = np.empty((self.dim, self.n), dtype=np.float32)
+            tid = np.empty(self.n, dtype=np.uint32)
+            check(self._lib.fkd_get_tables(self._h, _ptr(tab), _ptr(tid), MEM_HOST))
+            self._tables = (tab, tid)
+        return self._tables
+
+    def getDimensionVector(self, dimension: int) -> np.ndarray:
+        tab, _ = self.tables()
+        return tab[dimension] if 0 <= dimension < self.dim else tab[0]  # FKDTree_cpu.h:210-211
+
+    def getIdVector(self) -> np.ndarray:
+        return self.tables()[1]
+
+    # -- batched searches over (dim, q) SoA boxes
+    def _boxes(self, mins, maxs):
+        if _is_torch(mins):
+            return mins.contiguous(), maxs.contiguous(), MEM_DEVICE, int(mins.shape[-1])
+        mins = _host_f32(mins).reshape(self.dim, -1)
+        maxs = _host_f32(maxs).reshape(self.dim, -1)
+        return mins, maxs, MEM_HOST, int(mins.shape[1])
+
+    def count_boxes(self, mins, maxs) -> np.ndarray:
+        mins, maxs, mem, q = self._boxes(mins, maxs)
+        if mem == MEM_DEVICE:
+            import torch
+            counts = torch.empty(q, dtype=torch.int32, device=mins.device)
+        else:
+            counts = np.empty(q, dtype=np.uint32)
+        check(self._lib.fkd_search_count(self._h, _ptr(mins), _ptr(maxs), q, _ptr(counts), mem))
+        return counts
+
+    def search_boxes(self, mins, maxs, ordered: bool = True, capacity: int | None = None):
+        """Returns (offsets (q+1,) uint64, ids) with the ids of box j in
+        ids[offsets[j]:offsets[j+1]]; ``ordered`` gives the reference's
+        emission order (ascending heap index)."""
+        mins, maxs, mem, q = self._boxes(mins, maxs)
+        total = C.c_uint64(0)
+        if mem == MEM_DEVICE:
+            import torch
+            counts = self.count_boxes(mins, maxs)
+            offsets = torch.zeros(q + 1, dtype=torch.int64, device=mins.device)
+            offsets[1:] = torch.cumsum(counts.to(torch.int64), 0)
+            tot = int(offsets[-1].item())
+            out = torch.empty(max(tot, 1), dtype=torch.int32, device=mins.device)
+            check(self._lib.fkd_search_write(self._h, _ptr(mins), _ptr(maxs), q, _ptr(offsets), _ptr(out),
+                                             int(ordered), mem))
+            return offsets, out[:tot]
+        offsets = np.empty(q + 1, dtype=np.uint64)
+        if capacity is None:
+            counts = self.count_boxes(mins, maxs)
+            capacity = int(counts.sum(dtype=np.uint64))
+        out = np.empty(max(capacity, 1), dtype=np.uint32)
+        check(self._lib.fkd_search(self._h, _ptr(mins), _ptr(maxs), q, _ptr(offsets), _ptr(out), capacity,
+                                   C.byref(total), int(ordered), mem))
+        return offsets, out[:total.value]
+
+    def digest_boxes(self, mins, maxs):
+        mins, maxs, mem, q = self._boxes(mins, maxs)
+        if mem == MEM_DEVICE:
+            import torch
+            counts = torch.empty(q, dtype=torch.int32, device=mins.device)
+            dig = torch.empty(q, dtype=torch.int64, device=mins.device)
+        else:
+            counts = np.empty(q, dtype=np.uint32)
+            dig = np.empty(q, dtype=np.uint64)
+        check(self._lib.fkd_search_digest(self._h, _ptr(mins), _ptr(maxs), q, _ptr(counts), _ptr(dig), mem))
+        return counts, dig
+
+    # -- single-box searches, the reference's per-query API
+    def _one(self, minPoint, maxPoint, ordered=True) -> np.ndarray:
+        lo = _host_f32(minPoint).reshape(self.dim, 1)
+        hi = _host_f32(maxPoint).reshape(self.dim, 1)
+        _, ids = self.search_boxes(lo, hi, ordered=ordered)
+        return ids
+
+    def search_in_the_box(self, minPoint, maxPoint) -> np.ndarray:  # FKDTree_cpu.h:123-169
+        return self._one(minPoint, maxPoint)
+
+    def search_in_the_box_BFS(self, minPoint, maxPoint) -> np.ndarray:  # FKDTree_cpu.h:72-121
+        return self._one(minPoint, maxPoint)
+
+    def search_in_the_box_branchless(self, minPoint, maxPoint) -> np.ndarray:  # FKDTree_cpu.h:25-70
+        return self._one(minPoint, maxPoint)
+
+    def search_in_the_box_recursive(self, minPoint, maxPoint) -> np.ndarray:  # FKDTree_cpu.h:171-207
+        return self._one(minPoint, maxPoint)
+
+    def search_in_the_box_multiple(self, minPoints, maxPoints) -> np.ndarray:
+        """Per-box result counts, the OpenCL backend's semantics
+        (FKDTree_opencl.h:123-164); the CPU backend's stub returns nothing
+        (FKDTree_cpu.h:215-219)."""
+        return self.count_boxes(minPoints, maxPoints)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.fkd_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,440 @@
+// fkd_capi.cu -- the C ABI (include/fkdtree_b200.h) over the build and search
+// kernels: handle lifetime, device buffers, host staging and error latching.
+#include <stdio.h>
+#include <string.h>
+
+#include <new>
+#include <string>
+
+#include "../../include/fkdtree_b200.h"
+#include "fkd_internal.h"
+
+using namespace fkd;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+fkd_status fail(fkd_status s, const std::string& msg) {
+  g_last_error = msg;
+  return s;
+}
+
+#define FKD_CUDA(call)                                                                                    \
+  do {                                                                                                    \
+    cudaError_t e_ = (call);                                                                              \
+    if (e_ != cudaSuccess)                                                                                \
+      return fail(e_ == cudaErrorMemoryAllocation ? FKD_ERR_NOMEM : FKD_ERR_CUDA,                         \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                                    \
+  } while (0)
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  cudaError_t ensure(size_t want) {
+    if (want <= bytes && p) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    if (want == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e == cudaSuccess) bytes = want;
+    return e;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  template <class T>
+  T* as() const {
+    return (T*)p;
+  }
+};
+
+}  // namespace
+
+struct fkd_tree_s {
+  int dim = 3;
+  uint32_t flags = 0;
+  cudaStream_t stream = nullptr;
+  int device = 0;
+  uint64_t n = 0;
+  bool built = false;
+  DevBuf nodes, ids, work0, work1, sel, ghist, err, qctr;
+  DevBuf qlo, qhi, counts, offsets, partials, out, tmp, digests;
+  uint32_t* herr = nullptr;  // pinned mirror of err
+
+  ~fkd_tree_s() {
+    DevBuf* all[] = {&nodes, &ids, &work0, &work1, &sel, &ghist, &err, &qctr,
+                     &qlo, &qhi, &counts, &offsets, &partials, &out, &tmp, &digests};
+    for (DevBuf* b : all) b->release();
+    if (herr) cudaFreeHost(herr);
+  }
+};
+
+namespace {
+
+fkd_status check_err_word(fkd_tree h, const char* what) {
+  FKD_CUDA(cudaMemcpyAsync(h->herr, h->err.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+  FKD_CUDA(cudaStreamSynchronize(h->stream));
+  const uint32_t e = *h->herr;
+  if (e == 0) return FKD_OK;
+  char buf[160];
+  if (e & ERRB_NAN) {
+    snprintf(buf, sizeof buf, "%s: input coordinates contain NaN", what);
+    return fail(FKD_ERR_NAN, buf);
+  }
+  if (e & ERRB_CAPACITY) {
+    snprintf(buf, sizeof buf, "%s: a result or frontier capacity was exceeded", what);
+    return fail(FKD_ERR_CAPACITY, buf);
+  }
+  if (e & ERRB_TIMEOUT) {
+    snprintf(buf, sizeof buf, "%s: a bounded device wait gave up", what);
+    return fail(FKD_ERR_TIMEOUT, buf);
+  }
+  snprintf(buf, sizeof buf, "%s: device consistency check failed (0x%x)", what, e);
+  return fail(FKD_ERR_INTERNAL, buf);
+}
+
+fkd_status finish(fkd_tree h, const char* what, int mem) {
+  if (mem == FKD_MEM_DEVICE && (h->flags & FKD_FLAG_ASYNC)) return FKD_OK;
+  return check_err_word(h, what);
+}
+
+Table table_of(fkd_tree h) { return Table{h->nodes.as<uint4>(), h->ids.as<uint32_t>()}; }
+
+__global__ void k_tables_out(uint32_t n, int dim, const uint4* __restrict__ nodes, float* __restrict__ tab) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint4 v = nodes[i];
+  const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+  for (int c = 0; c < dim; ++c) tab[(uint64_t)c * n + i] = __uint_as_float(w[c]);
+}
+
+// Stages host boxes (or aliases device boxes).
+fkd_status stage_boxes(fkd_tree h, const float* mins, const float* maxs, uint64_t q, int mem, Boxes* b) {
+  b->q = q;
+  b->stride = q;
+  if (mem == FKD_MEM_DEVICE) {
+    b->lo = mins;
+    b->hi = maxs;
+    return FKD_OK;
+  }
+  const size_t bytes = (size_t)h->dim * q * sizeof(float);
+  FKD_CUDA(h->qlo.ensure(bytes ? bytes : 4));
+  FKD_CUDA(h->qhi.ensure(bytes ? bytes : 4));
+  if (bytes) {
+    FKD_CUDA(cudaMemcpyAsync(h->qlo.p, mins, bytes, cudaMemcpyHostToDevice, h->stream));
+    FKD_CUDA(cudaMemcpyAsync(h->qhi.p, maxs, bytes, cudaMemcpyHostToDevice, h->stream));
+  }
+  b->lo = h->qlo.as<float>();
+  b->hi = h->qhi.as<float>();
+  return FKD_OK;
+}
+
+SearchCtx search_ctx(fkd_tree h, const Boxes& b) {
+  SearchCtx sc;
+  memset(&sc, 0, sizeof sc);
+  sc.g = make_geom((uint32_t)h->n);
+  sc.tab = table_of(h);
+  sc.boxes = b;
+  sc.qcounter = h->qctr.as<uint32_t>();
+  sc.err = h->err.as<uint32_t>();
+  sc.stream = h->stream;
+  sc.capacity = ~0ull;
+  return sc;
+}
+
+fkd_status check_search_args(fkd_tree h, const float* mins, const float* maxs, uint64_t q, int mem) {
+  if (!h) return fail(FKD_ERR_ARG, "null handle");
+  if (!h->built) return fail(FKD_ERR_STATE, "search before build");
+  if (mem != FKD_MEM_HOST && mem != FKD_MEM_DEVICE) return fail(FKD_ERR_ARG, "mem must be FKD_MEM_HOST or FKD_MEM_DEVICE");
+  if (q > 0xffffffffull) return fail(FKD_ERR_ARG, "at most 2^32-1 boxes per call");
+  if (q && (!mins || !maxs)) return fail(FKD_ERR_ARG, "null box bounds");
+  return FKD_OK;
+}
+
+// count pass into h->counts (device); returns the device counts pointer
+fkd_status count_pass(fkd_tree h, const Boxes& b, uint32_t* dcounts) {
+  SearchCtx sc = search_ctx(h, b);
+  sc.counts = dcounts;
+  FKD_CUDA(launch_search(sc, h->dim, SEARCH_COUNT));
+  return FKD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* fkd_version(void) { return "fkdtree_b200 0.1 (sm_100a)"; }
+
+const char* fkd_last_error(void) { return g_last_error.c_str(); }
+
+fkd_status fkd_create(int dim, uint32_t flags, void* stream, fkd_tree* out) {
+  if (!out) return fail(FKD_ERR_ARG, "null output handle pointer");
+  *out = nullptr;
+  if (dim < 1 || dim > 4) return fail(FKD_ERR_ARG, "dim must be 1..4");
+  fkd_tree h = new (std::nothrow) fkd_tree_s();
+  if (!h) return fail(FKD_ERR_NOMEM, "host allocation failed");
+  h->dim = dim;
+  h->flags = flags;
+  h->stream = (cudaStream_t)stream;
+  cudaError_t e = cudaGetDevice(&h->device);
+  if (e == cudaSuccess) e = h->err.ensure(sizeof(uint32_t) * 4);
+  if (e == cudaSuccess) e = h->qctr.ensure(sizeof(uint32_t) * 4);
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&h->herr, sizeof(uint32_t) * 4);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->err.p, 0, sizeof(uint32_t), h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) {
+    delete h;
+    return fail(e == cudaErrorMemoryAllocation ? FKD_ERR_NOMEM : FKD_ERR_CUDA,
+                std::string("fkd_create: ") + cudaGetErrorString(e));
+  }
+  *out = h;
+  g_last_error.clear();
+  return FKD_OK;
+}
+
+fkd_status fkd_destroy(fkd_tree h) {
+  if (!h) return FKD_OK;
+  cudaStreamSynchronize(h->stream);
+  delete h;
+  return FKD_OK;
+}
+
+fkd_status fkd_set_stream(fkd_tree h, void* stream) {
+  if (!h) return fail(FKD_ERR_ARG, "null handle");
+  h->stream = (cudaStream_t)stream;
+  return FKD_OK;
+}
+
+fkd_status fkd_build(fkd_tree h, const float* coords, const uint32_t* ids, uint64_t n, int mem) {
+  if (!h) return fail(FKD_ERR_ARG, "null handle");
+  if (mem != FKD_MEM_HOST && mem != FKD_MEM_DEVICE) return fail(FKD_ERR_ARG, "mem must be FKD_MEM_HOST or FKD_MEM_DEVICE");
+  if (n >= (1ull << 31)) return fail(FKD_ERR_ARG, "at most 2^31-1 points per tree");
+  if (n && (!coords || !ids)) return fail(FKD_ERR_ARG, "null coords or ids");
+  h->built = false;
+  h->n = n;
+  if (n == 0) {
+    h->built = true;
+    return FKD_OK;
+  }
+  const int dim = h->dim;
+  const uint32_t d0 = build_global_levels((uint32_t)n, dim);
+  const size_t rec_bytes = (size_t)(dim + 1) * n * sizeof(uint32_t);
+  FKD_CUDA(h->nodes.ensure(n * sizeof(uint4)));
+  FKD_CUDA(h->ids.ensure(n * sizeof(uint32_t)));
+  FKD_CUDA(h->work1.ensure(rec_bytes));
+  if (d0 > 0) {
+    FKD_CUDA(h->work0.ensure(rec_bytes));
+    FKD_CUDA(h->sel.ensure(sizeof(SegSel) * (size_t)(1u << (d0 - 1))));
+    const size_t gw = build_ghist_words((uint32_t)n, dim);
+    FKD_CUDA(h->ghist.ensure(gw * sizeof(uint32_t)));
+    FKD_CUDA(cudaMemsetAsync(h->ghist.p, 0, gw * sizeof(uint32_t), h->stream));
+  }
+  FKD_CUDA(cudaMemsetAsync(h->err.p, 0, sizeof(uint32_t), h->stream));
+  BuildCtx bc;
+  bc.g = make_geom((uint32_t)n);
+  if (mem == FKD_MEM_HOST) {
+    uint32_t* w1 = h->work1.as<uint32_t>();
+    FKD_CUDA(cudaMemcpyAsync(w1, coords, (size_t)dim * n * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    FKD_CUDA(cudaMemcpyAsync(w1 + (size_t)dim * n, ids, n * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
+    bc.input = CSoA{w1, w1 + (size_t)dim * n, n};
+  } else {
+    bc.input = CSoA{(const uint32_t*)coords, ids, n};
+  }
+  uint32_t* w0 = h->work0.as<uint32_t>();
+  uint32_t* w1 = h->work1.as<uint32_t>();
+  bc.work[0] = SoA{w0, w0 ? w0 + (size_t)dim * n : nullptr, n};
+  bc.work[1] = SoA{w1, w1 + (size_t)dim * n, n};
+  bc.sel = h->sel.as<SegSel>();
+  bc.ghist = h->ghist.as<uint32_t>();
+  bc.tab = table_of(h);
+  bc.err = h->err.as<uint32_t>();
+  bc.stream = h->stream;
+  FKD_CUDA(launch_build(bc, dim));
+  h->built = true;
+  fkd_status s = finish(h, "fkd_build", mem);
+  if (s != FKD_OK) h->built = false;
+  return s;
+}
+
+fkd_status fkd_size(fkd_tree h, uint64_t* n) {
+  if (!h || !n) return fail(FKD_ERR_ARG, "null argument");
+  *n = h->built ? h->n : 0;
+  return FKD_OK;
+}
+
+fkd_status fkd_get_tables(fkd_tree h, float* tab, uint32_t* tab_ids, int mem) {
+  if (!h) return fail(FKD_ERR_ARG, "null handle");
+  if (!h->built) return fail(FKD_ERR_STATE, "tables requested before build");
+  if (mem != FKD_MEM_HOST && mem != FKD_MEM_DEVICE) return fail(FKD_ERR_ARG, "mem must be FKD_MEM_HOST or FKD_MEM_DEVICE");
+  const uint64_t n = h->n;
+  if (n == 0) return FKD_OK;
+  if (tab) {
+    float* dst = tab;
+    if (mem == FKD_MEM_HOST) {
+      FKD_CUDA(h->work0.ensure((size_t)(h->dim + 1) * n * sizeof(uint32_t)));
+      dst = h->work0.as<float>();
+    }
+    k_tables_out<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>((uint32_t)n, h->dim, h->nodes.as<uint4>(), dst);
+    FKD_CUDA(cudaGetLastError());
+    if (mem == FKD_MEM_HOST)
+      FKD_CUDA(cudaMemcpyAsync(tab, dst, (size_t)h->dim * n * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+  }
+  if (tab_ids)
+    FKD_CUDA(cudaMemcpyAsync(tab_ids, h->ids.p, n * sizeof(uint32_t),
+                             mem == FKD_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, h->stream));
+  if (mem == FKD_MEM_HOST || !(h->flags & FKD_FLAG_ASYNC)) FKD_CUDA(cudaStreamSynchronize(h->stream));
+  return FKD_OK;
+}
+
+fkd_status fkd_search_count(fkd_tree h, const float* mins, const float* maxs, uint64_t q, uint32_t* counts, int mem) {
+  fkd_status s = check_search_args(h, mins, maxs, q, mem);
+  if (s != FKD_OK) return s;
+  if (q && !counts) return fail(FKD_ERR_ARG, "null counts");
+  if (q == 0) return FKD_OK;
+  Boxes b;
+  if ((s = stage_boxes(h, mins, maxs, q, mem, &b)) != FKD_OK) return s;
+  uint32_t* dc = counts;
+  if (mem == FKD_MEM_HOST) {
+    FKD_CUDA(h->counts.ensure(q * sizeof(uint32_t)));
+    dc = h->counts.as<uint32_t>();
+  }
+  FKD_CUDA(cudaMemsetAsync(h->err.p, 0, sizeof(uint32_t), h->stream));
+  if ((s = count_pass(h, b, dc)) != FKD_OK) return s;
+  if (mem == FKD_MEM_HOST)
+    FKD_CUDA(cudaMemcpyAsync(counts, dc, q * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+  return finish(h, "fkd_search_count", mem);
+}
+
+static fkd_status write_pass(fkd_tree h, const Boxes& b, const uint64_t* doffsets, uint32_t* dout, uint64_t total,
+                             int ordered) {
+  SearchCtx sc = search_ctx(h, b);
+  sc.offsets = doffsets;
+  sc.out = dout;
+  sc.capacity = total;
+  sc.heap_out = ordered ? 1 : 0;
+  FKD_CUDA(launch_search(sc, h->dim, SEARCH_WRITE));
+  if (ordered) {
+    FKD_CUDA(h->tmp.ensure(total ? total * sizeof(uint32_t) : 4));
+    FKD_CUDA(launch_order_results(sc.g, sc.tab, doffsets, b.q, dout, h->tmp.as<uint32_t>(), sc.err, h->stream));
+  }
+  return FKD_OK;
+}
+
+fkd_status fkd_search_write(fkd_tree h, const float* mins, const float* maxs, uint64_t q, const uint64_t* offsets,
+                            uint32_t* ids_out, int ordered, int mem) {
+  fkd_status s = check_search_args(h, mins, maxs, q, mem);
+  if (s != FKD_OK) return s;
+  if (!offsets) return fail(FKD_ERR_ARG, "null offsets");
+  if (q == 0) return FKD_OK;
+  Boxes b;
+  if ((s = stage_boxes(h, mins, maxs, q, mem, &b)) != FKD_OK) return s;
+  const uint64_t* doff = offsets;
+  uint32_t* dout = ids_out;
+  uint64_t total = 0;
+  if (mem == FKD_MEM_HOST) {
+    total = offsets[q];
+    if (total && !ids_out) return fail(FKD_ERR_ARG, "null ids_out");
+    FKD_CUDA(h->offsets.ensure((q + 1) * sizeof(uint64_t)));
+    FKD_CUDA(cudaMemcpyAsync(h->offsets.p, offsets, (q + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, h->stream));
+    doff = h->offsets.as<uint64_t>();
+    FKD_CUDA(h->out.ensure(total ? total * sizeof(uint32_t) : 4));
+    dout = h->out.as<uint32_t>();
+  } else {
+    FKD_CUDA(cudaMemcpyAsync(h->herr + 2, offsets + q, sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
+    FKD_CUDA(cudaStreamSynchronize(h->stream));
+    memcpy(&total, h->herr + 2, sizeof(uint64_t));
+    if (total && !ids_out) return fail(FKD_ERR_ARG, "null ids_out");
+  }
+  FKD_CUDA(cudaMemsetAsync(h->err.p, 0, sizeof(uint32_t), h->stream));
+  if ((s = write_pass(h, b, doff, dout, total, ordered)) != FKD_OK) return s;
+  if (mem == FKD_MEM_HOST && total)
+    FKD_CUDA(cudaMemcpyAsync(ids_out, dout, total * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+  return finish(h, "fkd_search_write", mem);
+}
+
+fkd_status fkd_search(fkd_tree h, const float* mins, const float* maxs, uint64_t q, uint64_t* offsets_out,
+                      uint32_t* ids_out, uint64_t capacity, uint64_t* total, int ordered, int mem) {
+  fkd_status s = check_search_args(h, mins, maxs, q, mem);
+  if (s != FKD_OK) return s;
+  if (!offsets_out || !total) return fail(FKD_ERR_ARG, "null offsets_out or total");
+  Boxes b;
+  if ((s = stage_boxes(h, mins, maxs, q, mem, &b)) != FKD_OK) return s;
+  FKD_CUDA(h->counts.ensure(q ? q * sizeof(uint32_t) : 4));
+  FKD_CUDA(h->partials.ensure(scan_partials_words(q) * sizeof(unsigned long long)));
+  uint64_t* doff = offsets_out;
+  if (mem == FKD_MEM_HOST) {
+    FKD_CUDA(h->offsets.ensure((q + 1) * sizeof(uint64_t)));
+    doff = h->offsets.as<uint64_t>();
+  }
+  FKD_CUDA(cudaMemsetAsync(h->err.p, 0, sizeof(uint32_t), h->stream));
+  if (q && (s = count_pass(h, b, h->counts.as<uint32_t>())) != FKD_OK) return s;
+  FKD_CUDA(launch_scan_counts(h->counts.as<uint32_t>(), q, doff, h->partials.as<unsigned long long>(), h->stream));
+  FKD_CUDA(cudaMemcpyAsync(h->herr + 2, doff + q, sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
+  FKD_CUDA(cudaStreamSynchronize(h->stream));
+  uint64_t tot = 0;
+  memcpy(&tot, h->herr + 2, sizeof(uint64_t));
+  *total = tot;
+  if ((s = check_err_word(h, "fkd_search (count)")) != FKD_OK) return s;
+  if (mem == FKD_MEM_HOST)
+    FKD_CUDA(cudaMemcpyAsync(offsets_out, doff, (q + 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
+  if (tot > capacity) {
+    FKD_CUDA(cudaStreamSynchronize(h->stream));
+    char buf[128];
+    snprintf(buf, sizeof buf, "fkd_search: %llu results exceed the capacity of %llu ids", (unsigned long long)tot,
+             (unsigned long long)capacity);
+    return fail(FKD_ERR_CAPACITY, buf);
+  }
+  if (tot && !ids_out) return fail(FKD_ERR_ARG, "null ids_out");
+  if (tot == 0) {
+    FKD_CUDA(cudaStreamSynchronize(h->stream));
+    return FKD_OK;
+  }
+  uint32_t* dout = ids_out;
+  if (mem == FKD_MEM_HOST) {
+    FKD_CUDA(h->out.ensure(tot * sizeof(uint32_t)));
+    dout = h->out.as<uint32_t>();
+  }
+  if ((s = write_pass(h, b, doff, dout, tot, ordered)) != FKD_OK) return s;
+  if (mem == FKD_MEM_HOST)
+    FKD_CUDA(cudaMemcpyAsync(ids_out, dout, tot * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+  return finish(h, "fkd_search", mem);
+}
+
+fkd_status fkd_search_digest(fkd_tree h, const float* mins, const float* maxs, uint64_t q, uint32_t* counts,
+                             uint64_t* digests, int mem) {
+  fkd_status s = check_search_args(h, mins, maxs, q, mem);
+  if (s != FKD_OK) return s;
+  if (q && (!counts || !digests)) return fail(FKD_ERR_ARG, "null counts or digests");
+  if (q == 0) return FKD_OK;
+  Boxes b;
+  if ((s = stage_boxes(h, mins, maxs, q, mem, &b)) != FKD_OK) return s;
+  uint32_t* dc = counts;
+  uint64_t* dd = digests;
+  if (mem == FKD_MEM_HOST) {
+    FKD_CUDA(h->counts.ensure(q * sizeof(uint32_t)));
+    FKD_CUDA(h->digests.ensure(q * sizeof(uint64_t)));
+    dc = h->counts.as<uint32_t>();
+    dd = h->digests.as<uint64_t>();
+  }
+  FKD_CUDA(cudaMemsetAsync(h->err.p, 0, sizeof(uint32_t), h->stream));
+  SearchCtx sc = search_ctx(h, b);
+  sc.counts = dc;
+  sc.digests = (unsigned long long*)dd;
+  FKD_CUDA(launch_search(sc, h->dim, SEARCH_DIGEST));
+  if (mem == FKD_MEM_HOST) {
+    FKD_CUDA(cudaMemcpyAsync(counts, dc, q * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+    FKD_CUDA(cudaMemcpyAsync(digests, dd, q * sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
+  }
+  return finish(h, "fkd_search_digest", mem);
+}
+
+fkd_status fkd_sync(fkd_tree h) {
+  if (!h) return fail(FKD_ERR_ARG, "null handle");
+  return check_err_word(h, "fkd_sync");
+}
+
+}  // extern "C"

@@ -1,0 +1,517 @@
+// fkd_search.cu -- box search on the flat tree (sm_100a).
+//
+// Semantics: FKDTree_CPU::search_in_the_box (FKDTree_cpu.h:123-169) and its
+// BFS / branchless / recursive variants (:72-121, :25-70, :171-207) all return
+// the ids of exactly the points inside the closed box (intersects /
+// is_in_the_box, FKDTree_cpu.h:302-321): a child is skipped only when the
+// node's split value proves the whole subtree lies outside.  The GPU visits
+// the same children by the same tests -- left unless v < lo[c], right when
+// v < lo[c] or lo[c] <= v <= hi[c] -- so its result set is the reference's.
+//
+// Shape: one warp per box, boxes handed out by an atomic counter to a
+// persistent grid.  The frontier is a per-warp stack in shared memory (the
+// FQueue replacement): the warp pops up to 32 nodes, each lane tests one node
+// with a single 16-byte load, and the children are pushed back in lane order.
+// Popping the top 32 of a depth-sorted stack keeps it depth-sorted and leaves
+// at most 64 entries per depth, so 64*(H+1) entries can never overflow; the
+// bound is still checked and reported (FKD_ERR_CAPACITY) rather than trusted.
+//
+// Every node also carries a 2*dim-bit mask saying which sides of its cell
+// (the closed slab its ancestors' split values bound it by) already lie
+// inside the box.  A child whose mask is full is inside entirely: its
+// subtree is counted in closed form and, when ids are wanted, copied as one
+// contiguous run of the id table per level (in the heap layout the
+// descendants of node r at relative depth j are [(r+1)2^j - 1, (r+1)2^j - 1 + 2^j)).
+//
+// Two passes ("count then write"): SEARCH_COUNT fills counts, a prefix sum
+// turns them into offsets, SEARCH_WRITE writes every box's ids to its slice.
+// SEARCH_DIGEST replaces the write by a per-box order-independent digest.
+#include <math.h>
+
+#include "fkd_internal.h"
+
+namespace fkd {
+
+constexpr int QT = 128;  // threads per CTA
+constexpr int QW = QT / 32;
+constexpr int JOBS = 64;  // contained-subtree jobs per warp step (<= 2 per lane)
+
+__device__ __forceinline__ uint32_t lanemask_lt_s() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+__device__ __forceinline__ float sel4(uint32_t c, float a, float b, float d, float e) {
+  return c == 0 ? a : (c == 1 ? b : (c == 2 ? d : e));
+}
+
+__device__ __forceinline__ unsigned long long warp_sum64(unsigned long long v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__host__ __device__ inline uint32_t stack_cap(const Geom& g) { return 64u * (g.H + 1u) + 1u; }
+
+template <int DIM, int MODE>
+__global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ uint32_t jobs[QW][JOBS];
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  uint32_t* stk_node = (uint32_t*)smem_raw + (size_t)warp * cap;
+  uint8_t* stk_mask = (uint8_t*)((uint32_t*)smem_raw + (size_t)QW * cap) + (size_t)warp * cap;
+  const Geom g = sc.g;
+  const uint32_t n = g.n;
+  constexpr uint32_t FULL = (1u << (2 * DIM)) - 1u;
+  const uint32_t lt = lanemask_lt_s();
+
+  for (;;) {
+    uint32_t qi = 0;
+    if (lane == 0) qi = atomicAdd(sc.qcounter, 1u);
+    qi = __shfl_sync(0xffffffffu, qi, 0);
+    if ((uint64_t)qi >= sc.boxes.q) break;
+    const uint32_t qj = sc.order ? sc.order[qi] : qi;
+    float lo[4] = {0.f, 0.f, 0.f, 0.f}, hi[4] = {0.f, 0.f, 0.f, 0.f};
+    uint32_t mask0 = 0u;
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+      lo[c] = sc.boxes.lo[(uint64_t)c * sc.boxes.stride + qj];
+      hi[c] = sc.boxes.hi[(uint64_t)c * sc.boxes.stride + qj];
+      if (lo[c] == -INFINITY) mask0 |= 1u << (2 * c);
+      if (hi[c] == INFINITY) mask0 |= 2u << (2 * c);
+    }
+    unsigned long long acc = 0ull;   // count (COUNT) / digest (DIGEST)
+    unsigned long long acc2 = 0ull;  // count (DIGEST)
+    uint64_t cursor = 0, cend = 0;
+    if (MODE == SEARCH_WRITE) {
+      cursor = sc.offsets[qj];
+      cend = sc.offsets[qj + 1];
+    }
+    bool failed = false;
+
+    // Emits whole subtrees listed in jobs[warp][0..nj).
+    auto run_jobs = [&](uint32_t nj) {
+      for (uint32_t jb = 0; jb < nj; ++jb) {
+        const uint32_t r = jobs[warp][jb];
+        for (uint32_t j = 0;; ++j) {
+          const uint64_t a = ((uint64_t)(r + 1u) << j) - 1u;
+          if (a >= n) break;
+          const uint64_t b = (a + (1ull << j)) < (uint64_t)n ? (a + (1ull << j)) : (uint64_t)n;
+          for (uint64_t x = a + lane; x < b; x += 32u) {
+            const uint32_t id = __ldg(sc.tab.ids + x);
+            if (MODE == SEARCH_WRITE) {
+              const uint64_t pos = cursor + (x - a);
+              if (pos < cend && pos < sc.capacity)
+                sc.out[pos] = sc.heap_out ? (uint32_t)x : id;
+              else
+                failed = true;
+            } else {
+              acc += mix64(id);
+            }
+          }
+          cursor += b - a;
+        }
+      }
+    };
+
+    int top = 0;
+    if (n > 0) {
+      if (mask0 == FULL) {
+        if (MODE == SEARCH_COUNT) {
+          if (lane == 0) acc += n;
+        } else {
+          if (lane == 0) jobs[warp][0] = 0u;
+          if (MODE == SEARCH_DIGEST && lane == 0) acc2 += n;
+          __syncwarp();
+          run_jobs(1);
+          __syncwarp();
+        }
+      } else {
+        if (lane == 0) {
+          stk_node[0] = 0u;
+          stk_mask[0] = (uint8_t)mask0;
+        }
+        top = 1;
+      }
+    }
+    __syncwarp();
+
+    while (top > 0) {
+      const int gcount = top < 32 ? top : 32;
+      const int base = top - gcount;
+      const bool have = (int)lane < gcount;
+      uint32_t i = 0u, mask = 0u;
+      if (have) {
+        i = stk_node[base + lane];
+        mask = stk_mask[base + lane];
+      }
+      __syncwarp();
+      top = base;
+      bool emit = false, pushL = false, pushR = false, contL = false, contR = false;
+      uint32_t maskL = 0u, maskR = 0u, idv = 0u;
+      if (have) {
+        const uint32_t dep = floor_log2_u32(i + 1u);
+        const uint32_t c = dep % DIM;
+        const uint4 nd = __ldg(sc.tab.nodes + i);
+        const float x0 = __uint_as_float(nd.x), x1 = __uint_as_float(nd.y), x2 = __uint_as_float(nd.z),
+                    x3 = __uint_as_float(nd.w);
+        const float v = sel4(c, x0, x1, x2, x3);
+        const float loc = sel4(c, lo[0], lo[1], lo[2], lo[3]);
+        const float hic = sel4(c, hi[0], hi[1], hi[2], hi[3]);
+        const bool inter = v <= hic && v >= loc;
+        const bool lower = v < loc;
+        if (inter) {
+          bool in = true;
+          if (DIM > 0) in &= (x0 <= hi[0] && x0 >= lo[0]);
+          if (DIM > 1) in &= (x1 <= hi[1] && x1 >= lo[1]);
+          if (DIM > 2) in &= (x2 <= hi[2] && x2 >= lo[2]);
+          if (DIM > 3) in &= (x3 <= hi[3] && x3 >= lo[3]);
+          emit = in;
+        }
+        if (emit && MODE != SEARCH_COUNT) idv = DIM <= 3 ? nd.w : __ldg(sc.tab.ids + i);
+        const uint32_t l = 2u * i + 1u;
+        const bool visitL = !lower && l < n;
+        const bool visitR = (lower || inter) && l + 1u < n;
+        maskL = mask | (v <= hic ? (2u << (2 * c)) : 0u);
+        maskR = mask | (v >= loc ? (1u << (2 * c)) : 0u);
+        contL = visitL && maskL == FULL;
+        contR = visitR && maskR == FULL;
+        pushL = visitL && !contL;
+        pushR = visitR && !contR;
+      }
+      if (MODE == SEARCH_COUNT) {
+        acc += (emit ? 1u : 0u) + (contL ? subtree_size(g, 2u * i + 1u) : 0u) +
+               (contR ? subtree_size(g, 2u * i + 2u) : 0u);
+      } else {
+        if (MODE == SEARCH_DIGEST) {
+          if (emit) acc += mix64(idv);
+          acc2 += (emit ? 1u : 0u) + (contL ? subtree_size(g, 2u * i + 1u) : 0u) +
+                  (contR ? subtree_size(g, 2u * i + 2u) : 0u);
+        } else {
+          const uint32_t be = __ballot_sync(0xffffffffu, emit);
+          if (emit) {
+            const uint64_t pos = cursor + __popc(be & lt);
+            if (pos < cend && pos < sc.capacity)
+              sc.out[pos] = sc.heap_out ? i : idv;
+            else
+              failed = true;
+          }
+          cursor += __popc(be);
+        }
+        const uint32_t nj = (contL ? 1u : 0u) + (contR ? 1u : 0u);
+        uint32_t jincl = nj;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const uint32_t y = __shfl_up_sync(0xffffffffu, jincl, o);
+          if (lane >= (uint32_t)o) jincl += y;
+        }
+        const uint32_t jtot = __shfl_sync(0xffffffffu, jincl, 31);
+        if (jtot) {
+          uint32_t jp = jincl - nj;
+          if (contL) jobs[warp][jp++] = 2u * i + 1u;
+          if (contR) jobs[warp][jp] = 2u * i + 2u;
+          __syncwarp();
+          run_jobs(jtot);
+          __syncwarp();
+        }
+      }
+      const uint32_t np = (pushL ? 1u : 0u) + (pushR ? 1u : 0u);
+      uint32_t incl = np;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (uint32_t)o) incl += y;
+      }
+      const uint32_t tot = __shfl_sync(0xffffffffu, incl, 31);
+      if ((uint32_t)top + tot > cap) {
+        failed = true;
+        break;
+      }
+      uint32_t p = (uint32_t)top + incl - np;
+      if (pushL) {
+        stk_node[p] = 2u * i + 1u;
+        stk_mask[p] = (uint8_t)maskL;
+        ++p;
+      }
+      if (pushR) {
+        stk_node[p] = 2u * i + 2u;
+        stk_mask[p] = (uint8_t)maskR;
+      }
+      top += (int)tot;
+      __syncwarp();
+    }
+
+    const bool anyfail = __any_sync(0xffffffffu, failed);
+    if (MODE == SEARCH_COUNT) {
+      const unsigned long long tot = warp_sum64(acc);
+      if (lane == 0) sc.counts[qj] = (uint32_t)tot;
+      if (lane == 0 && tot > 0xffffffffull) atomicOr(sc.err, ERRB_CAPACITY);
+    } else if (MODE == SEARCH_DIGEST) {
+      const unsigned long long dg = warp_sum64(acc);
+      const unsigned long long ct = warp_sum64(acc2);
+      if (lane == 0) {
+        sc.digests[qj] = dg;
+        sc.counts[qj] = (uint32_t)ct;
+      }
+    } else {
+      if (lane == 0 && cursor != cend) atomicOr(sc.err, ERRB_INTERNAL);
+    }
+    if (anyfail && lane == 0) atomicOr(sc.err, ERRB_CAPACITY);
+    __syncwarp();
+  }
+}
+
+template <int DIM, int MODE>
+static cudaError_t run_search(SearchCtx& sc) {
+  const uint32_t cap = stack_cap(sc.g);
+  const size_t smem = (size_t)QW * cap * 5u;
+  cudaError_t e = cudaFuncSetAttribute(k_search<DIM, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_search<DIM, MODE>, QT, smem);
+  if (e != cudaSuccess) return e;
+  if (per < 1) per = 1;
+  uint64_t blocks = (uint64_t)sms * per;
+  const uint64_t need = (sc.boxes.q + QW - 1) / QW;
+  if (blocks > need) blocks = need ? need : 1;
+  e = cudaMemsetAsync(sc.qcounter, 0, sizeof(uint32_t), sc.stream);
+  if (e != cudaSuccess) return e;
+  k_search<DIM, MODE><<<(unsigned)blocks, QT, smem, sc.stream>>>(sc, cap);
+  return cudaGetLastError();
+}
+
+template <int DIM>
+static cudaError_t run_search_mode(SearchCtx& sc, int mode) {
+  switch (mode) {
+    case SEARCH_COUNT: return run_search<DIM, SEARCH_COUNT>(sc);
+    case SEARCH_WRITE: return run_search<DIM, SEARCH_WRITE>(sc);
+    default: return run_search<DIM, SEARCH_DIGEST>(sc);
+  }
+}
+
+cudaError_t launch_search(SearchCtx& sc, int dim, int mode) {
+  if (sc.boxes.q == 0) return cudaSuccess;
+  switch (dim) {
+    case 1: return run_search_mode<1>(sc, mode);
+    case 2: return run_search_mode<2>(sc, mode);
+    case 3: return run_search_mode<3>(sc, mode);
+    case 4: return run_search_mode<4>(sc, mode);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+// ------------------------------------------------------------------- scan
+
+constexpr int SCT = 256;
+constexpr int SCIPT = 16;
+constexpr int SCB = SCT * SCIPT;
+
+size_t scan_partials_words(uint64_t q) { return (q + SCB - 1) / SCB + 1; }
+
+__device__ __forceinline__ unsigned long long block_excl_scan64(unsigned long long v, unsigned long long* wsum,
+                                                                unsigned long long* total) {
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  unsigned long long incl = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned long long y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= (uint32_t)o) incl += y;
+  }
+  if (lane == 31u) wsum[warp] = incl;
+  __syncthreads();
+  unsigned long long base = 0ull, tot = 0ull;
+  for (uint32_t k = 0; k < blockDim.x / 32u; ++k) {
+    if (k < warp) base += wsum[k];
+    tot += wsum[k];
+  }
+  __syncthreads();
+  *total = tot;
+  return base + incl - v;
+}
+
+__global__ void __launch_bounds__(SCT) k_scan_partials(const uint32_t* __restrict__ counts, uint64_t q,
+                                                       unsigned long long* __restrict__ partials) {
+  __shared__ unsigned long long wsum[SCT / 32];
+  const uint64_t b0 = (uint64_t)blockIdx.x * SCB;
+  unsigned long long s = 0ull;
+#pragma unroll
+  for (int k = 0; k < SCIPT; ++k) {
+    const uint64_t i = b0 + (uint64_t)k * SCT + threadIdx.x;
+    if (i < q) s += counts[i];
+  }
+  unsigned long long tot;
+  block_excl_scan64(s, wsum, &tot);
+  if (threadIdx.x == 0) partials[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(1024) k_scan_top(unsigned long long* __restrict__ partials, uint64_t nb) {
+  __shared__ unsigned long long wsum[32];
+  unsigned long long carry = 0ull;
+  for (uint64_t c0 = 0; c0 < nb; c0 += blockDim.x) {
+    const uint64_t i = c0 + threadIdx.x;
+    const unsigned long long v = i < nb ? partials[i] : 0ull;
+    unsigned long long tot;
+    const unsigned long long ex = block_excl_scan64(v, wsum, &tot);
+    if (i < nb) partials[i] = carry + ex;
+    carry += tot;
+  }
+  if (threadIdx.x == 0) partials[nb] = carry;
+}
+
+__global__ void __launch_bounds__(SCT) k_scan_down(const uint32_t* __restrict__ counts, uint64_t q,
+                                                   const unsigned long long* __restrict__ partials,
+                                                   uint64_t* __restrict__ offsets, uint64_t nb) {
+  __shared__ unsigned long long wsum[SCT / 32];
+  const uint64_t b0 = (uint64_t)blockIdx.x * SCB;
+  // each thread owns SCIPT consecutive counts
+  const uint64_t t0 = b0 + (uint64_t)threadIdx.x * SCIPT;
+  uint32_t v[SCIPT];
+  unsigned long long s = 0ull;
+#pragma unroll
+  for (int k = 0; k < SCIPT; ++k) {
+    v[k] = (t0 + k < q) ? counts[t0 + k] : 0u;
+    s += v[k];
+  }
+  unsigned long long tot;
+  unsigned long long run = partials[blockIdx.x] + block_excl_scan64(s, wsum, &tot);
+#pragma unroll
+  for (int k = 0; k < SCIPT; ++k) {
+    if (t0 + k < q) offsets[t0 + k] = run;
+    run += v[k];
+  }
+  if (blockIdx.x == nb - 1 && threadIdx.x == 0) offsets[q] = partials[nb];
+}
+
+cudaError_t launch_scan_counts(const uint32_t* counts, uint64_t q, uint64_t* offsets, unsigned long long* partials,
+                               cudaStream_t stream) {
+  if (q == 0) return cudaMemsetAsync(offsets, 0, sizeof(uint64_t), stream);
+  const uint64_t nb = (q + SCB - 1) / SCB;
+  k_scan_partials<<<(unsigned)nb, SCT, 0, stream>>>(counts, q, partials);
+  k_scan_top<<<1, 1024, 0, stream>>>(partials, nb);
+  k_scan_down<<<(unsigned)nb, SCT, 0, stream>>>(counts, q, partials, offsets, nb);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------ ordered results
+//
+// search_in_the_box and its BFS / branchless variants emit the in-box nodes
+// level by level in frontier order, and the frontier of every level is sorted
+// by heap index (children are appended in order), so their output is the
+// in-box set sorted by heap index.  For that order the write pass stores heap
+// indices, this kernel sorts each box's slice and replaces the indices by ids.
+
+constexpr int OT = 256;
+constexpr int ORUN = 8192;  // slice length sorted in shared memory
+
+__device__ void bitonic_smem(uint32_t* a, uint32_t m) {  // m a power of two
+  for (uint32_t k = 2; k <= m; k <<= 1) {
+    for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+      for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
+        const uint32_t p = i ^ j;
+        if (p > i) {
+          const uint32_t x = a[i], y = a[p];
+          const bool up = (i & k) == 0;
+          if ((x > y) == up) {
+            a[i] = y;
+            a[p] = x;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// Merges sorted runs a[0,la) and b[0,lb) into o (distinct keys), CTA-wide by
+// merge-path partitioning.
+__device__ void merge_cta(const uint32_t* a, uint32_t la, const uint32_t* b, uint32_t lb, uint32_t* o) {
+  const uint32_t total = la + lb;
+  const uint32_t per = (total + blockDim.x - 1) / blockDim.x;
+  const uint32_t k0 = min(total, threadIdx.x * per), k1 = min(total, k0 + per);
+  if (k0 >= k1) return;
+  // find i in [max(0,k0-lb), min(k0,la)] with a[i-1] < b[k0-i] and b[k0-i-1] < a[i]
+  uint32_t lo = k0 > lb ? k0 - lb : 0u, hi = k0 < la ? k0 : la;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (a[mid] < b[k0 - mid - 1u])
+      lo = mid + 1u;
+    else
+      hi = mid;
+  }
+  uint32_t i = lo, j = k0 - lo;
+  for (uint32_t k = k0; k < k1; ++k) {
+    if (j >= lb || (i < la && a[i] < b[j]))
+      o[k] = a[i++];
+    else
+      o[k] = b[j++];
+  }
+}
+
+__global__ void __launch_bounds__(OT) k_order(Geom g, Table tab, const uint64_t* __restrict__ offsets, uint64_t q,
+                                              uint32_t* __restrict__ out, uint32_t* __restrict__ tmp,
+                                              uint32_t* __restrict__ err) {
+  __shared__ uint32_t buf[ORUN];
+  for (uint64_t qj = blockIdx.x; qj < q; qj += gridDim.x) {
+    const uint64_t s0 = offsets[qj];
+    const uint32_t len = (uint32_t)(offsets[qj + 1] - s0);
+    uint32_t* seg = out + s0;
+    uint32_t* alt = tmp + s0;
+    if (len > 1u) {
+      // sort runs of ORUN in shared memory
+      for (uint32_t r0 = 0; r0 < len; r0 += ORUN) {
+        const uint32_t rl = min((uint32_t)ORUN, len - r0);
+        uint32_t m = 1u;
+        while (m < rl) m <<= 1;
+        for (uint32_t i = threadIdx.x; i < m; i += OT) buf[i] = i < rl ? seg[r0 + i] : 0xffffffffu;
+        __syncthreads();
+        bitonic_smem(buf, m);
+        for (uint32_t i = threadIdx.x; i < rl; i += OT) seg[r0 + i] = buf[i];
+        __syncthreads();
+      }
+      // merge runs pairwise, ping-ponging between out and tmp
+      uint32_t* src = seg;
+      uint32_t* dst = alt;
+      for (uint32_t w = ORUN; w < len; w <<= 1) {
+        for (uint32_t a0 = 0; a0 < len; a0 += 2u * w) {
+          const uint32_t la = min(w, len - a0);
+          const uint32_t lb = (a0 + w < len) ? min(w, len - a0 - w) : 0u;
+          merge_cta(src + a0, la, src + a0 + la, lb, dst + a0);
+        }
+        __syncthreads();
+        uint32_t* t = src;
+        src = dst;
+        dst = t;
+      }
+      if (src != seg) {
+        for (uint32_t i = threadIdx.x; i < len; i += OT) seg[i] = src[i];
+        __syncthreads();
+      }
+    }
+    for (uint32_t i = threadIdx.x; i < len; i += OT) {
+      const uint32_t hidx = seg[i];
+      if (hidx < g.n) {
+        seg[i] = __ldg(tab.ids + hidx);
+      } else {
+        seg[i] = 0xffffffffu;
+        atomicOr(err, ERRB_INTERNAL);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+cudaError_t launch_order_results(const Geom& g, const Table& tab, const uint64_t* offsets, uint64_t q, uint32_t* out,
+                                 uint32_t* tmp, uint32_t* err, cudaStream_t stream) {
+  if (q == 0) return cudaSuccess;
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const uint64_t blocks = q < (uint64_t)sms * 8 ? q : (uint64_t)sms * 8;
+  k_order<<<(unsigned)blocks, OT, 0, stream>>>(g, tab, offsets, q, out, tmp, err);
+  return cudaGetLastError();
+}
+
+}  // namespace fkd

@@ -1,0 +1,146 @@
+/*
+ * fkdtree_b200.h -- C ABI of the B200 (sm_100a) FKDTree build and box search.
+ *
+ * The library (fkdtree_b200/libfkdtree_b200.so) builds the reference's flat,
+ * heap-ordered kd-tree on the GPU and answers axis-aligned box queries on it.
+ * The tree it builds is bit-identical to FKDTree_CPU::build
+ * (FKDTree_cpu.h:221-277 of te42kyfo/FKDTree): node i holds one input point,
+ * its split value is coordinate (depth(i) % dim) of that point, its children
+ * are 2i+1 and 2i+2, and the tables returned by fkd_get_tables are exactly
+ * theDimensions[d][i] / theIds[i] (FKDTree_cpu.h:323-326) -- provided the
+ * input ids are unique (with repeated ids the order among points whose
+ * split coordinate AND id tie is not defined by the reference either).
+ *
+ * Conventions
+ *  - every entry point returns an fkd_status; 0 is success.  No exception or
+ *    abort crosses the boundary.  fkd_last_error() describes the last failure
+ *    of the calling thread.
+ *  - coordinates are float32 and laid out SoA: coordinate c of point i is
+ *    coords[c*n + i] (the layout of getDimensionVector, FKDTree_cpu.h:209-213,
+ *    and of the OpenCL host upload, FKDTree_opencl.h:139-144).  Ids are uint32.
+ *  - box j is [mins[c*q + j], maxs[c*q + j]] in every dimension c, bounds
+ *    inclusive (FKDTree_cpu.h:302-321).
+ *  - `mem` says where the caller's buffers live: FKD_MEM_HOST (pageable or
+ *    pinned host memory; the call copies through the handle's device staging
+ *    buffers and is synchronous) or FKD_MEM_DEVICE (device pointers on the
+ *    handle's device; the call is stream-ordered on the handle's stream and,
+ *    unless the handle was created with FKD_FLAG_ASYNC, synchronises before it
+ *    returns so that errors can be reported).
+ *  - a handle is bound to one device and one stream; calls on one handle must
+ *    not overlap.  Different handles are independent.
+ *  - NaN coordinates are rejected (FKD_ERR_NAN): the reference comparator
+ *    (FKDTree_cpu.h:246-252) is not a strict weak order with NaN.  -0.0 and
+ *    +0.0 compare equal and tie on id, as in the reference.
+ *  - returned result ids are the tree's id values (theIds, FKDTree_cpu.h:148),
+ *    not array positions.
+ */
+#ifndef FKDTREE_B200_H_
+#define FKDTREE_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define FKD_API __attribute__((visibility("default")))
+#else
+#define FKD_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum fkd_status {
+  FKD_OK = 0,
+  FKD_ERR_ARG = 1,       /* bad argument (null pointer, unsupported dim, size) */
+  FKD_ERR_CUDA = 2,      /* a CUDA runtime call failed */
+  FKD_ERR_NOMEM = 3,     /* device or pinned allocation failed */
+  FKD_ERR_NAN = 4,       /* a coordinate is NaN */
+  FKD_ERR_STATE = 5,     /* e.g. search before build */
+  FKD_ERR_CAPACITY = 6,  /* a result or frontier bound was exceeded; nothing was silently dropped */
+  FKD_ERR_INTERNAL = 7,  /* a device-side consistency check failed */
+  FKD_ERR_TIMEOUT = 8    /* a bounded device-side wait gave up */
+} fkd_status;
+
+enum { FKD_MEM_HOST = 0, FKD_MEM_DEVICE = 1 };
+
+/* fkd_create flags */
+enum {
+  FKD_FLAG_ASYNC = 1u << 0 /* device-memory calls return without synchronising;
+                              errors are reported by fkd_sync */
+};
+
+typedef struct fkd_tree_s* fkd_tree;
+
+/* Version string of the library. */
+FKD_API const char* fkd_version(void);
+
+/* Description of the last failure on the calling thread ("" if none). */
+FKD_API const char* fkd_last_error(void);
+
+/* Creates an empty tree for points of `dim` coordinates (1..4) on the current
+ * CUDA device.  Replaces the FKDTree_CPU constructor (FKDTree_cpu.h:19-23);
+ * the points are passed to fkd_build instead.  `stream` is a cudaStream_t
+ * (NULL = the legacy default stream). */
+FKD_API fkd_status fkd_create(int dim, uint32_t flags, void* stream, fkd_tree* out);
+FKD_API fkd_status fkd_destroy(fkd_tree h);
+FKD_API fkd_status fkd_set_stream(fkd_tree h, void* stream);
+
+/* Builds the tree over n points.  Replaces FKDTree_CPU::build
+ * (FKDTree_cpu.h:221-277) together with the point copy of its constructor.
+ * coords: dim*n floats SoA; ids: n uint32.  n may be 0 (empty tree).  The
+ * library keeps its own copy; the caller's buffers may be reused on return
+ * (for FKD_MEM_DEVICE with FKD_FLAG_ASYNC: once the stream has passed the
+ * call). */
+FKD_API fkd_status fkd_build(fkd_tree h, const float* coords, const uint32_t* ids, uint64_t n, int mem);
+
+/* Number of points of the last build. */
+FKD_API fkd_status fkd_size(fkd_tree h, uint64_t* n);
+
+/* Copies the tables out: tab[c*n + i] = theDimensions[c][i], tab_ids[i] =
+ * theIds[i].  Replaces getDimensionVector / getIdVector
+ * (FKDTree_cpu.h:209-213; the OpenCL backend's lazy download,
+ * FKDTree_opencl.h:194-206).  Either pointer may be NULL. */
+FKD_API fkd_status fkd_get_tables(fkd_tree h, float* tab, uint32_t* tab_ids, int mem);
+
+/* Result count of every box (pass 1 of the two-pass search).  Replaces the
+ * per-box counts of FKDTree_OpenCL::search_in_the_box_multiple
+ * (FKDTree_opencl.h:123-164) and the counting half of CUDAKernelWrapper
+ * (searchInTheBoxCuda.cu:174-185, main.cpp:305). */
+FKD_API fkd_status fkd_search_count(fkd_tree h, const float* mins, const float* maxs, uint64_t q, uint32_t* counts,
+                            int mem);
+
+/* Writes the ids of box j to ids_out[offsets[j] .. offsets[j] + count_j)
+ * (pass 2).  offsets has q+1 entries (exclusive prefix sum of the counts of
+ * fkd_search_count, offsets[q] = total); ids_out holds offsets[q] ids.
+ * Within a box the ids come in ascending heap-index order, the order
+ * search_in_the_box / _BFS / _branchless emit them (FKDTree_cpu.h:123-169,
+ * 72-121, 25-70), when `ordered` is nonzero; otherwise in traversal order. */
+FKD_API fkd_status fkd_search_write(fkd_tree h, const float* mins, const float* maxs, uint64_t q, const uint64_t* offsets,
+                            uint32_t* ids_out, int ordered, int mem);
+
+/* Count, prefix sum and write in one call.  offsets_out receives q+1 entries;
+ * at most `capacity` ids are written; *total receives the number of results.
+ * Returns FKD_ERR_CAPACITY (and writes no ids) when total > capacity.
+ * Replaces search_in_the_box applied to a batch of boxes
+ * (FKDTree_cpu.h:123-169 under main.cpp:369-381) and the stub
+ * search_in_the_box_multiple (FKDTree_cpu.h:215-219). */
+FKD_API fkd_status fkd_search(fkd_tree h, const float* mins, const float* maxs, uint64_t q, uint64_t* offsets_out,
+                      uint32_t* ids_out, uint64_t capacity, uint64_t* total, int ordered, int mem);
+
+/* Per-box count and order-independent 64-bit digest of the id set (the
+ * wrap-around sum of a 64-bit finaliser of every id), for workloads whose
+ * result ids do not fit in memory.  No reference counterpart; it stands in
+ * for test_correct_search (FKDTree.h:54-86) at scale. */
+FKD_API fkd_status fkd_search_digest(fkd_tree h, const float* mins, const float* maxs, uint64_t q, uint32_t* counts,
+                             uint64_t* digests, int mem);
+
+/* Waits for the handle's stream and reports any device-side error latched by
+ * earlier asynchronous calls. */
+FKD_API fkd_status fkd_sync(fkd_tree h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FKDTREE_B200_H_ */

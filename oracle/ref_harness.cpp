@@ -1,0 +1,142 @@
+// ref_harness.cpp -- C entry points over the UNMODIFIED reference CPU tree.
+//
+// TEST INFRASTRUCTURE ONLY.  oracle/Makefile compiles this file against the
+// reference's own headers (FKDTree_cpu.h, FKDTree.h, FKDPoint.h, FQueue.h,
+// found through -I on the reference checkout) into oracle/_ref/libfkdref.so.
+// Nothing of the reference is copied here: this file only constructs
+// FKDTree_CPU<float, D>, calls its public methods and moves data in and out.
+// It serves two purposes:
+//   * pinning the C restatement (fkd_oracle.c) and generating the golden
+//     fixtures under tests/golden/ (tests/golden/make_golden.py);
+//   * the CPU baseline timed by bench.py: the reference build (serial by
+//     design, FKDTree_cpu.h:221-277) and its searches under an OpenMP
+//     parallel-for over boxes, the reference driver's `-p <threads>` loop
+//     (main.cpp:369-381) with OpenMP standing in for TBB as in test.cpp:71-76.
+//
+// It is compiled WITHOUT -DNDEBUG, so a FQueue overflow (FQueue.h:158) aborts
+// loudly rather than corrupting results; callers only run the level-order,
+// BFS and branchless variants on boxes whose frontier the C restatement has
+// shown to fit in FQueue's 1024 slots.
+#include <omp.h>
+#include <stdint.h>
+
+#include <chrono>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "FKDTree_cpu.h"
+
+namespace {
+
+struct HandleBase {
+  virtual ~HandleBase() {}
+  virtual int dim() const = 0;
+  virtual uint32_t size() const = 0;
+  virtual double build() = 0;
+  virtual void tables(float* tab_soa, uint32_t* ids) = 0;
+  virtual void search(int variant, uint64_t nq, const float* mins, const float* maxs, uint32_t* counts,
+                      const uint64_t* offsets, uint32_t* out, int threads, double* seconds) = 0;
+};
+
+template <int D>
+struct Handle : HandleBase {
+  std::vector<FKDPoint<float, D>> pts;
+  std::unique_ptr<FKDTree_CPU<float, D>> tree;
+
+  Handle(uint32_t n, const float* coords_soa, const uint32_t* ids) : pts(n) {
+    for (uint32_t i = 0; i < n; ++i) {
+      for (int c = 0; c < D; ++c) pts[i].setDimension(c, coords_soa[(size_t)c * n + i]);
+      pts[i].setId(ids[i]);
+    }
+  }
+  int dim() const override { return D; }
+  uint32_t size() const override { return (uint32_t)pts.size(); }
+
+  // Construction + build, the span main.cpp:201-207 times.
+  double build() override {
+    auto t0 = std::chrono::steady_clock::now();
+    tree.reset(new FKDTree_CPU<float, D>(pts));
+    tree->build();
+    auto t1 = std::chrono::steady_clock::now();
+    return std::chrono::duration<double>(t1 - t0).count();
+  }
+
+  void tables(float* tab_soa, uint32_t* ids) override {
+    const size_t n = pts.size();
+    for (int c = 0; c < D; ++c) {
+      const std::vector<float>& v = tree->getDimensionVector(c);
+      std::memcpy(tab_soa + (size_t)c * n, v.data(), n * sizeof(float));
+    }
+    const std::vector<unsigned int>& id = tree->getIdVector();
+    std::memcpy(ids, id.data(), n * sizeof(uint32_t));
+  }
+
+  std::vector<unsigned int> one(int variant, const FKDPoint<float, D>& lo, const FKDPoint<float, D>& hi) {
+    switch (variant) {
+      case 0: return tree->search_in_the_box(lo, hi);
+      case 1: return tree->search_in_the_box_BFS(lo, hi);
+      case 2: return tree->search_in_the_box_branchless(lo, hi);
+      default: {
+        std::vector<unsigned int> r;
+        tree->search_in_the_box_recursive(lo, hi, r);
+        return r;
+      }
+    }
+  }
+
+  void search(int variant, uint64_t nq, const float* mins, const float* maxs, uint32_t* counts,
+              const uint64_t* offsets, uint32_t* out, int threads, double* seconds) override {
+    std::vector<FKDPoint<float, D>> lo(nq), hi(nq);
+    for (uint64_t j = 0; j < nq; ++j)
+      for (int c = 0; c < D; ++c) {
+        lo[j].setDimension(c, mins[(size_t)c * nq + j]);
+        hi[j].setDimension(c, maxs[(size_t)c * nq + j]);
+      }
+    if (threads > 0) omp_set_num_threads(threads);
+    auto t0 = std::chrono::steady_clock::now();
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t j = 0; j < (int64_t)nq; ++j) {
+      std::vector<unsigned int> r = one(variant, lo[j], hi[j]);
+      if (counts) counts[j] = (uint32_t)r.size();
+      if (offsets && out && !r.empty()) std::memcpy(out + offsets[j], r.data(), r.size() * sizeof(uint32_t));
+    }
+    auto t1 = std::chrono::steady_clock::now();
+    if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+// Creates a reference tree over n points (coords_soa[c*n + i], ids[i]).
+void* fkdref_create(int dim, uint32_t n, const float* coords_soa, const uint32_t* ids) {
+  switch (dim) {
+    case 1: return new Handle<1>(n, coords_soa, ids);
+    case 2: return new Handle<2>(n, coords_soa, ids);
+    case 3: return new Handle<3>(n, coords_soa, ids);
+    case 4: return new Handle<4>(n, coords_soa, ids);
+    default: return nullptr;
+  }
+}
+
+void fkdref_destroy(void* h) { delete static_cast<HandleBase*>(h); }
+
+// FKDTree_CPU ctor + build(); returns the elapsed seconds (n must be > 0:
+// the reference build writes theIntervalMin[0] even for an empty input).
+double fkdref_build(void* h) { return static_cast<HandleBase*>(h)->build(); }
+
+// getDimensionVector(c) for every c, then getIdVector().
+void fkdref_tables(void* h, float* tab_soa, uint32_t* ids) { static_cast<HandleBase*>(h)->tables(tab_soa, ids); }
+
+// variant: 0 search_in_the_box, 1 _BFS, 2 _branchless, 3 _recursive.
+// counts may be null; ids are written to out[offsets[j]...] when both given.
+void fkdref_search(void* h, int variant, uint64_t nq, const float* mins_soa, const float* maxs_soa,
+                   uint32_t* counts, const uint64_t* offsets, uint32_t* out, int threads, double* seconds) {
+  static_cast<HandleBase*>(h)->search(variant, nq, mins_soa, maxs_soa, counts, offsets, out, threads, seconds);
+}
+
+int fkdref_max_threads(void) { return omp_get_max_threads(); }
+
+}  // extern "C"

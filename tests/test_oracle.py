@@ -1,0 +1,95 @@
+"""The C restatement (oracle/fkd_oracle.c) against the golden fixtures that
+the unmodified reference produced (tests/golden/make_golden.py).  CPU only."""
+import hashlib
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from fkdtree_b200 import workloads as W
+from tests._fixtures import GOLDEN, fixture_names, load, slices
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _built():
+    O.build_libs()
+
+
+@pytest.mark.parametrize("name", fixture_names())
+def test_oracle_build_matches_reference(name):
+    f = load(name)
+    tab, tid = O.build(f["coords"], f["ids"])
+    assert np.array_equal(tab.view(np.uint32), f["tab"].view(np.uint32)), "theDimensions differ"
+    assert np.array_equal(tid, f["tab_ids"]), "theIds differ"
+
+
+@pytest.mark.parametrize("name", fixture_names())
+def test_oracle_searches_match_reference(name):
+    f = load(name)
+    tab, tid = f["tab"], f["tab_ids"]
+    c, o, i, _ = O.search(tab, tid, f["mins"], f["maxs"], variant=O.RECURSIVE)
+    assert np.array_equal(c, f["rec_counts"]) and np.array_equal(i, f["rec_ids"])
+    for v, key in [(O.LEVEL_ORDER, "lvl"), (O.BFS, "bfs"), (O.BRANCHLESS, "bl")]:
+        mins, maxs = f["mins"], f["maxs"]
+        if f"{key}_sel" in f:
+            mins, maxs = mins[:, f[f"{key}_sel"]], maxs[:, f[f"{key}_sel"]]
+        c, o, i, _ = O.search(tab, tid, mins, maxs, variant=v)
+        assert np.array_equal(c, f[f"{key}_counts"]) and np.array_equal(i, f[f"{key}_ids"]), key
+
+
+@pytest.mark.parametrize("name", fixture_names())
+def test_every_variant_returns_the_brute_force_set(name):
+    """FKDTree.h:54-86: each result set equals the brute-force scan."""
+    f = load(name)
+    cb, ob, ib, _ = O.search(f["tab"], f["tab_ids"], f["mins"], f["maxs"], variant=O.BRUTE)
+    assert np.array_equal(cb, f["rec_counts"])
+    for a, b in zip(slices(ob, ib), slices(f["rec_offsets"], f["rec_ids"])):
+        assert np.array_equal(np.sort(a), np.sort(b))
+
+
+def test_level_order_is_ascending_heap_order():
+    """search_in_the_box emits in-box nodes sorted by heap index; the GPU's
+    ordered output relies on it."""
+    f = load("uniform3d_n1000")
+    pos = np.empty(f["tab_ids"].max() + 1, dtype=np.int64)
+    pos[f["tab_ids"]] = np.arange(f["tab_ids"].size)
+    for s in slices(f["lvl_offsets"], f["lvl_ids"]):
+        assert np.all(np.diff(pos[s]) > 0)
+
+
+def test_oracle_small_single_event_summary():
+    ev = W.uniform_event()
+    with np.load(GOLDEN / "uniform3d_n100000_summary.npz") as z:
+        tab, tid = O.build(ev.coords, ev.ids)
+        assert hashlib.sha256(tab.tobytes()).hexdigest() == str(z["tab_sha"])
+        assert hashlib.sha256(tid.tobytes()).hexdigest() == str(z["ids_sha"])
+        c, o, i, _ = O.search(tab, tid, ev.mins, ev.maxs, variant=O.LEVEL_ORDER)
+        assert np.array_equal(c, z["counts"])
+        assert hashlib.sha256(i.tobytes()).hexdigest() == str(z["lvl_ids_sha"])
+
+
+def test_digest_definition():
+    ids = np.array([0, 1, 2, 3, 0xFFFFFFFF], dtype=np.uint32)
+    m = O.mix64(ids)
+    for a, b in zip(ids, m):
+        assert O.lib().fkd_oracle_mix64(int(a)) == int(b)
+    f = load("uniform3d_n1000")
+    c, d = O.search_digest(f["tab"], f["tab_ids"], f["mins"], f["maxs"])
+    assert np.array_equal(c, f["rec_counts"])
+    assert np.array_equal(d, O.digest_of(f["rec_ids"], f["rec_offsets"]))
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference build not present")
+def test_oracle_matches_reference_on_random_inputs():
+    rng = np.random.default_rng(99)
+    for n in [10, 257, 4096, 30000]:
+        for dim in (2, 3, 4):
+            c = rng.random((dim, n), dtype=np.float32)
+            c[0] = np.round(c[0] * 64) / 64
+            ids = rng.permutation(n).astype(np.uint32)
+            t1 = O.build(c, ids)
+            r = O.RefTree(c, ids)
+            r.build()
+            t2 = r.tables()
+            r.close()
+            assert np.array_equal(t1[0].view(np.uint32), t2[0].view(np.uint32)) and np.array_equal(t1[1], t2[1])

@@ -1,0 +1,138 @@
+"""GPU search parity through the C ABI: per-box id lists equal the
+reference's (golden fixtures, in its emission order), sets equal the
+recursive search and the brute-force scan, counts and digests agree."""
+import hashlib
+
+import numpy as np
+import pytest
+
+import fkdtree_b200 as F
+from fkdtree_b200 import workloads as W
+from oracle import oracle as O
+from tests._fixtures import GOLDEN, fixture_names, load, slices
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name", fixture_names())
+def test_ordered_results_match_reference_lists(cuda, name):
+    f = load(name)
+    t = F.FKDTree(f["coords"], f["ids"]).build()
+    offs, ids = t.search_boxes(f["mins"], f["maxs"], ordered=True)
+    got = slices(offs, ids)
+    sel = f.get("lvl_sel")
+    want = slices(f["lvl_offsets"], f["lvl_ids"])
+    idx = range(len(got)) if sel is None else sel
+    for k, j in enumerate(idx):
+        assert np.array_equal(got[j], want[k]), f"box {j}"
+    # the recursive variant: same set
+    for a, b in zip(got, slices(f["rec_offsets"], f["rec_ids"])):
+        assert np.array_equal(np.sort(a), np.sort(b))
+    # per-box counts (search_in_the_box_multiple)
+    assert np.array_equal(t.search_in_the_box_multiple(f["mins"], f["maxs"]), f["rec_counts"])
+
+
+@pytest.mark.parametrize("name", ["uniform3d_n1000", "layers4d_n3000", "grid2d_n2000", "clustered3d_n20000"])
+def test_unordered_sets_and_digests(cuda, name):
+    f = load(name)
+    t = F.FKDTree(f["coords"], f["ids"]).build()
+    offs, ids = t.search_boxes(f["mins"], f["maxs"], ordered=False)
+    for a, b in zip(slices(offs, ids), slices(f["rec_offsets"], f["rec_ids"])):
+        assert np.array_equal(np.sort(a), np.sort(b))
+    c, d = t.digest_boxes(f["mins"], f["maxs"])
+    assert np.array_equal(c, f["rec_counts"])
+    assert np.array_equal(d, O.digest_of(f["rec_ids"], f["rec_offsets"]))
+
+
+def test_single_box_api(cuda):
+    f = load("uniform3d_n1000")
+    t = F.FKDTree(f["coords"], f["ids"]).build()
+    want = slices(f["lvl_offsets"], f["lvl_ids"])
+    for j in range(5):
+        lo, hi = f["mins"][:, j], f["maxs"][:, j]
+        assert np.array_equal(t.search_in_the_box(lo, hi), want[j])
+        assert np.array_equal(t.search_in_the_box_BFS(lo, hi), want[j])
+        assert np.array_equal(t.search_in_the_box_branchless(lo, hi), want[j])
+        assert np.array_equal(np.sort(t.search_in_the_box_recursive(lo, hi)), np.sort(want[j]))
+
+
+def test_small_single_event_against_reference_summary(cuda):
+    """100,000 uniform points, one box per point, half-width 0.01, seed 0."""
+    ev = W.uniform_event()
+    t = F.FKDTree(ev.coords, ev.ids).build()
+    tab, tid = t.tables()
+    offs, ids = t.search_boxes(ev.mins, ev.maxs, ordered=True)
+    with np.load(GOLDEN / "uniform3d_n100000_summary.npz") as z:
+        assert hashlib.sha256(tab.tobytes()).hexdigest() == str(z["tab_sha"])
+        assert hashlib.sha256(tid.tobytes()).hexdigest() == str(z["ids_sha"])
+        assert np.array_equal(np.diff(offs.astype(np.int64)), z["counts"].astype(np.int64))
+        assert hashlib.sha256(ids.tobytes()).hexdigest() == str(z["lvl_ids_sha"])
+
+
+@pytest.mark.parametrize("dim", [1, 2, 3, 4])
+def test_search_vs_brute_force_random(cuda, dim):
+    rng = np.random.default_rng(dim)
+    n = 50_000
+    c = rng.random((dim, n), dtype=np.float32)
+    ids = rng.permutation(n).astype(np.uint32)
+    q = 3000
+    ctr = c[:, rng.integers(0, n, q)]
+    hw = rng.uniform(0.0, 0.2, (dim, q)).astype(np.float32)
+    mins, maxs = (ctr - hw).astype(np.float32), (ctr + hw).astype(np.float32)
+    mins[:, :10] = -np.inf   # half-open and unbounded boxes
+    maxs[:, 5:15] = np.inf
+    mins[:, 20:25], maxs[:, 20:25] = maxs[:, 20:25].copy(), mins[:, 20:25].copy()  # empty boxes (lo > hi)
+    t = F.FKDTree(c, ids).build()
+    tab, tid = t.tables()
+    cb, ob, ib, _ = O.search(tab, tid, mins, maxs, variant=O.BRUTE)
+    offs, got = t.search_boxes(mins, maxs, ordered=True)
+    assert np.array_equal(offs, ob)
+    assert np.array_equal(got, ib)  # brute force scans in heap order too
+    c2, d2 = t.digest_boxes(mins, maxs)
+    assert np.array_equal(c2, cb) and np.array_equal(d2, O.digest_of(ib, ob))
+
+
+def test_whole_tree_and_nan_boxes(cuda):
+    rng = np.random.default_rng(3)
+    n = 10_000
+    c = rng.random((3, n), dtype=np.float32)
+    t = F.FKDTree(c).build()
+    mins = np.full((3, 3), -np.inf, np.float32)
+    maxs = np.full((3, 3), np.inf, np.float32)
+    mins[0, 1] = np.nan
+    maxs[2, 2] = np.nan
+    offs, got = t.search_boxes(mins, maxs, ordered=False)
+    assert offs[1] - offs[0] == n and np.array_equal(np.sort(got[:n]), np.arange(n))
+    assert offs[2] == offs[1] and offs[3] == offs[2]  # NaN bounds select nothing, like the reference
+
+
+def test_clustered_large_boxes_vs_recursive(cuda):
+    """Boxes containing whole dense clusters -- the regime where the
+    reference's FQueue overflows (FQueue.h:158); the GPU frontier must not
+    drop anything."""
+    ev = W.clustered_event(n=1 << 20, n_queries=4096, n_clusters=64, hw_lo=0.001, hw_hi=0.05, seed=4)
+    t = F.FKDTree(ev.coords, ev.ids).build()
+    tab, tid = t.tables()
+    cr, orr, ir, _ = O.search(tab, tid, ev.mins, ev.maxs, variant=O.RECURSIVE)
+    offs, got = t.search_boxes(ev.mins, ev.maxs, ordered=False)
+    assert np.array_equal(offs, orr)
+    ok = all(np.array_equal(np.sort(a), np.sort(b)) for a, b in zip(slices(offs, got), slices(orr, ir)))
+    assert ok
+    c, d = t.digest_boxes(ev.mins, ev.maxs)
+    assert np.array_equal(c, cr) and np.array_equal(d, O.digest_of(ir, orr))
+
+
+def test_device_memory_search_and_capacity_error(cuda):
+    import torch
+    ev = W.uniform_event(n=100_000, seed=8, half_width=0.02)
+    t = F.FKDTree(torch.from_numpy(ev.coords).to(cuda)).build()
+    mins = torch.from_numpy(ev.mins).to(cuda)
+    maxs = torch.from_numpy(ev.maxs).to(cuda)
+    offs, ids = t.search_boxes(mins, maxs, ordered=True)
+    tab, tid = t.tables()
+    cb, ob, ib, _ = O.search(tab, tid, ev.mins, ev.maxs, variant=O.LEVEL_ORDER)
+    assert np.array_equal(offs.cpu().numpy().astype(np.uint64), ob)
+    assert np.array_equal(ids.cpu().numpy().view(np.uint32), ib)
+    with pytest.raises(F.FKDError) as e:
+        t.search_boxes(ev.mins, ev.maxs, capacity=10)
+    assert e.value.status == 6
