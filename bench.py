@@ -1,0 +1,388 @@
+#!/usr/bin/env python
+"""FKDTree build + box search benchmark (B200).
+
+One step = build the flat kd-tree over the workload's points and answer all
+of its box queries (count pass, prefix sum, write pass) -- the reference's
+FKDTree_CPU::build (FKDTree_cpu.h:221-277) followed by search_in_the_box over
+every box (main.cpp:369-381).
+
+Default workload (single GPU): 16,777,216 float32 points in 3D, 80% from 4,096
+Gaussian clusters (sigma 0.002, Dirichlet(1) weights) + 20% uniform
+background, 1,048,576 boxes centred on random points with half-widths
+U[0.001, 0.02] per dim, seed 1 -- seeded synthetic data of the shapes and
+distributions the reference's benchmark description gives.  The point set
+(268 MB) and the result ids (~18 GB) are far larger than the 126 MB L2, so no
+L2 flush is needed between steps.
+
+Printed JSON line (rank 0):
+  value     build+search throughput over the whole job, Mpoints/s (points of
+            the tree built and queried per second; N GPUs run N replicas)
+  e2e       the same through the public C ABI with pinned host buffers:
+            host->device copy of points and boxes, build, table download,
+            search, device->host copy of offsets and every result id
+  roofline  achieved algorithmic GB/s of the dominant phase vs measured HBM peak
+  cpu_baseline  the reference CPU tree (oracle/_ref) on this host's cores
+
+`--impl reference` times the reference's own CPU implementation (the
+unmodified FKDTree_CPU compiled from its headers into oracle/_ref) on the
+same workload: serial build (the reference build is serial by design) plus
+search_in_the_box_recursive over a sample of the boxes on all host threads.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "build Mpoints/s + box queries/s, learned/batched vs plain GPU, exact results"
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="clustered16m", choices=["clustered16m", "uniform100k"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-queries", type=int, default=8192, help="box sample of the CPU baseline")
+    return ap.parse_args()
+
+
+def make_workload(name):
+    from fkdtree_b200 import workloads as W
+    if name == "uniform100k":
+        ev = W.uniform_event(n=100_000, half_width=0.01, seed=0)
+        cfg = {"workload": "uniform3d_100k", "n_points": ev.n, "n_boxes": ev.q, "dim": 3,
+               "points": "U[0,1)^3", "half_width": 0.01, "seed": 0}
+    else:
+        ev = W.clustered_event()
+        cfg = {"workload": "clustered3d_16m_boxes1m", "n_points": ev.n, "n_boxes": ev.q, "dim": 3,
+               "points": "80% of 4096 Gaussian clusters (sigma 0.002, Dirichlet(1)) + 20% U[0,1)^3",
+               "half_width": "U[0.001,0.02] per dim", "seed": 1}
+    cfg["l2"] = "inputs larger than L2 (no flush)" if ev.n * 16 > 126e6 else "inputs smaller than L2"
+    return ev, cfg
+
+
+def hbm_peak():
+    try:
+        with open(PEAKS_FILE) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def build_bytes(n, dim):
+    """Algorithmic bytes of one build: every record read and written once per
+    partition level plus the final table write, N*(4*dim+4)*(2*floor(log2 N)+1)."""
+    L = int(math.floor(math.log2(n))) if n > 0 else 0
+    return n * (4 * dim + 4) * (2 * L + 1)
+
+
+def search_bytes(n, dim, q, results):
+    """Tree read once, boxes + count + offset per box, result ids written."""
+    return n * (4 * dim + 4) + q * (8 * dim + 8) + 4 * results
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.p:
+            time.sleep(0.25)
+            self.p.terminate()
+            try:
+                self.out, _ = self.p.communicate(timeout=5)
+            except Exception:
+                self.p.kill()
+
+    def summary(self):
+        rows = [r.split(",") for r in (self.out or "").strip().splitlines() if r.count(",") >= 8]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = sorted(float(r[1]) for r in rows)
+        mx = max(float(r[2]) for r in rows)
+        reasons = set()
+        for r in rows:
+            for name, col in (("hw_slowdown", 5), ("hw_thermal_slowdown", 6), ("sw_thermal_slowdown", 7),
+                              ("sw_power_cap", 8)):
+                if r[col].strip().lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(rows)}
+
+
+# ------------------------------------------------------------------ our arm
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    from fkdtree_b200 import _capi
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    ev, cfg = make_workload(args.workload)
+    n, q, dim = ev.n, ev.q, ev.dim
+    L = _capi.lib()
+    stream = torch.cuda.current_stream(dev)
+    h = C.c_void_p()
+    _capi.check(L.fkd_create(dim, _capi.FLAG_ASYNC, C.c_void_p(stream.cuda_stream), C.byref(h)))
+    P = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+
+    coords = torch.from_numpy(ev.coords).to(dev)
+    ids = torch.from_numpy(ev.ids.view(np.int32)).to(dev)
+    mins = torch.from_numpy(ev.mins).to(dev)
+    maxs = torch.from_numpy(ev.maxs).to(dev)
+    offsets = torch.empty(q + 1, dtype=torch.int64, device=dev)
+    counts = torch.empty(q, dtype=torch.int32, device=dev)
+    # size the result buffer once
+    _capi.check(L.fkd_build(h, P(coords), P(ids), n, _capi.MEM_DEVICE))
+    _capi.check(L.fkd_search_count(h, P(mins), P(maxs), q, P(counts), _capi.MEM_DEVICE))
+    _capi.check(L.fkd_sync(h))
+    results = int(counts.to(torch.int64).sum().item())
+    out = torch.empty(max(results, 1), dtype=torch.int32, device=dev)
+    total = C.c_uint64(0)
+
+    ev_b0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ev_b1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ev_s1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+
+    def step(i=None):
+        if i is not None:
+            ev_b0[i].record(stream)
+        _capi.check(L.fkd_build(h, P(coords), P(ids), n, _capi.MEM_DEVICE))
+        if i is not None:
+            ev_b1[i].record(stream)
+        _capi.check(L.fkd_search(h, P(mins), P(maxs), q, P(offsets), P(out), results, C.byref(total), 0,
+                                 _capi.MEM_DEVICE))
+        if i is not None:
+            ev_s1[i].record(stream)
+
+    for _ in range(args.warmup):
+        step()
+    _capi.check(L.fkd_sync(h))
+    launches0 = L.fkd_kernel_launches()
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for i in range(args.steps):
+            step(i)
+        t1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    launches = L.fkd_kernel_launches() - launches0
+    _capi.check(L.fkd_sync(h))
+    assert total.value == results
+    ms = t0.elapsed_time(t1)
+    build_ms = float(np.mean([ev_b0[i].elapsed_time(ev_b1[i]) for i in range(args.steps)]))
+    search_ms = float(np.mean([ev_b1[i].elapsed_time(ev_s1[i]) for i in range(args.steps)]))
+    if world > 1:
+        tt = torch.tensor([ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    ms_step = ms / args.steps
+    value = world * n / (ms_step / 1e3) / 1e6
+
+    peak, peak_kind = hbm_peak()
+    bb = build_bytes(n, dim)
+    sb = search_bytes(n, dim, q, results)
+    phases = {
+        "build": {"ms": build_ms, "algorithmic_bytes": bb, "gbs": bb / build_ms / 1e6,
+                  "kernels": ["k_sel_init", "k_hist", "k_partition", "k_subtree"]},
+        "search": {"ms": search_ms, "algorithmic_bytes": sb, "gbs": sb / search_ms / 1e6,
+                   "kernels": ["k_box_keys", "k_box_scatter", "k_search<count>", "k_scan_*", "k_search<write>"]},
+    }
+    dom = "build" if build_ms >= search_ms else "search"
+    roof = {"bound": "hbm", "phase": dom, "achieved": phases[dom]["gbs"], "peak": peak, "unit": "GB/s",
+            "frac": phases[dom]["gbs"] / peak, "peak_kind": peak_kind, "traffic": None,
+            "algorithmic_bytes_per_launch": phases[dom]["algorithmic_bytes"]}
+
+    line = {"metric": METRIC, "value": value, "unit": "Mpoints/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator, fkdtree_b200/workloads.py)",
+            "config": dict(cfg, parallelism=f"replicas{world}", results_per_step=results),
+            "build_mpoints_per_s": n / build_ms / 1e3, "search_mboxes_per_s": q / search_ms / 1e3,
+            "phases": phases, "roofline": roof, "gpu_launches": int(launches)}
+    line["clocks"] = clk.summary()
+
+    if not args.no_e2e:
+        line["e2e"] = run_e2e(args, L, h, ev, results, stream, world, barrier, dev)
+    _capi.check(L.fkd_destroy(h))
+    if rank == 0 and world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(ev, args.cpu_queries)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def run_e2e(args, L, h, ev, results, stream, world, barrier, dev):
+    """The public C ABI with pinned host buffers: every step copies the points
+    and boxes in and the tables, offsets and every result id out."""
+    import torch
+
+    from fkdtree_b200 import _capi
+    n, q, dim = ev.n, ev.q, ev.dim
+    pin = lambda a: torch.from_numpy(a).pin_memory()  # noqa: E731
+    coords_h, ids_h = pin(ev.coords), pin(ev.ids.view(np.int32))
+    mins_h, maxs_h = pin(ev.mins), pin(ev.maxs)
+    tab_h = torch.empty((dim, n), dtype=torch.float32, pin_memory=True)
+    tid_h = torch.empty(n, dtype=torch.int32, pin_memory=True)
+    offs_h = torch.empty(q + 1, dtype=torch.int64, pin_memory=True)
+    out_h = torch.empty(max(results, 1), dtype=torch.int32, pin_memory=True)
+    P = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+    total = C.c_uint64(0)
+
+    def step():
+        _capi.check(L.fkd_build(h, P(coords_h), P(ids_h), n, _capi.MEM_HOST))
+        _capi.check(L.fkd_get_tables(h, P(tab_h), P(tid_h), _capi.MEM_HOST))
+        _capi.check(L.fkd_search(h, P(mins_h), P(maxs_h), q, P(offs_h), P(out_h), results, C.byref(total), 0,
+                                 _capi.MEM_HOST))
+
+    k = max(1, min(args.steps, 3))
+    step()
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(k):
+        step()
+    torch.cuda.synchronize()
+    sec = time.perf_counter() - t0
+    barrier()
+    if world > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([sec], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        sec = float(tt.item())
+    assert total.value == results
+    h2d = n * 4 * dim + n * 4 + 2 * q * 4 * dim
+    d2h = n * 4 * dim + n * 4 + (q + 1) * 8 + 4 * results
+    return {"value": world * n / (sec / k) / 1e6, "unit": "Mpoints/s", "steps": k, "ms_per_step": 1e3 * sec / k,
+            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+            "path": "fkd_build + fkd_get_tables + fkd_search, FKD_MEM_HOST (pinned)"}
+
+
+# ------------------------------------------------------------ reference arm
+
+def ref_step(oracle_mod, ev, nq_sample, threads):
+    """Reference FKDTree_CPU build of all points (serial) + recursive search of
+    a box sample on all threads; returns (build_s, search_s_extrapolated)."""
+    r = oracle_mod.RefTree(ev.coords, ev.ids)
+    tb = r.build()
+    sel = np.linspace(0, ev.q - 1, nq_sample).astype(np.int64)
+    _, _, _, ts = r.search(ev.mins[:, sel], ev.maxs[:, sel], variant=oracle_mod.RECURSIVE, want_ids=True,
+                           threads=threads)
+    r.close()
+    return tb, ts * ev.q / nq_sample
+
+
+def cpu_baseline(ev, nq_sample):
+    from oracle import oracle as O
+    if not O.ref_available():
+        return {"value": None, "unit": "Mpoints/s", "kind": "reference", "cores": 0,
+                "sample": "reference CPU build unavailable (oracle/_ref not built)"}
+    threads = O.host_threads()
+    tb, ts = ref_step(O, ev, nq_sample, threads)
+    return {"value": ev.n / (tb + ts) / 1e6, "unit": "Mpoints/s", "kind": "reference", "cores": threads,
+            "build_s": tb, "search_s": ts,
+            "sample": (f"FKDTree_CPU::build of all {ev.n} points (serial, as in the reference) + "
+                       f"search_in_the_box_recursive on {nq_sample} of {ev.q} boxes with {threads} OpenMP threads, "
+                       "search time scaled to all boxes")}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    if not O.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libfkdref.so not built"}), flush=True)
+        return
+    ev, cfg = make_workload(args.workload)
+    threads = O.host_threads()
+    nq = min(args.cpu_queries, ev.q)
+    # warm-up steps on a 1/16 sample of the points keep the run bounded
+    from fkdtree_b200 import workloads as W
+    sub = W.Event(ev.dim, np.ascontiguousarray(ev.coords[:, : ev.n // 16]), ev.ids[: ev.n // 16].copy(),
+                  ev.mins, ev.maxs)
+    for _ in range(args.warmup):
+        ref_step(O, sub, min(512, nq), threads)
+    tot_b = tot_s = 0.0
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        tb, ts = ref_step(O, ev, nq, threads)
+        tot_b += tb
+        tot_s += ts
+    wall = time.perf_counter() - t0
+    ms_step = 1e3 * (tot_b + tot_s) / args.steps
+    value = ev.n / (ms_step / 1e3) / 1e6
+    line = {"metric": METRIC, "value": value, "unit": "Mpoints/s", "n_gpus": 0, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator, fkdtree_b200/workloads.py)",
+            "config": dict(cfg, parallelism="cpu"), "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": "Mpoints/s", "kind": "reference", "cores": threads,
+                             "sample": (f"per step: FKDTree_CPU::build of all {ev.n} points (serial) + "
+                                        f"search_in_the_box_recursive on {nq} of {ev.q} boxes with {threads} "
+                                        "OpenMP threads, search time scaled to all boxes; warm-up steps on 1/16 "
+                                        "of the points"),
+                             "build_s_per_step": tot_b / args.steps, "search_s_per_step": tot_s / args.steps,
+                             "wall_s": wall},
+            "e2e": {"value": value, "unit": "Mpoints/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -24,6 +24,7 @@ _vp, _u32, _u64, _int = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int
 SIGNATURES = {
     "fkd_version": ([], C.c_char_p),
     "fkd_last_error": ([], C.c_char_p),
+    "fkd_kernel_launches": ([], C.c_uint64),
     "fkd_create": ([_int, _u32, _vp, C.POINTER(_vp)], _int),
     "fkd_destroy": ([_vp], _int),
     "fkd_set_stream": ([_vp, _vp], _int),

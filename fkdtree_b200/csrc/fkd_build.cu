@@ -33,7 +33,9 @@ namespace fkd {
 // ---------------------------------------------------------------- global
 
 constexpr int GT = 256;            // threads of the global-level kernels
-constexpr int GIPT = 16;           // records per thread
+constexpr int GIPT = 16;           // records per thread (digit passes)
+constexpr int PIPT = 8;            // records per thread (partition)
+constexpr int PTILE = GT * PIPT;
 constexpr int GTILE = GT * GIPT;   // records per CTA tile
 constexpr int GWARPS = GT / 32;
 constexpr int RBITS = 11;          // digit width of the global select
@@ -56,8 +58,13 @@ __device__ __forceinline__ void write_node(const Table& tab, uint32_t h, const u
   tab.ids[h] = rec[dim];
 }
 
-__global__ void k_sel_init(Geom g, uint32_t d, SegSel* __restrict__ sel) {
+__global__ void k_sel_init(Geom g, uint32_t d, SegSel* __restrict__ sel, uint32_t* __restrict__ pending) {
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s == 0) {
+    // pending[p] != 0: digit pass p has a segment to work on
+    pending[0] = 1u;
+    for (int p = 1; p <= RPASSES; ++p) pending[p] = 0u;
+  }
   if (s >= (1u << d)) return;
   const uint32_t len = seg_len(g, d, s);
   SegSel st;
@@ -75,10 +82,14 @@ __global__ void k_sel_init(Geom g, uint32_t d, SegSel* __restrict__ sel) {
 // One digit pass of the segmented select for every segment of depth d.
 template <int DIM>
 __global__ void __launch_bounds__(GT) k_hist(Geom g, uint32_t d, uint32_t tps, CSoA src, SegSel* __restrict__ sel,
-                                             uint32_t* __restrict__ ghist, uint32_t* __restrict__ err) {
+                                             uint32_t* __restrict__ ghist, const uint32_t* __restrict__ pending_now,
+                                             uint32_t* __restrict__ pending_next, uint32_t* __restrict__ err) {
   __shared__ uint32_t hist[RBINS];
   __shared__ uint32_t wsum[GWARPS];
   __shared__ uint32_t s_last;
+  // pending_now was raised by the previous pass when some segment still needs
+  // a digit; without it the whole launch is a no-op.
+  if (*(volatile const uint32_t*)pending_now == 0u) return;
   const uint32_t s = blockIdx.x / tps, t = blockIdx.x - s * tps;
   const uint32_t len = seg_len(g, d, s);
   const uint32_t ntiles = (len + GTILE - 1) / GTILE;
@@ -117,11 +128,16 @@ __global__ void __launch_bounds__(GT) k_hist(Geom g, uint32_t d, uint32_t tps, C
 #pragma unroll
   for (int k = 0; k < GIPT; ++k) {
     const uint32_t e = t0 + k * GT + threadIdx.x;
+    uint32_t dig = 0xffffffffu;  // no digit: outside the tile or prefix mismatch
     if (e < t1) {
       const uint64_t key = order_key(vb[k], idv[k]);
-      const bool match = bits == 0u || (key >> (64u - bits)) == prefix;
-      if (match) atomicAdd(&hist[(uint32_t)(key >> shift) & (nb - 1u)], 1u);
+      if (bits == 0u || (key >> (64u - bits)) == prefix) dig = (uint32_t)(key >> shift) & (nb - 1u);
     }
+    // lanes with the same digit add once (clustered data piles onto few bins);
+    // all 32 lanes take part in the match
+    const uint32_t peers = __match_any_sync(0xffffffffu, dig);
+    if (dig != 0xffffffffu && (threadIdx.x & 31u) == (uint32_t)(__ffs(peers) - 1))
+      atomicAdd(&hist[dig], (uint32_t)__popc(peers));
   }
   __syncthreads();
   uint32_t* gh = ghist + (uint64_t)s * RBINS;
@@ -171,6 +187,7 @@ __global__ void __launch_bounds__(GT) k_hist(Geom g, uint32_t d, uint32_t tps, C
       p->krem = krem - cum;
       p->cnt = h[k];
       p->done = (h[k] == 1u || nbits == 64u) ? 1u : 0u;
+      if (!p->done) *pending_next = 1u;
     }
     cum += h[k];
   }
@@ -181,70 +198,75 @@ __global__ void __launch_bounds__(GT) k_hist(Geom g, uint32_t d, uint32_t tps, C
   if (threadIdx.x == GT - 1 && krem >= wbase + incl) atomicOr(err, ERRB_INTERNAL);
 }
 
+template <int DIM>
+__device__ __forceinline__ uint32_t pick_coord(const uint32_t* rec, uint32_t c) {
+  uint32_t v = rec[0];
+#pragma unroll
+  for (int w = 1; w < DIM; ++w) v = (c == (uint32_t)w) ? rec[w] : v;
+  return v;
+}
+
 // Streams every record of depth-d segments once: records below the pivot go
 // to [start, start + rank), the pivot to the table, the rest above it.
 template <int DIM>
-__global__ void __launch_bounds__(GT) k_partition(Geom g, uint32_t d, uint32_t tps, CSoA src, SoA dst,
-                                                  SegSel* __restrict__ sel, Table tab, uint32_t* __restrict__ err) {
-  __shared__ uint32_t sL[GIPT * GWARPS], sR[GIPT * GWARPS];
+__global__ void __launch_bounds__(GT, 2) k_partition(Geom g, uint32_t d, uint32_t tps, CSoA src, SoA dst,
+                                                     SegSel* __restrict__ sel, Table tab, uint32_t* __restrict__ err) {
+  __shared__ uint32_t sL[PIPT * GWARPS], sR[PIPT * GWARPS];
   __shared__ uint32_t s_base[2];
   const uint32_t s = blockIdx.x / tps, t = blockIdx.x - s * tps;
   const uint32_t len = seg_len(g, d, s);
-  const uint32_t ntiles = (len + GTILE - 1) / GTILE;
+  const uint32_t ntiles = (len + PTILE - 1) / PTILE;
   if (t >= ntiles) return;
   const uint32_t start = seg_start(g, d, s);
   const uint32_t rank = seg_rank(g, d, s);
-  const uint32_t t0 = start + t * GTILE;
-  const uint32_t t1 = min(start + len, t0 + (uint32_t)GTILE);
+  const uint32_t t0 = start + t * PTILE;
+  const uint32_t t1 = min(start + len, t0 + (uint32_t)PTILE);
   const uint32_t bits = sel[s].bits;
   const unsigned long long prefix = sel[s].prefix;
   const uint32_t cnt = sel[s].cnt;
   const uint32_t c = d % DIM;
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
 
-  uint32_t rec[GIPT][DIM + 1];
+  uint32_t rec[PIPT][DIM + 1];
 #pragma unroll
-  for (int k = 0; k < GIPT; ++k) {
+  for (int k = 0; k < PIPT; ++k) {
     const uint32_t e = t0 + k * GT + threadIdx.x;
     const bool v = e < t1;
 #pragma unroll
     for (int w = 0; w < DIM; ++w) rec[k][w] = v ? __ldcs(src.base + (uint64_t)w * src.stride + e) : 0u;
     rec[k][DIM] = v ? __ldcs(src.ids + e) : 0u;
   }
-  uint32_t cls[GIPT];  // 0 below, 1 equal, 2 above, 3 none
+  uint32_t bl[PIPT], br[PIPT];
+  uint32_t eqmask = 0u;  // bit k: record k matches the pivot prefix
   bool nan = false;
 #pragma unroll
-  for (int k = 0; k < GIPT; ++k) {
+  for (int k = 0; k < PIPT; ++k) {
     const uint32_t e = t0 + k * GT + threadIdx.x;
-    if (e >= t1) {
-      cls[k] = 3u;
-      continue;
-    }
+    uint32_t cls = 3u;  // 0 below, 1 equal, 2 above, 3 none
+    if (e < t1) {
 #pragma unroll
-    for (int w = 0; w < DIM; ++w) nan |= is_nan_bits(rec[k][w]);
-    const uint64_t key = order_key(rec[k][c], rec[k][DIM]);
-    if (bits == 0u) {
-      cls[k] = 1u;
-    } else {
-      const uint64_t top = bits >= 64u ? key : (key >> (64u - bits));
-      cls[k] = top < prefix ? 0u : (top > prefix ? 2u : 1u);
+      for (int w = 0; w < DIM; ++w) nan |= is_nan_bits(rec[k][w]);
+      const uint64_t key = order_key(pick_coord<DIM>(rec[k], c), rec[k][DIM]);
+      if (bits == 0u) {
+        cls = 1u;
+      } else {
+        const uint64_t top = bits >= 64u ? key : (key >> (64u - bits));
+        cls = top < prefix ? 0u : (top > prefix ? 2u : 1u);
+      }
     }
-  }
-  if (nan) atomicOr(err, ERRB_NAN);
-  uint32_t bl[GIPT], br[GIPT];
-#pragma unroll
-  for (int k = 0; k < GIPT; ++k) {
-    bl[k] = __ballot_sync(0xffffffffu, cls[k] == 0u);
-    br[k] = __ballot_sync(0xffffffffu, cls[k] == 2u);
+    if (cls == 1u) eqmask |= 1u << k;
+    bl[k] = __ballot_sync(0xffffffffu, cls == 0u);
+    br[k] = __ballot_sync(0xffffffffu, cls == 2u);
     if (lane == 0) {
       sL[k * GWARPS + warp] = __popc(bl[k]);
       sR[k * GWARPS + warp] = __popc(br[k]);
     }
   }
+  if (nan) atomicOr(err, ERRB_NAN);
   __syncthreads();
   if (warp == 0) {
-    // exclusive scan over the GIPT*GWARPS (slot-major) warp counts
-    constexpr int PER = GIPT * GWARPS / 32;
+    // exclusive scan over the PIPT*GWARPS (slot-major) warp counts
+    constexpr int PER = PIPT * GWARPS / 32;
     uint32_t a[PER], b[PER], sa = 0u, sb = 0u;
 #pragma unroll
     for (int k = 0; k < PER; ++k) {
@@ -279,16 +301,17 @@ __global__ void __launch_bounds__(GT) k_partition(Geom g, uint32_t d, uint32_t t
   __syncthreads();
   const uint32_t lt = lanemask_lt();
   const uint32_t endL = start + rank, endR = start + len;
+  const uint32_t baseL = start + s_base[0], baseR = endL + 1u + s_base[1];
 #pragma unroll
-  for (int k = 0; k < GIPT; ++k) {
+  for (int k = 0; k < PIPT; ++k) {
     uint32_t pos = 0xffffffffu, lim = 0u;
-    if (cls[k] == 0u) {
-      pos = start + s_base[0] + sL[k * GWARPS + warp] + __popc(bl[k] & lt);
+    if ((bl[k] >> lane) & 1u) {
+      pos = baseL + sL[k * GWARPS + warp] + __popc(bl[k] & lt);
       lim = endL;
-    } else if (cls[k] == 2u) {
-      pos = endL + 1u + s_base[1] + sR[k * GWARPS + warp] + __popc(br[k] & lt);
+    } else if ((br[k] >> lane) & 1u) {
+      pos = baseR + sR[k * GWARPS + warp] + __popc(br[k] & lt);
       lim = endR;
-    } else if (cls[k] == 1u) {
+    } else if ((eqmask >> k) & 1u) {
       const uint32_t krem = sel[s].krem;
       uint32_t ticket = 0u;
       if (cnt != 1u) ticket = atomicAdd(&sel[s].curE, 1u);  // repeated (coordinate, id) keys only
@@ -305,8 +328,8 @@ __global__ void __launch_bounds__(GT) k_partition(Geom g, uint32_t d, uint32_t t
     if (pos != 0xffffffffu) {
       if (pos < lim) {
 #pragma unroll
-        for (int w = 0; w < DIM; ++w) dst.base[(uint64_t)w * dst.stride + pos] = rec[k][w];
-        dst.ids[pos] = rec[k][DIM];
+        for (int w = 0; w < DIM; ++w) __stcs(dst.base + (uint64_t)w * dst.stride + pos, rec[k][w]);
+        __stcs(dst.ids + pos, rec[k][DIM]);
       } else {
         atomicOr(err, ERRB_INTERNAL);
       }
@@ -455,12 +478,32 @@ __global__ void __launch_bounds__(ST, 1) k_subtree(Geom g, uint32_t d0, CSoA src
         sdup[u] = 0u;
       }
       __syncthreads();
-      for (uint32_t p = threadIdx.x; p < nloc; p += ST) {
-        const uint32_t u = segA[p];
-        if (u == DONE) continue;
-        const uint64_t key = skey<DIM>(bufA, p, c);
-        atomicMin(&smin[u], (unsigned long long)key);
-        atomicMax(&smax[u], (unsigned long long)key);
+      for (uint32_t p0 = 0; p0 < nloc; p0 += ST) {
+        const uint32_t p = p0 + threadIdx.x;
+        const uint32_t u = p < nloc ? segA[p] : DONE;
+        const bool valid = u != DONE;
+        unsigned long long kmin = valid ? skey<DIM>(bufA, p, c) : ~0ull;
+        unsigned long long kmax = valid ? kmin : 0ull;
+        // a warp whose lanes all sit in one segment reduces before the atomics
+        // (every lane executes the shuffle and the vote)
+        const uint32_t u0 = __shfl_sync(0xffffffffu, u, 0);
+        const bool same = valid && u == u0;
+        if (__all_sync(0xffffffffu, same)) {
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long a = __shfl_xor_sync(0xffffffffu, kmin, o);
+            const unsigned long long b = __shfl_xor_sync(0xffffffffu, kmax, o);
+            kmin = a < kmin ? a : kmin;
+            kmax = b > kmax ? b : kmax;
+          }
+          if (lane == 0) {
+            atomicMin(&smin[u], kmin);
+            atomicMax(&smax[u], kmax);
+          }
+        } else if (valid) {
+          atomicMin(&smin[u], kmin);
+          atomicMax(&smax[u], kmax);
+        }
       }
       __syncthreads();
       for (uint32_t u = threadIdx.x; u < nseg; u += ST) {
@@ -469,9 +512,6 @@ __global__ void __launch_bounds__(ST, 1) k_subtree(Geom g, uint32_t d0, CSoA src
         spre[u] = cp == 0u ? 0ull : (cp >= 64u ? lo : (lo >> (64u - cp)));
         sbits[u] = cp;
         scnt[u] = seg_len(g, d, t0 + u);
-        // with a common prefix of all 64 bits every point of the segment has
-        // the same key: nothing left to select
-        if (cp == 64u) scnt[u] = scnt[u];
       }
       __syncthreads();
       for (int pass = 0; pass < 64; ++pass) {
@@ -482,17 +522,25 @@ __global__ void __launch_bounds__(ST, 1) k_subtree(Geom g, uint32_t d0, CSoA src
         if (!__syncthreads_or(active)) break;
         for (uint32_t i = threadIdx.x; i < (nseg << hb) / 2u; i += ST) work[i] = 0u;
         __syncthreads();
-        for (uint32_t p = threadIdx.x; p < nloc; p += ST) {
-          const uint32_t u = segA[p];
-          if (u == DONE) continue;
-          const uint32_t bits = sbits[u];
-          if (scnt[u] <= 1u || bits >= 64u) continue;
-          const uint64_t key = skey<DIM>(bufA, p, c);
-          if (bits != 0u && (key >> (64u - bits)) != spre[u]) continue;
-          const uint32_t w = (64u - bits) < hb ? (64u - bits) : hb;
-          const uint32_t dig = (uint32_t)(key >> (64u - bits - w)) & ((1u << w) - 1u);
-          const uint32_t slot = (u << hb) + dig;
-          atomicAdd(&work[slot >> 1], 1u << (16u * (slot & 1u)));
+        for (uint32_t p0 = 0; p0 < nloc; p0 += ST) {
+          const uint32_t p = p0 + threadIdx.x;
+          uint32_t slot = 0xffffffffu;
+          const uint32_t u = p < nloc ? segA[p] : DONE;
+          if (u != DONE) {
+            const uint32_t bits = sbits[u];
+            if (scnt[u] > 1u && bits < 64u) {
+              const uint64_t key = skey<DIM>(bufA, p, c);
+              if (bits == 0u || (key >> (64u - bits)) == spre[u]) {
+                const uint32_t w = (64u - bits) < hb ? (64u - bits) : hb;
+                const uint32_t dig = (uint32_t)(key >> (64u - bits - w)) & ((1u << w) - 1u);
+                slot = (u << hb) + dig;
+              }
+            }
+          }
+          // lanes hitting the same counter add once
+          const uint32_t peers = __match_any_sync(0xffffffffu, slot);
+          if (slot != 0xffffffffu && lane == (uint32_t)(__ffs(peers) - 1))
+            atomicAdd(&work[slot >> 1], (uint32_t)__popc(peers) << (16u * (slot & 1u)));
         }
         __syncthreads();
         // warp per segment: find the digit holding krem
@@ -547,11 +595,8 @@ __global__ void __launch_bounds__(ST, 1) k_subtree(Geom g, uint32_t d0, CSoA src
       // Partition: exclusive scan of packed (below | above << 16) flags over
       // all positions, then each point moves to its side of its segment.
       uint32_t* scan = work;
-      uint32_t fl[PPT];
-      uint32_t tsum = 0u;
-#pragma unroll
-      for (int k = 0; k < PPT; ++k) {
-        const uint32_t p = threadIdx.x * PPT + k;
+      // flags in a strided pass (conflict-free), scan over contiguous chunks
+      for (uint32_t p = threadIdx.x; p < (uint32_t)SUBN; p += ST) {
         uint32_t f = 0u;
         if (p < nloc) {
           const uint32_t u = segA[p];
@@ -563,8 +608,15 @@ __global__ void __launch_bounds__(ST, 1) k_subtree(Geom g, uint32_t d0, CSoA src
             f = top < pre ? 1u : (top > pre ? (1u << 16) : 0u);
           }
         }
-        fl[k] = f;
-        tsum += f;
+        scan[p] = f;
+      }
+      __syncthreads();
+      uint32_t fl[PPT];
+      uint32_t tsum = 0u;
+#pragma unroll
+      for (int k = 0; k < PPT; ++k) {
+        fl[k] = scan[threadIdx.x * PPT + k];
+        tsum += fl[k];
       }
       uint32_t incl = tsum;
 #pragma unroll
@@ -579,8 +631,7 @@ __global__ void __launch_bounds__(ST, 1) k_subtree(Geom g, uint32_t d0, CSoA src
       uint32_t run = wb + incl - tsum;
 #pragma unroll
       for (int k = 0; k < PPT; ++k) {
-        const uint32_t p = threadIdx.x * PPT + k;
-        if (p < (uint32_t)SUBN) scan[p] = run;
+        scan[threadIdx.x * PPT + k] = run;
         run += fl[k];
       }
       uint32_t total = 0u;
@@ -663,12 +714,17 @@ static cudaError_t run_build(BuildCtx& bc) {
   for (uint32_t d = 0; d < d0; ++d) {
     const uint32_t S = 1u << d;
     const uint32_t tps = (seg_len(g, d, 0) + GTILE - 1) / GTILE;
-    const uint32_t grid = S * tps;
-    k_sel_init<<<(S + 255) / 256, 256, 0, bc.stream>>>(g, d, bc.sel);
-    for (int pass = 0; pass < RPASSES; ++pass)
-      k_hist<DIM><<<grid, GT, 0, bc.stream>>>(g, d, tps, src, bc.sel, bc.ghist, bc.err);
+    const uint32_t ptps = (seg_len(g, d, 0) + PTILE - 1) / PTILE;
+    k_sel_init<<<(S + 255) / 256, 256, 0, bc.stream>>>(g, d, bc.sel, bc.pending);
+    count_launches(1);
+    for (int pass = 0; pass < RPASSES; ++pass) {
+      k_hist<DIM><<<S * tps, GT, 0, bc.stream>>>(g, d, tps, src, bc.sel, bc.ghist, bc.pending + pass,
+                                                  bc.pending + pass + 1, bc.err);
+      count_launches(1);
+    }
     SoA dst = bufs[nb];
-    k_partition<DIM><<<grid, GT, 0, bc.stream>>>(g, d, tps, src, dst, bc.sel, bc.tab, bc.err);
+    k_partition<DIM><<<S * ptps, GT, 0, bc.stream>>>(g, d, ptps, src, dst, bc.sel, bc.tab, bc.err);
+    count_launches(1);
     src = CSoA{dst.base, dst.ids, dst.stride};
     nb ^= 1;
   }
@@ -676,6 +732,7 @@ static cudaError_t run_build(BuildCtx& bc) {
   cudaError_t e = cudaFuncSetAttribute(k_subtree<DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   k_subtree<DIM><<<1u << d0, ST, smem, bc.stream>>>(g, d0, src, bc.tab, bc.err);
+  count_launches(1);
   return cudaGetLastError();
 }
 

@@ -11,6 +11,12 @@
 
 using namespace fkd;
 
+namespace fkd {
+static unsigned long long g_launches = 0;
+void count_launches(uint64_t k) { __atomic_fetch_add(&g_launches, (unsigned long long)k, __ATOMIC_RELAXED); }
+uint64_t launches_total() { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
+}  // namespace fkd
+
 namespace {
 
 thread_local std::string g_last_error;
@@ -61,13 +67,13 @@ struct fkd_tree_s {
   int device = 0;
   uint64_t n = 0;
   bool built = false;
-  DevBuf nodes, ids, work0, work1, sel, ghist, err, qctr;
-  DevBuf qlo, qhi, counts, offsets, partials, out, tmp, digests;
+  DevBuf nodes, ids, work0, work1, sel, ghist, err, qctr, passflags;
+  DevBuf qlo, qhi, counts, offsets, partials, out, tmp, digests, qorder;
   uint32_t* herr = nullptr;  // pinned mirror of err
 
   ~fkd_tree_s() {
-    DevBuf* all[] = {&nodes, &ids, &work0, &work1, &sel, &ghist, &err, &qctr,
-                     &qlo, &qhi, &counts, &offsets, &partials, &out, &tmp, &digests};
+    DevBuf* all[] = {&nodes, &ids, &work0, &work1, &sel, &ghist, &err, &qctr, &passflags,
+                     &qlo, &qhi, &counts, &offsets, &partials, &out, &tmp, &digests, &qorder};
     for (DevBuf* b : all) b->release();
     if (herr) cudaFreeHost(herr);
   }
@@ -155,10 +161,21 @@ fkd_status check_search_args(fkd_tree h, const float* mins, const float* maxs, u
   return FKD_OK;
 }
 
-// count pass into h->counts (device); returns the device counts pointer
-fkd_status count_pass(fkd_tree h, const Boxes& b, uint32_t* dcounts) {
+// Spatial processing order of the boxes (fkd_search.cu: launch_box_order).
+fkd_status box_order(fkd_tree h, const Boxes& b, const uint32_t** order) {
+  FKD_CUDA(h->qorder.ensure(box_order_words(b.q) * sizeof(uint32_t)));
+  uint32_t* o = nullptr;
+  FKD_CUDA(launch_box_order(make_geom((uint32_t)h->n), table_of(h), b, h->dim, h->qorder.as<uint32_t>(), &o,
+                            h->stream));
+  *order = o;
+  return FKD_OK;
+}
+
+// count pass into dcounts (device)
+fkd_status count_pass(fkd_tree h, const Boxes& b, uint32_t* dcounts, const uint32_t* order) {
   SearchCtx sc = search_ctx(h, b);
   sc.counts = dcounts;
+  sc.order = order;
   FKD_CUDA(launch_search(sc, h->dim, SEARCH_COUNT));
   return FKD_OK;
 }
@@ -168,6 +185,8 @@ fkd_status count_pass(fkd_tree h, const Boxes& b, uint32_t* dcounts) {
 extern "C" {
 
 const char* fkd_version(void) { return "fkdtree_b200 0.1 (sm_100a)"; }
+
+uint64_t fkd_kernel_launches(void) { return launches_total(); }
 
 const char* fkd_last_error(void) { return g_last_error.c_str(); }
 
@@ -183,6 +202,7 @@ fkd_status fkd_create(int dim, uint32_t flags, void* stream, fkd_tree* out) {
   cudaError_t e = cudaGetDevice(&h->device);
   if (e == cudaSuccess) e = h->err.ensure(sizeof(uint32_t) * 4);
   if (e == cudaSuccess) e = h->qctr.ensure(sizeof(uint32_t) * 4);
+  if (e == cudaSuccess) e = h->passflags.ensure(sizeof(uint32_t) * 64);
   if (e == cudaSuccess) e = cudaMallocHost((void**)&h->herr, sizeof(uint32_t) * 4);
   if (e == cudaSuccess) e = cudaMemsetAsync(h->err.p, 0, sizeof(uint32_t), h->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
@@ -252,6 +272,7 @@ fkd_status fkd_build(fkd_tree h, const float* coords, const uint32_t* ids, uint6
   bc.ghist = h->ghist.as<uint32_t>();
   bc.tab = table_of(h);
   bc.err = h->err.as<uint32_t>();
+  bc.pending = h->passflags.as<uint32_t>();
   bc.stream = h->stream;
   FKD_CUDA(launch_build(bc, dim));
   h->built = true;
@@ -279,6 +300,7 @@ fkd_status fkd_get_tables(fkd_tree h, float* tab, uint32_t* tab_ids, int mem) {
       dst = h->work0.as<float>();
     }
     k_tables_out<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>((uint32_t)n, h->dim, h->nodes.as<uint4>(), dst);
+    count_launches(1);
     FKD_CUDA(cudaGetLastError());
     if (mem == FKD_MEM_HOST)
       FKD_CUDA(cudaMemcpyAsync(tab, dst, (size_t)h->dim * n * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
@@ -303,15 +325,18 @@ fkd_status fkd_search_count(fkd_tree h, const float* mins, const float* maxs, ui
     dc = h->counts.as<uint32_t>();
   }
   FKD_CUDA(cudaMemsetAsync(h->err.p, 0, sizeof(uint32_t), h->stream));
-  if ((s = count_pass(h, b, dc)) != FKD_OK) return s;
+  const uint32_t* order = nullptr;
+  if ((s = box_order(h, b, &order)) != FKD_OK) return s;
+  if ((s = count_pass(h, b, dc, order)) != FKD_OK) return s;
   if (mem == FKD_MEM_HOST)
     FKD_CUDA(cudaMemcpyAsync(counts, dc, q * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
   return finish(h, "fkd_search_count", mem);
 }
 
 static fkd_status write_pass(fkd_tree h, const Boxes& b, const uint64_t* doffsets, uint32_t* dout, uint64_t total,
-                             int ordered) {
+                             int ordered, const uint32_t* order) {
   SearchCtx sc = search_ctx(h, b);
+  sc.order = order;
   sc.offsets = doffsets;
   sc.out = dout;
   sc.capacity = total;
@@ -350,7 +375,9 @@ fkd_status fkd_search_write(fkd_tree h, const float* mins, const float* maxs, ui
     if (total && !ids_out) return fail(FKD_ERR_ARG, "null ids_out");
   }
   FKD_CUDA(cudaMemsetAsync(h->err.p, 0, sizeof(uint32_t), h->stream));
-  if ((s = write_pass(h, b, doff, dout, total, ordered)) != FKD_OK) return s;
+  const uint32_t* order = nullptr;
+  if ((s = box_order(h, b, &order)) != FKD_OK) return s;
+  if ((s = write_pass(h, b, doff, dout, total, ordered, order)) != FKD_OK) return s;
   if (mem == FKD_MEM_HOST && total)
     FKD_CUDA(cudaMemcpyAsync(ids_out, dout, total * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
   return finish(h, "fkd_search_write", mem);
@@ -371,7 +398,9 @@ fkd_status fkd_search(fkd_tree h, const float* mins, const float* maxs, uint64_t
     doff = h->offsets.as<uint64_t>();
   }
   FKD_CUDA(cudaMemsetAsync(h->err.p, 0, sizeof(uint32_t), h->stream));
-  if (q && (s = count_pass(h, b, h->counts.as<uint32_t>())) != FKD_OK) return s;
+  const uint32_t* order = nullptr;
+  if (q && (s = box_order(h, b, &order)) != FKD_OK) return s;
+  if (q && (s = count_pass(h, b, h->counts.as<uint32_t>(), order)) != FKD_OK) return s;
   FKD_CUDA(launch_scan_counts(h->counts.as<uint32_t>(), q, doff, h->partials.as<unsigned long long>(), h->stream));
   FKD_CUDA(cudaMemcpyAsync(h->herr + 2, doff + q, sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
   FKD_CUDA(cudaStreamSynchronize(h->stream));
@@ -398,7 +427,7 @@ fkd_status fkd_search(fkd_tree h, const float* mins, const float* maxs, uint64_t
     FKD_CUDA(h->out.ensure(tot * sizeof(uint32_t)));
     dout = h->out.as<uint32_t>();
   }
-  if ((s = write_pass(h, b, doff, dout, tot, ordered)) != FKD_OK) return s;
+  if ((s = write_pass(h, b, doff, dout, tot, ordered, order)) != FKD_OK) return s;
   if (mem == FKD_MEM_HOST)
     FKD_CUDA(cudaMemcpyAsync(ids_out, dout, tot * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
   return finish(h, "fkd_search", mem);
@@ -421,7 +450,10 @@ fkd_status fkd_search_digest(fkd_tree h, const float* mins, const float* maxs, u
     dd = h->digests.as<uint64_t>();
   }
   FKD_CUDA(cudaMemsetAsync(h->err.p, 0, sizeof(uint32_t), h->stream));
+  const uint32_t* order = nullptr;
+  if ((s = box_order(h, b, &order)) != FKD_OK) return s;
   SearchCtx sc = search_ctx(h, b);
+  sc.order = order;
   sc.counts = dc;
   sc.digests = (unsigned long long*)dd;
   FKD_CUDA(launch_search(sc, h->dim, SEARCH_DIGEST));

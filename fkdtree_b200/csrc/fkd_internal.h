@@ -7,6 +7,11 @@
 
 namespace fkd {
 
+// Process-wide count of kernel launches issued by this library (telemetry for
+// benchmarks: how many of the library's own kernels ran in a timed region).
+void count_launches(uint64_t k);
+uint64_t launches_total();
+
 // Per-segment state of the global-level radix select (one per node of the
 // level being split).
 struct SegSel {
@@ -26,6 +31,7 @@ struct BuildCtx {
   SoA work[2];    // ping-pong working records
   SegSel* sel;    // >= 2^(d0-1) entries
   uint32_t* ghist;
+  uint32_t* pending;  // one word per digit pass (+1): does that pass have work
   Table tab;
   uint32_t* err;
   cudaStream_t stream;
@@ -69,6 +75,11 @@ cudaError_t launch_search(SearchCtx& sc, int dim, int mode);
 // Sorts every box's result slice by heap index and maps it to ids.
 cudaError_t launch_order_results(const Geom& g, const Table& tab, const uint64_t* offsets, uint64_t q, uint32_t* out,
                                  uint32_t* tmp, uint32_t* err, cudaStream_t stream);
+// Processing order of the boxes (see fkd_search.cu); scratch holds
+// box_order_words(q) words; *order_out points into it.
+size_t box_order_words(uint64_t q);
+cudaError_t launch_box_order(const Geom& g, const Table& tab, const Boxes& b, int dim, uint32_t* scratch,
+                             uint32_t** order_out, cudaStream_t stream);
 // Exclusive prefix sum of q uint32 counts into q+1 uint64 offsets.
 cudaError_t launch_scan_counts(const uint32_t* counts, uint64_t q, uint64_t* offsets, unsigned long long* partials,
                                cudaStream_t stream);

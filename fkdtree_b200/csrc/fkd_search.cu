@@ -90,12 +90,43 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
     }
     bool failed = false;
 
-    // Emits whole subtrees listed in jobs[warp][0..nj).
+    // Emits whole subtrees listed in jobs[warp][0..nj).  Relative levels 0-4
+    // (runs of 1..16 nodes) are packed across jobs so every lane has a node;
+    // deeper levels are runs of >= 32 consecutive nodes copied warp-wide.
     auto run_jobs = [&](uint32_t nj) {
+      for (uint32_t j = 0; j < 5; ++j) {
+        const uint32_t total = nj << j;
+        uint32_t seen = 0u;
+        for (uint32_t e0 = 0; e0 < total; e0 += 32u) {
+          const uint32_t e = e0 + lane;
+          uint64_t node = ~0ull;
+          if (e < total) {
+            const uint32_t r = jobs[warp][e >> j];
+            node = (((uint64_t)r + 1u) << j) - 1u + (e & ((1u << j) - 1u));
+          }
+          const bool v = node < n;
+          const uint32_t bv = __ballot_sync(0xffffffffu, v);
+          seen |= bv;
+          if (v) {
+            const uint32_t id = __ldg(sc.tab.ids + node);
+            if (MODE == SEARCH_WRITE) {
+              const uint64_t pos = cursor + __popc(bv & lt);
+              if (pos < cend && pos < sc.capacity)
+                sc.out[pos] = sc.heap_out ? (uint32_t)node : id;
+              else
+                failed = true;
+            } else {
+              acc += mix64(id);
+            }
+          }
+          cursor += __popc(bv);
+        }
+        if (!seen) return;  // no job reaches this level, nor any deeper one
+      }
       for (uint32_t jb = 0; jb < nj; ++jb) {
         const uint32_t r = jobs[warp][jb];
-        for (uint32_t j = 0;; ++j) {
-          const uint64_t a = ((uint64_t)(r + 1u) << j) - 1u;
+        for (uint32_t j = 5;; ++j) {
+          const uint64_t a = (((uint64_t)r + 1u) << j) - 1u;
           if (a >= n) break;
           const uint64_t b = (a + (1ull << j)) < (uint64_t)n ? (a + (1ull << j)) : (uint64_t)n;
           for (uint64_t x = a + lane; x < b; x += 32u) {
@@ -280,6 +311,7 @@ static cudaError_t run_search(SearchCtx& sc) {
   e = cudaMemsetAsync(sc.qcounter, 0, sizeof(uint32_t), sc.stream);
   if (e != cudaSuccess) return e;
   k_search<DIM, MODE><<<(unsigned)blocks, QT, smem, sc.stream>>>(sc, cap);
+  count_launches(1);
   return cudaGetLastError();
 }
 
@@ -301,6 +333,80 @@ cudaError_t launch_search(SearchCtx& sc, int dim, int mode) {
     case 4: return run_search_mode<4>(sc, mode);
     default: return cudaErrorInvalidValue;
   }
+}
+
+// ------------------------------------------------------------ box order
+//
+// Boxes are processed in the order of the tree cell their centre falls in
+// (the root-to-depth-D path of the centre, D = min(H, 16)), so the warps
+// running at the same time walk neighbouring parts of the tree and share
+// its nodes in L2.  The order only changes which warp does which box, never
+// a box's result.
+
+constexpr int QO_BITS = 16;
+
+template <int DIM>
+__global__ void k_box_keys(Geom g, Table tab, Boxes b, uint32_t* __restrict__ keys, uint32_t* __restrict__ hist) {
+  const uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= b.q) return;
+  float ctr[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) ctr[c] = 0.5f * (b.lo[(uint64_t)c * b.stride + j] + b.hi[(uint64_t)c * b.stride + j]);
+  const uint32_t D = g.H < (uint32_t)QO_BITS ? g.H : (uint32_t)QO_BITS;
+  uint32_t i = 0u, path = 0u, dep = 0u;
+  while (dep < D) {
+    const uint32_t c = dep % DIM;
+    const uint4 nd = __ldg(tab.nodes + i);
+    const float v = sel4(c, __uint_as_float(nd.x), __uint_as_float(nd.y), __uint_as_float(nd.z), __uint_as_float(nd.w));
+    const uint32_t right = (sel4(c, ctr[0], ctr[1], ctr[2], ctr[3]) < v) ? 0u : 1u;
+    path = (path << 1) | right;
+    i = 2u * i + 1u + right;
+    ++dep;
+    if (i >= g.n) break;
+  }
+  const uint32_t key = path << (QO_BITS - dep);
+  keys[j] = key;
+  atomicAdd(&hist[key], 1u);
+}
+
+__global__ void k_box_scatter(uint64_t q, const uint32_t* __restrict__ keys, unsigned long long* __restrict__ offs,
+                              uint32_t* __restrict__ order) {
+  const uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= q) return;
+  const unsigned long long pos = atomicAdd(&offs[keys[j]], 1ull);
+  if (pos < q) order[pos] = (uint32_t)j;
+}
+
+size_t box_order_words(uint64_t q) {
+  // keys (q) + hist (2^16) + offsets (2^16 + 1, 64-bit) + partials + order (q)
+  return q + (1u << QO_BITS) + 2ull * ((1u << QO_BITS) + 1) + 2ull * scan_partials_words(1u << QO_BITS) + q + 16;
+}
+
+cudaError_t launch_box_order(const Geom& g, const Table& tab, const Boxes& b, int dim, uint32_t* scratch,
+                             uint32_t** order_out, cudaStream_t stream) {
+  *order_out = nullptr;
+  if (b.q == 0 || g.n == 0) return cudaSuccess;
+  uint32_t* keys = scratch;
+  uint32_t* hist = keys + b.q;
+  unsigned long long* offs = (unsigned long long*)(((uintptr_t)(hist + (1u << QO_BITS)) + 15) & ~(uintptr_t)15);
+  unsigned long long* partials = offs + (1u << QO_BITS) + 1;
+  uint32_t* order = (uint32_t*)(partials + scan_partials_words(1u << QO_BITS));
+  cudaError_t e = cudaMemsetAsync(hist, 0, sizeof(uint32_t) << QO_BITS, stream);
+  if (e != cudaSuccess) return e;
+  const unsigned blocks = (unsigned)((b.q + 255) / 256);
+  switch (dim) {
+    case 1: k_box_keys<1><<<blocks, 256, 0, stream>>>(g, tab, b, keys, hist); break;
+    case 2: k_box_keys<2><<<blocks, 256, 0, stream>>>(g, tab, b, keys, hist); break;
+    case 3: k_box_keys<3><<<blocks, 256, 0, stream>>>(g, tab, b, keys, hist); break;
+    default: k_box_keys<4><<<blocks, 256, 0, stream>>>(g, tab, b, keys, hist); break;
+  }
+  count_launches(1);
+  e = launch_scan_counts(hist, 1u << QO_BITS, (uint64_t*)offs, partials, stream);
+  if (e != cudaSuccess) return e;
+  k_box_scatter<<<blocks, 256, 0, stream>>>(b.q, keys, offs, order);
+  count_launches(1);
+  *order_out = order;
+  return cudaGetLastError();
 }
 
 // ------------------------------------------------------------------- scan
@@ -390,8 +496,11 @@ cudaError_t launch_scan_counts(const uint32_t* counts, uint64_t q, uint64_t* off
   if (q == 0) return cudaMemsetAsync(offsets, 0, sizeof(uint64_t), stream);
   const uint64_t nb = (q + SCB - 1) / SCB;
   k_scan_partials<<<(unsigned)nb, SCT, 0, stream>>>(counts, q, partials);
+  count_launches(1);
   k_scan_top<<<1, 1024, 0, stream>>>(partials, nb);
+  count_launches(1);
   k_scan_down<<<(unsigned)nb, SCT, 0, stream>>>(counts, q, partials, offsets, nb);
+  count_launches(1);
   return cudaGetLastError();
 }
 
@@ -511,6 +620,7 @@ cudaError_t launch_order_results(const Geom& g, const Table& tab, const uint64_t
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const uint64_t blocks = q < (uint64_t)sms * 8 ? q : (uint64_t)sms * 8;
   k_order<<<(unsigned)blocks, OT, 0, stream>>>(g, tab, offsets, q, out, tmp, err);
+  count_launches(1);
   return cudaGetLastError();
 }
 

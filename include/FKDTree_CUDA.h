@@ -1,0 +1,172 @@
+// FKDTree_CUDA.h -- drop-in replacement for the reference's FKDTree_CPU<TYPE, dim>
+// backed by the B200 library (include/fkdtree_b200.h).
+//
+// Usage is the reference's (main.cpp:203-205, :351-375):
+//
+//     #include "FKDTree_CUDA.h"          // needs FKDPoint.h / FKDTree.h on the include path
+//     std::unique_ptr<FKDTree<float, 3>> t(new FKDTree_CUDA<float, 3>(points));
+//     t->build();
+//     std::vector<unsigned int> ids = t->search_in_the_box(minPoint, maxPoint);
+//
+// It derives from the reference's abstract FKDTree<TYPE, dim> (FKDTree.h:6-22),
+// so code written against that interface -- including its test_correct_build
+// and test_correct_search helpers -- runs unchanged.  Semantics:
+//   * build() produces the reference's tables bit for bit (unique ids);
+//   * search_in_the_box / _BFS / _branchless return the reference's list in the
+//     reference's order (ascending heap index, FKDTree_cpu.h:123-169, 72-121,
+//     25-70); search_in_the_box_recursive appends the same set to foundPoints
+//     (in ascending heap order rather than the reference's depth-first order);
+//   * search_in_the_box_multiple returns per-box counts, the OpenCL backend's
+//     meaning (FKDTree_opencl.h:123-164) -- the CPU backend's is a stub;
+//   * search_in_the_box_batch is the bulk form (one GPU launch for all boxes);
+//   * getDimensionVector / getIdVector download the tables lazily after a
+//     build, like FKDTree_OpenCL (FKDTree_opencl.h:194-206);
+//   * failures throw std::runtime_error carrying fkd_last_error(); the
+//     reference aborts or prints instead.
+#ifndef FKDTREE_CUDA_H_
+#define FKDTREE_CUDA_H_
+
+#include <algorithm>  // FKDTree.h uses std::find without including it
+#include <iostream>
+#include <stdexcept>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "FKDPoint.h"
+#include "FKDTree.h"
+#include "fkdtree_b200.h"
+
+template <class TYPE, unsigned int numberOfDimensions>
+class FKDTree_CUDA : public FKDTree<TYPE, numberOfDimensions> {
+  static_assert(std::is_same<TYPE, float>::value, "the B200 tree stores float32 coordinates");
+  static_assert(numberOfDimensions >= 1 && numberOfDimensions <= 4, "1 to 4 dimensions");
+
+ public:
+  typedef FKDPoint<TYPE, numberOfDimensions> Point;
+
+  explicit FKDTree_CUDA(const std::vector<Point>& points, void* stream = nullptr)
+      : n_(points.size()), coords_(numberOfDimensions * points.size()), ids_(points.size()), synced_(false) {
+    for (size_t i = 0; i < n_; ++i) {
+      for (unsigned int c = 0; c < numberOfDimensions; ++c) coords_[c * n_ + i] = points[i][c];
+      ids_[i] = points[i].getId();
+    }
+    check(fkd_create((int)numberOfDimensions, 0u, stream, &h_));
+  }
+
+  ~FKDTree_CUDA() { fkd_destroy(h_); }
+  FKDTree_CUDA(const FKDTree_CUDA&) = delete;
+  FKDTree_CUDA& operator=(const FKDTree_CUDA&) = delete;
+
+  void build() override {
+    check(fkd_build(h_, coords_.data(), ids_.data(), n_, FKD_MEM_HOST));
+    synced_ = false;
+  }
+
+  std::vector<unsigned int> search_in_the_box(const Point& minPoint, const Point& maxPoint) override {
+    return one(minPoint, maxPoint);
+  }
+  std::vector<unsigned int> search_in_the_box_BFS(const Point& minPoint, const Point& maxPoint) {
+    return one(minPoint, maxPoint);
+  }
+  std::vector<unsigned int> search_in_the_box_branchless(const Point& minPoint, const Point& maxPoint) {
+    return one(minPoint, maxPoint);
+  }
+  void search_in_the_box_recursive(const Point& minPoint, const Point& maxPoint,
+                                   std::vector<unsigned int>& foundPoints, unsigned int = 0, int = 0) {
+    std::vector<unsigned int> r = one(minPoint, maxPoint);
+    foundPoints.insert(foundPoints.end(), r.begin(), r.end());
+  }
+
+  std::vector<unsigned int> search_in_the_box_multiple(const std::vector<Point>& minPoints,
+                                                       const std::vector<Point>& maxPoints) override {
+    std::vector<float> lo, hi;
+    soa(minPoints, maxPoints, lo, hi);
+    std::vector<unsigned int> counts(minPoints.size());
+    check(fkd_search_count(h_, lo.data(), hi.data(), minPoints.size(), counts.data(), FKD_MEM_HOST));
+    return counts;
+  }
+
+  // All boxes in one call: ids of box j are ids[offsets[j] .. offsets[j+1]).
+  void search_in_the_box_batch(const std::vector<Point>& minPoints, const std::vector<Point>& maxPoints,
+                               std::vector<uint64_t>& offsets, std::vector<unsigned int>& ids,
+                               bool ordered = true) {
+    std::vector<float> lo, hi;
+    soa(minPoints, maxPoints, lo, hi);
+    const uint64_t q = minPoints.size();
+    std::vector<unsigned int> counts(q);
+    check(fkd_search_count(h_, lo.data(), hi.data(), q, counts.data(), FKD_MEM_HOST));
+    offsets.assign(q + 1, 0);
+    for (uint64_t j = 0; j < q; ++j) offsets[j + 1] = offsets[j] + counts[j];
+    ids.resize(offsets[q]);
+    uint64_t total = 0;
+    check(fkd_search(h_, lo.data(), hi.data(), q, offsets.data(), ids.data(), ids.size(), &total, ordered ? 1 : 0,
+                     FKD_MEM_HOST));
+  }
+
+  std::vector<TYPE> const& getDimensionVector(const int dimension) override {
+    sync_tables();
+    if ((unsigned int)dimension < numberOfDimensions) return dims_[dimension];
+    return dims_[0];  // FKDTree_cpu.h:210-211
+  }
+  std::vector<unsigned int> const& getIdVector() override {
+    sync_tables();
+    return tab_ids_;
+  }
+
+  fkd_tree handle() const { return h_; }
+
+ private:
+  static void check(fkd_status s) {
+    if (s != FKD_OK) throw std::runtime_error(std::string("fkdtree_b200: ") + fkd_last_error());
+  }
+
+  static void soa(const std::vector<Point>& a, const std::vector<Point>& b, std::vector<float>& lo,
+                  std::vector<float>& hi) {
+    if (a.size() != b.size()) throw std::invalid_argument("minPoints and maxPoints differ in size");
+    const size_t q = a.size();
+    lo.resize(numberOfDimensions * q);
+    hi.resize(numberOfDimensions * q);
+    for (size_t j = 0; j < q; ++j)
+      for (unsigned int c = 0; c < numberOfDimensions; ++c) {
+        lo[c * q + j] = a[j][c];
+        hi[c * q + j] = b[j][c];
+      }
+  }
+
+  std::vector<unsigned int> one(const Point& minPoint, const Point& maxPoint) {
+    float lo[numberOfDimensions], hi[numberOfDimensions];
+    for (unsigned int c = 0; c < numberOfDimensions; ++c) {
+      lo[c] = minPoint[c];
+      hi[c] = maxPoint[c];
+    }
+    unsigned int count = 0;
+    check(fkd_search_count(h_, lo, hi, 1, &count, FKD_MEM_HOST));
+    std::vector<unsigned int> out(count);
+    uint64_t offsets[2] = {0, count};
+    uint64_t total = 0;
+    if (count) check(fkd_search(h_, lo, hi, 1, offsets, out.data(), count, &total, 1, FKD_MEM_HOST));
+    return out;
+  }
+
+  void sync_tables() {
+    if (synced_) return;
+    std::vector<float> flat(numberOfDimensions * n_);
+    tab_ids_.resize(n_);
+    check(fkd_get_tables(h_, flat.data(), tab_ids_.data(), FKD_MEM_HOST));
+    dims_.assign(numberOfDimensions, std::vector<TYPE>(n_));
+    for (unsigned int c = 0; c < numberOfDimensions; ++c)
+      for (size_t i = 0; i < n_; ++i) dims_[c][i] = flat[c * n_ + i];
+    synced_ = true;
+  }
+
+  size_t n_;
+  std::vector<float> coords_;
+  std::vector<unsigned int> ids_;
+  fkd_tree h_ = nullptr;
+  bool synced_;
+  std::vector<std::vector<TYPE>> dims_;
+  std::vector<unsigned int> tab_ids_;
+};
+
+#endif  // FKDTREE_CUDA_H_

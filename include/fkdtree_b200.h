@@ -75,6 +75,10 @@ typedef struct fkd_tree_s* fkd_tree;
 /* Version string of the library. */
 FKD_API const char* fkd_version(void);
 
+/* Number of CUDA kernels this library has launched in this process (all
+ * handles, all threads).  Telemetry for benchmarks; no reference counterpart. */
+FKD_API uint64_t fkd_kernel_launches(void);
+
 /* Description of the last failure on the calling thread ("" if none). */
 FKD_API const char* fkd_last_error(void);
 

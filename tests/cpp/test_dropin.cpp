@@ -1,0 +1,77 @@
+// Drop-in check: the reference's own FKDTree_CPU and FKDTree_CUDA side by side
+// behind the reference's FKDTree<T, dim> interface.  Built by oracle/Makefile
+// (target `dropin`, against the reference headers) into oracle/_ref/test_dropin;
+// run on a GPU by tests/test_dropin_gpu.py.  Prints "DROPIN OK" on success.
+#include <cstdio>
+#include <memory>
+#include <random>
+#include <vector>
+
+#include "FKDTree_CUDA.h"
+#include "FKDTree_cpu.h"
+
+template <unsigned D>
+static int run(unsigned n, unsigned seed, float hw) {
+  std::mt19937 gen(seed);
+  std::uniform_real_distribution<float> u(0.f, 1.f);
+  std::vector<FKDPoint<float, D>> pts(n), lo(n), hi(n);
+  for (unsigned i = 0; i < n; ++i) {
+    for (unsigned c = 0; c < D; ++c) {
+      float x = u(gen);
+      if (c == 3) x = (float)(int)(x * 16) / 16.f;  // a discrete fourth coordinate: heavy ties
+      pts[i].setDimension(c, x);
+      lo[i].setDimension(c, x - hw);
+      hi[i].setDimension(c, x + hw);
+    }
+    pts[i].setId(i);
+  }
+  FKDTree_CPU<float, D> cpu(pts);
+  cpu.build();
+  std::unique_ptr<FKDTree<float, D>> gpu(new FKDTree_CUDA<float, D>(pts));
+  gpu->build();
+  for (unsigned c = 0; c < D; ++c)
+    if (gpu->getDimensionVector(c) != cpu.getDimensionVector(c)) {
+      std::printf("dim %u: theDimensions differ\n", c);
+      return 1;
+    }
+  if (gpu->getIdVector() != cpu.getIdVector()) {
+    std::printf("theIds differ\n");
+    return 1;
+  }
+  if (!gpu->test_correct_build()) {
+    std::printf("test_correct_build failed\n");
+    return 1;
+  }
+  const unsigned q = n < 2000 ? n : 2000;
+  std::vector<unsigned> counts = gpu->search_in_the_box_multiple(
+      std::vector<FKDPoint<float, D>>(lo.begin(), lo.begin() + q), std::vector<FKDPoint<float, D>>(hi.begin(), hi.begin() + q));
+  auto* cu = static_cast<FKDTree_CUDA<float, D>*>(gpu.get());
+  std::vector<uint64_t> offs;
+  std::vector<unsigned> ids;
+  cu->search_in_the_box_batch(std::vector<FKDPoint<float, D>>(lo.begin(), lo.begin() + q),
+                              std::vector<FKDPoint<float, D>>(hi.begin(), hi.begin() + q), offs, ids, true);
+  for (unsigned j = 0; j < q; ++j) {
+    std::vector<unsigned> want = cpu.search_in_the_box(lo[j], hi[j]);  // the reference's order
+    std::vector<unsigned> got = gpu->search_in_the_box(lo[j], hi[j]);
+    std::vector<unsigned> batch(ids.begin() + offs[j], ids.begin() + offs[j + 1]);
+    if (got != want || batch != want || counts[j] != want.size()) {
+      std::printf("box %u: results differ (%zu vs %zu)\n", j, got.size(), want.size());
+      return 1;
+    }
+    if (j < 50 && !test_correct_search(pts, got, lo[j], hi[j])) {
+      std::printf("box %u: test_correct_search failed\n", j);
+      return 1;
+    }
+  }
+  std::printf("dim %u n %u: %u boxes identical\n", D, n, q);
+  return 0;
+}
+
+int main() {
+  int rc = 0;
+  rc |= run<3>(50000, 1, 0.02f);
+  rc |= run<4>(30000, 2, 0.05f);
+  rc |= run<2>(7777, 3, 0.01f);
+  if (rc == 0) std::printf("DROPIN OK\n");
+  return rc;
+}
