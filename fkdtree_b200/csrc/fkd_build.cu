@@ -30,15 +30,33 @@
 
 namespace fkd {
 
+#ifdef FKD_PROF
+// Phase cycle counters of the subtree kernel (profiling builds only).
+__device__ unsigned long long g_prof[8];
+extern "C" __attribute__((visibility("default"))) void fkd_prof_read(unsigned long long* out) {
+  cudaMemcpyFromSymbol(out, g_prof, sizeof(g_prof));
+}
+extern "C" __attribute__((visibility("default"))) void fkd_prof_reset() {
+  unsigned long long z[8] = {0};
+  cudaMemcpyToSymbol(g_prof, z, sizeof(z));
+}
+#define PROF_T(v) const unsigned long long v = clock64()
+#define PROF_ADD(slot, a, b) \
+  if (threadIdx.x == 0) atomicAdd(&g_prof[slot], (b) - (a))
+#else
+#define PROF_T(v)
+#define PROF_ADD(slot, a, b)
+#endif
+
 // ---------------------------------------------------------------- global
 
 constexpr int GT = 256;            // threads of the global-level kernels
 constexpr int GIPT = 16;           // records per thread (digit passes)
-constexpr int PIPT = 8;            // records per thread (partition)
+constexpr int PIPT = 4;            // records per thread (partition)
 constexpr int PTILE = GT * PIPT;
 constexpr int GTILE = GT * GIPT;   // records per CTA tile
 constexpr int GWARPS = GT / 32;
-constexpr int RBITS = 11;          // digit width of the global select
+constexpr int RBITS = 11;          // widest digit of the global select (11, 11, 10 per 32-bit word)
 constexpr int RBINS = 1 << RBITS;
 constexpr int RPASSES = 6;         // 5 * 11 + 9 >= 64
 
@@ -79,70 +97,84 @@ __global__ void k_sel_init(Geom g, uint32_t d, SegSel* __restrict__ sel, uint32_
   sel[s] = st;
 }
 
-// One digit pass of the segmented select for every segment of depth d.
+// One digit pass of the segmented select for every segment of depth d.  CTA
+// (s, t) counts the digits of tile t of segment s -- tiles are `ts` records
+// long, so that a level is covered by about four CTAs per SM whatever its
+// segment count -- into HCOPIES interleaved shared histograms (lane %
+// HCOPIES picks the copy, so lanes of clustered data do not all hit one
+// counter), then adds them to the segment's global histogram once.  The last
+// CTA of a segment picks the digit holding the pivot rank.
+constexpr int HCOPIES = 4;
+
 template <int DIM>
-__global__ void __launch_bounds__(GT) k_hist(Geom g, uint32_t d, uint32_t tps, CSoA src, SegSel* __restrict__ sel,
-                                             uint32_t* __restrict__ ghist, const uint32_t* __restrict__ pending_now,
+__global__ void __launch_bounds__(GT, 4) k_hist(Geom g, uint32_t d, uint32_t tps, uint32_t ts, CSoA src,
+                                             SegSel* __restrict__ sel, uint32_t* __restrict__ ghist,
+                                             const uint32_t* __restrict__ pending_now,
                                              uint32_t* __restrict__ pending_next, uint32_t* __restrict__ err) {
-  __shared__ uint32_t hist[RBINS];
+  __shared__ uint32_t hist[HCOPIES * RBINS];
   __shared__ uint32_t wsum[GWARPS];
   __shared__ uint32_t s_last;
   // pending_now was raised by the previous pass when some segment still needs
   // a digit; without it the whole launch is a no-op.
   if (*(volatile const uint32_t*)pending_now == 0u) return;
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   const uint32_t s = blockIdx.x / tps, t = blockIdx.x - s * tps;
   const uint32_t len = seg_len(g, d, s);
-  const uint32_t ntiles = (len + GTILE - 1) / GTILE;
+  const uint32_t ntiles = (len + ts - 1) / ts;
   if (t >= ntiles) return;
   if (sel[s].done) return;
   const uint32_t bits = sel[s].bits;
   const unsigned long long prefix = sel[s].prefix;
-  const uint32_t w = (64u - bits) < (uint32_t)RBITS ? (64u - bits) : (uint32_t)RBITS;
+  // digits never straddle the value/id boundary: 11, 11, 10 bits per word
+  const uint32_t inword = bits & 31u;
+  const uint32_t w = inword < 22u ? 11u : 10u;
   const uint32_t nb = 1u << w;
-  const uint32_t shift = 64u - bits - w;
-  const bool need_id = bits + w > 32u;
+  const bool need_id = bits >= 32u;
   const uint32_t c = d % DIM;
   const uint32_t start = seg_start(g, d, s);
-  const uint32_t t0 = start + t * GTILE;
-  const uint32_t t1 = min(start + len, t0 + (uint32_t)GTILE);
-  for (uint32_t i = threadIdx.x; i < nb; i += GT) hist[i] = 0u;
+  const uint32_t tend = min(start + len, start + t * ts + ts);
+  uint32_t* myhist = hist + (lane % HCOPIES) * RBINS;
+  for (uint32_t i = threadIdx.x; i < HCOPIES * RBINS; i += GT) hist[i] = 0u;
   __syncthreads();
-
   const uint32_t* X = src.base + (uint64_t)c * src.stride;
-  uint32_t vb[GIPT], idv[GIPT];
+  const uint32_t vpre = (uint32_t)(prefix >> (bits > 32u ? bits - 32u : 0u));  // value part of the prefix
+  const uint32_t vbits = bits < 32u ? bits : 32u;
+  constexpr int HIPT = 8;  // records per thread per step
+  for (uint32_t t0 = start + t * ts; t0 < tend; t0 += GT * HIPT) {
+    const uint32_t t1 = min(tend, t0 + (uint32_t)(GT * HIPT));
+    uint32_t vb[HIPT];
 #pragma unroll
-  for (int k = 0; k < GIPT; ++k) {
-    const uint32_t e = t0 + k * GT + threadIdx.x;
-    vb[k] = e < t1 ? __ldcs(X + e) : 0u;
-  }
-  if (need_id) {
-#pragma unroll
-    for (int k = 0; k < GIPT; ++k) {
+    for (int k = 0; k < HIPT; ++k) {
       const uint32_t e = t0 + k * GT + threadIdx.x;
-      idv[k] = e < t1 ? __ldcs(src.ids + e) : 0u;
+      vb[k] = e < t1 ? __ldcs(X + e) : 0u;
     }
-  } else {
 #pragma unroll
-    for (int k = 0; k < GIPT; ++k) idv[k] = 0u;
-  }
-#pragma unroll
-  for (int k = 0; k < GIPT; ++k) {
-    const uint32_t e = t0 + k * GT + threadIdx.x;
-    uint32_t dig = 0xffffffffu;  // no digit: outside the tile or prefix mismatch
-    if (e < t1) {
-      const uint64_t key = order_key(vb[k], idv[k]);
-      if (bits == 0u || (key >> (64u - bits)) == prefix) dig = (uint32_t)(key >> shift) & (nb - 1u);
+    for (int k = 0; k < HIPT; ++k) {
+      const uint32_t e = t0 + k * GT + threadIdx.x;
+      if (e < t1) {
+        const uint32_t mv = mono_bits(vb[k]);
+        // value bits first; the id is read only by points whose value matches
+        if (vbits == 0u || (mv >> (32u - vbits)) == vpre) {
+          uint32_t dig;
+          if (!need_id) {
+            dig = (mv >> (32u - bits - w)) & (nb - 1u);
+          } else {
+            const uint32_t id = __ldcs(src.ids + e);
+            const uint32_t ib = bits - 32u;  // id bits already fixed
+            if (ib != 0u && (id >> (32u - ib)) != (uint32_t)(prefix & ((1ull << ib) - 1u))) continue;
+            dig = (id >> (32u - ib - w)) & (nb - 1u);
+          }
+          atomicAdd(&myhist[dig], 1u);
+        }
+      }
     }
-    // lanes with the same digit add once (clustered data piles onto few bins);
-    // all 32 lanes take part in the match
-    const uint32_t peers = __match_any_sync(0xffffffffu, dig);
-    if (dig != 0xffffffffu && (threadIdx.x & 31u) == (uint32_t)(__ffs(peers) - 1))
-      atomicAdd(&hist[dig], (uint32_t)__popc(peers));
   }
   __syncthreads();
   uint32_t* gh = ghist + (uint64_t)s * RBINS;
   for (uint32_t i = threadIdx.x; i < nb; i += GT) {
-    const uint32_t v = hist[i];
+    uint32_t v = 0u;
+#pragma unroll
+    for (int cpy = 0; cpy < HCOPIES; ++cpy) v += hist[cpy * RBINS + i];
     if (v) atomicAdd(&gh[i], v);
   }
   __threadfence();
@@ -151,7 +183,6 @@ __global__ void __launch_bounds__(GT) k_hist(Geom g, uint32_t d, uint32_t tps, C
   __syncthreads();
   if (!s_last) return;
   __threadfence();
-
   // Last CTA of segment s: locate the digit holding rank krem.
   const uint32_t krem = *(volatile uint32_t*)&sel[s].krem;
   constexpr int BPT = RBINS / GT;  // bins per thread
@@ -163,8 +194,6 @@ __global__ void __launch_bounds__(GT) k_hist(Geom g, uint32_t d, uint32_t tps, C
     h[k] = b < nb ? __ldcg(gh + b) : 0u;
     mine += h[k];
   }
-  // block exclusive scan of `mine`
-  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   uint32_t incl = mine;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
@@ -182,7 +211,7 @@ __global__ void __launch_bounds__(GT) k_hist(Geom g, uint32_t d, uint32_t tps, C
     if (b < nb && krem >= cum && krem < cum + h[k]) {
       SegSel* p = &sel[s];
       const uint32_t nbits = bits + w;
-      p->prefix = (w == 64u ? 0ull : (prefix << w)) | (unsigned long long)b;
+      p->prefix = (prefix << w) | (unsigned long long)b;
       p->bits = nbits;
       p->krem = krem - cum;
       p->cnt = h[k];
@@ -193,8 +222,8 @@ __global__ void __launch_bounds__(GT) k_hist(Geom g, uint32_t d, uint32_t tps, C
   }
   for (uint32_t b = threadIdx.x; b < nb; b += GT) gh[b] = 0u;
   if (threadIdx.x == 0) sel[s].tiles_done = 0u;
-  // wbase + incl of the last thread is the number of matching records; it must
-  // cover krem, otherwise the select state is inconsistent.
+  // the last thread's inclusive sum is the number of matching records; it
+  // must cover krem, otherwise the select state is inconsistent.
   if (threadIdx.x == GT - 1 && krem >= wbase + incl) atomicOr(err, ERRB_INTERNAL);
 }
 
@@ -209,7 +238,7 @@ __device__ __forceinline__ uint32_t pick_coord(const uint32_t* rec, uint32_t c) 
 // Streams every record of depth-d segments once: records below the pivot go
 // to [start, start + rank), the pivot to the table, the rest above it.
 template <int DIM>
-__global__ void __launch_bounds__(GT, 2) k_partition(Geom g, uint32_t d, uint32_t tps, CSoA src, SoA dst,
+__global__ void __launch_bounds__(GT, 4) k_partition(Geom g, uint32_t d, uint32_t tps, CSoA src, SoA dst,
                                                      SegSel* __restrict__ sel, Table tab, uint32_t* __restrict__ err) {
   __shared__ uint32_t sL[PIPT * GWARPS], sR[PIPT * GWARPS];
   __shared__ uint32_t s_base[2];
@@ -339,27 +368,94 @@ __global__ void __launch_bounds__(GT, 2) k_partition(Geom g, uint32_t d, uint32_
 
 // ---------------------------------------------------------------- subtree
 
-constexpr int ST = 512;          // threads of the subtree kernel
+constexpr int ST = 1024;         // threads of the subtree kernel
 constexpr int SWARPS = ST / 32;
-constexpr int SMALL = 16;        // rank counting at or below this segment length
-constexpr int MAXSEG = 256;      // segments of a radix level (length > SMALL)
-constexpr int HWORDS = 8192;     // packed 16-bit digit counters (32 KB), also the scan buffer
+constexpr int WARPN = 32;        // segments of at most this many points finish in one warp
+constexpr int MAXSEG = 256;      // segments of a shared-memory radix level (length > WARPN)
+constexpr int HWORDS = 4096;     // packed 16-bit digit counters (16 KB); the scan buffer is bufB's spare row
 constexpr uint16_t DONE = 0xffffu;
 
 template <int DIM>
 struct SubCfg {
   static constexpr int SUBN = DIM <= 3 ? 4096 : 3072;
-  static constexpr int PPT = SUBN / ST;  // positions per thread in the scan
-  static constexpr size_t smem =
-      2ull * (DIM + 1) * SUBN * 4 + 2ull * SUBN * 2 + HWORDS * 4ull + MAXSEG * (8 + 8 + 8 + 4 + 4 + 4 + 4);
+  static constexpr int PPT = SUBN / ST;  // positions per thread
+  static constexpr int STAGE = DIM + 4;  // words per lane of the warp-phase staging area
+  static constexpr size_t smem = 2ull * (DIM + 1) * SUBN * 4 + 2ull * SUBN * 2 + HWORDS * 4ull +
+                                 MAXSEG * (4 * 4 + 8 + 4 + 4 + 4 + 4) + (size_t)SWARPS * 32 * STAGE * 4;
 };
 
 int sub_capacity(int dim) { return dim <= 3 ? SubCfg<3>::SUBN : SubCfg<4>::SUBN; }
 
+// Finishes one segment of at most 32 points (and every level below it) in the
+// registers of one warp.  Lane i starts with point i of the segment; per level
+// each lane counts the smaller keys of its segment through shuffles (all
+// pairs), the lane whose rank is the split rank writes its node, the others
+// move to position (segment start + rank) through a per-warp staging area.
 template <int DIM>
-__device__ __forceinline__ uint64_t skey(const uint32_t* buf, uint32_t p, uint32_t c) {
+__device__ void warp_finish(const Geom& g, uint32_t d1, uint32_t t1, const uint32_t* rec_base, uint32_t m0,
+                            uint32_t* stage, const Table& tab, uint32_t* err) {
   constexpr int SUBN = SubCfg<DIM>::SUBN;
-  return order_key(buf[c * SUBN + p], buf[DIM * SUBN + p]);
+  constexpr int W = SubCfg<DIM>::STAGE;
+  const uint32_t lane = threadIdx.x & 31u;
+  uint32_t rec[DIM + 1];
+  bool valid = lane < m0;
+#pragma unroll
+  for (int w = 0; w <= DIM; ++w) rec[w] = valid ? rec_base[w * SUBN + lane] : 0u;
+  uint32_t cur_t = t1, ls = 0u, m = m0;  // my segment: global index-in-level, first lane, length
+  for (uint32_t depth = d1;; ++depth) {
+    if (depth == g.H) {
+      if (valid) {
+        if (cur_t < g.M)
+          write_node(tab, (1u << g.H) - 1u + cur_t, rec, DIM);
+        else
+          atomicOr(err, ERRB_INTERNAL);
+      }
+      break;
+    }
+    const uint32_t c = depth % DIM;
+    const uint64_t key = order_key(pick_coord<DIM>(rec, c), rec[DIM]);
+    const uint32_t mmax = __reduce_max_sync(0xffffffffu, valid ? m : 0u);
+    if (mmax == 0u) break;
+    uint32_t r = 0u;
+    for (uint32_t i0 = 0; i0 < mmax; i0 += 4u) {
+      uint64_t kq[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) kq[u] = __shfl_sync(0xffffffffu, key, (ls + i0 + u) & 31u);
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const uint32_t i = i0 + u, srcl = (ls + i) & 31u;
+        r += (valid && i < m && (kq[u] < key || (kq[u] == key && srcl < lane))) ? 1u : 0u;
+      }
+    }
+    const uint32_t k = seg_rank(g, depth, cur_t);
+    stage[lane * W + DIM + 3] = 0u;  // slot empty unless a point moves in
+    __syncwarp();
+    if (valid) {
+      if (r == k) {
+        write_node(tab, (1u << depth) - 1u + cur_t, rec, DIM);
+      } else if (r < m) {
+        const uint32_t dst = ls + r;
+        const uint32_t ct = 2u * cur_t + (r > k ? 1u : 0u);
+        uint32_t* sl = stage + dst * W;
+#pragma unroll
+        for (int w = 0; w <= DIM; ++w) sl[w] = rec[w];
+        sl[DIM + 1] = ct;
+        sl[DIM + 2] = r < k ? ls : ls + k + 1u;
+        sl[DIM + 3] = 1u;
+      } else {
+        atomicOr(err, ERRB_INTERNAL);
+      }
+    }
+    __syncwarp();
+    const uint32_t* me = stage + lane * W;
+    valid = me[DIM + 3] != 0u;
+#pragma unroll
+    for (int w = 0; w <= DIM; ++w) rec[w] = me[w];
+    cur_t = me[DIM + 1];
+    ls = me[DIM + 2];
+    m = valid ? seg_len(g, depth + 1, cur_t) : 0u;
+    __syncwarp();
+  }
 }
 
 template <int DIM>
@@ -373,13 +469,16 @@ __global__ void __launch_bounds__(ST, 1) k_subtree(Geom g, uint32_t d0, CSoA src
   uint16_t* segA = (uint16_t*)(bufB + (DIM + 1) * SUBN);
   uint16_t* segB = segA + SUBN;
   uint32_t* work = (uint32_t*)(segB + SUBN);  // histograms / scan
-  unsigned long long* smin = (unsigned long long*)(work + HWORDS);
-  unsigned long long* smax = smin + MAXSEG;
-  unsigned long long* spre = smax + MAXSEG;
+  uint32_t* svmin = work + HWORDS;             // per-segment bounds of the value and id words
+  uint32_t* svmax = svmin + MAXSEG;
+  uint32_t* simin = svmax + MAXSEG;
+  uint32_t* simax = simin + MAXSEG;
+  unsigned long long* spre = (unsigned long long*)(simax + MAXSEG);
   uint32_t* sbits = (uint32_t*)(spre + MAXSEG);
   uint32_t* skrem = sbits + MAXSEG;
   uint32_t* scnt = skrem + MAXSEG;
   uint32_t* sdup = scnt + MAXSEG;
+  uint32_t* stage_all = sdup + MAXSEG;
   __shared__ uint32_t wtot[SWARPS];
 
   const uint32_t s0 = blockIdx.x;
@@ -402,215 +501,171 @@ __global__ void __launch_bounds__(ST, 1) k_subtree(Geom g, uint32_t d0, CSoA src
   }
   if (nan) atomicOr(err, ERRB_NAN);
   __syncthreads();
+  PROF_T(tp0);
 
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-  for (uint32_t j = 0;; ++j) {
+  uint32_t j = 0;
+  for (;; ++j) {
     const uint32_t d = d0 + j;
-    if (d == g.H) {
-      // Last level: every live position is a single-point node.
-      for (uint32_t p = threadIdx.x; p < nloc; p += ST) {
-        const uint32_t u = segA[p];
-        if (u == DONE) continue;
-        uint32_t rec[DIM + 1];
-#pragma unroll
-        for (int w = 0; w <= DIM; ++w) rec[w] = bufA[w * SUBN + p];
-        const uint32_t t = (s0 << j) + u;
-        if (t < g.M)
-          write_node(tab, (1u << g.H) - 1u + t, rec, DIM);
-        else
-          atomicOr(err, ERRB_INTERNAL);
-      }
-      break;
-    }
+    const uint32_t t0 = s0 << j;
+    if (d >= g.H || seg_len(g, d, t0) <= (uint32_t)WARPN) break;
     const uint32_t c = d % DIM;
     const uint32_t nseg = 1u << j;
-    const uint32_t t0 = s0 << j;
+    if (nseg > (uint32_t)MAXSEG) {
+      if (threadIdx.x == 0) atomicOr(err, ERRB_INTERNAL);
+      return;
+    }
+    PROF_T(tq0);
+    // the level's keys, cached in registers (positions p = tid + ST*k)
+    uint32_t kv[PPT], ki[PPT], ku[PPT];
+#pragma unroll
+    for (int k = 0; k < PPT; ++k) {
+      const uint32_t p = threadIdx.x + ST * k;
+      ku[k] = p < nloc ? segA[p] : DONE;
+      kv[k] = ku[k] != DONE ? mono_bits(bufA[c * SUBN + p]) : 0u;
+      ki[k] = ku[k] != DONE ? bufA[DIM * SUBN + p] : 0u;
+    }
+    // digit bits: about two counters per point of the widest segment, and the
+    // flattened (segment, digit) counters within 2*HWORDS
     const uint32_t lmax = seg_len(g, d, t0);
-
-    if (lmax <= (uint32_t)SMALL) {
-      // Rank counting: each point counts the smaller keys of its segment; the
-      // rank is its position, the rank-k point is the node.
-      for (uint32_t p = threadIdx.x; p < nloc; p += ST) {
-        const uint32_t u = segA[p];
-        if (u == DONE) {
-          segB[p] = DONE;
-          continue;
-        }
-        const uint32_t t = t0 + u;
-        const uint32_t ls = seg_start(g, d, t) - base;
-        const uint32_t m = seg_len(g, d, t);
-        const uint32_t k = seg_rank(g, d, t);
-        const uint64_t key = skey<DIM>(bufA, p, c);
-        uint32_t r = 0;
-        for (uint32_t q = ls; q < ls + m; ++q) {
-          const uint64_t kq = skey<DIM>(bufA, q, c);
-          r += (kq < key || (kq == key && q < p)) ? 1u : 0u;
-        }
-        const uint32_t dstp = ls + r;
-        if (dstp >= nloc) {
-          atomicOr(err, ERRB_INTERNAL);
-          continue;
-        }
-        uint32_t rec[DIM + 1];
+    uint32_t hb = floor_log2_u32(2u * lmax - 1u) + 1u;
+    if (hb > 12u) hb = 12u;
+    while ((nseg << hb) > 2u * HWORDS || (nseg << hb) < (uint32_t)ST) {
+      if ((nseg << hb) < (uint32_t)ST) ++hb; else --hb;
+    }
+    for (uint32_t u = threadIdx.x; u < nseg; u += ST) {
+      svmin[u] = simin[u] = 0xffffffffu;
+      svmax[u] = simax[u] = 0u;
+      skrem[u] = seg_rank(g, d, t0 + u);
+      scnt[u] = seg_len(g, d, t0 + u);
+      sdup[u] = 0u;
+    }
+    __syncthreads();
+    // bounds of the value and id words per segment (their common prefix is a
+    // common prefix of every key of the segment)
 #pragma unroll
-        for (int w = 0; w <= DIM; ++w) rec[w] = bufA[w * SUBN + p];
-        if (r == k) {
-          write_node(tab, (1u << d) - 1u + t, rec, DIM);
-          segB[dstp] = DONE;
-        } else {
-#pragma unroll
-          for (int w = 0; w <= DIM; ++w) bufB[w * SUBN + dstp] = rec[w];
-          segB[dstp] = (uint16_t)(r < k ? 2u * u : 2u * u + 1u);
+    for (int k = 0; k < PPT; ++k) {
+      const uint32_t u = ku[k];
+      const bool valid = u != DONE;
+      const uint32_t u0 = __shfl_sync(0xffffffffu, u, 0);
+      if (__all_sync(0xffffffffu, valid && u == u0)) {
+        const uint32_t a = __reduce_min_sync(0xffffffffu, kv[k]);
+        const uint32_t b = __reduce_max_sync(0xffffffffu, kv[k]);
+        const uint32_t e = __reduce_min_sync(0xffffffffu, ki[k]);
+        const uint32_t f = __reduce_max_sync(0xffffffffu, ki[k]);
+        if (lane == 0) {
+          atomicMin(&svmin[u], a);
+          atomicMax(&svmax[u], b);
+          atomicMin(&simin[u], e);
+          atomicMax(&simax[u], f);
         }
+      } else if (valid) {
+        atomicMin(&svmin[u], kv[k]);
+        atomicMax(&svmax[u], kv[k]);
+        atomicMin(&simin[u], ki[k]);
+        atomicMax(&simax[u], ki[k]);
       }
-    } else {
-      // Radix select per segment with a common-prefix skip.
-      if (nseg > (uint32_t)MAXSEG) {
-        if (threadIdx.x == 0) atomicOr(err, ERRB_INTERNAL);
-        return;
-      }
-      uint32_t hb = 8u;  // digit bits so that nseg << hb fits 2*HWORDS counters
-      while ((nseg << hb) > 2u * HWORDS) --hb;
-      for (uint32_t u = threadIdx.x; u < nseg; u += ST) {
-        smin[u] = ~0ull;
-        smax[u] = 0ull;
-        skrem[u] = seg_rank(g, d, t0 + u);
-        sdup[u] = 0u;
+    }
+    __syncthreads();
+    for (uint32_t u = threadIdx.x; u < nseg; u += ST) {
+      const unsigned long long lo = ((unsigned long long)svmin[u] << 32) | simin[u];
+      const unsigned long long hi = ((unsigned long long)svmax[u] << 32) | simax[u];
+      const uint32_t cp = lo == hi ? 64u : (uint32_t)__clzll((long long)(lo ^ hi));
+      spre[u] = cp == 0u ? 0ull : (cp >= 64u ? lo : (lo >> (64u - cp)));
+      sbits[u] = cp;
+    }
+    __syncthreads();
+    for (int pass = 0; pass < 64; ++pass) {
+      bool active = false;
+      for (uint32_t u = threadIdx.x; u < nseg; u += ST) active |= (scnt[u] > 1u && sbits[u] < 64u);
+      if (!__syncthreads_or(active)) break;
+      for (uint32_t i = threadIdx.x; i < (nseg << hb) / 2u; i += ST) work[i] = 0u;
+      __syncthreads();
+#pragma unroll
+      for (int k = 0; k < PPT; ++k) {
+        const uint32_t u = ku[k];
+        if (u == DONE) continue;
+        const uint32_t bits = sbits[u];
+        if (scnt[u] <= 1u || bits >= 64u) continue;
+        const uint64_t key = ((uint64_t)kv[k] << 32) | ki[k];
+        if (bits != 0u && (key >> (64u - bits)) != spre[u]) continue;
+        const uint32_t w = (64u - bits) < hb ? (64u - bits) : hb;
+        const uint32_t slot = (u << hb) + ((uint32_t)(key >> (64u - bits - w)) & ((1u << w) - 1u));
+        atomicAdd(&work[slot >> 1], 1u << (16u * (slot & 1u)));
       }
       __syncthreads();
-      for (uint32_t p0 = 0; p0 < nloc; p0 += ST) {
-        const uint32_t p = p0 + threadIdx.x;
-        const uint32_t u = p < nloc ? segA[p] : DONE;
-        const bool valid = u != DONE;
-        unsigned long long kmin = valid ? skey<DIM>(bufA, p, c) : ~0ull;
-        unsigned long long kmax = valid ? kmin : 0ull;
-        // a warp whose lanes all sit in one segment reduces before the atomics
-        // (every lane executes the shuffle and the vote)
-        const uint32_t u0 = __shfl_sync(0xffffffffu, u, 0);
-        const bool same = valid && u == u0;
-        if (__all_sync(0xffffffffu, same)) {
-#pragma unroll
-          for (int o = 16; o > 0; o >>= 1) {
-            const unsigned long long a = __shfl_xor_sync(0xffffffffu, kmin, o);
-            const unsigned long long b = __shfl_xor_sync(0xffffffffu, kmax, o);
-            kmin = a < kmin ? a : kmin;
-            kmax = b > kmax ? b : kmax;
-          }
-          if (lane == 0) {
-            atomicMin(&smin[u], kmin);
-            atomicMax(&smax[u], kmax);
-          }
-        } else if (valid) {
-          atomicMin(&smin[u], kmin);
-          atomicMax(&smax[u], kmax);
+      {
+        // CTA-wide digit search over the flattened (segment, digit) counters:
+        // thread t owns counters [t*cpt, (t+1)*cpt); every segment starts on a
+        // thread boundary (2^hb >= cpt).
+        const uint32_t T = nseg << hb;
+        const uint32_t cpt = T / ST;
+        uint32_t* segbase = sdup;  // reused as scratch: exclusive counter prefix at each segment start
+        uint32_t loc = 0u;
+        for (uint32_t k = 0; k < cpt; ++k) {
+          const uint32_t slot = threadIdx.x * cpt + k;
+          loc += (work[slot >> 1] >> (16u * (slot & 1u))) & 0xffffu;
         }
-      }
-      __syncthreads();
-      for (uint32_t u = threadIdx.x; u < nseg; u += ST) {
-        const unsigned long long lo = smin[u], hi = smax[u];
-        const uint32_t cp = lo == hi ? 64u : (uint32_t)__clzll((long long)(lo ^ hi));
-        spre[u] = cp == 0u ? 0ull : (cp >= 64u ? lo : (lo >> (64u - cp)));
-        sbits[u] = cp;
-        scnt[u] = seg_len(g, d, t0 + u);
-      }
-      __syncthreads();
-      for (int pass = 0; pass < 64; ++pass) {
-        // a segment is resolved when one point matches its prefix or the full
-        // key is known
-        bool active = false;
-        for (uint32_t u = threadIdx.x; u < nseg; u += ST) active |= (scnt[u] > 1u && sbits[u] < 64u);
-        if (!__syncthreads_or(active)) break;
-        for (uint32_t i = threadIdx.x; i < (nseg << hb) / 2u; i += ST) work[i] = 0u;
+        uint32_t incl = loc;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= (uint32_t)o) incl += y;
+        }
+        if (lane == 31u) wtot[warp] = incl;
         __syncthreads();
-        for (uint32_t p0 = 0; p0 < nloc; p0 += ST) {
-          const uint32_t p = p0 + threadIdx.x;
-          uint32_t slot = 0xffffffffu;
-          const uint32_t u = p < nloc ? segA[p] : DONE;
-          if (u != DONE) {
-            const uint32_t bits = sbits[u];
-            if (scnt[u] > 1u && bits < 64u) {
-              const uint64_t key = skey<DIM>(bufA, p, c);
-              if (bits == 0u || (key >> (64u - bits)) == spre[u]) {
-                const uint32_t w = (64u - bits) < hb ? (64u - bits) : hb;
-                const uint32_t dig = (uint32_t)(key >> (64u - bits - w)) & ((1u << w) - 1u);
-                slot = (u << hb) + dig;
-              }
-            }
-          }
-          // lanes hitting the same counter add once
-          const uint32_t peers = __match_any_sync(0xffffffffu, slot);
-          if (slot != 0xffffffffu && lane == (uint32_t)(__ffs(peers) - 1))
-            atomicAdd(&work[slot >> 1], (uint32_t)__popc(peers) << (16u * (slot & 1u)));
-        }
+        uint32_t excl = incl - loc;
+        for (uint32_t k = 0; k < warp; ++k) excl += wtot[k];
+        const uint32_t first = threadIdx.x * cpt;
+        if ((first & ((1u << hb) - 1u)) == 0u) segbase[first >> hb] = excl;
+        // read the segment state before anyone updates it
+        const uint32_t u = first >> hb;
+        const uint32_t bits = sbits[u];
+        const uint32_t cntu = scnt[u];
+        const uint32_t krem = skrem[u];
+        const unsigned long long pre = spre[u];
         __syncthreads();
-        // warp per segment: find the digit holding krem
-        for (uint32_t u = warp; u < nseg; u += SWARPS) {
-          const uint32_t bits = sbits[u];
-          if (scnt[u] <= 1u || bits >= 64u) continue;
+        uint32_t cum = excl - segbase[u];
+        // only the thread whose counters hold rank krem walks them
+        if (cntu > 1u && bits < 64u && krem >= cum && krem < cum + loc) {
           const uint32_t w = (64u - bits) < hb ? (64u - bits) : hb;
-          const uint32_t nb = 1u << w;
-          const uint32_t krem = skrem[u];
-          uint32_t found = 0xffffffffu, fcum = 0u, fh = 0u;
-          uint32_t carry = 0u;
-          for (uint32_t b0 = 0; b0 < nb; b0 += 32u) {
-            const uint32_t b = b0 + lane;
-            uint32_t h = 0u;
-            if (b < nb) {
-              const uint32_t slot = (u << hb) + b;
-              h = (work[slot >> 1] >> (16u * (slot & 1u))) & 0xffffu;
-            }
-            uint32_t incl = h;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-              const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-              if (lane >= (uint32_t)o) incl += y;
-            }
-            const uint32_t cum = carry + incl - h;
-            const bool hit = b < nb && krem >= cum && krem < cum + h;
-            const uint32_t bal = __ballot_sync(0xffffffffu, hit);
-            if (bal) {
-              const uint32_t src_lane = __ffs(bal) - 1u;
-              found = __shfl_sync(0xffffffffu, b, src_lane);
-              fcum = __shfl_sync(0xffffffffu, cum, src_lane);
-              fh = __shfl_sync(0xffffffffu, h, src_lane);
-              break;
-            }
-            carry += __shfl_sync(0xffffffffu, incl, 31);
-          }
-          if (lane == 0) {
-            if (found == 0xffffffffu) {
-              atomicOr(err, ERRB_INTERNAL);
-              scnt[u] = 1u;  // stop selecting; the partition check reports it
-            } else {
-              spre[u] = (bits == 0u ? 0ull : (spre[u] << w)) | found;
+          for (uint32_t k = 0; k < cpt; ++k) {
+            const uint32_t slot = first + k;
+            const uint32_t b = slot & ((1u << hb) - 1u);
+            const uint32_t h = (work[slot >> 1] >> (16u * (slot & 1u))) & 0xffffu;
+            if (b < (1u << w) && h && krem >= cum && krem < cum + h) {
+              spre[u] = (bits == 0u ? 0ull : (pre << w)) | b;
               sbits[u] = bits + w;
-              skrem[u] = krem - fcum;
-              scnt[u] = fh;
+              skrem[u] = krem - cum;
+              scnt[u] = h;
             }
+            cum += h;
           }
         }
         __syncthreads();
-      }
-
-      // Partition: exclusive scan of packed (below | above << 16) flags over
-      // all positions, then each point moves to its side of its segment.
-      uint32_t* scan = work;
-      // flags in a strided pass (conflict-free), scan over contiguous chunks
-      for (uint32_t p = threadIdx.x; p < (uint32_t)SUBN; p += ST) {
-        uint32_t f = 0u;
-        if (p < nloc) {
-          const uint32_t u = segA[p];
-          if (u != DONE) {
-            const uint32_t bits = sbits[u];
-            const uint64_t key = skey<DIM>(bufA, p, c);
-            const uint64_t top = bits >= 64u ? key : (bits == 0u ? 0ull : (key >> (64u - bits)));
-            const unsigned long long pre = bits == 0u ? 0ull : spre[u];
-            f = top < pre ? 1u : (top > pre ? (1u << 16) : 0u);
-          }
-        }
-        scan[p] = f;
+        for (uint32_t v = threadIdx.x; v < nseg; v += ST) sdup[v] = 0u;
       }
       __syncthreads();
+    }
+
+    PROF_T(tq1);
+    // Partition: flags (below | above << 16) per position, exclusive scan,
+    // then each point moves to its side of its segment.
+    uint32_t* scan = work;
+    for (uint32_t p = threadIdx.x; p < (uint32_t)SUBN; p += ST) scan[p] = 0u;
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < PPT; ++k) {
+      const uint32_t u = ku[k];
+      if (u == DONE) continue;
+      const uint32_t bits = sbits[u];
+      const uint64_t key = ((uint64_t)kv[k] << 32) | ki[k];
+      const uint64_t top = bits >= 64u ? key : (bits == 0u ? 0ull : (key >> (64u - bits)));
+      const unsigned long long pre = bits == 0u ? 0ull : spre[u];
+      scan[threadIdx.x + ST * k] = top < pre ? 1u : (top > pre ? (1u << 16) : 0u);
+    }
+    __syncthreads();
+    {
       uint32_t fl[PPT];
       uint32_t tsum = 0u;
 #pragma unroll
@@ -634,63 +689,69 @@ __global__ void __launch_bounds__(ST, 1) k_subtree(Geom g, uint32_t d0, CSoA src
         scan[threadIdx.x * PPT + k] = run;
         run += fl[k];
       }
-      uint32_t total = 0u;
-      for (uint32_t k = 0; k < (uint32_t)SWARPS; ++k) total += wtot[k];
-      __syncthreads();
-      for (uint32_t p = threadIdx.x; p < nloc; p += ST) {
-        const uint32_t u = segA[p];
-        if (u == DONE) {
-          segB[p] = DONE;
-          continue;
-        }
-        const uint32_t t = t0 + u;
-        const uint32_t ls = seg_start(g, d, t) - base;
-        const uint32_t m = seg_len(g, d, t);
-        const uint32_t k = seg_rank(g, d, t);
-        const uint32_t bits = sbits[u];
-        const uint64_t key = skey<DIM>(bufA, p, c);
-        const uint64_t top = bits >= 64u ? key : (bits == 0u ? 0ull : (key >> (64u - bits)));
-        const unsigned long long pre = bits == 0u ? 0ull : spre[u];
-        const uint32_t sp = scan[p], s0v = scan[ls];
-        uint32_t dstp;
-        bool pivot = false;
-        if (top < pre) {
-          dstp = ls + ((sp & 0xffffu) - (s0v & 0xffffu));
-        } else if (top > pre) {
-          dstp = ls + k + 1u + ((sp >> 16) - (s0v >> 16));
-        } else {
-          const uint32_t krem = skrem[u];
-          const uint32_t ticket = scnt[u] == 1u ? krem : atomicAdd(&sdup[u], 1u);
-          const uint32_t se = (ls + m < nloc) ? scan[ls + m] : total;
-          const uint32_t nbelow = (se & 0xffffu) - (s0v & 0xffffu);
-          const uint32_t nabove = (se >> 16) - (s0v >> 16);
-          if (ticket == krem) {
-            pivot = true;
-            dstp = ls + k;
-          } else if (ticket < krem) {
-            dstp = ls + nbelow + ticket;
-          } else {
-            dstp = ls + k + 1u + nabove + (ticket - krem - 1u);
-          }
-        }
-        if (dstp >= ls + m) {
-          atomicOr(err, ERRB_INTERNAL);
-          continue;
-        }
-        uint32_t rec[DIM + 1];
+    }
+    uint32_t total = 0u;
+    for (uint32_t k = 0; k < (uint32_t)SWARPS; ++k) total += wtot[k];
+    __syncthreads();
 #pragma unroll
-        for (int w = 0; w <= DIM; ++w) rec[w] = bufA[w * SUBN + p];
-        if (pivot) {
-          write_node(tab, (1u << d) - 1u + t, rec, DIM);
-          segB[dstp] = DONE;
+    for (int k = 0; k < PPT; ++k) {
+      const uint32_t p = threadIdx.x + ST * k;
+      if (p >= nloc) continue;
+      const uint32_t u = ku[k];
+      if (u == DONE) {
+        segB[p] = DONE;
+        continue;
+      }
+      const uint32_t t = t0 + u;
+      const uint32_t ls = seg_start(g, d, t) - base;
+      const uint32_t m = seg_len(g, d, t);
+      const uint32_t kr = seg_rank(g, d, t);
+      const uint32_t bits = sbits[u];
+      const uint64_t key = ((uint64_t)kv[k] << 32) | ki[k];
+      const uint64_t top = bits >= 64u ? key : (bits == 0u ? 0ull : (key >> (64u - bits)));
+      const unsigned long long pre = bits == 0u ? 0ull : spre[u];
+      const uint32_t sp = scan[p], s0v = scan[ls];
+      uint32_t dstp;
+      bool pivot = false;
+      if (top < pre) {
+        dstp = ls + ((sp & 0xffffu) - (s0v & 0xffffu));
+      } else if (top > pre) {
+        dstp = ls + kr + 1u + ((sp >> 16) - (s0v >> 16));
+      } else {
+        const uint32_t krem = skrem[u];
+        const uint32_t ticket = scnt[u] == 1u ? krem : atomicAdd(&sdup[u], 1u);  // repeated keys only
+        const uint32_t se = (ls + m < nloc) ? scan[ls + m] : total;
+        const uint32_t nbelow = (se & 0xffffu) - (s0v & 0xffffu);
+        const uint32_t nabove = (se >> 16) - (s0v >> 16);
+        if (ticket == krem) {
+          pivot = true;
+          dstp = ls + kr;
+        } else if (ticket < krem) {
+          dstp = ls + nbelow + ticket;
         } else {
-#pragma unroll
-          for (int w = 0; w <= DIM; ++w) bufB[w * SUBN + dstp] = rec[w];
-          segB[dstp] = (uint16_t)(dstp < ls + k ? 2u * u : 2u * u + 1u);
+          dstp = ls + kr + 1u + nabove + (ticket - krem - 1u);
         }
+      }
+      if (dstp >= ls + m) {
+        atomicOr(err, ERRB_INTERNAL);
+        continue;
+      }
+      uint32_t rec[DIM + 1];
+#pragma unroll
+      for (int w = 0; w <= DIM; ++w) rec[w] = bufA[w * SUBN + p];
+      if (pivot) {
+        write_node(tab, (1u << d) - 1u + t, rec, DIM);
+        segB[dstp] = DONE;
+      } else {
+#pragma unroll
+        for (int w = 0; w <= DIM; ++w) bufB[w * SUBN + dstp] = rec[w];
+        segB[dstp] = (uint16_t)(dstp < ls + kr ? 2u * u : 2u * u + 1u);
       }
     }
     __syncthreads();
+    PROF_T(tq2);
+    PROF_ADD(2, tq0, tq1);
+    PROF_ADD(3, tq1, tq2);
     uint32_t* tb = bufA;
     bufA = bufB;
     bufB = tb;
@@ -698,6 +759,26 @@ __global__ void __launch_bounds__(ST, 1) k_subtree(Geom g, uint32_t d0, CSoA src
     segA = segB;
     segB = ts;
   }
+
+  PROF_T(tp1);
+  PROF_ADD(0, tp0, tp1);
+  // Warp phase: every segment of level j is at most WARPN points long.
+  const uint32_t d1 = d0 + j;
+  const uint32_t t0 = s0 << j;
+  const uint32_t nseg = 1u << j;
+  uint32_t* stage = stage_all + warp * 32 * SubCfg<DIM>::STAGE;
+  for (uint32_t u = warp; u < nseg; u += SWARPS) {
+    const uint32_t t = t0 + u;
+    const uint32_t m = seg_len(g, d1, t);
+    if (m > (uint32_t)WARPN) {
+      if (lane == 0) atomicOr(err, ERRB_INTERNAL);
+      continue;
+    }
+    const uint32_t ls = seg_start(g, d1, t) - base;
+    warp_finish<DIM>(g, d1, t, bufA + ls, m, stage, tab, err);
+  }
+  PROF_T(tp2);
+  PROF_ADD(1, tp1, tp2);
 }
 
 // ---------------------------------------------------------------- host
@@ -710,15 +791,24 @@ static cudaError_t run_build(BuildCtx& bc) {
   while (seg_len(g, d0, 0) > (uint32_t)SUBN) ++d0;
   CSoA src = bc.input;
   SoA bufs[2] = {bc.work[0], bc.work[1]};
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const uint32_t hist_grid = (uint32_t)sms * 4u;
   int nb = 0;
   for (uint32_t d = 0; d < d0; ++d) {
     const uint32_t S = 1u << d;
-    const uint32_t tps = (seg_len(g, d, 0) + GTILE - 1) / GTILE;
-    const uint32_t ptps = (seg_len(g, d, 0) + PTILE - 1) / PTILE;
+    // digit passes: about hist_grid CTAs per level, tiles a multiple of GTILE
+    const uint32_t lmax = seg_len(g, d, 0);
+    const uint32_t want = (hist_grid + S - 1) / S;
+    const uint32_t chunks = (lmax + GTILE - 1) / GTILE;
+    const uint32_t tps = want < chunks ? want : chunks;
+    const uint32_t ts = ((chunks + tps - 1) / tps) * GTILE;
+    const uint32_t ptps = (lmax + PTILE - 1) / PTILE;
     k_sel_init<<<(S + 255) / 256, 256, 0, bc.stream>>>(g, d, bc.sel, bc.pending);
     count_launches(1);
     for (int pass = 0; pass < RPASSES; ++pass) {
-      k_hist<DIM><<<S * tps, GT, 0, bc.stream>>>(g, d, tps, src, bc.sel, bc.ghist, bc.pending + pass,
+      k_hist<DIM><<<S * tps, GT, 0, bc.stream>>>(g, d, tps, ts, src, bc.sel, bc.ghist, bc.pending + pass,
                                                   bc.pending + pass + 1, bc.err);
       count_launches(1);
     }

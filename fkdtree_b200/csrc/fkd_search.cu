@@ -34,7 +34,8 @@ namespace fkd {
 
 constexpr int QT = 128;  // threads per CTA
 constexpr int QW = QT / 32;
-constexpr int JOBS = 64;  // contained-subtree jobs per warp step (<= 2 per lane)
+constexpr int JOBS = 256;      // contained-subtree jobs buffered per warp
+constexpr int JFLUSH = JOBS - 64;  // one step adds at most 64
 
 __device__ __forceinline__ uint32_t lanemask_lt_s() {
   uint32_t m;
@@ -58,6 +59,7 @@ template <int DIM, int MODE>
 __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ uint32_t jobs[QW][JOBS];
+  __shared__ uint32_t jsort[QW][JOBS];
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   uint32_t* stk_node = (uint32_t*)smem_raw + (size_t)warp * cap;
   uint8_t* stk_mask = (uint8_t*)((uint32_t*)smem_raw + (size_t)QW * cap) + (size_t)warp * cap;
@@ -89,61 +91,104 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
       cend = sc.offsets[qj + 1];
     }
     bool failed = false;
+    uint32_t njobs = 0;  // warp-uniform
 
-    // Emits whole subtrees listed in jobs[warp][0..nj).  Relative levels 0-4
-    // (runs of 1..16 nodes) are packed across jobs so every lane has a node;
-    // deeper levels are runs of >= 32 consecutive nodes copied warp-wide.
-    auto run_jobs = [&](uint32_t nj) {
-      for (uint32_t j = 0; j < 5; ++j) {
-        const uint32_t total = nj << j;
-        uint32_t seen = 0u;
-        for (uint32_t e0 = 0; e0 < total; e0 += 32u) {
-          const uint32_t e = e0 + lane;
-          uint64_t node = ~0ull;
-          if (e < total) {
-            const uint32_t r = jobs[warp][e >> j];
-            node = (((uint64_t)r + 1u) << j) - 1u + (e & ((1u << j) - 1u));
-          }
-          const bool v = node < n;
-          const uint32_t bv = __ballot_sync(0xffffffffu, v);
-          seen |= bv;
-          if (v) {
-            const uint32_t id = __ldg(sc.tab.ids + node);
-            if (MODE == SEARCH_WRITE) {
-              const uint64_t pos = cursor + __popc(bv & lt);
-              if (pos < cend && pos < sc.capacity)
-                sc.out[pos] = sc.heap_out ? (uint32_t)node : id;
-              else
-                failed = true;
-            } else {
-              acc += mix64(id);
-            }
-          }
-          cursor += __popc(bv);
+    // Emits one id per lane with v set, packed at the cursor.
+    auto emit_ballot = [&](bool v, uint32_t node, uint32_t id) {
+      const uint32_t bv = __ballot_sync(0xffffffffu, v);
+      if (v) {
+        if (MODE == SEARCH_WRITE) {
+          const uint64_t pos = cursor + __popc(bv & lt);
+          if (pos < cend && pos < sc.capacity)
+            sc.out[pos] = sc.heap_out ? node : id;
+          else
+            failed = true;
+        } else {
+          acc += mix64(id);
         }
-        if (!seen) return;  // no job reaches this level, nor any deeper one
       }
-      for (uint32_t jb = 0; jb < nj; ++jb) {
-        const uint32_t r = jobs[warp][jb];
+      cursor += __popc(bv);
+    };
+
+    // Emits the whole subtrees buffered in jobs[warp][0..nj).  The jobs are
+    // first sorted by height (1, 3, 7, 15 nodes, taller) so that the short
+    // runs of the small subtrees are packed 32 nodes per warp step with no
+    // empty slots; the levels of taller subtrees are runs of >= 32 (below
+    // their fifth level) copied warp-wide.
+    auto run_jobs = [&](uint32_t nj) {
+      uint32_t cnt[5] = {0u, 0u, 0u, 0u, 0u};
+      for (uint32_t e0 = 0; e0 < nj; e0 += 32u) {
+        const uint32_t e = e0 + lane;
+        const uint32_t h = e < nj ? g.H - floor_log2_u32(jobs[warp][e] + 1u) : 99u;
+#pragma unroll
+        for (uint32_t c = 0; c < 5; ++c) cnt[c] += __popc(__ballot_sync(0xffffffffu, c < 4 ? h == c : (h >= 4u && h != 99u)));
+      }
+      uint32_t off[5];
+      off[0] = 0u;
+#pragma unroll
+      for (uint32_t c = 1; c < 5; ++c) off[c] = off[c - 1] + cnt[c - 1];
+      uint32_t fill[5] = {off[0], off[1], off[2], off[3], off[4]};
+      for (uint32_t e0 = 0; e0 < nj; e0 += 32u) {
+        const uint32_t e = e0 + lane;
+        const uint32_t r = e < nj ? jobs[warp][e] : 0u;
+        const uint32_t h = e < nj ? g.H - floor_log2_u32(r + 1u) : 99u;
+#pragma unroll
+        for (uint32_t c = 0; c < 5; ++c) {
+          const bool mine = c < 4 ? h == c : (h >= 4u && h != 99u);
+          const uint32_t b = __ballot_sync(0xffffffffu, mine);
+          if (mine) jsort[warp][fill[c] + __popc(b & lt)] = r;
+          fill[c] += __popc(b);
+        }
+      }
+      __syncwarp();
+      // classes 0-3: whole subtrees; class 4: the top five levels (31 nodes)
+      // of each taller subtree -- all packed 32 slots per step
+#pragma unroll
+      for (uint32_t c = 0; c < 5; ++c) {
+        const uint32_t per = (2u << c) - 1u;
+        const uint32_t total = cnt[c] * per;
+        for (uint32_t e0 = 0; e0 < total; e0 += 64u) {
+          uint64_t node[2];
+          uint32_t id[2];
+#pragma unroll
+          for (int u = 0; u < 2; ++u) {
+            const uint32_t e = e0 + 32u * u + lane;
+            node[u] = ~0ull;
+            if (e < total) {
+              const uint32_t jb = e / per, k = e - jb * per;
+              const uint32_t rl = floor_log2_u32(k + 1u);
+              const uint32_t r = jsort[warp][off[c] + jb];
+              node[u] = (((uint64_t)r + 1u) << rl) - 1u + (k + 1u - (1u << rl));
+            }
+            id[u] = node[u] < n ? __ldg(sc.tab.ids + node[u]) : 0u;
+          }
+#pragma unroll
+          for (int u = 0; u < 2; ++u) emit_ballot(node[u] < n, (uint32_t)node[u], id[u]);
+        }
+      }
+      // levels >= 5 of the tall subtrees: runs of >= 32 consecutive slots
+      for (uint32_t jb = 0; jb < cnt[4]; ++jb) {
+        const uint32_t r = jsort[warp][off[4] + jb];
         for (uint32_t j = 5;; ++j) {
           const uint64_t a = (((uint64_t)r + 1u) << j) - 1u;
           if (a >= n) break;
           const uint64_t b = (a + (1ull << j)) < (uint64_t)n ? (a + (1ull << j)) : (uint64_t)n;
-          for (uint64_t x = a + lane; x < b; x += 32u) {
-            const uint32_t id = __ldg(sc.tab.ids + x);
-            if (MODE == SEARCH_WRITE) {
-              const uint64_t pos = cursor + (x - a);
-              if (pos < cend && pos < sc.capacity)
-                sc.out[pos] = sc.heap_out ? (uint32_t)x : id;
-              else
-                failed = true;
-            } else {
-              acc += mix64(id);
+          for (uint64_t x0 = a; x0 < b; x0 += 64u) {
+            uint32_t id[2];
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+              const uint64_t x = x0 + 32u * u + lane;
+              id[u] = x < b ? __ldg(sc.tab.ids + x) : 0u;
+            }
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+              const uint64_t x = x0 + 32u * u + lane;
+              emit_ballot(x < b, (uint32_t)x, id[u]);
             }
           }
-          cursor += b - a;
         }
       }
+      __syncwarp();
     };
 
     int top = 0;
@@ -154,8 +199,7 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
         } else {
           if (lane == 0) jobs[warp][0] = 0u;
           if (MODE == SEARCH_DIGEST && lane == 0) acc2 += n;
-          __syncwarp();
-          run_jobs(1);
+          njobs = 1;
           __syncwarp();
         }
       } else {
@@ -220,46 +264,28 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
           acc2 += (emit ? 1u : 0u) + (contL ? subtree_size(g, 2u * i + 1u) : 0u) +
                   (contR ? subtree_size(g, 2u * i + 2u) : 0u);
         } else {
-          const uint32_t be = __ballot_sync(0xffffffffu, emit);
-          if (emit) {
-            const uint64_t pos = cursor + __popc(be & lt);
-            if (pos < cend && pos < sc.capacity)
-              sc.out[pos] = sc.heap_out ? i : idv;
-            else
-              failed = true;
-          }
-          cursor += __popc(be);
+          emit_ballot(emit, i, idv);
         }
-        const uint32_t nj = (contL ? 1u : 0u) + (contR ? 1u : 0u);
-        uint32_t jincl = nj;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const uint32_t y = __shfl_up_sync(0xffffffffu, jincl, o);
-          if (lane >= (uint32_t)o) jincl += y;
-        }
-        const uint32_t jtot = __shfl_sync(0xffffffffu, jincl, 31);
-        if (jtot) {
-          uint32_t jp = jincl - nj;
-          if (contL) jobs[warp][jp++] = 2u * i + 1u;
-          if (contR) jobs[warp][jp] = 2u * i + 2u;
+        // buffer the contained subtrees; emit them in bulk when the buffer fills
+        const uint32_t bl = __ballot_sync(0xffffffffu, contL), br = __ballot_sync(0xffffffffu, contR);
+        const uint32_t jp = njobs + __popc(bl & lt) + __popc(br & lt);
+        if (contL) jobs[warp][jp] = 2u * i + 1u;
+        if (contR) jobs[warp][jp + (contL ? 1u : 0u)] = 2u * i + 2u;
+        njobs += __popc(bl) + __popc(br);
+        if (njobs > (uint32_t)JFLUSH) {
           __syncwarp();
-          run_jobs(jtot);
-          __syncwarp();
+          run_jobs(njobs);
+          njobs = 0;
         }
       }
-      const uint32_t np = (pushL ? 1u : 0u) + (pushR ? 1u : 0u);
-      uint32_t incl = np;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= (uint32_t)o) incl += y;
-      }
-      const uint32_t tot = __shfl_sync(0xffffffffu, incl, 31);
+      // push the children in lane order (keeps the stack depth-sorted)
+      const uint32_t bpl = __ballot_sync(0xffffffffu, pushL), bpr = __ballot_sync(0xffffffffu, pushR);
+      const uint32_t tot = __popc(bpl) + __popc(bpr);
       if ((uint32_t)top + tot > cap) {
         failed = true;
         break;
       }
-      uint32_t p = (uint32_t)top + incl - np;
+      uint32_t p = (uint32_t)top + __popc(bpl & lt) + __popc(bpr & lt);
       if (pushL) {
         stk_node[p] = 2u * i + 1u;
         stk_mask[p] = (uint8_t)maskL;
@@ -273,6 +299,10 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
       __syncwarp();
     }
 
+    if (MODE != SEARCH_COUNT && njobs) {
+      __syncwarp();
+      run_jobs(njobs);
+    }
     const bool anyfail = __any_sync(0xffffffffu, failed);
     if (MODE == SEARCH_COUNT) {
       const unsigned long long tot = warp_sum64(acc);
