@@ -36,6 +36,7 @@ constexpr int QT = 128;  // threads per CTA
 constexpr int QW = QT / 32;
 constexpr int JOBS = 256;      // contained-subtree jobs buffered per warp
 constexpr int JFLUSH = JOBS - 64;  // one step adds at most 64
+constexpr int EU = 2;              // emission steps with loads in flight (measured best of 1, 2, 4, 8)
 
 __device__ __forceinline__ uint32_t lanemask_lt_s() {
   uint32_t m;
@@ -142,16 +143,17 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
       }
       __syncwarp();
       // classes 0-3: whole subtrees; class 4: the top five levels (31 nodes)
-      // of each taller subtree -- all packed 32 slots per step
+      // of each taller subtree -- all packed 32 slots per lane step, EU steps
+      // of loads in flight before their stores
 #pragma unroll
       for (uint32_t c = 0; c < 5; ++c) {
         const uint32_t per = (2u << c) - 1u;
         const uint32_t total = cnt[c] * per;
-        for (uint32_t e0 = 0; e0 < total; e0 += 64u) {
-          uint64_t node[2];
-          uint32_t id[2];
+        for (uint32_t e0 = 0; e0 < total; e0 += 32u * EU) {
+          uint64_t node[EU];
+          uint32_t id[EU];
 #pragma unroll
-          for (int u = 0; u < 2; ++u) {
+          for (int u = 0; u < EU; ++u) {
             const uint32_t e = e0 + 32u * u + lane;
             node[u] = ~0ull;
             if (e < total) {
@@ -160,10 +162,11 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
               const uint32_t r = jsort[warp][off[c] + jb];
               node[u] = (((uint64_t)r + 1u) << rl) - 1u + (k + 1u - (1u << rl));
             }
-            id[u] = node[u] < n ? __ldg(sc.tab.ids + node[u]) : 0u;
           }
 #pragma unroll
-          for (int u = 0; u < 2; ++u) emit_ballot(node[u] < n, (uint32_t)node[u], id[u]);
+          for (int u = 0; u < EU; ++u) id[u] = node[u] < n ? __ldg(sc.tab.ids + node[u]) : 0u;
+#pragma unroll
+          for (int u = 0; u < EU; ++u) emit_ballot(node[u] < n, (uint32_t)node[u], id[u]);
         }
       }
       // levels >= 5 of the tall subtrees: runs of >= 32 consecutive slots
@@ -173,15 +176,15 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
           const uint64_t a = (((uint64_t)r + 1u) << j) - 1u;
           if (a >= n) break;
           const uint64_t b = (a + (1ull << j)) < (uint64_t)n ? (a + (1ull << j)) : (uint64_t)n;
-          for (uint64_t x0 = a; x0 < b; x0 += 64u) {
-            uint32_t id[2];
+          for (uint64_t x0 = a; x0 < b; x0 += 32u * EU) {
+            uint32_t id[EU];
 #pragma unroll
-            for (int u = 0; u < 2; ++u) {
+            for (int u = 0; u < EU; ++u) {
               const uint64_t x = x0 + 32u * u + lane;
               id[u] = x < b ? __ldg(sc.tab.ids + x) : 0u;
             }
 #pragma unroll
-            for (int u = 0; u < 2; ++u) {
+            for (int u = 0; u < EU; ++u) {
               const uint64_t x = x0 + 32u * u + lane;
               emit_ballot(x < b, (uint32_t)x, id[u]);
             }
