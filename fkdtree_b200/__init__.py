@@ -25,7 +25,7 @@ import numpy as np
 from . import _capi
 from ._capi import FKDError, MEM_DEVICE, MEM_HOST, FLAG_ASYNC, check, lib
 
-__all__ = ["FKDTree", "FKDError", "lib", "version"]
+__all__ = ["FKDTree", "Batch", "FKDError", "lib", "version"]
 
 
 def version() -> str:
@@ -195,6 +195,81 @@ class FKDTree:
     def close(self) -> None:
         if getattr(self, "_h", None):
             self._lib.fkd_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many independent events built and searched together (fkd_batch_* in
+    include/fkdtree_b200.h).  ``dims`` (E,), ``pt_off`` / ``q_off`` (E+1,)
+    describe the layout of fkdtree_b200.workloads.Batch: event e owns points
+    [pt_off[e], pt_off[e+1]) and boxes [q_off[e], q_off[e+1]); its coordinates
+    (and boxes) are an SoA slice of the flat arrays."""
+
+    def __init__(self, dims, pt_off, q_off, stream=None, flags: int = 0):
+        self._lib = lib()
+        self.dims = np.ascontiguousarray(dims, dtype=np.uint32)
+        self.pt_off = np.ascontiguousarray(pt_off, dtype=np.uint64)
+        self.q_off = np.ascontiguousarray(q_off, dtype=np.uint64)
+        self.n_events = int(self.dims.shape[0])
+        n = np.diff(self.pt_off.astype(np.int64))
+        self.n_coords = int((n * self.dims).sum())
+        self.n_points = int(self.pt_off[-1])
+        self.n_boxes = int(self.q_off[-1])
+        h = C.c_void_p()
+        check(self._lib.fkd_batch_create(self.n_events, _ptr(self.dims), _ptr(self.pt_off), _ptr(self.q_off), flags,
+                                         _stream_handle(stream), C.byref(h)))
+        self._h = h
+
+    @classmethod
+    def of(cls, wb, **kw) -> "Batch":
+        return cls(wb.dims, wb.pt_off, wb.q_off, **kw)
+
+    def set_param(self, name: str, value: int) -> None:
+        check(self._lib.fkd_batch_set_param(self._h, name.encode(), int(value)))
+
+    def build(self, coords, ids) -> "Batch":
+        if _is_torch(coords):
+            check(self._lib.fkd_batch_build(self._h, _ptr(coords), _ptr(ids), MEM_DEVICE))
+        else:
+            c = _host_f32(coords)
+            i = np.ascontiguousarray(ids, dtype=np.uint32)
+            check(self._lib.fkd_batch_build(self._h, _ptr(c), _ptr(i), MEM_HOST))
+        return self
+
+    def tables(self):
+        tab = np.empty(self.n_coords, dtype=np.float32)
+        tid = np.empty(self.n_points, dtype=np.uint32)
+        check(self._lib.fkd_batch_get_tables(self._h, _ptr(tab), _ptr(tid), MEM_HOST))
+        return tab, tid
+
+    def search_digest(self, mins, maxs):
+        if _is_torch(mins):
+            import torch
+            counts = torch.empty(self.n_boxes, dtype=torch.int32, device=mins.device)
+            dig = torch.empty(self.n_boxes, dtype=torch.int64, device=mins.device)
+            check(self._lib.fkd_batch_search_digest(self._h, _ptr(mins), _ptr(maxs), _ptr(counts), _ptr(dig),
+                                                    MEM_DEVICE))
+            return counts, dig
+        lo, hi = _host_f32(mins), _host_f32(maxs)
+        counts = np.empty(self.n_boxes, dtype=np.uint32)
+        dig = np.empty(self.n_boxes, dtype=np.uint64)
+        check(self._lib.fkd_batch_search_digest(self._h, _ptr(lo), _ptr(hi), _ptr(counts), _ptr(dig), MEM_HOST))
+        return counts, dig
+
+    def run(self, coords, ids, mins, maxs, counts, digests) -> None:
+        """Build + digest search of CUDA tensors as one CUDA graph launch."""
+        check(self._lib.fkd_batch_run(self._h, _ptr(coords), _ptr(ids), _ptr(mins), _ptr(maxs), _ptr(counts),
+                                      _ptr(digests)))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.fkd_batch_destroy(self._h)
             self._h = None
 
     def __del__(self):

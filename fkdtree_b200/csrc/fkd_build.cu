@@ -51,10 +51,9 @@ extern "C" __attribute__((visibility("default"))) void fkd_prof_reset() {
 // ---------------------------------------------------------------- global
 
 constexpr int GT = 256;            // threads of the global-level kernels
-constexpr int GIPT = 16;           // records per thread (digit passes)
 constexpr int PIPT = 4;            // records per thread (partition)
 constexpr int PTILE = GT * PIPT;
-constexpr int GTILE = GT * GIPT;   // records per CTA tile
+static_assert(PTILE == (int)PART_TILE, "partition tile");
 constexpr int GWARPS = GT / 32;
 constexpr int RBITS = 11;          // widest digit of the global select (11, 11, 10 per 32-bit word)
 constexpr int RBINS = 1 << RBITS;
@@ -76,19 +75,22 @@ __device__ __forceinline__ void write_node(const Table& tab, uint32_t h, const u
   tab.ids[h] = rec[dim];
 }
 
-__global__ void k_sel_init(Geom g, uint32_t d, SegSel* __restrict__ sel, uint32_t* __restrict__ pending) {
+__global__ void k_sel_init(uint32_t d, const EvDesc* __restrict__ evs, const uint2* __restrict__ segs, uint32_t nseg,
+                           SegSel* __restrict__ sel, uint32_t* __restrict__ pending) {
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s == 0) {
     // pending[p] != 0: digit pass p has a segment to work on
     pending[0] = 1u;
     for (int p = 1; p <= RPASSES; ++p) pending[p] = 0u;
   }
-  if (s >= (1u << d)) return;
-  const uint32_t len = seg_len(g, d, s);
+  if (s >= nseg) return;
+  const uint2 sd = segs[s];
+  const Geom g = evs[sd.x].g;
+  const uint32_t len = seg_len(g, d, sd.y);
   SegSel st;
   st.prefix = 0ull;
   st.bits = 0u;
-  st.krem = (d < g.H) ? seg_rank(g, d, s) : 0u;
+  st.krem = (d < g.H) ? seg_rank(g, d, sd.y) : 0u;
   st.cnt = len;
   st.done = len <= 1u ? 1u : 0u;
   st.tiles_done = 0u;
@@ -107,10 +109,11 @@ __global__ void k_sel_init(Geom g, uint32_t d, SegSel* __restrict__ sel, uint32_
 constexpr int HCOPIES = 4;
 
 template <int DIM>
-__global__ void __launch_bounds__(GT, 4) k_hist(Geom g, uint32_t d, uint32_t tps, uint32_t ts, CSoA src,
-                                             SegSel* __restrict__ sel, uint32_t* __restrict__ ghist,
-                                             const uint32_t* __restrict__ pending_now,
-                                             uint32_t* __restrict__ pending_next, uint32_t* __restrict__ err) {
+__global__ void __launch_bounds__(GT, 4) k_hist(uint32_t d, const EvDesc* __restrict__ evs,
+                                                const uint2* __restrict__ segs, const uint2* __restrict__ tiles,
+                                                uint32_t ts, CSoA src, SegSel* __restrict__ sel,
+                                                uint32_t* __restrict__ ghist, const uint32_t* __restrict__ pending_now,
+                                                uint32_t* __restrict__ pending_next, uint32_t* __restrict__ err) {
   __shared__ uint32_t hist[HCOPIES * RBINS];
   __shared__ uint32_t wsum[GWARPS];
   __shared__ uint32_t s_last;
@@ -118,8 +121,12 @@ __global__ void __launch_bounds__(GT, 4) k_hist(Geom g, uint32_t d, uint32_t tps
   // a digit; without it the whole launch is a no-op.
   if (*(volatile const uint32_t*)pending_now == 0u) return;
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-  const uint32_t s = blockIdx.x / tps, t = blockIdx.x - s * tps;
-  const uint32_t len = seg_len(g, d, s);
+  const uint2 tl = tiles[blockIdx.x];
+  const uint32_t s = tl.x, t = tl.y;
+  const uint2 sd = segs[s];
+  const Geom eg = evs[sd.x].g;
+  const uint32_t ebase = evs[sd.x].base;
+  const uint32_t len = seg_len(eg, d, sd.y);
   const uint32_t ntiles = (len + ts - 1) / ts;
   if (t >= ntiles) return;
   if (sel[s].done) return;
@@ -131,7 +138,7 @@ __global__ void __launch_bounds__(GT, 4) k_hist(Geom g, uint32_t d, uint32_t tps
   const uint32_t nb = 1u << w;
   const bool need_id = bits >= 32u;
   const uint32_t c = d % DIM;
-  const uint32_t start = seg_start(g, d, s);
+  const uint32_t start = ebase + seg_start(eg, d, sd.y);
   const uint32_t tend = min(start + len, start + t * ts + ts);
   uint32_t* myhist = hist + (lane % HCOPIES) * RBINS;
   for (uint32_t i = threadIdx.x; i < HCOPIES * RBINS; i += GT) hist[i] = 0u;
@@ -238,16 +245,23 @@ __device__ __forceinline__ uint32_t pick_coord(const uint32_t* rec, uint32_t c) 
 // Streams every record of depth-d segments once: records below the pivot go
 // to [start, start + rank), the pivot to the table, the rest above it.
 template <int DIM>
-__global__ void __launch_bounds__(GT, 4) k_partition(Geom g, uint32_t d, uint32_t tps, CSoA src, SoA dst,
-                                                     SegSel* __restrict__ sel, Table tab, uint32_t* __restrict__ err) {
+__global__ void __launch_bounds__(GT, 4) k_partition(uint32_t d, const EvDesc* __restrict__ evs,
+                                                     const uint2* __restrict__ segs, const uint2* __restrict__ tiles,
+                                                     CSoA src, SoA dst, SegSel* __restrict__ sel, Table tab,
+                                                     uint32_t* __restrict__ err) {
   __shared__ uint32_t sL[PIPT * GWARPS], sR[PIPT * GWARPS];
   __shared__ uint32_t s_base[2];
-  const uint32_t s = blockIdx.x / tps, t = blockIdx.x - s * tps;
-  const uint32_t len = seg_len(g, d, s);
+  const uint2 tl = tiles[blockIdx.x];
+  const uint32_t s = tl.x, t = tl.y;
+  const uint2 sd = segs[s];
+  const Geom eg = evs[sd.x].g;
+  const uint32_t ebase = evs[sd.x].base;
+  const uint32_t len = seg_len(eg, d, sd.y);
   const uint32_t ntiles = (len + PTILE - 1) / PTILE;
   if (t >= ntiles) return;
-  const uint32_t start = seg_start(g, d, s);
-  const uint32_t rank = seg_rank(g, d, s);
+  const uint32_t start = ebase + seg_start(eg, d, sd.y);
+  const uint32_t rank = seg_rank(eg, d, sd.y);
+  const uint32_t node = ebase + (1u << d) - 1u + sd.y;  // this segment's node
   const uint32_t t0 = start + t * PTILE;
   const uint32_t t1 = min(start + len, t0 + (uint32_t)PTILE);
   const uint32_t bits = sel[s].bits;
@@ -345,7 +359,7 @@ __global__ void __launch_bounds__(GT, 4) k_partition(Geom g, uint32_t d, uint32_
       uint32_t ticket = 0u;
       if (cnt != 1u) ticket = atomicAdd(&sel[s].curE, 1u);  // repeated (coordinate, id) keys only
       if (ticket == krem) {
-        write_node(tab, (1u << d) - 1u + s, rec[k], DIM);
+        write_node(tab, node, rec[k], DIM);
       } else if (ticket < krem) {
         pos = start + atomicAdd(&sel[s].curL, 1u);
         lim = endL;
@@ -459,7 +473,8 @@ __device__ void warp_finish(const Geom& g, uint32_t d1, uint32_t t1, const uint3
 }
 
 template <int DIM>
-__global__ void __launch_bounds__(ST, 1) k_subtree(Geom g, uint32_t d0, CSoA src, Table tab,
+__global__ void __launch_bounds__(ST, 1) k_subtree(const EvDesc* __restrict__ evs, const uint2* __restrict__ subs,
+                                                   CSoA src_in, CSoA src_b0, CSoA src_b1, Table tab_all,
                                                    uint32_t* __restrict__ err) {
   constexpr int SUBN = SubCfg<DIM>::SUBN;
   constexpr int PPT = SubCfg<DIM>::PPT;
@@ -481,7 +496,18 @@ __global__ void __launch_bounds__(ST, 1) k_subtree(Geom g, uint32_t d0, CSoA src
   uint32_t* stage_all = sdup + MAXSEG;
   __shared__ uint32_t wtot[SWARPS];
 
-  const uint32_t s0 = blockIdx.x;
+  // this CTA's subtree: event sb.x, root (d0, s0); positions and node indices
+  // below are local to the event
+  const uint2 sb = subs[blockIdx.x];
+  const EvDesc ev = evs[sb.x];
+  const Geom g = ev.g;
+  const uint32_t d0 = ev.d0;
+  const uint32_t s0 = sb.y;
+  // an event's records sit where its last global level wrote them: the input
+  // (no global level), buffer 0 (odd d0) or buffer 1 (even d0 >= 2)
+  const CSoA src_all = d0 == 0u ? src_in : ((d0 & 1u) ? src_b0 : src_b1);
+  const CSoA src{src_all.base + ev.base, src_all.ids + ev.base, src_all.stride};
+  const Table tab{tab_all.nodes + ev.base, tab_all.ids + ev.base};
   const uint32_t base = seg_start(g, d0, s0);
   const uint32_t nloc = seg_len(g, d0, s0);
   if (nloc > (uint32_t)SUBN) {
@@ -785,35 +811,23 @@ __global__ void __launch_bounds__(ST, 1) k_subtree(Geom g, uint32_t d0, CSoA src
 
 template <int DIM>
 static cudaError_t run_build(BuildCtx& bc) {
-  const Geom g = bc.g;
-  const int SUBN = SubCfg<DIM>::SUBN;
-  uint32_t d0 = 0;
-  while (seg_len(g, d0, 0) > (uint32_t)SUBN) ++d0;
   CSoA src = bc.input;
   SoA bufs[2] = {bc.work[0], bc.work[1]};
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const uint32_t hist_grid = (uint32_t)sms * 4u;
+  const CSoA b0{bufs[0].base, bufs[0].ids, bufs[0].stride}, b1{bufs[1].base, bufs[1].ids, bufs[1].stride};
   int nb = 0;
-  for (uint32_t d = 0; d < d0; ++d) {
-    const uint32_t S = 1u << d;
-    // digit passes: about hist_grid CTAs per level, tiles a multiple of GTILE
-    const uint32_t lmax = seg_len(g, d, 0);
-    const uint32_t want = (hist_grid + S - 1) / S;
-    const uint32_t chunks = (lmax + GTILE - 1) / GTILE;
-    const uint32_t tps = want < chunks ? want : chunks;
-    const uint32_t ts = ((chunks + tps - 1) / tps) * GTILE;
-    const uint32_t ptps = (lmax + PTILE - 1) / PTILE;
-    k_sel_init<<<(S + 255) / 256, 256, 0, bc.stream>>>(g, d, bc.sel, bc.pending);
+  for (uint32_t d = 0; d < bc.nlevels; ++d) {
+    const LevelPlan& lp = bc.levels[d];
+    if (lp.nseg == 0) continue;
+    k_sel_init<<<(lp.nseg + 255) / 256, 256, 0, bc.stream>>>(d, bc.evs, lp.segs, lp.nseg, bc.sel, bc.pending);
     count_launches(1);
     for (int pass = 0; pass < RPASSES; ++pass) {
-      k_hist<DIM><<<S * tps, GT, 0, bc.stream>>>(g, d, tps, ts, src, bc.sel, bc.ghist, bc.pending + pass,
-                                                  bc.pending + pass + 1, bc.err);
+      k_hist<DIM><<<lp.nhtile, GT, 0, bc.stream>>>(d, bc.evs, lp.segs, lp.htiles, lp.hts, src, bc.sel, bc.ghist,
+                                                    bc.pending + pass, bc.pending + pass + 1, bc.err);
       count_launches(1);
     }
     SoA dst = bufs[nb];
-    k_partition<DIM><<<S * ptps, GT, 0, bc.stream>>>(g, d, ptps, src, dst, bc.sel, bc.tab, bc.err);
+    k_partition<DIM><<<lp.nptile, GT, 0, bc.stream>>>(d, bc.evs, lp.segs, lp.ptiles, src, dst, bc.sel, bc.tab,
+                                                        bc.err);
     count_launches(1);
     src = CSoA{dst.base, dst.ids, dst.stride};
     nb ^= 1;
@@ -821,27 +835,23 @@ static cudaError_t run_build(BuildCtx& bc) {
   const size_t smem = SubCfg<DIM>::smem;
   cudaError_t e = cudaFuncSetAttribute(k_subtree<DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  k_subtree<DIM><<<1u << d0, ST, smem, bc.stream>>>(g, d0, src, bc.tab, bc.err);
-  count_launches(1);
+  if (bc.nsub) {
+    k_subtree<DIM><<<bc.nsub, ST, smem, bc.stream>>>(bc.evs, bc.subs, bc.input, b0, b1, bc.tab, bc.err);
+    count_launches(1);
+  }
   return cudaGetLastError();
 }
 
 uint32_t build_global_levels(uint32_t n, int dim) {
+  if (n == 0) return 0;
   const Geom g = make_geom(n);
   const uint32_t subn = (uint32_t)sub_capacity(dim);
   uint32_t d0 = 0;
-  if (n == 0) return 0;
   while (seg_len(g, d0, 0) > subn) ++d0;
   return d0;
 }
 
-size_t build_ghist_words(uint32_t n, int dim) {
-  const uint32_t d0 = build_global_levels(n, dim);
-  return d0 ? (size_t)(1u << (d0 - 1)) * RBINS : 0;
-}
-
 cudaError_t launch_build(BuildCtx& bc, int dim) {
-  if (bc.g.n == 0) return cudaSuccess;
   switch (dim) {
     case 1: return run_build<1>(bc);
     case 2: return run_build<2>(bc);

@@ -8,10 +8,13 @@
 
 #include "../../include/fkdtree_b200.h"
 #include "fkd_internal.h"
+#include "fkd_plan.h"
 
 using namespace fkd;
 
 namespace fkd {
+fkd_status capi_fail(fkd_status s, const std::string& msg);
+fkd_status capi_status_from_err(uint32_t e, const char* what);
 static unsigned long long g_launches = 0;
 void count_launches(uint64_t k) { __atomic_fetch_add(&g_launches, (unsigned long long)k, __ATOMIC_RELAXED); }
 uint64_t launches_total() { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
@@ -70,6 +73,9 @@ struct fkd_tree_s {
   DevBuf nodes, ids, work0, work1, sel, ghist, err, qctr, passflags;
   DevBuf qlo, qhi, counts, offsets, partials, out, tmp, digests, qorder;
   uint32_t* herr = nullptr;  // pinned mirror of err
+  PlanDev plan;              // build plan of the last size built
+  uint64_t plan_n = ~0ull;
+  uint32_t hist_ctas = 0;    // digit-pass CTAs per level (0: four per SM)
 
   ~fkd_tree_s() {
     DevBuf* all[] = {&nodes, &ids, &work0, &work1, &sel, &ghist, &err, &qctr, &passflags,
@@ -81,10 +87,7 @@ struct fkd_tree_s {
 
 namespace {
 
-fkd_status check_err_word(fkd_tree h, const char* what) {
-  FKD_CUDA(cudaMemcpyAsync(h->herr, h->err.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
-  FKD_CUDA(cudaStreamSynchronize(h->stream));
-  const uint32_t e = *h->herr;
+fkd_status status_from_err(uint32_t e, const char* what) {
   if (e == 0) return FKD_OK;
   char buf[160];
   if (e & ERRB_NAN) {
@@ -101,6 +104,12 @@ fkd_status check_err_word(fkd_tree h, const char* what) {
   }
   snprintf(buf, sizeof buf, "%s: device consistency check failed (0x%x)", what, e);
   return fail(FKD_ERR_INTERNAL, buf);
+}
+
+fkd_status check_err_word(fkd_tree h, const char* what) {
+  FKD_CUDA(cudaMemcpyAsync(h->herr, h->err.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+  FKD_CUDA(cudaStreamSynchronize(h->stream));
+  return status_from_err(*h->herr, what);
 }
 
 fkd_status finish(fkd_tree h, const char* what, int mem) {
@@ -182,6 +191,11 @@ fkd_status count_pass(fkd_tree h, const Boxes& b, uint32_t* dcounts, const uint3
 
 }  // namespace
 
+namespace fkd {
+fkd_status capi_fail(fkd_status s, const std::string& msg) { return fail(s, msg); }
+fkd_status capi_status_from_err(uint32_t e, const char* what) { return status_from_err(e, what); }
+}  // namespace fkd
+
 extern "C" {
 
 const char* fkd_version(void) { return "fkdtree_b200 0.1 (sm_100a)"; }
@@ -241,21 +255,28 @@ fkd_status fkd_build(fkd_tree h, const float* coords, const uint32_t* ids, uint6
     return FKD_OK;
   }
   const int dim = h->dim;
-  const uint32_t d0 = build_global_levels((uint32_t)n, dim);
+  if (h->plan_n != n) {
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
+    PlanHost ph;
+    const uint32_t n32 = (uint32_t)n, base0 = 0u;
+    plan_build(&n32, &base0, 1, dim, h->hist_ctas ? h->hist_ctas : 4u * (uint32_t)sms, ph);
+    FKD_CUDA(h->plan.upload(ph, h->stream));
+    h->plan_n = n;
+  }
   const size_t rec_bytes = (size_t)(dim + 1) * n * sizeof(uint32_t);
   FKD_CUDA(h->nodes.ensure(n * sizeof(uint4)));
   FKD_CUDA(h->ids.ensure(n * sizeof(uint32_t)));
   FKD_CUDA(h->work1.ensure(rec_bytes));
-  if (d0 > 0) {
+  if (!h->plan.levels.empty()) {
     FKD_CUDA(h->work0.ensure(rec_bytes));
-    FKD_CUDA(h->sel.ensure(sizeof(SegSel) * (size_t)(1u << (d0 - 1))));
-    const size_t gw = build_ghist_words((uint32_t)n, dim);
+    FKD_CUDA(h->sel.ensure(sizeof(SegSel) * (size_t)h->plan.maxseg));
+    const size_t gw = (size_t)h->plan.maxseg * HIST_BINS;
     FKD_CUDA(h->ghist.ensure(gw * sizeof(uint32_t)));
     FKD_CUDA(cudaMemsetAsync(h->ghist.p, 0, gw * sizeof(uint32_t), h->stream));
   }
   FKD_CUDA(cudaMemsetAsync(h->err.p, 0, sizeof(uint32_t), h->stream));
   BuildCtx bc;
-  bc.g = make_geom((uint32_t)n);
   if (mem == FKD_MEM_HOST) {
     uint32_t* w1 = h->work1.as<uint32_t>();
     FKD_CUDA(cudaMemcpyAsync(w1, coords, (size_t)dim * n * sizeof(float), cudaMemcpyHostToDevice, h->stream));
@@ -268,6 +289,11 @@ fkd_status fkd_build(fkd_tree h, const float* coords, const uint32_t* ids, uint6
   uint32_t* w1 = h->work1.as<uint32_t>();
   bc.work[0] = SoA{w0, w0 ? w0 + (size_t)dim * n : nullptr, n};
   bc.work[1] = SoA{w1, w1 + (size_t)dim * n, n};
+  bc.evs = h->plan.evs;
+  bc.nlevels = (uint32_t)h->plan.levels.size();
+  bc.levels = h->plan.levels.data();
+  bc.subs = h->plan.subs;
+  bc.nsub = h->plan.nsub;
   bc.sel = h->sel.as<SegSel>();
   bc.ghist = h->ghist.as<uint32_t>();
   bc.tab = table_of(h);

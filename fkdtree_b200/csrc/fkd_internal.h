@@ -25,11 +25,41 @@ struct SegSel {
   uint32_t pad;
 };
 
-struct BuildCtx {
+// One event (one independent tree) of a build: its geometry, the position of
+// its first point in the concatenated working arrays / node tables, the number
+// of levels the global kernels split (d0), and where its boxes are.
+struct EvDesc {
   Geom g;
-  CSoA input;     // the points to build from (device)
+  uint32_t base;     // first point / node of the event
+  uint32_t d0;       // global levels of this event
+  uint32_t nq;       // boxes of the event
+  uint64_t qbase;    // index of the event's first box in the launch's box space
+  uint64_t qcbase;   // offset of the event's box coordinates (SoA slice: [c*nq + j])
+  uint64_t qout;     // index of the event's first box in the caller's output arrays
+};
+
+// Device-side plan of a (batched) build: per global level the list of
+// (event, segment) pairs and the CTA -> (segment, tile) maps of the digit and
+// partition kernels; the list of (event, subtree) roots of the subtree kernel.
+struct LevelPlan {
+  const uint2* segs;    // (event, index-in-level)
+  uint32_t nseg;
+  const uint2* htiles;  // digit-pass CTA -> (segment, tile)
+  uint32_t nhtile;
+  uint32_t hts;         // digit-pass tile length
+  const uint2* ptiles;  // partition CTA -> (segment, tile)
+  uint32_t nptile;
+};
+
+struct BuildCtx {
+  const EvDesc* evs;
+  uint32_t nlevels;
+  const LevelPlan* levels;  // host array of nlevels
+  const uint2* subs;        // (event, subtree index at the event's d0)
+  uint32_t nsub;
+  CSoA input;     // the points to build from (device, SoA with stride = total points)
   SoA work[2];    // ping-pong working records
-  SegSel* sel;    // >= 2^(d0-1) entries
+  SegSel* sel;    // >= max segments of a level
   uint32_t* ghist;
   uint32_t* pending;  // one word per digit pass (+1): does that pass have work
   Table tab;
@@ -40,8 +70,10 @@ struct BuildCtx {
 // Number of levels split by the global kernels (the first level whose
 // intervals all fit the shared-memory subtree kernel).
 uint32_t build_global_levels(uint32_t n, int dim);
-size_t build_ghist_words(uint32_t n, int dim);
 int sub_capacity(int dim);
+constexpr uint32_t HIST_BINS = 2048;  // global digit histogram per segment
+constexpr uint32_t PART_TILE = 1024;  // records per partition CTA
+constexpr uint32_t HIST_STEP = 2048;  // digit-pass tile granularity
 cudaError_t launch_build(BuildCtx& bc, int dim);
 
 // ------------------------------------------------------------------ search
@@ -59,6 +91,8 @@ struct SearchCtx {
   Geom g;
   Table tab;
   Boxes boxes;
+  const EvDesc* evs;       // batched search: per-event geometry / bases (null: one event, g + tab)
+  uint32_t nev;
   const uint32_t* order;   // optional processing order of the boxes (null: 0..q-1)
   uint32_t* counts;        // SEARCH_COUNT / SEARCH_DIGEST
   const uint64_t* offsets; // SEARCH_WRITE

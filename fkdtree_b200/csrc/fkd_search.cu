@@ -64,10 +64,9 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   uint32_t* stk_node = (uint32_t*)smem_raw + (size_t)warp * cap;
   uint8_t* stk_mask = (uint8_t*)((uint32_t*)smem_raw + (size_t)QW * cap) + (size_t)warp * cap;
-  const Geom g = sc.g;
-  const uint32_t n = g.n;
   constexpr uint32_t FULL = (1u << (2 * DIM)) - 1u;
   const uint32_t lt = lanemask_lt_s();
+  uint32_t cur_ev = 0;  // batched search: the event of the last box (boxes come in increasing order)
 
   for (;;) {
     uint32_t qi = 0;
@@ -75,12 +74,31 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
     qi = __shfl_sync(0xffffffffu, qi, 0);
     if ((uint64_t)qi >= sc.boxes.q) break;
     const uint32_t qj = sc.order ? sc.order[qi] : qi;
+    uint64_t oj = qj;  // output slot of this box
+    Geom g = sc.g;
+    Table tab = sc.tab;
+    const float* blo = sc.boxes.lo;
+    const float* bhi = sc.boxes.hi;
+    uint64_t bstride = sc.boxes.stride, bj = qj;
+    if (sc.evs) {
+      while (cur_ev + 1u < sc.nev && (uint64_t)qj >= sc.evs[cur_ev + 1u].qbase) ++cur_ev;
+      const EvDesc& ev = sc.evs[cur_ev];
+      g = ev.g;
+      tab.nodes = sc.tab.nodes + ev.base;
+      tab.ids = sc.tab.ids + ev.base;
+      blo = sc.boxes.lo + ev.qcbase;
+      bhi = sc.boxes.hi + ev.qcbase;
+      bstride = ev.nq;
+      bj = qj - ev.qbase;
+      oj = ev.qout + bj;
+    }
+    const uint32_t n = g.n;
     float lo[4] = {0.f, 0.f, 0.f, 0.f}, hi[4] = {0.f, 0.f, 0.f, 0.f};
     uint32_t mask0 = 0u;
 #pragma unroll
     for (int c = 0; c < DIM; ++c) {
-      lo[c] = sc.boxes.lo[(uint64_t)c * sc.boxes.stride + qj];
-      hi[c] = sc.boxes.hi[(uint64_t)c * sc.boxes.stride + qj];
+      lo[c] = blo[(uint64_t)c * bstride + bj];
+      hi[c] = bhi[(uint64_t)c * bstride + bj];
       if (lo[c] == -INFINITY) mask0 |= 1u << (2 * c);
       if (hi[c] == INFINITY) mask0 |= 2u << (2 * c);
     }
@@ -88,8 +106,8 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
     unsigned long long acc2 = 0ull;  // count (DIGEST)
     uint64_t cursor = 0, cend = 0;
     if (MODE == SEARCH_WRITE) {
-      cursor = sc.offsets[qj];
-      cend = sc.offsets[qj + 1];
+      cursor = sc.offsets[oj];
+      cend = sc.offsets[oj + 1];
     }
     bool failed = false;
     uint32_t njobs = 0;  // warp-uniform
@@ -164,7 +182,7 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
             }
           }
 #pragma unroll
-          for (int u = 0; u < EU; ++u) id[u] = node[u] < n ? __ldg(sc.tab.ids + node[u]) : 0u;
+          for (int u = 0; u < EU; ++u) id[u] = node[u] < n ? __ldg(tab.ids + node[u]) : 0u;
 #pragma unroll
           for (int u = 0; u < EU; ++u) emit_ballot(node[u] < n, (uint32_t)node[u], id[u]);
         }
@@ -181,7 +199,7 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
 #pragma unroll
             for (int u = 0; u < EU; ++u) {
               const uint64_t x = x0 + 32u * u + lane;
-              id[u] = x < b ? __ldg(sc.tab.ids + x) : 0u;
+              id[u] = x < b ? __ldg(tab.ids + x) : 0u;
             }
 #pragma unroll
             for (int u = 0; u < EU; ++u) {
@@ -231,7 +249,7 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
       if (have) {
         const uint32_t dep = floor_log2_u32(i + 1u);
         const uint32_t c = dep % DIM;
-        const uint4 nd = __ldg(sc.tab.nodes + i);
+        const uint4 nd = __ldg(tab.nodes + i);
         const float x0 = __uint_as_float(nd.x), x1 = __uint_as_float(nd.y), x2 = __uint_as_float(nd.z),
                     x3 = __uint_as_float(nd.w);
         const float v = sel4(c, x0, x1, x2, x3);
@@ -247,7 +265,7 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
           if (DIM > 3) in &= (x3 <= hi[3] && x3 >= lo[3]);
           emit = in;
         }
-        if (emit && MODE != SEARCH_COUNT) idv = DIM <= 3 ? nd.w : __ldg(sc.tab.ids + i);
+        if (emit && MODE != SEARCH_COUNT) idv = DIM <= 3 ? nd.w : __ldg(tab.ids + i);
         const uint32_t l = 2u * i + 1u;
         const bool visitL = !lower && l < n;
         const bool visitR = (lower || inter) && l + 1u < n;
@@ -309,14 +327,14 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
     const bool anyfail = __any_sync(0xffffffffu, failed);
     if (MODE == SEARCH_COUNT) {
       const unsigned long long tot = warp_sum64(acc);
-      if (lane == 0) sc.counts[qj] = (uint32_t)tot;
+      if (lane == 0) sc.counts[oj] = (uint32_t)tot;
       if (lane == 0 && tot > 0xffffffffull) atomicOr(sc.err, ERRB_CAPACITY);
     } else if (MODE == SEARCH_DIGEST) {
       const unsigned long long dg = warp_sum64(acc);
       const unsigned long long ct = warp_sum64(acc2);
       if (lane == 0) {
-        sc.digests[qj] = dg;
-        sc.counts[qj] = (uint32_t)ct;
+        sc.digests[oj] = dg;
+        sc.counts[oj] = (uint32_t)ct;
       }
     } else {
       if (lane == 0 && cursor != cend) atomicOr(sc.err, ERRB_INTERNAL);

@@ -143,6 +143,43 @@ FKD_API fkd_status fkd_search_digest(fkd_tree h, const float* mins, const float*
  * earlier asynchronous calls. */
 FKD_API fkd_status fkd_sync(fkd_tree h);
 
+/* ---------------------------------------------------------------- batches
+ * Many independent events (one tree each) built and searched together.  No
+ * reference counterpart: the reference constructs one FKDTree_CPU per event
+ * (FKDTree_cpu.h:19-23) and calls build() (:221-277) and search_in_the_box
+ * (:123-169) on each.
+ *
+ * Layout: event e owns points [pt_off[e], pt_off[e+1]) and boxes
+ * [q_off[e], q_off[e+1]) of the concatenated id / count / digest arrays; its
+ * coordinates form their own SoA slice of the concatenated coordinate array:
+ * coordinate c of its point i is coords[coff(e) + c*n_e + i] with
+ * coff(e) = sum over e' < e of dims[e'] * n_e' (boxes likewise with q_e).
+ * Events may mix dimensions (1..4). */
+typedef struct fkd_batch_s* fkd_batch;
+
+/* Plans the batch from its sizes (the plan is reused by every later call). */
+FKD_API fkd_status fkd_batch_create(uint32_t n_events, const uint32_t* dims, const uint64_t* pt_off,
+                                    const uint64_t* q_off, uint32_t flags, void* stream, fkd_batch* out);
+FKD_API fkd_status fkd_batch_destroy(fkd_batch b);
+/* Tuning knob used by the autotuner: "hist_ctas" (digit-pass CTAs per level,
+ * 0 = four per SM).  Re-plans the batch. */
+FKD_API fkd_status fkd_batch_set_param(fkd_batch b, const char* name, int64_t value);
+/* Builds every event; the tables equal one FKDTree_CPU::build per event. */
+FKD_API fkd_status fkd_batch_build(fkd_batch b, const float* coords, const uint32_t* ids, int mem);
+/* Tables of every event in the coordinate / id layout above. */
+FKD_API fkd_status fkd_batch_get_tables(fkd_batch b, float* tab, uint32_t* tab_ids, int mem);
+/* Per-box result count and order-independent digest (see fkd_search_digest);
+ * each box searches its own event's tree. */
+FKD_API fkd_status fkd_batch_search_digest(fkd_batch b, const float* mins, const float* maxs, uint32_t* counts,
+                                           uint64_t* digests, int mem);
+/* Build + digest search of device buffers as ONE CUDA graph launch; the graph
+ * is captured on the first call and replayed while the buffers stay the same.
+ * The batch's stream must not be the legacy default stream (a NULL stream at
+ * fkd_batch_create gives the batch its own stream). */
+FKD_API fkd_status fkd_batch_run(fkd_batch b, const float* coords, const uint32_t* ids, const float* mins,
+                                 const float* maxs, uint32_t* counts, uint64_t* digests);
+FKD_API fkd_status fkd_batch_sync(fkd_batch b);
+
 #ifdef __cplusplus
 }
 #endif
