@@ -25,7 +25,7 @@ import numpy as np
 from . import _capi
 from ._capi import FKDError, MEM_DEVICE, MEM_HOST, FLAG_ASYNC, check, lib
 
-__all__ = ["FKDTree", "Batch", "FKDError", "lib", "version"]
+__all__ = ["FKDTree", "Batch", "MLP", "FKDError", "lib", "version"]
 
 
 def version() -> str:
@@ -192,6 +192,17 @@ class FKDTree:
         (FKDTree_cpu.h:215-219)."""
         return self.count_boxes(minPoints, maxPoints)
 
+    def set_mlp(self, mlp, delta: float = 0.05) -> "FKDTree":
+        """Learned split for later builds (None: plain radix select)."""
+        self._mlp = mlp
+        check(self._lib.fkd_set_mlp(self._h, mlp._h if mlp else None, float(delta)))
+        return self
+
+    def learn_stats(self, reset: bool = False) -> dict:
+        st = np.zeros(4, dtype=np.uint64)
+        check(self._lib.fkd_learn_stats(self._h, _ptr(st), int(reset)))
+        return dict(brackets=int(st[0]), verified=int(st[1]), fallbacks=int(st[2]), bits=int(st[3]))
+
     def close(self) -> None:
         if getattr(self, "_h", None):
             self._lib.fkd_destroy(self._h)
@@ -262,6 +273,33 @@ class Batch:
         check(self._lib.fkd_batch_search_digest(self._h, _ptr(lo), _ptr(hi), _ptr(counts), _ptr(dig), MEM_HOST))
         return counts, dig
 
+    def set_mlp(self, mlp, delta: float = 0.05) -> "Batch":
+        self._mlp = mlp
+        check(self._lib.fkd_batch_set_mlp(self._h, mlp._h if mlp else None, float(delta)))
+        return self
+
+    def learn_stats(self, reset: bool = False) -> dict:
+        st = np.zeros(4, dtype=np.uint64)
+        check(self._lib.fkd_batch_learn_stats(self._h, _ptr(st), int(reset)))
+        return dict(brackets=int(st[0]), verified=int(st[1]), fallbacks=int(st[2]), bits=int(st[3]))
+
+    def record(self, coords, ids, cap: int | None = None):
+        """Exact build that records (features, target) of every globally split
+        node; returns (x (m, 40) float32, t (m,) float32)."""
+        cap = cap if cap is not None else max(1024, self.n_points // 512)
+        x = np.empty((cap, MLP.IN), dtype=np.float32)
+        t = np.empty(cap, dtype=np.float32)
+        n = C.c_uint64(0)
+        if _is_torch(coords):
+            check(self._lib.fkd_batch_record(self._h, _ptr(coords), _ptr(ids), _ptr(x), _ptr(t), cap, C.byref(n),
+                                             MEM_DEVICE))
+        else:
+            c = _host_f32(coords)
+            i = np.ascontiguousarray(ids, dtype=np.uint32)
+            check(self._lib.fkd_batch_record(self._h, _ptr(c), _ptr(i), _ptr(x), _ptr(t), cap, C.byref(n), MEM_HOST))
+        m = min(int(n.value), cap)
+        return x[:m], t[:m]
+
     def run(self, coords, ids, mins, maxs, counts, digests) -> None:
         """Build + digest search of CUDA tensors as one CUDA graph launch."""
         check(self._lib.fkd_batch_run(self._h, _ptr(coords), _ptr(ids), _ptr(mins), _ptr(maxs), _ptr(counts),
@@ -270,6 +308,66 @@ class Batch:
     def close(self) -> None:
         if getattr(self, "_h", None):
             self._lib.fkd_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class MLP:
+    """The learned split predictor (fkd_mlp_* in include/fkdtree_b200.h):
+    40 -> 64 -> 64 -> 1, GELU, bf16 tensor-core products with fp32
+    accumulation, trained on the GPU."""
+
+    IN = 40
+
+    def __init__(self, seed: int = 0):
+        self._lib = lib()
+        h = C.c_void_p()
+        check(self._lib.fkd_mlp_create(seed, C.byref(h)))
+        self._h = h
+        self.n_params = int(self._lib.fkd_mlp_param_count())
+
+    @property
+    def params(self) -> np.ndarray:
+        p = np.empty(self.n_params, dtype=np.float32)
+        check(self._lib.fkd_mlp_get_params(self._h, _ptr(p)))
+        return p
+
+    @params.setter
+    def params(self, p) -> None:
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        assert p.shape == (self.n_params,)
+        check(self._lib.fkd_mlp_set_params(self._h, _ptr(p)))
+
+    def forward(self, x) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, self.IN)
+        y = np.empty(x.shape[0], dtype=np.float32)
+        check(self._lib.fkd_mlp_forward(self._h, _ptr(x), x.shape[0], _ptr(y), MEM_HOST))
+        return y
+
+    def grad(self, x, t):
+        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, self.IN)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        g = np.empty(self.n_params, dtype=np.float32)
+        loss = C.c_float(0.0)
+        check(self._lib.fkd_mlp_grad(self._h, _ptr(x), _ptr(t), x.shape[0], _ptr(g), C.byref(loss), MEM_HOST))
+        return g, float(loss.value)
+
+    def train(self, x, t, epochs: int = 30, batch: int = 256, lr: float = 2e-3, seed: int = 0) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, self.IN)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        losses = np.empty(epochs, dtype=np.float32)
+        check(self._lib.fkd_mlp_train(self._h, _ptr(x), _ptr(t), x.shape[0], epochs, batch, float(lr), seed,
+                                      _ptr(losses), MEM_HOST))
+        return losses
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.fkd_mlp_destroy(self._h)
             self._h = None
 
     def __del__(self):

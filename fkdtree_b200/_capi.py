@@ -44,6 +44,19 @@ SIGNATURES = {
     "fkd_batch_search_digest": ([_vp, _vp, _vp, _vp, _vp, _int], _int),
     "fkd_batch_run": ([_vp, _vp, _vp, _vp, _vp, _vp, _vp], _int),
     "fkd_batch_sync": ([_vp], _int),
+    "fkd_mlp_create": ([_u32, C.POINTER(_vp)], _int),
+    "fkd_mlp_destroy": ([_vp], _int),
+    "fkd_mlp_param_count": ([], _u64),
+    "fkd_mlp_get_params": ([_vp, _vp], _int),
+    "fkd_mlp_set_params": ([_vp, _vp], _int),
+    "fkd_mlp_forward": ([_vp, _vp, _u64, _vp, _int], _int),
+    "fkd_mlp_grad": ([_vp, _vp, _vp, _u64, _vp, _vp, _int], _int),
+    "fkd_mlp_train": ([_vp, _vp, _vp, _u64, _u32, _u32, C.c_float, _u32, _vp, _int], _int),
+    "fkd_set_mlp": ([_vp, _vp, C.c_float], _int),
+    "fkd_batch_set_mlp": ([_vp, _vp, C.c_float], _int),
+    "fkd_learn_stats": ([_vp, _vp, _int], _int),
+    "fkd_batch_learn_stats": ([_vp, _vp, _int], _int),
+    "fkd_batch_record": ([_vp, _vp, _vp, _vp, _vp, _u64, _vp, _int], _int),
 }
 
 

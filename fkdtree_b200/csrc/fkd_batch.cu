@@ -22,6 +22,7 @@
 #include "../../include/fkdtree_b200.h"
 #include "fkd_internal.h"
 #include "fkd_plan.h"
+#include "fkd_mlp.h"
 
 using namespace fkd;
 
@@ -112,7 +113,7 @@ struct Part {
   uint64_t npts = 0, nq = 0;
   uint32_t maxn = 0;  // largest event (sizes the search stack)
   PlanDev plan;
-  Buf io, chunks, work0, work1, nodes, ids, sel, ghist;
+  Buf io, chunks, work0, work1, nodes, ids, sel, ghist, lfeat, lyhat, lrange;
   uint32_t nchunks = 0;
 };
 
@@ -132,6 +133,15 @@ struct fkd_batch_s {
   bool built = false;
   // tuning knobs (fkd_batch_set_param)
   uint32_t hist_ctas = 0;
+  // learned split
+  fkd_mlp mlp = nullptr;
+  float mlp_delta = 0.f;
+  Buf lstats;
+  // recording of training targets (fkd_batch_record)
+  float* rec_x = nullptr;
+  float* rec_t = nullptr;
+  unsigned long long* rec_n = nullptr;
+  uint64_t rec_cap = 0;
   // captured build+search graph and the pointers it was captured with
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
@@ -194,7 +204,11 @@ fkd_status batch_plan(fkd_batch b) {
     BCUDA(p.ids.ensure(p.npts * 4));
     BCUDA(p.sel.ensure(sizeof(SegSel) * (size_t)p.plan.maxseg));
     BCUDA(p.ghist.ensure((size_t)p.plan.maxseg * HIST_BINS * 4));
+    BCUDA(p.lfeat.ensure((size_t)p.plan.maxseg * FKD_MLP_FEATURES * 4));
+    BCUDA(p.lyhat.ensure((size_t)p.plan.maxseg * 4));
+    BCUDA(p.lrange.ensure((size_t)p.plan.maxseg * sizeof(float2)));
   }
+  BCUDA(b->lstats.ensure(64));
   BCUDA(cudaStreamSynchronize(b->stream));
   return FKD_OK;
 }
@@ -238,6 +252,23 @@ fkd_status enqueue_build(fkd_batch b, const float* coords, const uint32_t* ids) 
     bc.err = b->err.as<uint32_t>();
     bc.pending = b->passflags.as<uint32_t>();
     bc.stream = b->stream;
+    memset(&bc.learn, 0, sizeof bc.learn);
+    if (b->mlp || b->rec_x) {
+      bc.learn.feat = p.lfeat.as<float>();
+      bc.learn.yhat = p.lyhat.as<float>();
+      bc.learn.range = p.lrange.as<float2>();
+      bc.learn.stats = b->lstats.as<unsigned long long>();
+    }
+    if (b->mlp) {
+      bc.learn.params = mlp_params(b->mlp);
+      bc.learn.delta = b->mlp_delta;
+    }
+    if (b->rec_x) {
+      bc.learn.rec_x = b->rec_x;
+      bc.learn.rec_t = b->rec_t;
+      bc.learn.rec_n = b->rec_n;
+      bc.learn.rec_cap = b->rec_cap;
+    }
     BCUDA(launch_build(bc, p.dim));
   }
   return FKD_OK;
@@ -482,6 +513,59 @@ fkd_status fkd_batch_run(fkd_batch b, const float* coords, const uint32_t* ids, 
   BCUDA(cudaGraphLaunch(b->gexec, b->stream));
   b->built = true;
   return batch_finish(b, "fkd_batch_run", FKD_MEM_DEVICE);
+}
+
+fkd_status fkd_batch_set_mlp(fkd_batch b, fkd_mlp m, float delta) {
+  if (!b) return capi_fail(FKD_ERR_ARG, "null handle");
+  if (m && !(delta > 0.f)) return capi_fail(FKD_ERR_ARG, "delta must be positive");
+  b->mlp = m;
+  b->mlp_delta = delta;
+  if (b->gexec) cudaGraphExecDestroy(b->gexec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->gexec = nullptr;
+  b->graph = nullptr;
+  BCUDA(cudaMemsetAsync(b->lstats.p, 0, 32, b->stream));
+  BCUDA(cudaStreamSynchronize(b->stream));
+  return FKD_OK;
+}
+
+fkd_status fkd_batch_learn_stats(fkd_batch b, uint64_t* stats, int reset) {
+  if (!b || !stats) return capi_fail(FKD_ERR_ARG, "null argument");
+  BCUDA(cudaMemcpyAsync(stats, b->lstats.p, 4 * sizeof(uint64_t), cudaMemcpyDeviceToHost, b->stream));
+  if (reset) BCUDA(cudaMemsetAsync(b->lstats.p, 0, 32, b->stream));
+  BCUDA(cudaStreamSynchronize(b->stream));
+  return FKD_OK;
+}
+
+fkd_status fkd_batch_record(fkd_batch b, const float* coords, const uint32_t* ids, float* x_out, float* t_out,
+                            uint64_t cap, uint64_t* n_out, int mem) {
+  if (!b || !n_out || (cap && (!x_out || !t_out))) return capi_fail(FKD_ERR_ARG, "null argument");
+  Buf dx, dt, dn;
+  BCUDA(dx.ensure((cap ? cap : 1) * FKD_MLP_FEATURES * 4));
+  BCUDA(dt.ensure((cap ? cap : 1) * 4));
+  BCUDA(dn.ensure(8));
+  BCUDA(cudaMemsetAsync(dn.p, 0, 8, b->stream));
+  fkd_mlp saved = b->mlp;
+  b->mlp = nullptr;  // recording needs the plain (exact, unpredicted) select
+  b->rec_x = dx.as<float>();
+  b->rec_t = dt.as<float>();
+  b->rec_n = dn.as<unsigned long long>();
+  b->rec_cap = cap;
+  fkd_status s = fkd_batch_build(b, coords, ids, mem);
+  b->mlp = saved;
+  b->rec_x = b->rec_t = nullptr;
+  b->rec_n = nullptr;
+  b->rec_cap = 0;
+  if (s != FKD_OK) return s;
+  unsigned long long n = 0;
+  BCUDA(cudaMemcpy(&n, dn.p, 8, cudaMemcpyDeviceToHost));
+  *n_out = n;
+  const uint64_t m = n < cap ? n : cap;
+  if (m) {
+    BCUDA(cudaMemcpy(x_out, dx.p, m * FKD_MLP_FEATURES * 4, cudaMemcpyDeviceToHost));
+    BCUDA(cudaMemcpy(t_out, dt.p, m * 4, cudaMemcpyDeviceToHost));
+  }
+  return FKD_OK;
 }
 
 fkd_status fkd_batch_sync(fkd_batch b) {

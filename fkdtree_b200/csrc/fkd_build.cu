@@ -27,6 +27,7 @@
 //    to the table as it is decided.  One HBM read + one table write for the
 //    bottom ~12 levels.
 #include "fkd_internal.h"
+#include "fkd_mlp.h"
 
 namespace fkd {
 
@@ -57,7 +58,7 @@ static_assert(PTILE == (int)PART_TILE, "partition tile");
 constexpr int GWARPS = GT / 32;
 constexpr int RBITS = 11;          // widest digit of the global select (11, 11, 10 per 32-bit word)
 constexpr int RBINS = 1 << RBITS;
-constexpr int RPASSES = 6;         // 5 * 11 + 9 >= 64
+constexpr int RPASSES = 7;         // 11,11,10 | 11,11,10 bits, plus a verifying pass of a predicted block
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
   uint32_t m;
@@ -95,6 +96,9 @@ __global__ void k_sel_init(uint32_t d, const EvDesc* __restrict__ evs, const uin
   st.done = len <= 1u ? 1u : 0u;
   st.tiles_done = 0u;
   st.curL = st.curR = st.curE = 0u;
+  st.verify = 0u;
+  st.below = 0u;
+  st.kfull = st.krem;
   st.pad = 0u;
   sel[s] = st;
 }
@@ -113,7 +117,8 @@ __global__ void __launch_bounds__(GT, 4) k_hist(uint32_t d, const EvDesc* __rest
                                                 const uint2* __restrict__ segs, const uint2* __restrict__ tiles,
                                                 uint32_t ts, CSoA src, SegSel* __restrict__ sel,
                                                 uint32_t* __restrict__ ghist, const uint32_t* __restrict__ pending_now,
-                                                uint32_t* __restrict__ pending_next, uint32_t* __restrict__ err) {
+                                                uint32_t* __restrict__ pending_next, uint32_t* __restrict__ err,
+                                                unsigned long long* __restrict__ lstats) {
   __shared__ uint32_t hist[HCOPIES * RBINS];
   __shared__ uint32_t wsum[GWARPS];
   __shared__ uint32_t s_last;
@@ -132,9 +137,11 @@ __global__ void __launch_bounds__(GT, 4) k_hist(uint32_t d, const EvDesc* __rest
   if (sel[s].done) return;
   const uint32_t bits = sel[s].bits;
   const unsigned long long prefix = sel[s].prefix;
-  // digits never straddle the value/id boundary: 11, 11, 10 bits per word
+  // digits never straddle the value/id boundary: at most 11 bits, up to the
+  // end of the current 32-bit word (11, 11, 10 from a word start)
   const uint32_t inword = bits & 31u;
-  const uint32_t w = inword < 22u ? 11u : 10u;
+  const uint32_t w = (32u - inword) < 11u ? (32u - inword) : 11u;
+  const bool verify = sel[s].verify != 0u;  // prefix is a predicted block (value bits only)
   const uint32_t nb = 1u << w;
   const bool need_id = bits >= 32u;
   const uint32_t c = d % DIM;
@@ -146,6 +153,7 @@ __global__ void __launch_bounds__(GT, 4) k_hist(uint32_t d, const EvDesc* __rest
   const uint32_t* X = src.base + (uint64_t)c * src.stride;
   const uint32_t vpre = (uint32_t)(prefix >> (bits > 32u ? bits - 32u : 0u));  // value part of the prefix
   const uint32_t vbits = bits < 32u ? bits : 32u;
+  uint32_t nbelow = 0u;  // verify pass: points below the predicted block
   constexpr int HIPT = 8;  // records per thread per step
   for (uint32_t t0 = start + t * ts; t0 < tend; t0 += GT * HIPT) {
     const uint32_t t1 = min(tend, t0 + (uint32_t)(GT * HIPT));
@@ -160,6 +168,7 @@ __global__ void __launch_bounds__(GT, 4) k_hist(uint32_t d, const EvDesc* __rest
       const uint32_t e = t0 + k * GT + threadIdx.x;
       if (e < t1) {
         const uint32_t mv = mono_bits(vb[k]);
+        if (verify && vbits != 0u && (mv >> (32u - vbits)) < vpre) ++nbelow;
         // value bits first; the id is read only by points whose value matches
         if (vbits == 0u || (mv >> (32u - vbits)) == vpre) {
           uint32_t dig;
@@ -176,6 +185,10 @@ __global__ void __launch_bounds__(GT, 4) k_hist(uint32_t d, const EvDesc* __rest
       }
     }
   }
+  if (verify) {
+    for (int o = 16; o > 0; o >>= 1) nbelow += __shfl_xor_sync(0xffffffffu, nbelow, o);
+    if (lane == 0 && nbelow) atomicAdd(&sel[s].below, nbelow);
+  }
   __syncthreads();
   uint32_t* gh = ghist + (uint64_t)s * RBINS;
   for (uint32_t i = threadIdx.x; i < nb; i += GT) {
@@ -191,7 +204,7 @@ __global__ void __launch_bounds__(GT, 4) k_hist(uint32_t d, const EvDesc* __rest
   if (!s_last) return;
   __threadfence();
   // Last CTA of segment s: locate the digit holding rank krem.
-  const uint32_t krem = *(volatile uint32_t*)&sel[s].krem;
+  uint32_t krem = *(volatile uint32_t*)&sel[s].krem;
   constexpr int BPT = RBINS / GT;  // bins per thread
   uint32_t h[BPT];
   uint32_t mine = 0u;
@@ -209,8 +222,40 @@ __global__ void __launch_bounds__(GT, 4) k_hist(uint32_t d, const EvDesc* __rest
   }
   if (lane == 31u) wsum[warp] = incl;
   __syncthreads();
-  uint32_t wbase = 0u;
-  for (uint32_t k = 0; k < warp; ++k) wbase += wsum[k];
+  uint32_t wbase = 0u, total = 0u;
+  for (uint32_t k = 0; k < (uint32_t)GWARPS; ++k) {
+    if (k < warp) wbase += wsum[k];
+    total += wsum[k];
+  }
+  if (verify) {
+    // the predicted block holds the pivot iff below <= k < below + total
+    const uint32_t below = *(volatile uint32_t*)&sel[s].below;
+    if (krem >= below && krem - below < total) {
+      krem -= below;
+      if (threadIdx.x == 0) {
+        sel[s].verify = 0u;
+        if (lstats) {
+          atomicAdd(&lstats[1], 1ull);
+          atomicAdd(&lstats[3], (unsigned long long)bits);  // key bits the prediction resolved
+        }
+      }
+    } else {
+      // miss: restart this segment as the plain radix select
+      for (uint32_t b = threadIdx.x; b < nb; b += GT) gh[b] = 0u;
+      if (threadIdx.x == 0) {
+        SegSel* p = &sel[s];
+        p->prefix = 0ull;
+        p->bits = 0u;
+        p->krem = p->kfull;
+        p->cnt = len;
+        p->verify = 0u;
+        p->tiles_done = 0u;
+        *pending_next = 1u;
+        if (lstats) atomicAdd(&lstats[2], 1ull);
+      }
+      return;
+    }
+  }
   uint32_t cum = wbase + incl - mine;
 #pragma unroll
   for (int k = 0; k < BPT; ++k) {
@@ -231,7 +276,7 @@ __global__ void __launch_bounds__(GT, 4) k_hist(uint32_t d, const EvDesc* __rest
   if (threadIdx.x == 0) sel[s].tiles_done = 0u;
   // the last thread's inclusive sum is the number of matching records; it
   // must cover krem, otherwise the select state is inconsistent.
-  if (threadIdx.x == GT - 1 && krem >= wbase + incl) atomicOr(err, ERRB_INTERNAL);
+  if (threadIdx.x == GT - 1 && krem >= total) atomicOr(err, ERRB_INTERNAL);
 }
 
 template <int DIM>
@@ -820,15 +865,34 @@ static cudaError_t run_build(BuildCtx& bc) {
     if (lp.nseg == 0) continue;
     k_sel_init<<<(lp.nseg + 255) / 256, 256, 0, bc.stream>>>(d, bc.evs, lp.segs, lp.nseg, bc.sel, bc.pending);
     count_launches(1);
-    for (int pass = 0; pass < RPASSES; ++pass) {
+    const LearnCtx& lc = bc.learn;
+    if (lc.params || lc.rec_x) {
+      cudaError_t e = launch_features(d, bc.evs, lp.segs, lp.nseg, src, DIM, lc.feat, lc.range, bc.stream);
+      if (e != cudaSuccess) return e;
+    }
+    if (lc.params) {
+      cudaError_t e = mlp_infer(lc.params, lc.feat, lp.nseg, lc.yhat, bc.stream);
+      if (e == cudaSuccess)
+        e = launch_bracket(d, bc.evs, lp.segs, lp.nseg, lc.yhat, lc.range, lc.delta, bc.sel, lc.stats, bc.stream);
+      if (e != cudaSuccess) return e;
+    }
+    // the plain select needs at most 6 passes; a failed prediction costs one more
+    const int passes = lc.params ? RPASSES : RPASSES - 1;
+    for (int pass = 0; pass < passes; ++pass) {
       k_hist<DIM><<<lp.nhtile, GT, 0, bc.stream>>>(d, bc.evs, lp.segs, lp.htiles, lp.hts, src, bc.sel, bc.ghist,
-                                                    bc.pending + pass, bc.pending + pass + 1, bc.err);
+                                                    bc.pending + pass, bc.pending + pass + 1, bc.err,
+                                                    lc.params ? lc.stats : nullptr);
       count_launches(1);
     }
     SoA dst = bufs[nb];
     k_partition<DIM><<<lp.nptile, GT, 0, bc.stream>>>(d, bc.evs, lp.segs, lp.ptiles, src, dst, bc.sel, bc.tab,
                                                         bc.err);
     count_launches(1);
+    if (lc.rec_x) {
+      cudaError_t e = launch_record(d, bc.evs, lp.segs, lp.nseg, DIM, bc.tab, lc.feat, lc.range, lc.rec_x, lc.rec_t,
+                                    lc.rec_n, lc.rec_cap, bc.stream);
+      if (e != cudaSuccess) return e;
+    }
     src = CSoA{dst.base, dst.ids, dst.stride};
     nb ^= 1;
   }

@@ -9,6 +9,7 @@
 #include "../../include/fkdtree_b200.h"
 #include "fkd_internal.h"
 #include "fkd_plan.h"
+#include "fkd_mlp.h"
 
 using namespace fkd;
 
@@ -76,10 +77,14 @@ struct fkd_tree_s {
   PlanDev plan;              // build plan of the last size built
   uint64_t plan_n = ~0ull;
   uint32_t hist_ctas = 0;    // digit-pass CTAs per level (0: four per SM)
+  fkd_mlp mlp = nullptr;     // learned split (null: plain radix select)
+  float mlp_delta = 0.f;
+  DevBuf lfeat, lyhat, lrange, lstats;
 
   ~fkd_tree_s() {
     DevBuf* all[] = {&nodes, &ids, &work0, &work1, &sel, &ghist, &err, &qctr, &passflags,
-                     &qlo, &qhi, &counts, &offsets, &partials, &out, &tmp, &digests, &qorder};
+                     &qlo, &qhi, &counts, &offsets, &partials, &out, &tmp, &digests, &qorder,
+                     &lfeat, &lyhat, &lrange, &lstats};
     for (DevBuf* b : all) b->release();
     if (herr) cudaFreeHost(herr);
   }
@@ -300,6 +305,20 @@ fkd_status fkd_build(fkd_tree h, const float* coords, const uint32_t* ids, uint6
   bc.err = h->err.as<uint32_t>();
   bc.pending = h->passflags.as<uint32_t>();
   bc.stream = h->stream;
+  memset(&bc.learn, 0, sizeof bc.learn);
+  if (h->mlp && !h->plan.levels.empty()) {
+    const size_t ms = h->plan.maxseg;
+    FKD_CUDA(h->lfeat.ensure(ms * FKD_MLP_FEATURES * sizeof(float)));
+    FKD_CUDA(h->lyhat.ensure(ms * sizeof(float)));
+    FKD_CUDA(h->lrange.ensure(ms * sizeof(float2)));
+    FKD_CUDA(h->lstats.ensure(4 * sizeof(unsigned long long)));
+    bc.learn.params = mlp_params(h->mlp);
+    bc.learn.delta = h->mlp_delta;
+    bc.learn.feat = h->lfeat.as<float>();
+    bc.learn.yhat = h->lyhat.as<float>();
+    bc.learn.range = h->lrange.as<float2>();
+    bc.learn.stats = h->lstats.as<unsigned long long>();
+  }
   FKD_CUDA(launch_build(bc, dim));
   h->built = true;
   fkd_status s = finish(h, "fkd_build", mem);
@@ -488,6 +507,28 @@ fkd_status fkd_search_digest(fkd_tree h, const float* mins, const float* maxs, u
     FKD_CUDA(cudaMemcpyAsync(digests, dd, q * sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
   }
   return finish(h, "fkd_search_digest", mem);
+}
+
+fkd_status fkd_set_mlp(fkd_tree h, fkd_mlp m, float delta) {
+  if (!h) return fail(FKD_ERR_ARG, "null handle");
+  if (m && !(delta > 0.f)) return fail(FKD_ERR_ARG, "delta must be positive");
+  h->mlp = m;
+  h->mlp_delta = delta;
+  if (m) {
+    FKD_CUDA(h->lstats.ensure(4 * sizeof(unsigned long long)));
+    FKD_CUDA(cudaMemsetAsync(h->lstats.p, 0, 4 * sizeof(unsigned long long), h->stream));
+  }
+  return FKD_OK;
+}
+
+fkd_status fkd_learn_stats(fkd_tree h, uint64_t* stats, int reset) {
+  if (!h || !stats) return fail(FKD_ERR_ARG, "null argument");
+  stats[0] = stats[1] = stats[2] = stats[3] = 0;
+  if (!h->lstats.p) return FKD_OK;
+  FKD_CUDA(cudaMemcpyAsync(stats, h->lstats.p, 4 * sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
+  if (reset) FKD_CUDA(cudaMemsetAsync(h->lstats.p, 0, 4 * sizeof(unsigned long long), h->stream));
+  FKD_CUDA(cudaStreamSynchronize(h->stream));
+  return FKD_OK;
 }
 
 fkd_status fkd_sync(fkd_tree h) {

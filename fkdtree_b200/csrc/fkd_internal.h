@@ -22,7 +22,27 @@ struct SegSel {
   uint32_t done;              // the pivot key is determined
   uint32_t tiles_done;        // CTAs of the current pass that finished
   uint32_t curL, curR, curE;  // partition cursors
+  uint32_t verify;            // 1: prefix is a predicted block, the next pass verifies it
+  uint32_t below;             // verify pass: points whose key lies below the block
+  uint32_t kfull;             // the pivot rank within the segment (fallback restart)
   uint32_t pad;
+};
+
+constexpr int FKD_MLP_FEATURES = 40;  // node summary width (== FKD_MLP_IN of the C ABI)
+
+// Learned-split state of a build (all null / zero for the plain build).
+struct LearnCtx {
+  const float* params;  // MLP parameters (null: plain radix select)
+  float delta;          // bracket half-width, in units of the sample range
+  float* feat;          // >= maxseg * 40 features
+  float* yhat;          // >= maxseg predictions
+  float2* range;        // >= maxseg sample ranges (min, max) along the split dimension
+  unsigned long long* stats;  // [0] brackets tried, [1] verified, [2] fell back
+  // recording mode (training data): targets of every global segment
+  float* rec_x;         // features of recorded segments (rows of 40)
+  float* rec_t;         // their targets
+  unsigned long long* rec_n;  // running count
+  uint64_t rec_cap;
 };
 
 // One event (one independent tree) of a build: its geometry, the position of
@@ -65,6 +85,7 @@ struct BuildCtx {
   Table tab;
   uint32_t* err;
   cudaStream_t stream;
+  LearnCtx learn;
 };
 
 // Number of levels split by the global kernels (the first level whose
@@ -75,6 +96,15 @@ constexpr uint32_t HIST_BINS = 2048;  // global digit histogram per segment
 constexpr uint32_t PART_TILE = 1024;  // records per partition CTA
 constexpr uint32_t HIST_STEP = 2048;  // digit-pass tile granularity
 cudaError_t launch_build(BuildCtx& bc, int dim);
+// fkd_features.cu: node summaries, bracket initialisation, target recording
+cudaError_t launch_features(uint32_t d, const EvDesc* evs, const uint2* segs, uint32_t nseg, CSoA src, int dim,
+                            float* feat, float2* range, cudaStream_t stream);
+cudaError_t launch_bracket(uint32_t d, const EvDesc* evs, const uint2* segs, uint32_t nseg, const float* yhat,
+                           const float2* range, float delta, SegSel* sel, unsigned long long* stats,
+                           cudaStream_t stream);
+cudaError_t launch_record(uint32_t d, const EvDesc* evs, const uint2* segs, uint32_t nseg, int dim, Table tab,
+                          const float* feat, const float2* range, float* rec_x, float* rec_t,
+                          unsigned long long* rec_n, uint64_t rec_cap, cudaStream_t stream);
 
 // ------------------------------------------------------------------ search
 

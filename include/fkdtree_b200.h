@@ -180,6 +180,52 @@ FKD_API fkd_status fkd_batch_run(fkd_batch b, const float* coords, const uint32_
                                  const float* maxs, uint32_t* counts, uint64_t* digests);
 FKD_API fkd_status fkd_batch_sync(fkd_batch b);
 
+/* -------------------------------------------------------- learned split
+ * A 40 -> 64 -> 64 -> 1 MLP (GELU, bf16 operands, fp32 accumulation) that
+ * predicts where a node's split value lies, from cheap summaries of the node:
+ * the bounding box of a 256-point sample (6 floats), log2 of the point count,
+ * the depth and a 32-bin histogram of the sample along the split dimension
+ * (FKD_MLP_IN = 40 features, layout in fkd_features.cu).  The prediction only
+ * chooses where the exact radix select starts; a verifying count decides
+ * whether it holds and the plain select runs when it does not, so the tree is
+ * bit-identical either way.  No reference counterpart.
+ *
+ * Parameters (fkd_mlp_param_count() floats): W1[48][64] (rows 40..47 zero),
+ * b1[64], W2[64][64], b2[64], w3[64], b3. */
+#define FKD_MLP_IN 40
+typedef struct fkd_mlp_s* fkd_mlp;
+
+FKD_API fkd_status fkd_mlp_create(uint32_t seed, fkd_mlp* out);
+FKD_API fkd_status fkd_mlp_destroy(fkd_mlp m);
+FKD_API uint64_t fkd_mlp_param_count(void);
+FKD_API fkd_status fkd_mlp_get_params(fkd_mlp m, float* params);
+FKD_API fkd_status fkd_mlp_set_params(fkd_mlp m, const float* params);
+/* y[i] = MLP(x[i*40 .. i*40+39]) */
+FKD_API fkd_status fkd_mlp_forward(fkd_mlp m, const float* x, uint64_t n, float* y, int mem);
+/* Gradient of mean((y - t)^2)/2 w.r.t. every parameter (host output). */
+FKD_API fkd_status fkd_mlp_grad(fkd_mlp m, const float* x, const float* t, uint64_t n, float* grad, float* loss,
+                                int mem);
+/* Adam training on the GPU; losses[epoch] receives the mean batch loss. */
+FKD_API fkd_status fkd_mlp_train(fkd_mlp m, const float* x, const float* t, uint64_t n, uint32_t epochs,
+                                 uint32_t batch, float lr, uint32_t seed, float* losses, int mem);
+/* Learned split for later builds of a tree / batch (m NULL: plain radix
+ * select).  delta is the bracket half-width in units of the node's sample
+ * range along the split dimension.  The model must outlive its use. */
+FKD_API fkd_status fkd_set_mlp(fkd_tree h, fkd_mlp m, float delta);
+FKD_API fkd_status fkd_batch_set_mlp(fkd_batch b, fkd_mlp m, float delta);
+/* stats[0] brackets predicted, [1] verified (the select started inside the
+ * predicted block), [2] fell back to the plain select, [3] key bits resolved
+ * by the verified predictions (sum); cumulative until reset. */
+FKD_API fkd_status fkd_learn_stats(fkd_tree h, uint64_t* stats, int reset);
+FKD_API fkd_status fkd_batch_learn_stats(fkd_batch b, uint64_t* stats, int reset);
+/* Exact (plain) build of a batch that also records, for every node the
+ * global kernels split, its features and target (the split value's position
+ * in the node's sample range): training data for the learned split.  At most
+ * cap rows are written (host arrays x_out: cap*40, t_out: cap); *n_out
+ * receives the number of recorded nodes. */
+FKD_API fkd_status fkd_batch_record(fkd_batch b, const float* coords, const uint32_t* ids, float* x_out,
+                                    float* t_out, uint64_t cap, uint64_t* n_out, int mem);
+
 #ifdef __cplusplus
 }
 #endif
