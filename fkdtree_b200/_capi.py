@@ -30,6 +30,8 @@ SIGNATURES = {
     "fkd_set_stream": ([_vp, _vp], _int),
     "fkd_build": ([_vp, _vp, _vp, _u64, _int], _int),
     "fkd_size": ([_vp, C.POINTER(_u64)], _int),
+    "fkd_build_noalloc": ([_int, _vp, _vp, _u32, _vp, _vp, _vp], _int),
+    "fkd_build_noalloc_max_points": ([_int], _u32),
     "fkd_get_tables": ([_vp, _vp, _vp, _int], _int),
     "fkd_search_count": ([_vp, _vp, _vp, _u64, _vp, _int], _int),
     "fkd_search_write": ([_vp, _vp, _vp, _u64, _vp, _vp, _int, _int], _int),

@@ -915,6 +915,28 @@ uint32_t build_global_levels(uint32_t n, int dim) {
   return d0;
 }
 
+template <int DIM>
+static cudaError_t run_subtree_direct(const EvDesc* evs, const uint2* subs, uint32_t nsub, CSoA src, Table tab,
+                                     uint32_t* err, cudaStream_t stream) {
+  const size_t smem = SubCfg<DIM>::smem;
+  cudaError_t e = cudaFuncSetAttribute(k_subtree<DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  k_subtree<DIM><<<nsub, ST, smem, stream>>>(evs, subs, src, src, src, tab, err);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_subtree_direct(const EvDesc* evs, const uint2* subs, uint32_t nsub, CSoA src, Table tab,
+                                  uint32_t* err, int dim, cudaStream_t stream) {
+  switch (dim) {
+    case 1: return run_subtree_direct<1>(evs, subs, nsub, src, tab, err, stream);
+    case 2: return run_subtree_direct<2>(evs, subs, nsub, src, tab, err, stream);
+    case 3: return run_subtree_direct<3>(evs, subs, nsub, src, tab, err, stream);
+    case 4: return run_subtree_direct<4>(evs, subs, nsub, src, tab, err, stream);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
 cudaError_t launch_build(BuildCtx& bc, int dim) {
   switch (dim) {
     case 1: return run_build<1>(bc);

@@ -96,6 +96,10 @@ constexpr uint32_t HIST_BINS = 2048;  // global digit histogram per segment
 constexpr uint32_t PART_TILE = 1024;  // records per partition CTA
 constexpr uint32_t HIST_STEP = 2048;  // digit-pass tile granularity
 cudaError_t launch_build(BuildCtx& bc, int dim);
+// The shared-memory subtree kernel alone, for events whose d0 is 0 (reads
+// every event from `src`).
+cudaError_t launch_subtree_direct(const EvDesc* evs, const uint2* subs, uint32_t nsub, CSoA src, Table tab,
+                                  uint32_t* err, int dim, cudaStream_t stream);
 // fkd_features.cu: node summaries, bracket initialisation, target recording
 cudaError_t launch_features(uint32_t d, const EvDesc* evs, const uint2* segs, uint32_t nseg, CSoA src, int dim,
                             float* feat, float2* range, cudaStream_t stream);

@@ -98,6 +98,24 @@ FKD_API fkd_status fkd_set_stream(fkd_tree h, void* stream);
  * call). */
 FKD_API fkd_status fkd_build(fkd_tree h, const float* coords, const uint32_t* ids, uint64_t n, int mem);
 
+/* Builds one small tree without allocating any memory (no counterpart in the
+ * reference).  For callers that may not call cudaMalloc / cudaFree while
+ * they work -- code inside a framework that owns all device memory through
+ * its own pool, where those calls would synchronise the device or could fail
+ * mid-event.  All buffers are the caller's device memory: coords (dim*n SoA),
+ * ids (n) in; tab (dim*n SoA, theDimensions) and tab_ids (n, theIds) out, the
+ * same tables fkd_build + fkd_get_tables produce.  The library works in a
+ * fixed scratch array of its own (one per device, kept until exit), so n is
+ * limited to fkd_build_noalloc_max_points(dim) (4096, or 3072 for dim 4);
+ * larger n is rejected with FKD_ERR_ARG.  The first call on a device looks up
+ * the scratch address -- make it before any stream capture.  Calls share the
+ * scratch: calls whose GPU work overlaps (other streams or threads on the same
+ * device) race and must be serialised by the caller.  Synchronises `stream`
+ * before returning, to report device-side errors. */
+FKD_API fkd_status fkd_build_noalloc(int dim, const float* coords, const uint32_t* ids, uint32_t n, float* tab,
+                                     uint32_t* tab_ids, void* stream);
+FKD_API uint32_t fkd_build_noalloc_max_points(int dim);
+
 /* Number of points of the last build. */
 FKD_API fkd_status fkd_size(fkd_tree h, uint64_t* n);
 
