@@ -113,7 +113,7 @@ struct Part {
   uint64_t npts = 0, nq = 0;
   uint32_t maxn = 0;  // largest event (sizes the search stack)
   PlanDev plan;
-  Buf io, chunks, work0, work1, nodes, ids, sel, ghist, lfeat, lyhat, lrange;
+  Buf io, chunks, work0, work1, nodes, ids, sel, ghist, lfeat, lyhat, lrange, sdig;
   uint32_t nchunks = 0;
 };
 
@@ -204,6 +204,7 @@ fkd_status batch_plan(fkd_batch b) {
     BCUDA(p.ids.ensure(p.npts * 4));
     BCUDA(p.sel.ensure(sizeof(SegSel) * (size_t)p.plan.maxseg));
     BCUDA(p.ghist.ensure((size_t)p.plan.maxseg * HIST_BINS * 4));
+    BCUDA(p.sdig.ensure(p.npts * sizeof(unsigned long long)));
     BCUDA(p.lfeat.ensure((size_t)p.plan.maxseg * FKD_MLP_FEATURES * 4));
     BCUDA(p.lyhat.ensure((size_t)p.plan.maxseg * 4));
     BCUDA(p.lrange.ensure((size_t)p.plan.maxseg * sizeof(float2)));
@@ -278,10 +279,12 @@ fkd_status enqueue_digest(fkd_batch b, const float* mins, const float* maxs, uin
   for (auto& pp : b->parts) {
     Part& p = *pp;
     if (p.nq == 0) continue;
+    Table tab{p.nodes.as<uint4>(), p.ids.as<uint32_t>(), p.sdig.as<unsigned long long>()};
+    BCUDA(launch_subtree_digests(p.plan.evs, p.plan.nev, p.maxn, tab, b->stream));
     SearchCtx sc;
     memset(&sc, 0, sizeof sc);
     sc.g = make_geom(p.maxn);  // per-box geometry comes from the event; this sizes the stack
-    sc.tab = Table{p.nodes.as<uint4>(), p.ids.as<uint32_t>()};
+    sc.tab = tab;
     sc.boxes = Boxes{mins, maxs, 0, p.nq};
     sc.evs = p.plan.evs;
     sc.nev = p.plan.nev;

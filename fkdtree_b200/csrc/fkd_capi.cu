@@ -79,12 +79,13 @@ struct fkd_tree_s {
   uint32_t hist_ctas = 0;    // digit-pass CTAs per level (0: four per SM)
   fkd_mlp mlp = nullptr;     // learned split (null: plain radix select)
   float mlp_delta = 0.f;
-  DevBuf lfeat, lyhat, lrange, lstats;
+  DevBuf lfeat, lyhat, lrange, lstats, sdig;
+  bool sdig_valid = false;
 
   ~fkd_tree_s() {
     DevBuf* all[] = {&nodes, &ids, &work0, &work1, &sel, &ghist, &err, &qctr, &passflags,
                      &qlo, &qhi, &counts, &offsets, &partials, &out, &tmp, &digests, &qorder,
-                     &lfeat, &lyhat, &lrange, &lstats};
+                     &lfeat, &lyhat, &lrange, &lstats, &sdig};
     for (DevBuf* b : all) b->release();
     if (herr) cudaFreeHost(herr);
   }
@@ -254,6 +255,7 @@ fkd_status fkd_build(fkd_tree h, const float* coords, const uint32_t* ids, uint6
   if (n >= (1ull << 31)) return fail(FKD_ERR_ARG, "at most 2^31-1 points per tree");
   if (n && (!coords || !ids)) return fail(FKD_ERR_ARG, "null coords or ids");
   h->built = false;
+  h->sdig_valid = false;
   h->n = n;
   if (n == 0) {
     h->built = true;
@@ -495,9 +497,17 @@ fkd_status fkd_search_digest(fkd_tree h, const float* mins, const float* maxs, u
     dd = h->digests.as<uint64_t>();
   }
   FKD_CUDA(cudaMemsetAsync(h->err.p, 0, sizeof(uint32_t), h->stream));
+  if (!h->sdig_valid && h->n) {
+    FKD_CUDA(h->sdig.ensure(h->n * sizeof(unsigned long long)));
+    Table t = table_of(h);
+    t.sdig = h->sdig.as<unsigned long long>();
+    FKD_CUDA(launch_subtree_digests(h->plan.evs, 1, (uint32_t)h->n, t, h->stream));
+    h->sdig_valid = true;
+  }
   const uint32_t* order = nullptr;
   if ((s = box_order(h, b, &order)) != FKD_OK) return s;
   SearchCtx sc = search_ctx(h, b);
+  sc.tab.sdig = h->sdig.as<unsigned long long>();
   sc.order = order;
   sc.counts = dc;
   sc.digests = (unsigned long long*)dd;

@@ -116,6 +116,9 @@ struct CSoA {
 struct Table {
   uint4* nodes;
   uint32_t* ids;
+  // optional: sdig[i] = sum of mix64(id) over the subtree of node i (mod 2^64),
+  // filled by launch_subtree_digests before a digest search
+  unsigned long long* sdig = nullptr;
 };
 
 }  // namespace fkd

@@ -140,6 +140,8 @@ struct SearchCtx {
 };
 
 cudaError_t launch_search(SearchCtx& sc, int dim, int mode);
+// Fills tab.sdig (subtree digests) for every event; required by SEARCH_DIGEST.
+cudaError_t launch_subtree_digests(const EvDesc* evs, uint32_t nev, uint32_t max_n, Table tab, cudaStream_t stream);
 // Sorts every box's result slice by heap index and maps it to ids.
 cudaError_t launch_order_results(const Geom& g, const Table& tab, const uint64_t* offsets, uint64_t q, uint32_t* out,
                                  uint32_t* tmp, uint32_t* err, cudaStream_t stream);

@@ -86,6 +86,7 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
       g = ev.g;
       tab.nodes = sc.tab.nodes + ev.base;
       tab.ids = sc.tab.ids + ev.base;
+      tab.sdig = sc.tab.sdig ? sc.tab.sdig + ev.base : nullptr;
       blo = sc.boxes.lo + ev.qcbase;
       bhi = sc.boxes.hi + ev.qcbase;
       bstride = ev.nq;
@@ -217,9 +218,13 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
       if (mask0 == FULL) {
         if (MODE == SEARCH_COUNT) {
           if (lane == 0) acc += n;
+        } else if (MODE == SEARCH_DIGEST) {
+          if (lane == 0) {
+            acc2 += n;
+            acc += tab.sdig[0];
+          }
         } else {
           if (lane == 0) jobs[warp][0] = 0u;
-          if (MODE == SEARCH_DIGEST && lane == 0) acc2 += n;
           njobs = 1;
           __syncwarp();
         }
@@ -281,13 +286,17 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
                (contR ? subtree_size(g, 2u * i + 2u) : 0u);
       } else {
         if (MODE == SEARCH_DIGEST) {
+          // a contained subtree's digest is one table entry (sdig)
           if (emit) acc += mix64(idv);
+          if (contL) acc += tab.sdig[2u * i + 1u];
+          if (contR) acc += tab.sdig[2u * i + 2u];
           acc2 += (emit ? 1u : 0u) + (contL ? subtree_size(g, 2u * i + 1u) : 0u) +
                   (contR ? subtree_size(g, 2u * i + 2u) : 0u);
         } else {
           emit_ballot(emit, i, idv);
         }
         // buffer the contained subtrees; emit them in bulk when the buffer fills
+        if (MODE == SEARCH_WRITE) {
         const uint32_t bl = __ballot_sync(0xffffffffu, contL), br = __ballot_sync(0xffffffffu, contR);
         const uint32_t jp = njobs + __popc(bl & lt) + __popc(br & lt);
         if (contL) jobs[warp][jp] = 2u * i + 1u;
@@ -297,6 +306,7 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
           __syncwarp();
           run_jobs(njobs);
           njobs = 0;
+        }
         }
       }
       // push the children in lane order (keeps the stack depth-sorted)
@@ -384,6 +394,45 @@ cudaError_t launch_search(SearchCtx& sc, int dim, int mode) {
     case 4: return run_search_mode<4>(sc, mode);
     default: return cudaErrorInvalidValue;
   }
+}
+
+// ---------------------------------------------------------- subtree digests
+//
+// sdig[i] = mix64(id_i) + sdig[2i+1] + sdig[2i+2] (mod 2^64), level by level
+// from the deepest level up.  Block x handles event x (grid.y blocks share an
+// event's level).  With it a digest search adds one entry per contained
+// subtree instead of hashing every id in it.
+
+__global__ void k_sdig_level(uint32_t d, const EvDesc* __restrict__ evs, Table tab) {
+  const EvDesc ev = evs[blockIdx.x];
+  const uint32_t n = ev.g.n;
+  if (d > ev.g.H || n == 0) return;
+  const uint32_t a = (1u << d) - 1u;
+  const uint32_t b = min(n, (2u << d) - 1u);
+  const uint32_t* ids = tab.ids + ev.base;
+  unsigned long long* sd = tab.sdig + ev.base;
+  for (uint32_t i = a + blockIdx.y * blockDim.x + threadIdx.x; i < b; i += gridDim.y * blockDim.x) {
+    unsigned long long v = mix64(ids[i]);
+    const uint32_t l = 2u * i + 1u;
+    if (l < n) v += sd[l];
+    if (l + 1u < n) v += sd[l + 1u];
+    sd[i] = v;
+  }
+}
+
+cudaError_t launch_subtree_digests(const EvDesc* evs, uint32_t nev, uint32_t max_n, Table tab, cudaStream_t stream) {
+  if (nev == 0 || max_n == 0) return cudaSuccess;
+  const uint32_t H = floor_log2_u32(max_n);
+  for (int d = (int)H; d >= 0; --d) {
+    const uint32_t width = 1u << d;
+    uint32_t gy = (width + 255u) / 256u;
+    const uint32_t cap = nev >= 1024u ? 1u : 4096u / nev;
+    if (gy > cap) gy = cap;
+    if (gy < 1u) gy = 1u;
+    k_sdig_level<<<dim3(nev, gy), 256, 0, stream>>>((uint32_t)d, evs, tab);
+    count_launches(1);
+  }
+  return cudaGetLastError();
 }
 
 // ------------------------------------------------------------ box order
