@@ -59,6 +59,8 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-queries", type=int, default=8192, help="box sample of the CPU baseline")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched / learned events report")
+    ap.add_argument("--batched-events", type=int, default=4096)
     return ap.parse_args()
 
 
@@ -140,6 +142,150 @@ class ClockSampler:
                 if r[col].strip().lower().startswith("active"):
                     reasons.add(name)
         return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(rows)}
+
+
+# ------------------------------------------------------- batched events
+
+def batched_report(dev, n_events=4096, steps=3, train_events=2000):
+    """The batched events workload (4,096 events, log-normal sizes median
+    20,000 clipped to [1,000, 200,000], 50-500 clusters each, every point a
+    box of half-width 0.01 on its own event; eval seed 20) three ways:
+
+      plain    one fkd_build + fkd_search_digest per event (the plain
+               single-event GPU path), every event, device buffers
+      batched  fkd_batch_run: all builds and searches as one CUDA graph launch,
+               launch knobs from the autotuner
+      learned  the same graph with the learned split (MLP trained on the GPU on
+               splits recorded from 2,000 training events, seed 10)
+
+    Exactness: per-box counts and digests of the batched runs equal the plain
+    path's; the learned tables equal the plain batched tables."""
+    import torch
+
+    import fkdtree_b200 as F
+    from fkdtree_b200 import _capi
+    from fkdtree_b200 import workloads as W
+
+    t0 = time.perf_counter()
+    wb = W.event_batch(n_events=n_events, seed=20)
+    tr = W.event_batch(n_events=train_events, seed=10, queries=False)
+    gen_s = time.perf_counter() - t0
+    L = _capi.lib()
+    P = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+    coords = torch.from_numpy(wb.coords).to(dev)
+    ids = torch.from_numpy(wb.ids.view(np.int32)).to(dev)
+    mins = torch.from_numpy(wb.mins).to(dev)
+    maxs = torch.from_numpy(wb.maxs).to(dev)
+    nq = wb.n_queries
+
+    def timed(fn, k):
+        fn()
+        torch.cuda.synchronize()
+        best = float("inf")
+        for _ in range(k):
+            a = time.perf_counter()
+            fn()
+            torch.cuda.synchronize()
+            best = min(best, time.perf_counter() - a)
+        return best
+
+    # plain single-event path over every event
+    pc = torch.empty(nq, dtype=torch.int32, device=dev)
+    pd = torch.empty(nq, dtype=torch.int64, device=dev)
+    hd = {}
+    sh = C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+
+    def plain():
+        for e in range(wb.n_events):
+            d = int(wb.dims[e])
+            if d not in hd:
+                hh = C.c_void_p()
+                _capi.check(L.fkd_create(d, _capi.FLAG_ASYNC, sh, C.byref(hh)))
+                hd[d] = hh
+            hh = hd[d]
+            n = int(wb.pt_off[e + 1] - wb.pt_off[e])
+            q = int(wb.q_off[e + 1] - wb.q_off[e])
+            c0, p0, qc0, q0 = int(wb.coord_off[e]), int(wb.pt_off[e]), int(wb.qcoord_off[e]), int(wb.q_off[e])
+            _capi.check(L.fkd_build(hh, P(coords[c0:c0 + d * n]), P(ids[p0:p0 + n]), n, _capi.MEM_DEVICE))
+            if q:
+                _capi.check(L.fkd_search_digest(hh, P(mins[qc0:qc0 + d * q]), P(maxs[qc0:qc0 + d * q]), q,
+                                                P(pc[q0:q0 + q]), P(pd[q0:q0 + q]), _capi.MEM_DEVICE))
+        for hh in hd.values():
+            _capi.check(L.fkd_sync(hh))
+
+    plain_s = timed(plain, 1)
+    for hh in hd.values():
+        _capi.check(L.fkd_destroy(hh))
+    results = int(pc.to(torch.int64).sum().item())
+
+    # batched, autotuned
+    b = F.Batch.of(wb)
+    tune = b.autotune(coords, ids, mins, maxs, use_cache=False, reps=1)
+    bc = torch.empty(nq, dtype=torch.int32, device=dev)
+    bd = torch.empty(nq, dtype=torch.int64, device=dev)
+    batched_s = timed(lambda: b.run(coords, ids, mins, maxs, bc, bd), steps)
+    exact_batched = bool(torch.equal(bc, pc) and torch.equal(bd, pd))
+    tab0 = torch.empty(wb.coords.size, dtype=torch.float32, device=dev)
+    tid0 = torch.empty(wb.n_points, dtype=torch.int32, device=dev)
+    _capi.check(L.fkd_batch_get_tables(b._h, P(tab0), P(tid0), _capi.MEM_DEVICE))
+    build_s = timed(lambda: b.build(coords, ids), steps)
+    digest_s = timed(lambda: b.search_digest(mins, maxs), 1)
+    launches0 = L.fkd_kernel_launches()
+    b.build(coords, ids)
+    b.search_digest(mins, maxs)
+    batched_launches = L.fkd_kernel_launches() - launches0
+
+    # learned split: record on the training events, train on the GPU
+    t0 = time.perf_counter()
+    btr = F.Batch.of(tr)
+    trc = torch.from_numpy(tr.coords).to(dev)
+    tri = torch.from_numpy(tr.ids.view(np.int32)).to(dev)
+    x, t = btr.record(trc, tri)
+    record_s = time.perf_counter() - t0
+    mlp = F.MLP(seed=1)
+    t0 = time.perf_counter()
+    losses = mlp.train(x, t, epochs=60, batch=256, lr=2e-3)
+    train_s = time.perf_counter() - t0
+    del btr, trc, tri
+    delta = 0.1
+    b.set_mlp(mlp, delta=delta)
+    lc = torch.empty(nq, dtype=torch.int32, device=dev)
+    ld = torch.empty(nq, dtype=torch.int64, device=dev)
+    learned_s = timed(lambda: b.run(coords, ids, mins, maxs, lc, ld), steps)
+    st = b.learn_stats(reset=True)
+    tab1 = torch.empty_like(tab0)
+    tid1 = torch.empty_like(tid0)
+    _capi.check(L.fkd_batch_get_tables(b._h, P(tab1), P(tid1), _capi.MEM_DEVICE))
+    exact_learned = bool(torch.equal(lc, pc) and torch.equal(ld, pd) and
+                         torch.equal(tab0.view(torch.int32), tab1.view(torch.int32)) and torch.equal(tid0, tid1))
+    learned_build_s = timed(lambda: b.build(coords, ids), steps)
+    b.learn_stats(reset=True)
+    b.set_mlp(None)
+    runs = steps + 1
+    hit = st["verified"] / st["brackets"] if st["brackets"] else 0.0
+    return {
+        "workload": ("events4096: 4,096 3D events, sizes LogNormal(ln 20000, 1.0) clipped to [1000, 200000], "
+                     "50-500 clusters each, every point a box of half-width 0.01 on its own event, seed 20"),
+        "events": wb.n_events, "points": wb.n_points, "boxes": nq, "results": results, "generate_s": gen_s,
+        "plain_single_event_ms": 1e3 * plain_s,
+        "batched_graph_ms": 1e3 * batched_s,
+        "batched_build_ms": 1e3 * build_s, "batched_digest_ms": 1e3 * digest_s,
+        "learned_graph_ms": 1e3 * learned_s, "learned_build_ms": 1e3 * learned_build_s,
+        "speedup_batched_vs_plain": plain_s / batched_s,
+        "speedup_learned_batched_vs_plain": plain_s / learned_s,
+        "batched_mpoints_per_s": wb.n_points / batched_s / 1e6,
+        "batched_mboxes_per_s": nq / batched_s / 1e6,
+        "kernels_per_batched_run": int(batched_launches),
+        "exact": {"batched_counts_digests_equal_plain": exact_batched,
+                  "learned_counts_digests_tables_equal_plain": exact_learned},
+        "autotune": {"hist_ctas": tune["hist_ctas"], "search_lanes": tune["search_lanes"],
+                     "build_s": tune["build_s"], "search_s": tune["search_s"]},
+        "learned": {"delta": delta, "train_events": train_events, "train_seed": 10, "train_rows": int(x.shape[0]),
+                    "record_s": record_s, "train_s": train_s, "loss_first": float(losses[0]),
+                    "loss_last": float(losses[-1]),
+                    "brackets_per_run": st["brackets"] // runs, "hit_rate": hit, "fallback_rate": 1.0 - hit,
+                    "fallbacks_per_run": st["fallbacks"] // runs},
+    }
 
 
 # ------------------------------------------------------------------ our arm
@@ -253,6 +399,10 @@ def run_ours(args):
     if not args.no_e2e:
         line["e2e"] = run_e2e(args, L, h, ev, results, stream, world, barrier, dev)
     _capi.check(L.fkd_destroy(h))
+    del coords, ids, mins, maxs, offsets, counts, out
+    torch.cuda.empty_cache()
+    if rank == 0 and world == 1 and not args.no_batched:
+        line["batched"] = batched_report(dev, n_events=args.batched_events)
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(ev, args.cpu_queries)
     if rank == 0:

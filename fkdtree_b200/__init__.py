@@ -192,6 +192,11 @@ class FKDTree:
         (FKDTree_cpu.h:215-219)."""
         return self.count_boxes(minPoints, maxPoints)
 
+    def set_param(self, name: str, value: int) -> "FKDTree":
+        """Tuning knob ("hist_ctas", "search_lanes"; fkd_set_param)."""
+        check(self._lib.fkd_set_param(self._h, name.encode(), int(value)))
+        return self
+
     def set_mlp(self, mlp, delta: float = 0.05) -> "FKDTree":
         """Learned split for later builds (None: plain radix select)."""
         self._mlp = mlp
@@ -243,6 +248,12 @@ class Batch:
 
     def set_param(self, name: str, value: int) -> None:
         check(self._lib.fkd_batch_set_param(self._h, name.encode(), int(value)))
+
+    def autotune(self, coords, ids, mins, maxs, **kw) -> dict:
+        """Sweeps the launch knobs on these inputs and keeps the fastest
+        (fkdtree_b200.autotune.tune_batch)."""
+        from . import autotune
+        return autotune.tune_batch(self, coords, ids, mins, maxs, **kw)
 
     def build(self, coords, ids) -> "Batch":
         if _is_torch(coords):

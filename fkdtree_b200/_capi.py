@@ -41,6 +41,7 @@ SIGNATURES = {
     "fkd_batch_create": ([_u32, _vp, _vp, _vp, _u32, _vp, C.POINTER(_vp)], _int),
     "fkd_batch_destroy": ([_vp], _int),
     "fkd_batch_set_param": ([_vp, C.c_char_p, C.c_int64], _int),
+    "fkd_set_param": ([_vp, C.c_char_p, C.c_int64], _int),
     "fkd_batch_build": ([_vp, _vp, _vp, _int], _int),
     "fkd_batch_get_tables": ([_vp, _vp, _vp, _int], _int),
     "fkd_batch_search_digest": ([_vp, _vp, _vp, _vp, _vp, _int], _int),

@@ -133,6 +133,7 @@ struct fkd_batch_s {
   bool built = false;
   // tuning knobs (fkd_batch_set_param)
   uint32_t hist_ctas = 0;
+  uint32_t search_lanes = 0;
   // learned split
   fkd_mlp mlp = nullptr;
   float mlp_delta = 0.f;
@@ -293,6 +294,7 @@ fkd_status enqueue_digest(fkd_batch b, const float* mins, const float* maxs, uin
     sc.qcounter = b->qctr.as<uint32_t>();
     sc.err = b->err.as<uint32_t>();
     sc.capacity = ~0ull;
+    sc.lanes = b->search_lanes;
     sc.stream = b->stream;
     BCUDA(launch_search(sc, p.dim, SEARCH_DIGEST));
   }
@@ -375,9 +377,7 @@ fkd_status fkd_batch_destroy(fkd_batch b) {
 
 fkd_status fkd_batch_set_param(fkd_batch b, const char* name, int64_t value) {
   if (!b || !name) return capi_fail(FKD_ERR_ARG, "null argument");
-  if (strcmp(name, "hist_ctas") == 0) {
-    if (value < 0 || value > (1 << 20)) return capi_fail(FKD_ERR_ARG, "hist_ctas out of range");
-    b->hist_ctas = (uint32_t)value;
+  auto drop_graph = [b]() {
     if (b->gexec) {
       cudaGraphExecDestroy(b->gexec);
       b->gexec = nullptr;
@@ -386,7 +386,19 @@ fkd_status fkd_batch_set_param(fkd_batch b, const char* name, int64_t value) {
       cudaGraphDestroy(b->graph);
       b->graph = nullptr;
     }
+  };
+  if (strcmp(name, "hist_ctas") == 0) {
+    if (value < 0 || value > (1 << 20)) return capi_fail(FKD_ERR_ARG, "hist_ctas out of range");
+    b->hist_ctas = (uint32_t)value;
+    drop_graph();
     return batch_plan(b);
+  }
+  if (strcmp(name, "search_lanes") == 0) {
+    if (value != 0 && value != 1 && value != 2 && value != 4 && value != 8 && value != 16 && value != 32)
+      return capi_fail(FKD_ERR_ARG, "search_lanes must be 0, 1, 2, 4, 8, 16 or 32");
+    b->search_lanes = (uint32_t)value;
+    drop_graph();
+    return FKD_OK;
   }
   return capi_fail(FKD_ERR_ARG, std::string("unknown parameter ") + name);
 }

@@ -77,6 +77,7 @@ struct fkd_tree_s {
   PlanDev plan;              // build plan of the last size built
   uint64_t plan_n = ~0ull;
   uint32_t hist_ctas = 0;    // digit-pass CTAs per level (0: four per SM)
+  uint32_t search_lanes = 0; // count / digest lanes per box (0: one warp)
   fkd_mlp mlp = nullptr;     // learned split (null: plain radix select)
   float mlp_delta = 0.f;
   DevBuf lfeat, lyhat, lrange, lstats, sdig;
@@ -164,6 +165,7 @@ SearchCtx search_ctx(fkd_tree h, const Boxes& b) {
   sc.err = h->err.as<uint32_t>();
   sc.stream = h->stream;
   sc.capacity = ~0ull;
+  sc.lanes = h->search_lanes;
   return sc;
 }
 
@@ -517,6 +519,23 @@ fkd_status fkd_search_digest(fkd_tree h, const float* mins, const float* maxs, u
     FKD_CUDA(cudaMemcpyAsync(digests, dd, q * sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
   }
   return finish(h, "fkd_search_digest", mem);
+}
+
+fkd_status fkd_set_param(fkd_tree h, const char* name, int64_t value) {
+  if (!h || !name) return fail(FKD_ERR_ARG, "null argument");
+  if (strcmp(name, "hist_ctas") == 0) {
+    if (value < 0 || value > (1 << 20)) return fail(FKD_ERR_ARG, "hist_ctas out of range");
+    h->hist_ctas = (uint32_t)value;
+    h->plan_n = ~0ull;  // re-plan at the next build
+    return FKD_OK;
+  }
+  if (strcmp(name, "search_lanes") == 0) {
+    if (value != 0 && value != 1 && value != 2 && value != 4 && value != 8 && value != 16 && value != 32)
+      return fail(FKD_ERR_ARG, "search_lanes must be 0, 1, 2, 4, 8, 16 or 32");
+    h->search_lanes = (uint32_t)value;
+    return FKD_OK;
+  }
+  return fail(FKD_ERR_ARG, std::string("unknown parameter ") + name);
 }
 
 fkd_status fkd_set_mlp(fkd_tree h, fkd_mlp m, float delta) {

@@ -136,6 +136,7 @@ struct SearchCtx {
   uint32_t* qcounter;      // work counter (zeroed by the launcher)
   uint32_t* err;
   int heap_out;            // write heap indices instead of ids
+  uint32_t lanes;          // count / digest: lanes per box (1, 2, 4, 8, 16; 0 or 32: one warp per box)
   cudaStream_t stream;
 };
 

@@ -354,6 +354,221 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
   }
 }
 
+// Count / digest with G < 32 lanes per box (G = 1: a thread per box): a warp
+// holds 32/G boxes, each group with its own depth-sorted stack (popping the
+// top G keeps at most 2G entries per depth, so 2G*(H+1) + 1 bound it), and a
+// group that finishes takes the next box at once.  Small boxes near the root
+// keep only a few nodes in flight; packing several per warp fills the lanes
+// those steps leave idle.  Same node tests and accumulation as k_search.
+__host__ __device__ inline uint32_t stack_cap_lanes(const Geom& g, uint32_t G) { return 2u * G * (g.H + 1u) + 1u; }
+
+template <int DIM, int MODE, int G>
+__global__ void __launch_bounds__(QT) k_search_grp(SearchCtx sc, uint32_t cap) {
+  static_assert(G == 1 || G == 2 || G == 4 || G == 8 || G == 16, "group width");
+  constexpr int NG = QT / G;
+  constexpr uint32_t GM = (1u << G) - 1u;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t grp = threadIdx.x / G, gl = threadIdx.x % G;
+  const uint32_t gsh = lane & ~(uint32_t)(G - 1);
+  const uint32_t gmask = GM << gsh;
+  const uint32_t glt = (1u << gl) - 1u;
+  uint32_t* stk_node = (uint32_t*)smem_raw + (size_t)grp * cap;
+  uint8_t* stk_mask = (uint8_t*)((uint32_t*)smem_raw + (size_t)NG * cap) + (size_t)grp * cap;
+  constexpr uint32_t FULL = (1u << (2 * DIM)) - 1u;
+
+  uint32_t cur_ev = 0;
+  bool active = false, exhausted = false, failed = false;
+  int top = 0;
+  uint64_t oj = 0;
+  Geom g = sc.g;
+  Table tab = sc.tab;
+  float lo[4] = {0.f, 0.f, 0.f, 0.f}, hi[4] = {0.f, 0.f, 0.f, 0.f};
+  unsigned long long acc = 0ull, acc2 = 0ull;
+
+  // the group's result for its current box (group-uniform call)
+  auto finish = [&]() {
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) {
+      acc += __shfl_xor_sync(gmask, acc, o);
+      if (MODE == SEARCH_DIGEST) acc2 += __shfl_xor_sync(gmask, acc2, o);
+    }
+    const bool anyfail = __any_sync(gmask, failed);
+    if (gl == 0) {
+      if (MODE == SEARCH_COUNT) {
+        sc.counts[oj] = (uint32_t)acc;
+        if (acc > 0xffffffffull) atomicOr(sc.err, ERRB_CAPACITY);
+      } else {
+        sc.digests[oj] = acc;
+        sc.counts[oj] = (uint32_t)acc2;
+      }
+      if (anyfail) atomicOr(sc.err, ERRB_CAPACITY);
+    }
+    active = false;
+    failed = false;
+  };
+
+  for (;;) {
+    // groups without a box take boxes until one needs a traversal
+    while (!active && !exhausted) {
+      uint32_t qi = 0;
+      if (gl == 0) qi = atomicAdd(sc.qcounter, 1u);
+      qi = __shfl_sync(gmask, qi, 0, G);
+      if ((uint64_t)qi >= sc.boxes.q) {
+        exhausted = true;
+        break;
+      }
+      const uint32_t qj = sc.order ? sc.order[qi] : qi;
+      oj = qj;
+      g = sc.g;
+      tab = sc.tab;
+      const float* blo = sc.boxes.lo;
+      const float* bhi = sc.boxes.hi;
+      uint64_t bstride = sc.boxes.stride, bj = qj;
+      if (sc.evs) {
+        while (cur_ev + 1u < sc.nev && (uint64_t)qj >= sc.evs[cur_ev + 1u].qbase) ++cur_ev;
+        const EvDesc& ev = sc.evs[cur_ev];
+        g = ev.g;
+        tab.nodes = sc.tab.nodes + ev.base;
+        tab.ids = sc.tab.ids + ev.base;
+        tab.sdig = sc.tab.sdig ? sc.tab.sdig + ev.base : nullptr;
+        blo = sc.boxes.lo + ev.qcbase;
+        bhi = sc.boxes.hi + ev.qcbase;
+        bstride = ev.nq;
+        bj = qj - ev.qbase;
+        oj = ev.qout + bj;
+      }
+      uint32_t mask0 = 0u;
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) {
+        lo[c] = blo[(uint64_t)c * bstride + bj];
+        hi[c] = bhi[(uint64_t)c * bstride + bj];
+        if (lo[c] == -INFINITY) mask0 |= 1u << (2 * c);
+        if (hi[c] == INFINITY) mask0 |= 2u << (2 * c);
+      }
+      acc = 0ull;
+      acc2 = 0ull;
+      if (g.n == 0) {
+        finish();
+      } else if (mask0 == FULL) {
+        if (gl == 0) {
+          if (MODE == SEARCH_COUNT) {
+            acc = g.n;
+          } else {
+            acc = tab.sdig[0];
+            acc2 = g.n;
+          }
+        }
+        finish();
+      } else {
+        if (gl == 0) {
+          stk_node[0] = 0u;
+          stk_mask[0] = (uint8_t)mask0;
+        }
+        top = 1;
+        active = true;
+      }
+    }
+    if (!__any_sync(0xffffffffu, active)) break;
+    __syncwarp();
+
+    const int gcount = top < G ? top : G;
+    const int base = top - gcount;
+    const bool have = (int)gl < gcount;
+    uint32_t i = 0u, mask = 0u;
+    if (have) {
+      i = stk_node[base + gl];
+      mask = stk_mask[base + gl];
+    }
+    __syncwarp();
+    top = base;
+    bool pushL = false, pushR = false;
+    uint32_t maskL = 0u, maskR = 0u;
+    if (have) {
+      const uint32_t dep = floor_log2_u32(i + 1u);
+      const uint32_t c = dep % DIM;
+      const uint4 nd = __ldg(tab.nodes + i);
+      const float x0 = __uint_as_float(nd.x), x1 = __uint_as_float(nd.y), x2 = __uint_as_float(nd.z),
+                  x3 = __uint_as_float(nd.w);
+      const float v = sel4(c, x0, x1, x2, x3);
+      const float loc = sel4(c, lo[0], lo[1], lo[2], lo[3]);
+      const float hic = sel4(c, hi[0], hi[1], hi[2], hi[3]);
+      const bool inter = v <= hic && v >= loc;
+      const bool lower = v < loc;
+      bool emit = false;
+      if (inter) {
+        bool in = true;
+        if (DIM > 0) in &= (x0 <= hi[0] && x0 >= lo[0]);
+        if (DIM > 1) in &= (x1 <= hi[1] && x1 >= lo[1]);
+        if (DIM > 2) in &= (x2 <= hi[2] && x2 >= lo[2]);
+        if (DIM > 3) in &= (x3 <= hi[3] && x3 >= lo[3]);
+        emit = in;
+      }
+      const uint32_t l = 2u * i + 1u;
+      const bool visitL = !lower && l < g.n;
+      const bool visitR = (lower || inter) && l + 1u < g.n;
+      maskL = mask | (v <= hic ? (2u << (2 * c)) : 0u);
+      maskR = mask | (v >= loc ? (1u << (2 * c)) : 0u);
+      const bool contL = visitL && maskL == FULL;
+      const bool contR = visitR && maskR == FULL;
+      pushL = visitL && !contL;
+      pushR = visitR && !contR;
+      const uint32_t cnt = (emit ? 1u : 0u) + (contL ? subtree_size(g, l) : 0u) + (contR ? subtree_size(g, l + 1u) : 0u);
+      if (MODE == SEARCH_COUNT) {
+        acc += cnt;
+      } else {
+        acc2 += cnt;
+        if (emit) acc += mix64(DIM <= 3 ? nd.w : __ldg(tab.ids + i));
+        if (contL) acc += tab.sdig[l];
+        if (contR) acc += tab.sdig[l + 1u];
+      }
+    }
+    const uint32_t bpl = (__ballot_sync(0xffffffffu, pushL) >> gsh) & GM;
+    const uint32_t bpr = (__ballot_sync(0xffffffffu, pushR) >> gsh) & GM;
+    const uint32_t tot = __popc(bpl) + __popc(bpr);
+    if ((uint32_t)top + tot > cap) {
+      failed = true;  // group-uniform: abandon the box, report capacity
+      top = 0;
+    } else {
+      uint32_t p = (uint32_t)top + __popc(bpl & glt) + __popc(bpr & glt);
+      if (pushL) {
+        stk_node[p] = 2u * i + 1u;
+        stk_mask[p] = (uint8_t)maskL;
+        ++p;
+      }
+      if (pushR) {
+        stk_node[p] = 2u * i + 2u;
+        stk_mask[p] = (uint8_t)maskR;
+      }
+      top += (int)tot;
+    }
+    __syncwarp();
+    if (active && top == 0) finish();
+  }
+}
+
+template <int DIM, int MODE, int G>
+static cudaError_t run_search_grp(SearchCtx& sc) {
+  const uint32_t cap = stack_cap_lanes(sc.g, G);
+  const size_t smem = (size_t)(QT / G) * cap * 5u;
+  cudaError_t e = cudaFuncSetAttribute(k_search_grp<DIM, MODE, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_search_grp<DIM, MODE, G>, QT, smem);
+  if (e != cudaSuccess) return e;
+  if (per < 1) per = 1;
+  uint64_t blocks = (uint64_t)sms * per;
+  const uint64_t need = (sc.boxes.q + (QT / G) - 1) / (QT / G);
+  if (blocks > need) blocks = need ? need : 1;
+  e = cudaMemsetAsync(sc.qcounter, 0, sizeof(uint32_t), sc.stream);
+  if (e != cudaSuccess) return e;
+  k_search_grp<DIM, MODE, G><<<(unsigned)blocks, QT, smem, sc.stream>>>(sc, cap);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
 template <int DIM, int MODE>
 static cudaError_t run_search(SearchCtx& sc) {
   const uint32_t cap = stack_cap(sc.g);
@@ -376,8 +591,24 @@ static cudaError_t run_search(SearchCtx& sc) {
   return cudaGetLastError();
 }
 
+template <int DIM, int MODE>
+static cudaError_t run_search_lanes(SearchCtx& sc) {
+  switch (sc.lanes) {
+    case 1: return run_search_grp<DIM, MODE, 1>(sc);
+    case 2: return run_search_grp<DIM, MODE, 2>(sc);
+    case 4: return run_search_grp<DIM, MODE, 4>(sc);
+    case 8: return run_search_grp<DIM, MODE, 8>(sc);
+    case 16: return run_search_grp<DIM, MODE, 16>(sc);
+    default: return run_search<DIM, MODE>(sc);
+  }
+}
+
 template <int DIM>
 static cudaError_t run_search_mode(SearchCtx& sc, int mode) {
+  if (sc.lanes != 0 && sc.lanes != 32) {
+    if (mode == SEARCH_COUNT) return run_search_lanes<DIM, SEARCH_COUNT>(sc);
+    if (mode == SEARCH_DIGEST) return run_search_lanes<DIM, SEARCH_DIGEST>(sc);
+  }
   switch (mode) {
     case SEARCH_COUNT: return run_search<DIM, SEARCH_COUNT>(sc);
     case SEARCH_WRITE: return run_search<DIM, SEARCH_WRITE>(sc);

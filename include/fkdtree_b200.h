@@ -161,6 +161,11 @@ FKD_API fkd_status fkd_search_digest(fkd_tree h, const float* mins, const float*
  * earlier asynchronous calls. */
 FKD_API fkd_status fkd_sync(fkd_tree h);
 
+/* Tuning knobs of one tree, same names and ranges as fkd_batch_set_param
+ * ("hist_ctas" takes effect at the next build; "search_lanes" applies to
+ * fkd_search_count / fkd_search_digest).  No reference counterpart. */
+FKD_API fkd_status fkd_set_param(fkd_tree h, const char* name, int64_t value);
+
 /* ---------------------------------------------------------------- batches
  * Many independent events (one tree each) built and searched together.  No
  * reference counterpart: the reference constructs one FKDTree_CPU per event
@@ -179,8 +184,11 @@ typedef struct fkd_batch_s* fkd_batch;
 FKD_API fkd_status fkd_batch_create(uint32_t n_events, const uint32_t* dims, const uint64_t* pt_off,
                                     const uint64_t* q_off, uint32_t flags, void* stream, fkd_batch* out);
 FKD_API fkd_status fkd_batch_destroy(fkd_batch b);
-/* Tuning knob used by the autotuner: "hist_ctas" (digit-pass CTAs per level,
- * 0 = four per SM).  Re-plans the batch. */
+/* Tuning knobs used by the autotuner (fkdtree_b200/autotune.py):
+ *   "hist_ctas"    digit-pass CTAs per level (0 = four per SM); re-plans the batch
+ *   "search_lanes" lanes per box of the count / digest search: 1, 2, 4, 8, 16
+ *                  or 32 (0 = 32, one warp per box)
+ * No reference counterpart (the reference has one fixed launch shape). */
 FKD_API fkd_status fkd_batch_set_param(fkd_batch b, const char* name, int64_t value);
 /* Builds every event; the tables equal one FKDTree_CPU::build per event. */
 FKD_API fkd_status fkd_batch_build(fkd_batch b, const float* coords, const uint32_t* ids, int mem);

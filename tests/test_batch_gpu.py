@@ -20,11 +20,12 @@ def check_batch(wb, gpu_tab, gpu_tid, counts, digests):
     assert np.array_equal(np.asarray(digests).astype(np.uint64), od), "digests differ"
 
 
-@pytest.mark.parametrize("frac_4d", [0.0, 0.5])
-def test_batch_matches_per_event_oracle(cuda, frac_4d):
+@pytest.mark.parametrize("frac_4d,lanes", [(0.0, 0), (0.5, 0), (0.5, 1), (0.0, 2), (0.5, 4), (0.0, 8), (0.5, 16)])
+def test_batch_matches_per_event_oracle(cuda, frac_4d, lanes):
     wb = W.event_batch(n_events=64, median=6000, size_lo=1, size_hi=60_000, clusters_lo=5, clusters_hi=50,
                        half_width=0.01, seed=21, frac_4d=frac_4d)
     b = F.Batch.of(wb)
+    b.set_param("search_lanes", lanes)
     b.build(wb.coords, wb.ids)
     tab, tid = b.tables()
     c, d = b.search_digest(wb.mins, wb.maxs)
@@ -82,4 +83,29 @@ def test_batch_graph_run_device(cuda):
         dig.zero_()
         b.run(coords, ids, mins, maxs, counts, dig)
     tab, tid = b.tables()
+    check_batch(wb, tab, tid, counts.cpu().numpy().view(np.uint32), dig.cpu().numpy().view(np.uint64))
+
+
+def test_autotuned_batch_graph(cuda, tmp_path):
+    """The autotuner sweeps the knobs on the batch itself, caches the choice,
+    and the graph launched with the chosen knobs still gives exact results."""
+    import torch
+    wb = W.event_batch(n_events=96, median=8_000, size_lo=500, size_hi=60_000, clusters_lo=20, clusters_hi=200,
+                       half_width=0.01, seed=34, frac_4d=0.25)
+    b = F.Batch.of(wb)
+    dev = cuda
+    coords = torch.from_numpy(wb.coords).to(dev)
+    ids = torch.from_numpy(wb.ids.view(np.int32)).to(dev)
+    mins = torch.from_numpy(wb.mins).to(dev)
+    maxs = torch.from_numpy(wb.maxs).to(dev)
+    cache = str(tmp_path / "tune.json")
+    r = b.autotune(coords, ids, mins, maxs, cache_file=cache, reps=1, hist_ctas=[148, 592])
+    assert not r["cached"] and r["search_lanes"] in (1, 2, 4, 8, 16, 32) and r["hist_ctas"] in (148, 592)
+    b2 = F.Batch.of(wb)
+    r2 = b2.autotune(coords, ids, mins, maxs, cache_file=cache)
+    assert r2["cached"] and r2["search_lanes"] == r["search_lanes"]
+    counts = torch.empty(wb.n_queries, dtype=torch.int32, device=dev)
+    dig = torch.empty(wb.n_queries, dtype=torch.int64, device=dev)
+    b2.run(coords, ids, mins, maxs, counts, dig)
+    tab, tid = b2.tables()
     check_batch(wb, tab, tid, counts.cpu().numpy().view(np.uint32), dig.cpu().numpy().view(np.uint64))

@@ -136,3 +136,30 @@ def test_device_memory_search_and_capacity_error(cuda):
     with pytest.raises(F.FKDError) as e:
         t.search_boxes(ev.mins, ev.maxs, capacity=10)
     assert e.value.status == 6
+
+
+@pytest.mark.parametrize("lanes", [1, 2, 4, 8, 16])
+@pytest.mark.parametrize("dim", [1, 3, 4])
+def test_search_lanes_per_box(cuda, dim, lanes):
+    """Count and digest with several boxes per warp (search_lanes) equal the
+    brute-force scan, unbounded, empty and whole-tree boxes included."""
+    rng = np.random.default_rng(40 + dim)
+    n = 30_000
+    c = rng.random((dim, n), dtype=np.float32)
+    ids = rng.permutation(n).astype(np.uint32)
+    q = 2000
+    ctr = c[:, rng.integers(0, n, q)]
+    hw = rng.uniform(0.0, 0.15, (dim, q)).astype(np.float32)
+    mins, maxs = (ctr - hw).astype(np.float32), (ctr + hw).astype(np.float32)
+    mins[:, :10] = -np.inf
+    maxs[:, 5:15] = np.inf
+    mins[:, 20:25], maxs[:, 20:25] = maxs[:, 20:25].copy(), mins[:, 20:25].copy()
+    t = F.FKDTree(c, ids).build()
+    tab, tid = t.tables()
+    cb, ob, ib, _ = O.search(tab, tid, mins, maxs, variant=O.BRUTE)
+    t.set_param("search_lanes", lanes)
+    assert np.array_equal(t.count_boxes(mins, maxs), cb)
+    c2, d2 = t.digest_boxes(mins, maxs)
+    assert np.array_equal(c2, cb) and np.array_equal(d2, O.digest_of(ib, ob))
+    with pytest.raises(F.FKDError):
+        t.set_param("search_lanes", 3)
