@@ -60,19 +60,21 @@ def parse_args():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-queries", type=int, default=8192, help="box sample of the CPU baseline")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched / learned events report")
+    ap.add_argument("--queries", type=int, default=0,
+                    help="box count of the 16M-point workload (0: 1,048,576; smaller cases are for profiling)")
     ap.add_argument("--batched-events", type=int, default=4096)
     return ap.parse_args()
 
 
-def make_workload(name):
+def make_workload(name, queries=None):
     from fkdtree_b200 import workloads as W
     if name == "uniform100k":
         ev = W.uniform_event(n=100_000, half_width=0.01, seed=0)
         cfg = {"workload": "uniform3d_100k", "n_points": ev.n, "n_boxes": ev.q, "dim": 3,
                "points": "U[0,1)^3", "half_width": 0.01, "seed": 0}
     else:
-        ev = W.clustered_event()
-        cfg = {"workload": "clustered3d_16m_boxes1m", "n_points": ev.n, "n_boxes": ev.q, "dim": 3,
+        ev = W.clustered_event() if not queries else W.clustered_event(n_queries=queries)
+        cfg = {"workload": "clustered3d_16m_boxes1m" if not queries else f"clustered3d_16m_boxes{queries}", "n_points": ev.n, "n_boxes": ev.q, "dim": 3,
                "points": "80% of 4096 Gaussian clusters (sigma 0.002, Dirichlet(1)) + 20% U[0,1)^3",
                "half_width": "U[0.001,0.02] per dim", "seed": 1}
     cfg["l2"] = "inputs larger than L2 (no flush)" if ev.n * 16 > 126e6 else "inputs smaller than L2"
@@ -309,12 +311,14 @@ def run_ours(args):
         if world > 1:
             dist.barrier()
 
-    ev, cfg = make_workload(args.workload)
+    ev, cfg = make_workload(args.workload, args.queries)
     n, q, dim = ev.n, ev.q, ev.dim
     L = _capi.lib()
     stream = torch.cuda.current_stream(dev)
     h = C.c_void_p()
     _capi.check(L.fkd_create(dim, _capi.FLAG_ASYNC, C.c_void_p(stream.cuda_stream), C.byref(h)))
+    # CUDA events around the library's kernels (read back after the timed region)
+    _capi.check(L.fkd_set_param(h, b"kernel_events", 1))
     P = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
 
     coords = torch.from_numpy(ev.coords).to(dev)
@@ -364,6 +368,10 @@ def run_ours(args):
     launches = L.fkd_kernel_launches() - launches0
     _capi.check(L.fkd_sync(h))
     assert total.value == results
+    kt = np.zeros((min(args.steps, 63), 5), dtype=np.float32)
+    for b in range(kt.shape[0]):
+        _capi.check(L.fkd_kernel_times(h, b, kt[b].ctypes.data_as(C.c_void_p)))
+    kms = [float(x) for x in kt.mean(axis=0)]  # count, write, build, global levels, subtree
     ms = t0.elapsed_time(t1)
     build_ms = float(np.mean([ev_b0[i].elapsed_time(ev_b1[i]) for i in range(args.steps)]))
     search_ms = float(np.mean([ev_b1[i].elapsed_time(ev_s1[i]) for i in range(args.steps)]))
@@ -383,17 +391,34 @@ def run_ours(args):
         "search": {"ms": search_ms, "algorithmic_bytes": sb, "gbs": sb / search_ms / 1e6,
                    "kernels": ["k_box_keys", "k_box_scatter", "k_search<count>", "k_scan_*", "k_search<write>"]},
     }
-    dom = "build" if build_ms >= search_ms else "search"
-    roof = {"bound": "hbm", "phase": dom, "achieved": phases[dom]["gbs"], "peak": peak, "unit": "GB/s",
-            "frac": phases[dom]["gbs"] / peak, "peak_kind": peak_kind, "traffic": None,
-            "algorithmic_bytes_per_launch": phases[dom]["algorithmic_bytes"]}
+    # per kernel (CUDA events inside the library, same stream, every timed step)
+    kern = {
+        "k_search<write>": {"ms": float(kms[1]), "algorithmic_bytes": n * (4 * dim + 4) + q * (8 * dim + 8) + 4 * results,
+                            "bytes_rule": "tree once + boxes + offsets + 4 B per result id"},
+        "k_search<count>": {"ms": float(kms[0]), "algorithmic_bytes": n * (4 * dim + 4) + q * (8 * dim + 4),
+                            "bytes_rule": "tree once + boxes + one count per box"},
+        "build (k_hist + k_partition + k_subtree)": {"ms": float(kms[2]), "algorithmic_bytes": bb,
+                                                     "bytes_rule": "N*(4*dim+4)*(2*floor(log2 N)+1)"},
+        "global levels (k_sel_init + k_hist + k_partition)": {"ms": float(kms[3])},
+        "k_subtree": {"ms": float(kms[4])},
+    }
+    for v in kern.values():
+        if "algorithmic_bytes" in v and v["ms"] > 0:
+            v["gbs"] = v["algorithmic_bytes"] / v["ms"] / 1e6
+    dom = max(("k_search<write>", "k_search<count>", "build (k_hist + k_partition + k_subtree)"),
+              key=lambda k: kern[k]["ms"])
+    roof = {"bound": "hbm", "kernel": dom, "achieved": kern[dom]["gbs"], "peak": peak, "unit": "GB/s",
+            "frac": kern[dom]["gbs"] / peak, "peak_kind": f"{peak_kind} (copy bandwidth, MEASURED_PEAKS.json)",
+            "traffic": None, "algorithmic_bytes_per_launch": kern[dom]["algorithmic_bytes"],
+            "launch_ms": kern[dom]["ms"],
+            "build_frac": bb / kms[2] / 1e6 / peak if kms[2] > 0 else None}
 
     line = {"metric": METRIC, "value": value, "unit": "Mpoints/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator, fkdtree_b200/workloads.py)",
             "config": dict(cfg, parallelism=f"replicas{world}", results_per_step=results),
             "build_mpoints_per_s": n / build_ms / 1e3, "search_mboxes_per_s": q / search_ms / 1e3,
-            "phases": phases, "roofline": roof, "gpu_launches": int(launches)}
+            "phases": phases, "kernels": kern, "roofline": roof, "gpu_launches": int(launches)}
     line["clocks"] = clk.summary()
 
     if not args.no_e2e:
@@ -493,7 +518,7 @@ def run_reference(args):
     if not O.ref_available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libfkdref.so not built"}), flush=True)
         return
-    ev, cfg = make_workload(args.workload)
+    ev, cfg = make_workload(args.workload, args.queries)
     threads = O.host_threads()
     nq = min(args.cpu_queries, ev.q)
     # warm-up steps on a 1/16 sample of the points keep the run bounded

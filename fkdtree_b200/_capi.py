@@ -42,6 +42,7 @@ SIGNATURES = {
     "fkd_batch_destroy": ([_vp], _int),
     "fkd_batch_set_param": ([_vp, C.c_char_p, C.c_int64], _int),
     "fkd_set_param": ([_vp, C.c_char_p, C.c_int64], _int),
+    "fkd_kernel_times": ([_vp, C.c_uint32, _vp], _int),
     "fkd_batch_build": ([_vp, _vp, _vp, _int], _int),
     "fkd_batch_get_tables": ([_vp, _vp, _vp, _int], _int),
     "fkd_batch_search_digest": ([_vp, _vp, _vp, _vp, _vp, _int], _int),

@@ -899,6 +899,10 @@ static cudaError_t run_build(BuildCtx& bc) {
   const size_t smem = SubCfg<DIM>::smem;
   cudaError_t e = cudaFuncSetAttribute(k_subtree<DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
+  if (bc.ev_sub) {
+    e = cudaEventRecord(bc.ev_sub, bc.stream);
+    if (e != cudaSuccess) return e;
+  }
   if (bc.nsub) {
     k_subtree<DIM><<<bc.nsub, ST, smem, bc.stream>>>(bc.evs, bc.subs, bc.input, b0, b1, bc.tab, bc.err);
     count_launches(1);

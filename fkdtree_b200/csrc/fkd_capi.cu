@@ -5,6 +5,7 @@
 
 #include <new>
 #include <string>
+#include <vector>
 
 #include "../../include/fkdtree_b200.h"
 #include "fkd_internal.h"
@@ -80,16 +81,25 @@ struct fkd_tree_s {
   uint32_t search_lanes = 0; // count / digest lanes per box (0: one warp)
   fkd_mlp mlp = nullptr;     // learned split (null: plain radix select)
   float mlp_delta = 0.f;
-  DevBuf lfeat, lyhat, lrange, lstats, sdig;
+  DevBuf lfeat, lyhat, lrange, lstats, sdig, dids, dnode;
   bool sdig_valid = false;
+  bool inorder_valid = false;
+  // optional per-kernel timing (fkd_set_param "kernel_events"): a ring of
+  // KEV_RING event sets, one per build / search call
+  static constexpr uint32_t KEV_RING = 64;
+  std::vector<cudaEvent_t> kev;  // [slot * 7 + k]: 0 count start, 1 count end, 2 write start, 3 write end,
+                                 //                  4 build start, 5 subtree start, 6 build end
+  uint64_t kev_builds = 0, kev_searches = 0;
 
   ~fkd_tree_s() {
     DevBuf* all[] = {&nodes, &ids, &work0, &work1, &sel, &ghist, &err, &qctr, &passflags,
                      &qlo, &qhi, &counts, &offsets, &partials, &out, &tmp, &digests, &qorder,
-                     &lfeat, &lyhat, &lrange, &lstats, &sdig};
+                     &lfeat, &lyhat, &lrange, &lstats, &sdig, &dids, &dnode};
     for (DevBuf* b : all) b->release();
     if (herr) cudaFreeHost(herr);
+    for (cudaEvent_t e : kev) cudaEventDestroy(e);
   }
+  cudaEvent_t kev_at(uint64_t call, int k) { return kev[(size_t)(call % KEV_RING) * 7 + k]; }
 };
 
 namespace {
@@ -258,6 +268,7 @@ fkd_status fkd_build(fkd_tree h, const float* coords, const uint32_t* ids, uint6
   if (n && (!coords || !ids)) return fail(FKD_ERR_ARG, "null coords or ids");
   h->built = false;
   h->sdig_valid = false;
+  h->inorder_valid = false;
   h->n = n;
   if (n == 0) {
     h->built = true;
@@ -323,7 +334,16 @@ fkd_status fkd_build(fkd_tree h, const float* coords, const uint32_t* ids, uint6
     bc.learn.range = h->lrange.as<float2>();
     bc.learn.stats = h->lstats.as<unsigned long long>();
   }
+  const bool kt = !h->kev.empty();
+  if (kt) {
+    FKD_CUDA(cudaEventRecord(h->kev_at(h->kev_builds, 4), h->stream));
+    bc.ev_sub = h->kev_at(h->kev_builds, 5);
+  }
   FKD_CUDA(launch_build(bc, dim));
+  if (kt) {
+    FKD_CUDA(cudaEventRecord(h->kev_at(h->kev_builds, 6), h->stream));
+    ++h->kev_builds;
+  }
   h->built = true;
   fkd_status s = finish(h, "fkd_build", mem);
   if (s != FKD_OK) h->built = false;
@@ -382,9 +402,27 @@ fkd_status fkd_search_count(fkd_tree h, const float* mins, const float* maxs, ui
   return finish(h, "fkd_search_count", mem);
 }
 
+// In-order id / heap-index tables of the current tree (built once per tree,
+// before the first write pass).
+static fkd_status ensure_inorder(fkd_tree h) {
+  if (h->inorder_valid || h->n == 0) return FKD_OK;
+  FKD_CUDA(h->dids.ensure(h->n * sizeof(uint32_t)));
+  FKD_CUDA(h->dnode.ensure(h->n * sizeof(uint32_t)));
+  Table t = table_of(h);
+  t.dids = h->dids.as<uint32_t>();
+  t.dnode = h->dnode.as<uint32_t>();
+  FKD_CUDA(launch_inorder(make_geom((uint32_t)h->n), t, h->stream));
+  h->inorder_valid = true;
+  return FKD_OK;
+}
+
 static fkd_status write_pass(fkd_tree h, const Boxes& b, const uint64_t* doffsets, uint32_t* dout, uint64_t total,
                              int ordered, const uint32_t* order) {
+  fkd_status s0 = ensure_inorder(h);
+  if (s0 != FKD_OK) return s0;
   SearchCtx sc = search_ctx(h, b);
+  sc.tab.dids = h->dids.as<uint32_t>();
+  sc.tab.dnode = h->dnode.as<uint32_t>();
   sc.order = order;
   sc.offsets = doffsets;
   sc.out = dout;
@@ -449,7 +487,11 @@ fkd_status fkd_search(fkd_tree h, const float* mins, const float* maxs, uint64_t
   FKD_CUDA(cudaMemsetAsync(h->err.p, 0, sizeof(uint32_t), h->stream));
   const uint32_t* order = nullptr;
   if (q && (s = box_order(h, b, &order)) != FKD_OK) return s;
+  if ((s = ensure_inorder(h)) != FKD_OK) return s;
+  const bool kt = !h->kev.empty();
+  if (kt) FKD_CUDA(cudaEventRecord(h->kev_at(h->kev_searches, 0), h->stream));
   if (q && (s = count_pass(h, b, h->counts.as<uint32_t>(), order)) != FKD_OK) return s;
+  if (kt) FKD_CUDA(cudaEventRecord(h->kev_at(h->kev_searches, 1), h->stream));
   FKD_CUDA(launch_scan_counts(h->counts.as<uint32_t>(), q, doff, h->partials.as<unsigned long long>(), h->stream));
   FKD_CUDA(cudaMemcpyAsync(h->herr + 2, doff + q, sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
   FKD_CUDA(cudaStreamSynchronize(h->stream));
@@ -468,6 +510,11 @@ fkd_status fkd_search(fkd_tree h, const float* mins, const float* maxs, uint64_t
   }
   if (tot && !ids_out) return fail(FKD_ERR_ARG, "null ids_out");
   if (tot == 0) {
+    if (kt) {
+      FKD_CUDA(cudaEventRecord(h->kev_at(h->kev_searches, 2), h->stream));
+      FKD_CUDA(cudaEventRecord(h->kev_at(h->kev_searches, 3), h->stream));
+      ++h->kev_searches;
+    }
     FKD_CUDA(cudaStreamSynchronize(h->stream));
     return FKD_OK;
   }
@@ -476,7 +523,12 @@ fkd_status fkd_search(fkd_tree h, const float* mins, const float* maxs, uint64_t
     FKD_CUDA(h->out.ensure(tot * sizeof(uint32_t)));
     dout = h->out.as<uint32_t>();
   }
+  if (kt) FKD_CUDA(cudaEventRecord(h->kev_at(h->kev_searches, 2), h->stream));
   if ((s = write_pass(h, b, doff, dout, tot, ordered, order)) != FKD_OK) return s;
+  if (kt) {
+    FKD_CUDA(cudaEventRecord(h->kev_at(h->kev_searches, 3), h->stream));
+    ++h->kev_searches;
+  }
   if (mem == FKD_MEM_HOST)
     FKD_CUDA(cudaMemcpyAsync(ids_out, dout, tot * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
   return finish(h, "fkd_search", mem);
@@ -535,7 +587,50 @@ fkd_status fkd_set_param(fkd_tree h, const char* name, int64_t value) {
     h->search_lanes = (uint32_t)value;
     return FKD_OK;
   }
+  if (strcmp(name, "kernel_events") == 0) {
+    if (value != 0 && value != 1) return fail(FKD_ERR_ARG, "kernel_events must be 0 or 1");
+    FKD_CUDA(cudaStreamSynchronize(h->stream));
+    for (cudaEvent_t e : h->kev) cudaEventDestroy(e);
+    h->kev.clear();
+    h->kev_builds = h->kev_searches = 0;
+    if (value) {
+      FKD_CUDA(cudaSetDevice(h->device));
+      h->kev.resize((size_t)fkd_tree_s::KEV_RING * 7, nullptr);
+      for (cudaEvent_t& e : h->kev) {
+        cudaError_t ce = cudaEventCreate(&e);
+        if (ce != cudaSuccess) {
+          e = nullptr;
+          for (cudaEvent_t x : h->kev)
+            if (x) cudaEventDestroy(x);
+          h->kev.clear();
+          return fail(FKD_ERR_CUDA, std::string("kernel_events: ") + cudaGetErrorString(ce));
+        }
+      }
+    }
+    return FKD_OK;
+  }
   return fail(FKD_ERR_ARG, std::string("unknown parameter ") + name);
+}
+
+fkd_status fkd_kernel_times(fkd_tree h, uint32_t back, float* ms) {
+  if (!h || !ms) return fail(FKD_ERR_ARG, "null argument");
+  if (h->kev.empty()) return fail(FKD_ERR_STATE, "kernel_events is off");
+  float v[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+  if (back < fkd_tree_s::KEV_RING && back < h->kev_searches) {
+    const uint64_t c = h->kev_searches - 1 - back;
+    FKD_CUDA(cudaEventSynchronize(h->kev_at(c, 3)));
+    FKD_CUDA(cudaEventElapsedTime(&v[0], h->kev_at(c, 0), h->kev_at(c, 1)));
+    FKD_CUDA(cudaEventElapsedTime(&v[1], h->kev_at(c, 2), h->kev_at(c, 3)));
+  }
+  if (back < fkd_tree_s::KEV_RING && back < h->kev_builds) {
+    const uint64_t c = h->kev_builds - 1 - back;
+    FKD_CUDA(cudaEventSynchronize(h->kev_at(c, 6)));
+    FKD_CUDA(cudaEventElapsedTime(&v[2], h->kev_at(c, 4), h->kev_at(c, 6)));
+    FKD_CUDA(cudaEventElapsedTime(&v[3], h->kev_at(c, 4), h->kev_at(c, 5)));
+    FKD_CUDA(cudaEventElapsedTime(&v[4], h->kev_at(c, 5), h->kev_at(c, 6)));
+  }
+  memcpy(ms, v, sizeof v);
+  return FKD_OK;
 }
 
 fkd_status fkd_set_mlp(fkd_tree h, fkd_mlp m, float delta) {

@@ -119,6 +119,10 @@ struct Table {
   // optional: sdig[i] = sum of mix64(id) over the subtree of node i (mod 2^64),
   // filled by launch_subtree_digests before a digest search
   unsigned long long* sdig = nullptr;
+  // optional: ids / heap indices in in-order position (launch_inorder), for
+  // the write pass
+  uint32_t* dids = nullptr;
+  uint32_t* dnode = nullptr;
 };
 
 }  // namespace fkd

@@ -86,6 +86,7 @@ struct BuildCtx {
   uint32_t* err;
   cudaStream_t stream;
   LearnCtx learn;
+  cudaEvent_t ev_sub = nullptr;  // optional: recorded right before the subtree kernel
 };
 
 // Number of levels split by the global kernels (the first level whose
@@ -141,6 +142,8 @@ struct SearchCtx {
 };
 
 cudaError_t launch_search(SearchCtx& sc, int dim, int mode);
+// Fills tab.dids / tab.dnode (in-order tables); required by SEARCH_WRITE.
+cudaError_t launch_inorder(const Geom& g, Table tab, cudaStream_t stream);
 // Fills tab.sdig (subtree digests) for every event; required by SEARCH_DIGEST.
 cudaError_t launch_subtree_digests(const EvDesc* evs, uint32_t nev, uint32_t max_n, Table tab, cudaStream_t stream);
 // Sorts every box's result slice by heap index and maps it to ids.

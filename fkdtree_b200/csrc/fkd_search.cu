@@ -20,8 +20,9 @@
 // (the closed slab its ancestors' split values bound it by) already lie
 // inside the box.  A child whose mask is full is inside entirely: its
 // subtree is counted in closed form and, when ids are wanted, copied as one
-// contiguous run of the id table per level (in the heap layout the
-// descendants of node r at relative depth j are [(r+1)2^j - 1, (r+1)2^j - 1 + 2^j)).
+// contiguous run of the in-order id table (k_inorder): the subtree of node
+// (d, t) holds exactly the in-order positions [start(d,t), start(d,t) + len(d,t)),
+// the interval the build gave it.
 //
 // Two passes ("count then write"): SEARCH_COUNT fills counts, a prefix sum
 // turns them into offsets, SEARCH_WRITE writes every box's ids to its slice.
@@ -36,7 +37,7 @@ constexpr int QT = 128;  // threads per CTA
 constexpr int QW = QT / 32;
 constexpr int JOBS = 256;      // contained-subtree jobs buffered per warp
 constexpr int JFLUSH = JOBS - 64;  // one step adds at most 64
-constexpr int EU = 2;              // emission steps with loads in flight (measured best of 1, 2, 4, 8)
+constexpr int EU = 2;              // emission windows with loads in flight
 
 __device__ __forceinline__ uint32_t lanemask_lt_s() {
   uint32_t m;
@@ -59,8 +60,9 @@ __host__ __device__ inline uint32_t stack_cap(const Geom& g) { return 64u * (g.H
 template <int DIM, int MODE>
 __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ uint32_t jobs[QW][JOBS];
-  __shared__ uint32_t jsort[QW][JOBS];
+  __shared__ uint32_t jst[QW][JOBS];   // write pass: in-order start of each buffered subtree
+  __shared__ uint32_t jlen[QW][JOBS];  // its size
+  __shared__ uint32_t jpre[QW][JOBS];  // exclusive prefix of the sizes
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   uint32_t* stk_node = (uint32_t*)smem_raw + (size_t)warp * cap;
   uint8_t* stk_mask = (uint8_t*)((uint32_t*)smem_raw + (size_t)QW * cap) + (size_t)warp * cap;
@@ -130,86 +132,67 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
       cursor += __popc(bv);
     };
 
-    // Emits the whole subtrees buffered in jobs[warp][0..nj).  The jobs are
-    // first sorted by height (1, 3, 7, 15 nodes, taller) so that the short
-    // runs of the small subtrees are packed 32 nodes per warp step with no
-    // empty slots; the levels of taller subtrees are runs of >= 32 (below
-    // their fifth level) copied warp-wide.
+    // Emits the whole subtrees buffered in the job list: job k is the run
+    // [jst[k], jst[k] + jlen[k]) of the in-order table (tab.dids, or tab.dnode
+    // for heap indices), where every subtree is one contiguous range.  The
+    // runs are concatenated at the cursor; each lane step writes 32
+    // consecutive output slots, a lane finds its job from the bitmask of the
+    // jobs that start inside the window (EU windows with loads in flight).
     auto run_jobs = [&](uint32_t nj) {
-      uint32_t cnt[5] = {0u, 0u, 0u, 0u, 0u};
+      uint32_t carry = 0u;
       for (uint32_t e0 = 0; e0 < nj; e0 += 32u) {
         const uint32_t e = e0 + lane;
-        const uint32_t h = e < nj ? g.H - floor_log2_u32(jobs[warp][e] + 1u) : 99u;
+        const uint32_t len = e < nj ? jlen[warp][e] : 0u;
+        uint32_t incl = len;
 #pragma unroll
-        for (uint32_t c = 0; c < 5; ++c) cnt[c] += __popc(__ballot_sync(0xffffffffu, c < 4 ? h == c : (h >= 4u && h != 99u)));
-      }
-      uint32_t off[5];
-      off[0] = 0u;
-#pragma unroll
-      for (uint32_t c = 1; c < 5; ++c) off[c] = off[c - 1] + cnt[c - 1];
-      uint32_t fill[5] = {off[0], off[1], off[2], off[3], off[4]};
-      for (uint32_t e0 = 0; e0 < nj; e0 += 32u) {
-        const uint32_t e = e0 + lane;
-        const uint32_t r = e < nj ? jobs[warp][e] : 0u;
-        const uint32_t h = e < nj ? g.H - floor_log2_u32(r + 1u) : 99u;
-#pragma unroll
-        for (uint32_t c = 0; c < 5; ++c) {
-          const bool mine = c < 4 ? h == c : (h >= 4u && h != 99u);
-          const uint32_t b = __ballot_sync(0xffffffffu, mine);
-          if (mine) jsort[warp][fill[c] + __popc(b & lt)] = r;
-          fill[c] += __popc(b);
+        for (int o = 1; o < 32; o <<= 1) {
+          const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= (uint32_t)o) incl += y;
         }
+        if (e < nj) jpre[warp][e] = carry + incl - len;
+        carry += __shfl_sync(0xffffffffu, incl, 31);
       }
       __syncwarp();
-      // classes 0-3: whole subtrees; class 4: the top five levels (31 nodes)
-      // of each taller subtree -- all packed 32 slots per lane step, EU steps
-      // of loads in flight before their stores
+      const uint32_t total = carry;
+      const uint32_t* srct = sc.heap_out ? tab.dnode : tab.dids;
+      uint32_t jb = 0u;  // the job holding output slot o0 (warp-uniform)
+      for (uint32_t o0 = 0; o0 < total; o0 += 32u * EU) {
+        uint32_t src[EU];
+        bool ok[EU];
 #pragma unroll
-      for (uint32_t c = 0; c < 5; ++c) {
-        const uint32_t per = (2u << c) - 1u;
-        const uint32_t total = cnt[c] * per;
-        for (uint32_t e0 = 0; e0 < total; e0 += 32u * EU) {
-          uint64_t node[EU];
-          uint32_t id[EU];
-#pragma unroll
-          for (int u = 0; u < EU; ++u) {
-            const uint32_t e = e0 + 32u * u + lane;
-            node[u] = ~0ull;
-            if (e < total) {
-              const uint32_t jb = e / per, k = e - jb * per;
-              const uint32_t rl = floor_log2_u32(k + 1u);
-              const uint32_t r = jsort[warp][off[c] + jb];
-              node[u] = (((uint64_t)r + 1u) << rl) - 1u + (k + 1u - (1u << rl));
-            }
-          }
-#pragma unroll
-          for (int u = 0; u < EU; ++u) id[u] = node[u] < n ? __ldg(tab.ids + node[u]) : 0u;
-#pragma unroll
-          for (int u = 0; u < EU; ++u) emit_ballot(node[u] < n, (uint32_t)node[u], id[u]);
+        for (int u = 0; u < EU; ++u) {
+          const uint32_t w0 = o0 + 32u * u;
+          const uint32_t k = jb + lane;
+          const bool kv = k < nj;
+          const uint32_t pk = kv ? jpre[warp][k] : total;
+          const uint32_t sk = kv ? jst[warp][k] : 0u;
+          // jobs after jb start after w0 (every job holds at least one id)
+          const uint32_t B = __reduce_or_sync(0xffffffffu, (lane > 0u && kv && pk < w0 + 32u) ? (1u << (pk - w0)) : 0u);
+          const uint32_t jl = __popc(B & (0xffffffffu >> (31u - lane)));
+          const uint32_t mp = __shfl_sync(0xffffffffu, pk, jl);
+          const uint32_t ms = __shfl_sync(0xffffffffu, sk, jl);
+          ok[u] = w0 + lane < total;
+          src[u] = ms + (w0 + lane - mp);
+          // the job holding w0 + 32: the one holding w0 + 31, or the next if it starts there
+          uint32_t nb = jb + __popc(B);
+          if (nb + 1u < nj && jpre[warp][nb + 1u] == w0 + 32u) ++nb;
+          jb = nb;
         }
-      }
-      // levels >= 5 of the tall subtrees: runs of >= 32 consecutive slots
-      for (uint32_t jb = 0; jb < cnt[4]; ++jb) {
-        const uint32_t r = jsort[warp][off[4] + jb];
-        for (uint32_t j = 5;; ++j) {
-          const uint64_t a = (((uint64_t)r + 1u) << j) - 1u;
-          if (a >= n) break;
-          const uint64_t b = (a + (1ull << j)) < (uint64_t)n ? (a + (1ull << j)) : (uint64_t)n;
-          for (uint64_t x0 = a; x0 < b; x0 += 32u * EU) {
-            uint32_t id[EU];
+        uint32_t v[EU];
 #pragma unroll
-            for (int u = 0; u < EU; ++u) {
-              const uint64_t x = x0 + 32u * u + lane;
-              id[u] = x < b ? __ldg(tab.ids + x) : 0u;
-            }
+        for (int u = 0; u < EU; ++u) v[u] = ok[u] ? __ldg(srct + src[u]) : 0u;
 #pragma unroll
-            for (int u = 0; u < EU; ++u) {
-              const uint64_t x = x0 + 32u * u + lane;
-              emit_ballot(x < b, (uint32_t)x, id[u]);
-            }
+        for (int u = 0; u < EU; ++u) {
+          if (ok[u]) {
+            const uint64_t pos = cursor + o0 + 32u * u + lane;
+            if (pos < cend && pos < sc.capacity)
+              sc.out[pos] = v[u];
+            else
+              failed = true;
           }
         }
       }
+      cursor += total;
       __syncwarp();
     };
 
@@ -224,7 +207,10 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
             acc += tab.sdig[0];
           }
         } else {
-          if (lane == 0) jobs[warp][0] = 0u;
+          if (lane == 0) {
+            jst[warp][0] = 0u;
+            jlen[warp][0] = n;
+          }
           njobs = 1;
           __syncwarp();
         }
@@ -299,8 +285,20 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
         if (MODE == SEARCH_WRITE) {
         const uint32_t bl = __ballot_sync(0xffffffffu, contL), br = __ballot_sync(0xffffffffu, contR);
         const uint32_t jp = njobs + __popc(bl & lt) + __popc(br & lt);
-        if (contL) jobs[warp][jp] = 2u * i + 1u;
-        if (contR) jobs[warp][jp + (contL ? 1u : 0u)] = 2u * i + 2u;
+        if (contL || contR) {
+          // the children of node (dep, t) are (dep + 1, 2t) and (dep + 1, 2t + 1)
+          const uint32_t dc = floor_log2_u32(i + 1u) + 1u;
+          const uint32_t tl = 2u * (i + 1u - (1u << (dc - 1u)));
+          if (contL) {
+            jst[warp][jp] = seg_start(g, dc, tl);
+            jlen[warp][jp] = seg_len(g, dc, tl);
+          }
+          if (contR) {
+            const uint32_t q2 = jp + (contL ? 1u : 0u);
+            jst[warp][q2] = seg_start(g, dc, tl + 1u);
+            jlen[warp][q2] = seg_len(g, dc, tl + 1u);
+          }
+        }
         njobs += __popc(bl) + __popc(br);
         if (njobs > (uint32_t)JFLUSH) {
           __syncwarp();
@@ -625,6 +623,38 @@ cudaError_t launch_search(SearchCtx& sc, int dim, int mode) {
     case 4: return run_search_mode<4>(sc, mode);
     default: return cudaErrorInvalidValue;
   }
+}
+
+// ----------------------------------------------------------- in-order table
+//
+// Node (d, t) owns the interval [start(d,t), start(d,t) + len(d,t)) of the
+// build's working order and sits at start + rank(d,t) inside it (its left
+// subtree before it, its right subtree after it): the in-order position.
+// dids / dnode list the ids / heap indices in that order, so every subtree
+// is one contiguous range of them.
+
+__global__ void k_inorder(Geom g, const uint32_t* __restrict__ ids, uint32_t* __restrict__ dids,
+                          uint32_t* __restrict__ dnode) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x) {
+    const uint32_t d = floor_log2_u32(i + 1u);
+    const uint32_t t = i + 1u - (1u << d);
+    const uint32_t p = seg_start(g, d, t) + (d < g.H ? seg_rank(g, d, t) : 0u);
+    dids[p] = ids[i];
+    dnode[p] = i;
+  }
+}
+
+cudaError_t launch_inorder(const Geom& g, Table tab, cudaStream_t stream) {
+  if (g.n == 0) return cudaSuccess;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  uint32_t blocks = (g.n + 255u) / 256u;
+  const uint32_t cap = (uint32_t)sms * 8u;
+  if (blocks > cap) blocks = cap;
+  k_inorder<<<blocks, 256, 0, stream>>>(g, tab.ids, tab.dids, tab.dnode);
+  count_launches(1);
+  return cudaGetLastError();
 }
 
 // ---------------------------------------------------------- subtree digests

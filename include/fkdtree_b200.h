@@ -163,8 +163,16 @@ FKD_API fkd_status fkd_sync(fkd_tree h);
 
 /* Tuning knobs of one tree, same names and ranges as fkd_batch_set_param
  * ("hist_ctas" takes effect at the next build; "search_lanes" applies to
- * fkd_search_count / fkd_search_digest).  No reference counterpart. */
+ * fkd_search_count / fkd_search_digest), plus "kernel_events" (0/1): record
+ * CUDA events around the kernels of every fkd_build and fkd_search call for
+ * fkd_kernel_times.  No reference counterpart. */
 FKD_API fkd_status fkd_set_param(fkd_tree h, const char* name, int64_t value);
+/* Device times (ms) of the kernels of the build / search `back` calls ago
+ * (0 = the last; at most 63), measured by CUDA events on the handle's stream:
+ * ms[0] count pass, ms[1] write pass (fkd_search), ms[2] whole build,
+ * ms[3] global levels, ms[4] shared-memory subtree kernel (fkd_build).
+ * Requires "kernel_events" = 1.  No reference counterpart. */
+FKD_API fkd_status fkd_kernel_times(fkd_tree h, uint32_t back, float* ms);
 
 /* ---------------------------------------------------------------- batches
  * Many independent events (one tree each) built and searched together.  No
