@@ -113,7 +113,7 @@ struct Part {
   uint64_t npts = 0, nq = 0;
   uint32_t maxn = 0;  // largest event (sizes the search stack)
   PlanDev plan;
-  Buf io, chunks, work0, work1, nodes, ids, sel, ghist, lfeat, lyhat, lrange, sdig;
+  Buf io, chunks, work0, work1, nodes, ids, sel, ghist, lfeat, lyhat, lrange, sdig, bnd;
   uint32_t nchunks = 0;
 };
 
@@ -204,6 +204,7 @@ fkd_status batch_plan(fkd_batch b) {
     BCUDA(p.nodes.ensure(p.npts * sizeof(uint4)));
     BCUDA(p.ids.ensure(p.npts * 4));
     BCUDA(p.sel.ensure(sizeof(SegSel) * (size_t)p.plan.maxseg));
+    BCUDA(p.bnd.ensure(2 * sizeof(uint2) * (size_t)p.plan.maxseg));
     BCUDA(p.ghist.ensure((size_t)p.plan.maxseg * HIST_BINS * 4));
     BCUDA(p.sdig.ensure(p.npts * sizeof(unsigned long long)));
     BCUDA(p.lfeat.ensure((size_t)p.plan.maxseg * FKD_MLP_FEATURES * 4));
@@ -253,6 +254,8 @@ fkd_status enqueue_build(fkd_batch b, const float* coords, const uint32_t* ids) 
     bc.tab = Table{p.nodes.as<uint4>(), p.ids.as<uint32_t>()};
     bc.err = b->err.as<uint32_t>();
     bc.pending = b->passflags.as<uint32_t>();
+    bc.bnd = p.bnd.as<uint2>();
+    bc.bnd_stride = p.plan.maxseg;
     bc.stream = b->stream;
     memset(&bc.learn, 0, sizeof bc.learn);
     if (b->mlp || b->rec_x) {

@@ -44,9 +44,12 @@ extern "C" __attribute__((visibility("default"))) void fkd_prof_reset() {
 #define PROF_T(v) const unsigned long long v = clock64()
 #define PROF_ADD(slot, a, b) \
   if (threadIdx.x == 0) atomicAdd(&g_prof[slot], (b) - (a))
+#define PROF_CNT(slot) \
+  if (threadIdx.x == 0) atomicAdd(&g_prof[slot], 1ull)
 #else
 #define PROF_T(v)
 #define PROF_ADD(slot, a, b)
+#define PROF_CNT(slot)
 #endif
 
 // ---------------------------------------------------------------- global
@@ -77,7 +80,8 @@ __device__ __forceinline__ void write_node(const Table& tab, uint32_t h, const u
 }
 
 __global__ void k_sel_init(uint32_t d, const EvDesc* __restrict__ evs, const uint2* __restrict__ segs, uint32_t nseg,
-                           SegSel* __restrict__ sel, uint32_t* __restrict__ pending) {
+                           SegSel* __restrict__ sel, uint32_t* __restrict__ pending, const uint2* __restrict__ bnd_in,
+                           uint2* __restrict__ bnd_out, const uint32_t* __restrict__ child) {
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s == 0) {
     // pending[p] != 0: digit pass p has a segment to work on
@@ -91,6 +95,18 @@ __global__ void k_sel_init(uint32_t d, const EvDesc* __restrict__ evs, const uin
   SegSel st;
   st.prefix = 0ull;
   st.bits = 0u;
+  if (bnd_in) {
+    // every key of the segment shares the common prefix of its smallest and
+    // largest split coordinate: the select starts below it
+    const uint2 b = bnd_in[s];
+    if (b.x <= b.y) {
+      const uint32_t cp = b.x == b.y ? 32u : (uint32_t)__clz(b.x ^ b.y);
+      st.bits = cp;
+      st.prefix = cp == 0u ? 0ull : (unsigned long long)(b.x >> (32u - cp));
+    }
+  }
+  st.bits0 = st.bits;
+  st.prefix0 = st.prefix;
   st.krem = (d < g.H) ? seg_rank(g, d, sd.y) : 0u;
   st.cnt = len;
   st.done = len <= 1u ? 1u : 0u;
@@ -99,8 +115,11 @@ __global__ void k_sel_init(uint32_t d, const EvDesc* __restrict__ evs, const uin
   st.verify = 0u;
   st.below = 0u;
   st.kfull = st.krem;
-  st.pad = 0u;
   sel[s] = st;
+  if (bnd_out && child[s] != ~0u) {
+    bnd_out[child[s]] = make_uint2(0xffffffffu, 0u);
+    bnd_out[child[s] + 1u] = make_uint2(0xffffffffu, 0u);
+  }
 }
 
 // One digit pass of the segmented select for every segment of depth d.  CTA
@@ -244,8 +263,8 @@ __global__ void __launch_bounds__(GT, 4) k_hist(uint32_t d, const EvDesc* __rest
       for (uint32_t b = threadIdx.x; b < nb; b += GT) gh[b] = 0u;
       if (threadIdx.x == 0) {
         SegSel* p = &sel[s];
-        p->prefix = 0ull;
-        p->bits = 0u;
+        p->prefix = p->prefix0;
+        p->bits = p->bits0;
         p->krem = p->kfull;
         p->cnt = len;
         p->verify = 0u;
@@ -293,7 +312,8 @@ template <int DIM>
 __global__ void __launch_bounds__(GT, 4) k_partition(uint32_t d, const EvDesc* __restrict__ evs,
                                                      const uint2* __restrict__ segs, const uint2* __restrict__ tiles,
                                                      CSoA src, SoA dst, SegSel* __restrict__ sel, Table tab,
-                                                     uint32_t* __restrict__ err) {
+                                                     uint32_t* __restrict__ err, uint2* __restrict__ bnd_out,
+                                                     const uint32_t* __restrict__ child) {
   __shared__ uint32_t sL[PIPT * GWARPS], sR[PIPT * GWARPS];
   __shared__ uint32_t s_base[2];
   const uint2 tl = tiles[blockIdx.x];
@@ -389,6 +409,10 @@ __global__ void __launch_bounds__(GT, 4) k_partition(uint32_t d, const EvDesc* _
   __syncthreads();
   const uint32_t lt = lanemask_lt();
   const uint32_t endL = start + rank, endR = start + len;
+  // bounds of the children's split coordinate (the next level's select starts below their common prefix)
+  const uint32_t cnext = (d + 1u) % DIM;
+  const uint32_t ch = bnd_out ? child[s] : ~0u;
+  uint32_t mnL = 0xffffffffu, mxL = 0u, mnR = 0xffffffffu, mxR = 0u;
   const uint32_t baseL = start + s_base[0], baseR = endL + 1u + s_base[1];
 #pragma unroll
   for (int k = 0; k < PIPT; ++k) {
@@ -418,8 +442,48 @@ __global__ void __launch_bounds__(GT, 4) k_partition(uint32_t d, const EvDesc* _
 #pragma unroll
         for (int w = 0; w < DIM; ++w) __stcs(dst.base + (uint64_t)w * dst.stride + pos, rec[k][w]);
         __stcs(dst.ids + pos, rec[k][DIM]);
+        const uint32_t mv = mono_bits(pick_coord<DIM>(rec[k], cnext));
+        if (lim == endL) {
+          mnL = min(mnL, mv);
+          mxL = max(mxL, mv);
+        } else {
+          mnR = min(mnR, mv);
+          mxR = max(mxR, mv);
+        }
       } else {
         atomicOr(err, ERRB_INTERNAL);
+      }
+    }
+  }
+  if (ch != ~0u) {  // CTA-uniform
+    // warp, then CTA reduction; one global atomic per bound per CTA
+    mnL = __reduce_min_sync(0xffffffffu, mnL);
+    mxL = __reduce_max_sync(0xffffffffu, mxL);
+    mnR = __reduce_min_sync(0xffffffffu, mnR);
+    mxR = __reduce_max_sync(0xffffffffu, mxR);
+    __shared__ uint32_t sb[4];
+    if (threadIdx.x == 0) {
+      sb[0] = 0xffffffffu;
+      sb[1] = 0u;
+      sb[2] = 0xffffffffu;
+      sb[3] = 0u;
+    }
+    __syncthreads();
+    if (lane == 0u) {
+      atomicMin(&sb[0], mnL);
+      atomicMax(&sb[1], mxL);
+      atomicMin(&sb[2], mnR);
+      atomicMax(&sb[3], mxR);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      if (sb[0] <= sb[1]) {
+        atomicMin(&bnd_out[ch].x, sb[0]);
+        atomicMax(&bnd_out[ch].y, sb[1]);
+      }
+      if (sb[2] <= sb[3]) {
+        atomicMin(&bnd_out[ch + 1u].x, sb[2]);
+        atomicMax(&bnd_out[ch + 1u].y, sb[3]);
       }
     }
   }
@@ -587,6 +651,7 @@ __global__ void __launch_bounds__(ST, 1) k_subtree(const EvDesc* __restrict__ ev
       return;
     }
     PROF_T(tq0);
+    PROF_CNT(6);
     // the level's keys, cached in registers (positions p = tid + ST*k)
     uint32_t kv[PPT], ki[PPT], ku[PPT];
 #pragma unroll
@@ -650,6 +715,7 @@ __global__ void __launch_bounds__(ST, 1) k_subtree(const EvDesc* __restrict__ ev
       bool active = false;
       for (uint32_t u = threadIdx.x; u < nseg; u += ST) active |= (scnt[u] > 1u && sbits[u] < 64u);
       if (!__syncthreads_or(active)) break;
+      PROF_CNT(5);
       for (uint32_t i = threadIdx.x; i < (nseg << hb) / 2u; i += ST) work[i] = 0u;
       __syncthreads();
 #pragma unroll
@@ -863,7 +929,12 @@ static cudaError_t run_build(BuildCtx& bc) {
   for (uint32_t d = 0; d < bc.nlevels; ++d) {
     const LevelPlan& lp = bc.levels[d];
     if (lp.nseg == 0) continue;
-    k_sel_init<<<(lp.nseg + 255) / 256, 256, 0, bc.stream>>>(d, bc.evs, lp.segs, lp.nseg, bc.sel, bc.pending);
+    // per-segment bounds: written by level d - 1's partition into bnd[d & 1],
+    // by level d's partition into bnd[(d + 1) & 1]
+    const uint2* bnd_in = (bc.bnd && d > 0) ? bc.bnd + (size_t)(d & 1u) * bc.bnd_stride : nullptr;
+    uint2* bnd_out = bc.bnd ? bc.bnd + (size_t)((d + 1u) & 1u) * bc.bnd_stride : nullptr;
+    k_sel_init<<<(lp.nseg + 255) / 256, 256, 0, bc.stream>>>(d, bc.evs, lp.segs, lp.nseg, bc.sel, bc.pending, bnd_in,
+                                                            bnd_out, lp.child);
     count_launches(1);
     const LearnCtx& lc = bc.learn;
     if (lc.params || lc.rec_x) {
@@ -886,7 +957,7 @@ static cudaError_t run_build(BuildCtx& bc) {
     }
     SoA dst = bufs[nb];
     k_partition<DIM><<<lp.nptile, GT, 0, bc.stream>>>(d, bc.evs, lp.segs, lp.ptiles, src, dst, bc.sel, bc.tab,
-                                                        bc.err);
+                                                        bc.err, bnd_out, lp.child);
     count_launches(1);
     if (lc.rec_x) {
       cudaError_t e = launch_record(d, bc.evs, lp.segs, lp.nseg, DIM, bc.tab, lc.feat, lc.range, lc.rec_x, lc.rec_t,

@@ -3,6 +3,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <new>
 #include <string>
 #include <vector>
@@ -81,7 +82,9 @@ struct fkd_tree_s {
   uint32_t search_lanes = 0; // count / digest lanes per box (0: one warp)
   fkd_mlp mlp = nullptr;     // learned split (null: plain radix select)
   float mlp_delta = 0.f;
-  DevBuf lfeat, lyhat, lrange, lstats, sdig, dids, dnode;
+  DevBuf lfeat, lyhat, lrange, lstats, sdig, dids, dnode, bnd, pool_st, pool_len, pool_s, brec, jctr, rflags;
+  // run pool of fkd_search, sized by the previous call's demand
+  uint64_t pool_want = 0, pool_s_want = 0, brec_want = 0;
   bool sdig_valid = false;
   bool inorder_valid = false;
   // optional per-kernel timing (fkd_set_param "kernel_events"): a ring of
@@ -94,7 +97,8 @@ struct fkd_tree_s {
   ~fkd_tree_s() {
     DevBuf* all[] = {&nodes, &ids, &work0, &work1, &sel, &ghist, &err, &qctr, &passflags,
                      &qlo, &qhi, &counts, &offsets, &partials, &out, &tmp, &digests, &qorder,
-                     &lfeat, &lyhat, &lrange, &lstats, &sdig, &dids, &dnode};
+                     &lfeat, &lyhat, &lrange, &lstats, &sdig, &dids, &dnode, &bnd, &pool_st, &pool_len, &pool_s,
+                     &brec, &jctr, &rflags};
     for (DevBuf* b : all) b->release();
     if (herr) cudaFreeHost(herr);
     for (cudaEvent_t e : kev) cudaEventDestroy(e);
@@ -199,10 +203,25 @@ fkd_status box_order(fkd_tree h, const Boxes& b, const uint32_t** order) {
 }
 
 // count pass into dcounts (device)
-fkd_status count_pass(fkd_tree h, const Boxes& b, uint32_t* dcounts, const uint32_t* order) {
+// rec (optional): the run pool fields of a recording count pass
+fkd_status count_pass(fkd_tree h, const Boxes& b, uint32_t* dcounts, const uint32_t* order,
+                      const SearchCtx* rec = nullptr) {
   SearchCtx sc = search_ctx(h, b);
   sc.counts = dcounts;
   sc.order = order;
+  if (rec) {
+    sc.pool_st = rec->pool_st;
+    sc.pool_len = rec->pool_len;
+    sc.pool_s = rec->pool_s;
+    sc.pool_ctr = rec->pool_ctr;
+    sc.pool_cap = rec->pool_cap;
+    sc.pool_cap_s = rec->pool_cap_s;
+    sc.brec = rec->brec;
+    sc.brec_ctr = rec->brec_ctr;
+    sc.brec_cap = rec->brec_cap;
+    sc.flags = rec->flags;
+    sc.flag_ctr = rec->flag_ctr;
+  }
   FKD_CUDA(launch_search(sc, h->dim, SEARCH_COUNT));
   return FKD_OK;
 }
@@ -235,7 +254,7 @@ fkd_status fkd_create(int dim, uint32_t flags, void* stream, fkd_tree* out) {
   if (e == cudaSuccess) e = h->err.ensure(sizeof(uint32_t) * 4);
   if (e == cudaSuccess) e = h->qctr.ensure(sizeof(uint32_t) * 4);
   if (e == cudaSuccess) e = h->passflags.ensure(sizeof(uint32_t) * 64);
-  if (e == cudaSuccess) e = cudaMallocHost((void**)&h->herr, sizeof(uint32_t) * 4);
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&h->herr, sizeof(uint32_t) * 16);
   if (e == cudaSuccess) e = cudaMemsetAsync(h->err.p, 0, sizeof(uint32_t), h->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess) {
@@ -291,6 +310,7 @@ fkd_status fkd_build(fkd_tree h, const float* coords, const uint32_t* ids, uint6
   if (!h->plan.levels.empty()) {
     FKD_CUDA(h->work0.ensure(rec_bytes));
     FKD_CUDA(h->sel.ensure(sizeof(SegSel) * (size_t)h->plan.maxseg));
+    FKD_CUDA(h->bnd.ensure(2 * sizeof(uint2) * (size_t)h->plan.maxseg));
     const size_t gw = (size_t)h->plan.maxseg * HIST_BINS;
     FKD_CUDA(h->ghist.ensure(gw * sizeof(uint32_t)));
     FKD_CUDA(cudaMemsetAsync(h->ghist.p, 0, gw * sizeof(uint32_t), h->stream));
@@ -319,6 +339,8 @@ fkd_status fkd_build(fkd_tree h, const float* coords, const uint32_t* ids, uint6
   bc.tab = table_of(h);
   bc.err = h->err.as<uint32_t>();
   bc.pending = h->passflags.as<uint32_t>();
+  bc.bnd = h->plan.levels.empty() ? nullptr : h->bnd.as<uint2>();
+  bc.bnd_stride = h->plan.maxseg;
   bc.stream = h->stream;
   memset(&bc.learn, 0, sizeof bc.learn);
   if (h->mlp && !h->plan.levels.empty()) {
@@ -416,8 +438,11 @@ static fkd_status ensure_inorder(fkd_tree h) {
   return FKD_OK;
 }
 
+// rec: the run pool the count pass filled (null: traverse every box); with
+// it, k_expand writes the recorded runs and the traversal only revisits the
+// nflag boxes whose runs did not fit.
 static fkd_status write_pass(fkd_tree h, const Boxes& b, const uint64_t* doffsets, uint32_t* dout, uint64_t total,
-                             int ordered, const uint32_t* order) {
+                             int ordered, const uint32_t* order, const SearchCtx* rec = nullptr, uint32_t nflag = 0) {
   fkd_status s0 = ensure_inorder(h);
   if (s0 != FKD_OK) return s0;
   SearchCtx sc = search_ctx(h, b);
@@ -428,7 +453,19 @@ static fkd_status write_pass(fkd_tree h, const Boxes& b, const uint64_t* doffset
   sc.out = dout;
   sc.capacity = total;
   sc.heap_out = ordered ? 1 : 0;
-  FKD_CUDA(launch_search(sc, h->dim, SEARCH_WRITE));
+  if (rec) {
+    SearchCtx x = sc;
+    x.pool_st = rec->pool_st;
+    x.pool_len = rec->pool_len;
+    x.pool_s = rec->pool_s;
+    x.brec = rec->brec;
+    x.brec_ctr = rec->brec_ctr;
+    x.brec_cap = rec->brec_cap;
+    FKD_CUDA(launch_expand(x));
+    sc.order = rec->flags;
+    sc.boxes.q = nflag;
+  }
+  if (sc.boxes.q) FKD_CUDA(launch_search(sc, h->dim, SEARCH_WRITE));
   if (ordered) {
     FKD_CUDA(h->tmp.ensure(total ? total * sizeof(uint32_t) : 4));
     FKD_CUDA(launch_order_results(sc.g, sc.tab, doffsets, b.q, dout, h->tmp.as<uint32_t>(), sc.err, h->stream));
@@ -490,13 +527,69 @@ fkd_status fkd_search(fkd_tree h, const float* mins, const float* maxs, uint64_t
   if ((s = ensure_inorder(h)) != FKD_OK) return s;
   const bool kt = !h->kev.empty();
   if (kt) FKD_CUDA(cudaEventRecord(h->kev_at(h->kev_searches, 0), h->stream));
-  if (q && (s = count_pass(h, b, h->counts.as<uint32_t>(), order)) != FKD_OK) return s;
+  // The count pass records every box's result as runs of the in-order table
+  // (fkd_search.cu: k_search, k_expand) into a pool sized by the previous
+  // call's demand; boxes that do not fit are traversed again by the write pass.
+  SearchCtx rec;
+  memset(&rec, 0, sizeof rec);
+  bool rec_on = q > 0 && (h->search_lanes == 0 || h->search_lanes == 32);
+  if (rec_on) {
+    uint64_t pw = h->pool_want ? h->pool_want : 64 * q + (1u << 22);
+    uint64_t sw = h->pool_s_want ? h->pool_s_want : 256 * q + (1u << 22);
+    if (pw > 0xffffffffull) pw = 0xffffffffull;
+    if (sw > 0xffffffffull) sw = 0xffffffffull;
+    const uint64_t bw = h->brec_want ? h->brec_want : q + (1u << 16);
+    cudaError_t ae = h->pool_st.ensure(pw * sizeof(uint32_t));
+    if (ae == cudaSuccess) ae = h->pool_len.ensure(pw * sizeof(uint32_t));
+    if (ae == cudaSuccess) ae = h->pool_s.ensure(sw * sizeof(uint32_t));
+    if (ae == cudaSuccess) ae = h->brec.ensure(2 * bw * sizeof(uint4));
+    if (ae == cudaSuccess) ae = h->rflags.ensure(q * sizeof(uint32_t));
+    if (ae == cudaSuccess) ae = h->jctr.ensure(4 * sizeof(unsigned long long));
+    if (ae != cudaSuccess) {
+      // no room for the pool: traverse twice
+      (void)cudaGetLastError();
+      h->pool_st.release();
+      h->pool_len.release();
+      h->pool_s.release();
+      h->brec.release();
+      h->pool_want = h->pool_s_want = h->brec_want = 0;
+      rec_on = false;
+    } else {
+      FKD_CUDA(cudaMemsetAsync(h->jctr.p, 0, 4 * sizeof(unsigned long long), h->stream));
+      // chunk records are reserved in blocks; the unused tail of a block must read as empty
+      FKD_CUDA(cudaMemsetAsync(h->brec.p, 0, h->brec.bytes, h->stream));
+      unsigned long long* ctr = h->jctr.as<unsigned long long>();
+      rec.pool_st = h->pool_st.as<uint32_t>();
+      rec.pool_len = h->pool_len.as<uint32_t>();
+      rec.pool_s = h->pool_s.as<uint32_t>();
+      rec.pool_ctr = ctr;  // [0] runs, [1] singles
+      rec.pool_cap = h->pool_st.bytes / sizeof(uint32_t);
+      rec.pool_cap_s = h->pool_s.bytes / sizeof(uint32_t);
+      rec.brec = h->brec.as<uint4>();
+      rec.brec_ctr = ctr + 2;
+      rec.brec_cap = h->brec.bytes / (2 * sizeof(uint4));
+      rec.flags = h->rflags.as<uint32_t>();
+      rec.flag_ctr = (uint32_t*)(ctr + 3);
+    }
+  }
+  if (q && (s = count_pass(h, b, h->counts.as<uint32_t>(), order, rec_on ? &rec : nullptr)) != FKD_OK) return s;
   if (kt) FKD_CUDA(cudaEventRecord(h->kev_at(h->kev_searches, 1), h->stream));
   FKD_CUDA(launch_scan_counts(h->counts.as<uint32_t>(), q, doff, h->partials.as<unsigned long long>(), h->stream));
   FKD_CUDA(cudaMemcpyAsync(h->herr + 2, doff + q, sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
+  if (rec_on) FKD_CUDA(cudaMemcpyAsync(h->herr + 4, h->jctr.p, 4 * sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
   FKD_CUDA(cudaStreamSynchronize(h->stream));
   uint64_t tot = 0;
   memcpy(&tot, h->herr + 2, sizeof(uint64_t));
+  uint32_t nflag = 0;
+  if (rec_on) {
+    uint64_t dem[4];
+    memcpy(dem, h->herr + 4, sizeof dem);
+    nflag = (uint32_t)dem[3];
+    // the next call's pools hold this call's demand with room to spare
+    h->pool_want = std::max<uint64_t>(h->pool_want, dem[0] + dem[0] / 4 + (1u << 22));
+    h->pool_s_want = std::max<uint64_t>(h->pool_s_want, dem[1] + dem[1] / 4 + (1u << 22));
+    h->brec_want = std::max<uint64_t>(h->brec_want, dem[2] + dem[2] / 4 + (1u << 16));
+  }
   *total = tot;
   if ((s = check_err_word(h, "fkd_search (count)")) != FKD_OK) return s;
   if (mem == FKD_MEM_HOST)
@@ -524,7 +617,7 @@ fkd_status fkd_search(fkd_tree h, const float* mins, const float* maxs, uint64_t
     dout = h->out.as<uint32_t>();
   }
   if (kt) FKD_CUDA(cudaEventRecord(h->kev_at(h->kev_searches, 2), h->stream));
-  if ((s = write_pass(h, b, doff, dout, tot, ordered, order)) != FKD_OK) return s;
+  if ((s = write_pass(h, b, doff, dout, tot, ordered, order, rec_on ? &rec : nullptr, nflag)) != FKD_OK) return s;
   if (kt) {
     FKD_CUDA(cudaEventRecord(h->kev_at(h->kev_searches, 3), h->stream));
     ++h->kev_searches;

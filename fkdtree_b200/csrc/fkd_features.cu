@@ -126,6 +126,9 @@ __global__ void k_bracket(uint32_t d, const EvDesc* __restrict__ evs, const uint
   const uint32_t cp = lk == hk ? 32u : (uint32_t)__clz(lk ^ hk);
   if (cp < 4u) return;  // a block wider than 1/16 of the key space saves nothing
   SegSel* p = &sel[s];
+  // the segment's common prefix may already fix as many bits, or exclude the block
+  if (p->bits >= cp) return;
+  if (p->bits != 0u && (lk >> (32u - p->bits)) != (uint32_t)p->prefix) return;
   p->prefix = (unsigned long long)(lk >> (32u - cp));
   p->bits = cp;
   p->verify = 1u;

@@ -25,7 +25,8 @@ struct SegSel {
   uint32_t verify;            // 1: prefix is a predicted block, the next pass verifies it
   uint32_t below;             // verify pass: points whose key lies below the block
   uint32_t kfull;             // the pivot rank within the segment (fallback restart)
-  uint32_t pad;
+  uint32_t bits0;             // the common prefix every key of the segment shares (restart point)
+  unsigned long long prefix0;
 };
 
 constexpr int FKD_MLP_FEATURES = 40;  // node summary width (== FKD_MLP_IN of the C ABI)
@@ -69,6 +70,7 @@ struct LevelPlan {
   uint32_t hts;         // digit-pass tile length
   const uint2* ptiles;  // partition CTA -> (segment, tile)
   uint32_t nptile;
+  const uint32_t* child;  // per segment: its left child's index in the next level (~0u: not a global segment)
 };
 
 struct BuildCtx {
@@ -82,6 +84,9 @@ struct BuildCtx {
   SegSel* sel;    // >= max segments of a level
   uint32_t* ghist;
   uint32_t* pending;  // one word per digit pass (+1): does that pass have work
+  uint2* bnd = nullptr;    // 2 x bnd_stride: per-segment (min, max) of the split coordinate's
+                           // order bits, written by the previous level's partition (null: unused)
+  uint32_t bnd_stride = 0; // >= max segments of a level
   Table tab;
   uint32_t* err;
   cudaStream_t stream;
@@ -138,10 +143,26 @@ struct SearchCtx {
   uint32_t* err;
   int heap_out;            // write heap indices instead of ids
   uint32_t lanes;          // count / digest: lanes per box (1, 2, 4, 8, 16; 0 or 32: one warp per box)
+  // count pass with a run pool: every box's result recorded as runs of the
+  // in-order table, in chunks that k_expand writes out (null pool: no record)
+  uint32_t* pool_st;             // in-order start of every run
+  uint32_t* pool_len;            // its length
+  uint32_t* pool_s;              // in-order position of every single (in-box node without a contained child)
+  unsigned long long* pool_ctr;  // [0] runs, [1] singles reserved (zeroed by the caller; count past the caps)
+  uint64_t pool_cap;             // runs
+  uint64_t pool_cap_s;           // singles
+  uint4* brec;                   // two uint4 per chunk: (box, offset within the box, singles position,
+                                 // singles), (runs position, runs, 0, 0)
+  unsigned long long* brec_ctr;  // chunks reserved (zeroed by the caller; counts past brec_cap)
+  uint64_t brec_cap;
+  uint32_t* flags;               // boxes whose runs did not fit (the write pass traverses them)
+  uint32_t* flag_ctr;            // (zeroed by the caller)
   cudaStream_t stream;
 };
 
 cudaError_t launch_search(SearchCtx& sc, int dim, int mode);
+// Writes the results of the runs a recording count pass stored (no-op without a pool).
+cudaError_t launch_expand(const SearchCtx& sc);
 // Fills tab.dids / tab.dnode (in-order tables); required by SEARCH_WRITE.
 cudaError_t launch_inorder(const Geom& g, Table tab, cudaStream_t stream);
 // Fills tab.sdig (subtree digests) for every event; required by SEARCH_DIGEST.

@@ -29,6 +29,17 @@ void plan_build(const uint32_t* n_ev, const uint32_t* base_ev, uint32_t nev, int
     if (n_ev[e] && d.d0 > maxd0) maxd0 = d.d0;
   }
   out.levels.resize(maxd0);
+  // first[L][e]: index of event e's first segment in level L's list
+  std::vector<std::vector<uint32_t>> first(maxd0 + 1, std::vector<uint32_t>(nev, ~0u));
+  for (uint32_t L = 0; L < maxd0; ++L) {
+    uint32_t k = 0;
+    for (uint32_t e = 0; e < nev; ++e) {
+      const EvDesc& d = out.evs[e];
+      if (d.g.n == 0 || d.d0 <= L) continue;
+      first[L][e] = k;
+      k += 1u << L;
+    }
+  }
   for (uint32_t L = 0; L < maxd0; ++L) {
     PlanLevel& lv = out.levels[L];
     uint64_t total = 0;
@@ -37,6 +48,7 @@ void plan_build(const uint32_t* n_ev, const uint32_t* base_ev, uint32_t nev, int
       if (d.g.n == 0 || d.d0 <= L) continue;
       for (uint32_t t = 0; t < (1u << L); ++t) {
         lv.segs.push_back(make_uint2(e, t));
+        lv.child.push_back(d.d0 > L + 1 ? first[L + 1][e] + 2u * t : ~0u);
         total += seg_len(d.g, L, t);
       }
     }
@@ -61,23 +73,26 @@ void plan_build(const uint32_t* n_ev, const uint32_t* base_ev, uint32_t nev, int
 }
 
 cudaError_t PlanDev::upload(const PlanHost& h, cudaStream_t stream) {
-  size_t words = h.evs.size() * (sizeof(EvDesc) / 4) + 2 * h.subs.size();
-  for (const PlanLevel& lv : h.levels) words += 2 * (lv.segs.size() + lv.htiles.size() + lv.ptiles.size());
+  // every array starts on a 16-byte boundary (uint2 / EvDesc loads need 8)
+  size_t words = h.evs.size() * (sizeof(EvDesc) / 4) + 2 * h.subs.size() + 8;
+  for (const PlanLevel& lv : h.levels)
+    words += 2 * (lv.segs.size() + lv.htiles.size() + lv.ptiles.size()) + lv.child.size() + 16;
   host.assign(words + 16, 0u);
   size_t pos = 0;
   auto put = [&](const void* src, size_t bytes) {
     const size_t at = pos;
-    memcpy(host.data() + pos, src, bytes);
-    pos += (bytes + 3) / 4;
+    if (bytes) memcpy(host.data() + pos, src, bytes);
+    pos += ((bytes + 15) / 16) * 4;
     return at;
   };
   const size_t evs_at = put(h.evs.data(), h.evs.size() * sizeof(EvDesc));
   const size_t subs_at = put(h.subs.data(), h.subs.size() * sizeof(uint2));
-  std::vector<size_t> at(h.levels.size() * 3);
+  std::vector<size_t> at(h.levels.size() * 4);
   for (size_t L = 0; L < h.levels.size(); ++L) {
-    at[3 * L] = put(h.levels[L].segs.data(), h.levels[L].segs.size() * sizeof(uint2));
-    at[3 * L + 1] = put(h.levels[L].htiles.data(), h.levels[L].htiles.size() * sizeof(uint2));
-    at[3 * L + 2] = put(h.levels[L].ptiles.data(), h.levels[L].ptiles.size() * sizeof(uint2));
+    at[4 * L] = put(h.levels[L].segs.data(), h.levels[L].segs.size() * sizeof(uint2));
+    at[4 * L + 1] = put(h.levels[L].htiles.data(), h.levels[L].htiles.size() * sizeof(uint2));
+    at[4 * L + 2] = put(h.levels[L].ptiles.data(), h.levels[L].ptiles.size() * sizeof(uint2));
+    at[4 * L + 3] = put(h.levels[L].child.data(), h.levels[L].child.size() * sizeof(uint32_t));
   }
   const size_t bytes = pos * 4 + 16;
   if (bytes > cap) {
@@ -98,13 +113,14 @@ cudaError_t PlanDev::upload(const PlanHost& h, cudaStream_t stream) {
   levels.resize(h.levels.size());
   for (size_t L = 0; L < h.levels.size(); ++L) {
     LevelPlan& lp = levels[L];
-    lp.segs = (const uint2*)(d + at[3 * L]);
+    lp.segs = (const uint2*)(d + at[4 * L]);
     lp.nseg = (uint32_t)h.levels[L].segs.size();
-    lp.htiles = (const uint2*)(d + at[3 * L + 1]);
+    lp.htiles = (const uint2*)(d + at[4 * L + 1]);
     lp.nhtile = (uint32_t)h.levels[L].htiles.size();
     lp.hts = h.levels[L].hts;
-    lp.ptiles = (const uint2*)(d + at[3 * L + 2]);
+    lp.ptiles = (const uint2*)(d + at[4 * L + 2]);
     lp.nptile = (uint32_t)h.levels[L].ptiles.size();
+    lp.child = (const uint32_t*)(d + at[4 * L + 3]);
   }
   maxseg = h.maxseg;
   return cudaSuccess;

@@ -10,6 +10,7 @@ namespace fkd {
 
 struct PlanLevel {
   std::vector<uint2> segs, htiles, ptiles;
+  std::vector<uint32_t> child;  // per segment: index of its left child in the next level's list (~0u: none)
   uint32_t hts = HIST_STEP;
 };
 

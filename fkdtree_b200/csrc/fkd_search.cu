@@ -38,6 +38,10 @@ constexpr int QW = QT / 32;
 constexpr int JOBS = 256;      // contained-subtree jobs buffered per warp
 constexpr int JFLUSH = JOBS - 64;  // one step adds at most 64
 constexpr int EU = 2;              // emission windows with loads in flight
+constexpr uint32_t SBLK = 4096;  // recording count pass: singles reserved per warp at a time
+constexpr uint32_t RBLK = 2048;  // runs reserved per warp at a time
+constexpr uint32_t CBLK = 64;    // chunk records reserved per warp at a time
+constexpr uint32_t RCAP = 4096;  // results per chunk record before a new one starts
 
 __device__ __forceinline__ uint32_t lanemask_lt_s() {
   uint32_t m;
@@ -55,20 +59,79 @@ __device__ __forceinline__ unsigned long long warp_sum64(unsigned long long v) {
   return v;
 }
 
-__host__ __device__ inline uint32_t stack_cap(const Geom& g) { return 64u * (g.H + 1u) + 1u; }
+// Popping the top 32 of a depth-sorted stack leaves at most 64 entries per
+// depth, and depth d has only 2^d nodes: sum over d of min(64, 2^d), plus one.
+__host__ __device__ inline uint32_t stack_cap(const Geom& g) {
+  uint32_t c = 1u;
+  for (uint32_t d = 0; d <= g.H; ++d) c += d < 6u ? (1u << d) : 64u;
+  return c;
+}
 
-template <int DIM, int MODE>
+// Copies the concatenation of nj runs of the in-order table srct -- run k
+// starts at srct[st[k]] and lands at out[base + pre[k]], pre being the
+// exclusive prefix of the run lengths and total their sum -- with one warp.
+// Each lane step writes 32 consecutive output slots; a lane finds its run
+// from the bitmask of the runs that start inside the window (EU windows with
+// loads in flight).  st / pre live in shared memory; slots at or past
+// `limit` are not written and set `failed`.
+__device__ __forceinline__ void copy_runs(const uint32_t* st, const uint32_t* pre, uint32_t nj, uint32_t total,
+                                          const uint32_t* __restrict__ srct, uint32_t* __restrict__ out,
+                                          uint64_t base, uint64_t limit, bool& failed) {
+  const uint32_t lane = threadIdx.x & 31u;
+  uint32_t jb = 0u;  // the run holding output slot o0 (warp-uniform)
+  for (uint32_t o0 = 0; o0 < total; o0 += 32u * EU) {
+    uint32_t src[EU];
+    bool ok[EU];
+#pragma unroll
+    for (int u = 0; u < EU; ++u) {
+      const uint32_t w0 = o0 + 32u * u;
+      const uint32_t k = jb + lane;
+      const bool kv = k < nj;
+      const uint32_t pk = kv ? pre[k] : total;
+      const uint32_t sk = kv ? st[k] : 0u;
+      // runs after jb start after w0 (every run holds at least one id)
+      const uint32_t B = __reduce_or_sync(0xffffffffu, (lane > 0u && kv && pk < w0 + 32u) ? (1u << (pk - w0)) : 0u);
+      const uint32_t jl = __popc(B & (0xffffffffu >> (31u - lane)));
+      const uint32_t mp = __shfl_sync(0xffffffffu, pk, jl);
+      const uint32_t ms = __shfl_sync(0xffffffffu, sk, jl);
+      ok[u] = w0 + lane < total;
+      src[u] = ms + (w0 + lane - mp);
+      // the run holding w0 + 32: the one holding w0 + 31, or the next if it starts there
+      uint32_t nb = jb + __popc(B);
+      if (nb + 1u < nj && pre[nb + 1u] == w0 + 32u) ++nb;
+      jb = nb;
+    }
+    uint32_t v[EU];
+#pragma unroll
+    for (int u = 0; u < EU; ++u) v[u] = ok[u] ? __ldg(srct + src[u]) : 0u;
+#pragma unroll
+    for (int u = 0; u < EU; ++u) {
+      if (ok[u]) {
+        const uint64_t pos = base + o0 + 32u * u + lane;
+        if (pos < limit)
+          out[pos] = v[u];
+        else
+          failed = true;
+      }
+    }
+  }
+}
+
+template <int DIM, int MODE, bool REC = false>
 __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ uint32_t jst[QW][JOBS];   // write pass: in-order start of each buffered subtree
-  __shared__ uint32_t jlen[QW][JOBS];  // its size
-  __shared__ uint32_t jpre[QW][JOBS];  // exclusive prefix of the sizes
+  constexpr int JN = REC ? JOBS / 2 : JOBS;  // the recording count pass flushes twice as often (occupancy)
+  __shared__ uint32_t jst[QW][JN];   // in-order start of each buffered subtree (write pass, recording count)
+  __shared__ uint32_t jlen[QW][JN];  // its size
+  __shared__ uint32_t jpre[QW][JN];  // write pass: exclusive prefix of the sizes; recording count: single positions
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   uint32_t* stk_node = (uint32_t*)smem_raw + (size_t)warp * cap;
   uint8_t* stk_mask = (uint8_t*)((uint32_t*)smem_raw + (size_t)QW * cap) + (size_t)warp * cap;
   constexpr uint32_t FULL = (1u << (2 * DIM)) - 1u;
   const uint32_t lt = lanemask_lt_s();
   uint32_t cur_ev = 0;  // batched search: the event of the last box (boxes come in increasing order)
+  // recording count pass: this warp's current pool blocks and chunk-record block
+  uint32_t s_cur = 0u, s_end = 0u, r_cur = 0u, r_end = 0u, c_cur = 0u, c_end = 0u;
 
   for (;;) {
     uint32_t qi = 0;
@@ -134,10 +197,8 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
 
     // Emits the whole subtrees buffered in the job list: job k is the run
     // [jst[k], jst[k] + jlen[k]) of the in-order table (tab.dids, or tab.dnode
-    // for heap indices), where every subtree is one contiguous range.  The
-    // runs are concatenated at the cursor; each lane step writes 32
-    // consecutive output slots, a lane finds its job from the bitmask of the
-    // jobs that start inside the window (EU windows with loads in flight).
+    // for heap indices), where every subtree is one contiguous range; the
+    // runs are concatenated at the cursor.
     auto run_jobs = [&](uint32_t nj) {
       uint32_t carry = 0u;
       for (uint32_t e0 = 0; e0 < nj; e0 += 32u) {
@@ -153,46 +214,96 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
         carry += __shfl_sync(0xffffffffu, incl, 31);
       }
       __syncwarp();
-      const uint32_t total = carry;
-      const uint32_t* srct = sc.heap_out ? tab.dnode : tab.dids;
-      uint32_t jb = 0u;  // the job holding output slot o0 (warp-uniform)
-      for (uint32_t o0 = 0; o0 < total; o0 += 32u * EU) {
-        uint32_t src[EU];
-        bool ok[EU];
-#pragma unroll
-        for (int u = 0; u < EU; ++u) {
-          const uint32_t w0 = o0 + 32u * u;
-          const uint32_t k = jb + lane;
-          const bool kv = k < nj;
-          const uint32_t pk = kv ? jpre[warp][k] : total;
-          const uint32_t sk = kv ? jst[warp][k] : 0u;
-          // jobs after jb start after w0 (every job holds at least one id)
-          const uint32_t B = __reduce_or_sync(0xffffffffu, (lane > 0u && kv && pk < w0 + 32u) ? (1u << (pk - w0)) : 0u);
-          const uint32_t jl = __popc(B & (0xffffffffu >> (31u - lane)));
-          const uint32_t mp = __shfl_sync(0xffffffffu, pk, jl);
-          const uint32_t ms = __shfl_sync(0xffffffffu, sk, jl);
-          ok[u] = w0 + lane < total;
-          src[u] = ms + (w0 + lane - mp);
-          // the job holding w0 + 32: the one holding w0 + 31, or the next if it starts there
-          uint32_t nb = jb + __popc(B);
-          if (nb + 1u < nj && jpre[warp][nb + 1u] == w0 + 32u) ++nb;
-          jb = nb;
+      const uint64_t limit = cend < sc.capacity ? cend : sc.capacity;
+      copy_runs(jst[warp], jpre[warp], nj, carry, sc.heap_out ? tab.dnode : tab.dids, sc.out, cursor, limit, failed);
+      cursor += carry;
+      __syncwarp();
+    };
+
+    // Recording count pass (REC): the result of the box is also recorded in
+    // the in-order table -- an in-box node whose children are not contained
+    // as its position ("single"), a contained subtree (merged with an
+    // adjacent in-box node) as a run -- handed to k_expand in chunks
+    // (box, offset within the box, singles, runs), so the write pass needs
+    // no second traversal.  A box whose record does not fit the pools is
+    // listed in sc.flags for the traversing write pass.
+    constexpr bool record = REC && MODE == SEARCH_COUNT;
+    bool recfail = false;
+    uint32_t relcur = 0u;  // results of the box recorded so far
+    uint32_t nsing = 0u;   // singles buffered in jpre[warp] (warp-uniform)
+    bool ropen = false;    // this box has an open chunk record (rb) that later flushes may extend
+    uint32_t rb = 0u, rs0 = 0u, rns = 0u, rr0 = 0u, rnr = 0u, rrel = 0u, rcnt = 0u;
+    auto flush_runs = [&](uint32_t nj) {
+      uint32_t tot = nsing;
+      {
+        uint32_t t = 0u;
+        for (uint32_t e = lane; e < nj; e += 32u) t += jlen[warp][e];
+        tot += __reduce_add_sync(0xffffffffu, t);
+      }
+      if (!recfail) {
+        // pool space comes in per-warp blocks (one atomic per block, not per flush)
+        bool ok = true;
+        if (s_cur + nsing > s_end) {
+          const uint32_t want = nsing > SBLK ? nsing : SBLK;
+          unsigned long long b = 0ull;
+          if (lane == 0) b = atomicAdd(sc.pool_ctr + 1, (unsigned long long)want);
+          b = __shfl_sync(0xffffffffu, b, 0);
+          ok = b + want <= sc.pool_cap_s;
+          s_cur = ok ? (uint32_t)b : 0u;
+          s_end = ok ? (uint32_t)(b + want) : 0u;
+          ropen = false;  // the next chunk cannot continue the last one
         }
-        uint32_t v[EU];
-#pragma unroll
-        for (int u = 0; u < EU; ++u) v[u] = ok[u] ? __ldg(srct + src[u]) : 0u;
-#pragma unroll
-        for (int u = 0; u < EU; ++u) {
-          if (ok[u]) {
-            const uint64_t pos = cursor + o0 + 32u * u + lane;
-            if (pos < cend && pos < sc.capacity)
-              sc.out[pos] = v[u];
-            else
-              failed = true;
+        if (ok && r_cur + nj > r_end) {
+          const uint32_t want = nj > RBLK ? nj : RBLK;
+          unsigned long long b = 0ull;
+          if (lane == 0) b = atomicAdd(sc.pool_ctr, (unsigned long long)want);
+          b = __shfl_sync(0xffffffffu, b, 0);
+          ok = b + want <= sc.pool_cap;
+          r_cur = ok ? (uint32_t)b : 0u;
+          r_end = ok ? (uint32_t)(b + want) : 0u;
+          ropen = false;
+        }
+        if (ropen && rcnt >= RCAP) ropen = false;  // keep records short: k_expand balances by records
+        if (ok && !ropen) {
+          if (c_cur == c_end) {
+            unsigned long long b = 0ull;
+            if (lane == 0) b = atomicAdd(sc.brec_ctr, (unsigned long long)CBLK);
+            b = __shfl_sync(0xffffffffu, b, 0);
+            ok = b + CBLK <= sc.brec_cap;
+            c_cur = ok ? (uint32_t)b : 0u;
+            c_end = ok ? (uint32_t)(b + CBLK) : 0u;
+          }
+          if (ok) {
+            rb = c_cur++;
+            rs0 = s_cur;
+            rr0 = r_cur;
+            rns = rnr = 0u;
+            rcnt = 0u;
+            rrel = relcur;
+            ropen = true;
           }
         }
+        if (ok) {
+          for (uint32_t e = lane; e < nj; e += 32u) {
+            sc.pool_st[r_cur + e] = jst[warp][e];
+            sc.pool_len[r_cur + e] = jlen[warp][e];
+          }
+          for (uint32_t e = lane; e < nsing; e += 32u) sc.pool_s[s_cur + e] = jpre[warp][e];
+          s_cur += nsing;
+          r_cur += nj;
+          rns += nsing;
+          rnr += nj;
+          rcnt += tot;
+          if (lane == 0) {
+            sc.brec[2ull * rb] = make_uint4((uint32_t)oj, rrel, rs0, rns);
+            sc.brec[2ull * rb + 1ull] = make_uint4(rr0, rnr, 0u, 0u);
+          }
+        } else {
+          recfail = true;
+        }
       }
-      cursor += total;
+      relcur += tot;
+      nsing = 0u;
       __syncwarp();
     };
 
@@ -200,7 +311,15 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
     if (n > 0) {
       if (mask0 == FULL) {
         if (MODE == SEARCH_COUNT) {
-          if (lane == 0) acc += n;
+          if (lane == 0) {
+            acc += n;
+            if (record) {
+              jst[warp][0] = 0u;
+              jlen[warp][0] = n;
+            }
+          }
+          if (record) njobs = 1;
+          __syncwarp();
         } else if (MODE == SEARCH_DIGEST) {
           if (lane == 0) {
             acc2 += n;
@@ -268,8 +387,74 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
         pushR = visitR && !contR;
       }
       if (MODE == SEARCH_COUNT) {
-        acc += (emit ? 1u : 0u) + (contL ? subtree_size(g, 2u * i + 1u) : 0u) +
-               (contR ? subtree_size(g, 2u * i + 2u) : 0u);
+        if (!record) {
+          acc += (emit ? 1u : 0u) + (contL ? subtree_size(g, 2u * i + 1u) : 0u) +
+                 (contR ? subtree_size(g, 2u * i + 2u) : 0u);
+        } else {
+          // node (dep, t) owns in-order [S, S + len); its left subtree is
+          // [S, S + K), itself S + K, its right subtree the rest (32-bit
+          // arithmetic: every position is below n < 2^31)
+          uint32_t s1 = 0u, l1 = 0u, s2 = 0u, l2 = 0u, sg = 0u;
+          const bool single = emit && !contL && !contR;
+          if (emit || contL || contR) {
+            const uint32_t dep = 31u - (uint32_t)__clz(i + 1u);
+            const uint32_t t = i + 1u - (1u << dep);
+            const uint32_t sh = g.H - dep;
+            const uint32_t tw = t << sh;
+            const uint32_t S = tw + min(g.M, tw);
+            uint32_t K = 0u, W = 0u;
+            if (sh != 0u) {  // len(dep + 1, 2t); (2t) * 2^(H-dep-1) = t * 2^(H-dep)
+              W = 1u << (sh - 1u);
+              K = W - 1u + (g.M > tw ? min(g.M - tw, W) : 0u);
+            }
+            const uint32_t P = S + K;
+            sg = P;
+            if (!single) {
+              const uint32_t tw3 = tw + W;  // (2t + 1) * 2^(H-dep-1)
+              const uint32_t lenR = contR ? W - 1u + (g.M > tw3 ? min(g.M - tw3, W) : 0u) : 0u;
+              if (contL) {
+                s1 = S;
+                l1 = K;
+              }
+              if (emit) {
+                if (l1 == 0u) s1 = P;
+                l1 += 1u;
+              }
+              if (contR) {
+                if (l1 == 0u) {
+                  s1 = P + 1u;
+                  l1 = lenR;
+                } else if (emit) {
+                  l1 += lenR;
+                } else {
+                  s2 = P + 1u;
+                  l2 = lenR;
+                }
+              }
+            }
+          }
+          acc += (single ? 1u : 0u) + l1 + l2;
+          const uint32_t b1 = __ballot_sync(0xffffffffu, l1 != 0u), b2 = __ballot_sync(0xffffffffu, l2 != 0u);
+          const uint32_t bs = __ballot_sync(0xffffffffu, single);
+          uint32_t jp = njobs + __popc(b1 & lt) + __popc(b2 & lt);
+          if (l1) {
+            jst[warp][jp] = s1;
+            jlen[warp][jp] = l1;
+            ++jp;
+          }
+          if (l2) {
+            jst[warp][jp] = s2;
+            jlen[warp][jp] = l2;
+          }
+          if (single) jpre[warp][nsing + __popc(bs & lt)] = sg;
+          njobs += __popc(b1) + __popc(b2);
+          nsing += __popc(bs);
+          if (njobs > (uint32_t)(JN - 64) || nsing > (uint32_t)(JN - 32)) {
+            __syncwarp();
+            flush_runs(njobs);
+            njobs = 0;
+          }
+        }
       } else {
         if (MODE == SEARCH_DIGEST) {
           // a contained subtree's digest is one table entry (sdig)
@@ -328,9 +513,24 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
       __syncwarp();
     }
 
-    if (MODE != SEARCH_COUNT && njobs) {
+    if (MODE == SEARCH_WRITE && njobs) {
       __syncwarp();
       run_jobs(njobs);
+    }
+    if (record) {
+      if (njobs || nsing) {
+        __syncwarp();
+        flush_runs(njobs);
+      }
+      if (recfail) {
+        // a chunk this box already wrote stays valid: zero its counts, the
+        // traversing write pass writes the whole box
+        if (ropen && lane == 0) {
+          sc.brec[2ull * rb] = make_uint4((uint32_t)oj, 0u, 0u, 0u);
+          sc.brec[2ull * rb + 1ull] = make_uint4(0u, 0u, 0u, 0u);
+        }
+        if (lane == 0) sc.flags[atomicAdd(sc.flag_ctr, 1u)] = qj;
+      }
     }
     const bool anyfail = __any_sync(0xffffffffu, failed);
     if (MODE == SEARCH_COUNT) {
@@ -350,6 +550,103 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
     if (anyfail && lane == 0) atomicOr(sc.err, ERRB_CAPACITY);
     __syncwarp();
   }
+}
+
+// Writes every box's result from what its count pass recorded: a warp per
+// chunk record (box, offset within the box, singles, runs) -- the singles'
+// ids first, one per lane, then the runs, JOBS at a time -- with no
+// traversal state, so the copy runs at full occupancy.  Records never
+// written (the tail of a warp's record block) are zero and skipped.
+constexpr int XT = 256;  // threads of k_expand
+constexpr int EXU = 4;   // k_expand: single ids with loads in flight per lane
+__global__ void __launch_bounds__(XT) k_expand(const uint4* __restrict__ brec,
+                                               const unsigned long long* __restrict__ brec_ctr, uint64_t brec_cap,
+                                               const uint32_t* __restrict__ pool_s,
+                                               const uint32_t* __restrict__ pool_st,
+                                               const uint32_t* __restrict__ pool_len,
+                                               const uint64_t* __restrict__ offsets,
+                                               const uint32_t* __restrict__ srct, uint32_t* __restrict__ out,
+                                               uint64_t capacity, uint32_t* __restrict__ err) {
+  __shared__ uint32_t st[XT / 32][JOBS];
+  __shared__ uint32_t pre[XT / 32][JOBS];
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint64_t nrec = *brec_ctr < brec_cap ? *brec_ctr : brec_cap;
+  bool failed = false;
+  for (uint64_t r = (uint64_t)blockIdx.x * (XT / 32) + warp; r < nrec; r += (uint64_t)gridDim.x * (XT / 32)) {
+    const uint4 R = brec[2 * r], R2 = brec[2 * r + 1];
+    const uint32_t ns = R.w, nj = R2.y;
+    if (ns == 0u && nj == 0u) continue;
+    const uint64_t lo = offsets[R.x], hi = offsets[R.x + 1u];
+    const uint64_t limit = hi < capacity ? hi : capacity;
+    uint64_t base = lo + R.y;
+    // singles
+    for (uint32_t e0 = 0; e0 < ns; e0 += 32u * EXU) {
+      uint32_t v[EXU];
+#pragma unroll
+      for (int u = 0; u < EXU; ++u) {
+        const uint32_t e = e0 + 32u * u + lane;
+        v[u] = e < ns ? __ldg(pool_s + R.z + e) : 0u;
+      }
+#pragma unroll
+      for (int u = 0; u < EXU; ++u) {
+        const uint32_t e = e0 + 32u * u + lane;
+        if (e < ns) v[u] = __ldg(srct + v[u]);
+      }
+#pragma unroll
+      for (int u = 0; u < EXU; ++u) {
+        const uint32_t e = e0 + 32u * u + lane;
+        if (e < ns) {
+          if (base + e < limit)
+            out[base + e] = v[u];
+          else
+            failed = true;
+        }
+      }
+    }
+    base += ns;
+    // runs, JOBS at a time
+    for (uint32_t k0 = 0; k0 < nj; k0 += (uint32_t)JOBS) {
+      const uint32_t m = (nj - k0) < (uint32_t)JOBS ? (nj - k0) : (uint32_t)JOBS;
+      const uint64_t pb = (uint64_t)R2.x + k0;
+      uint32_t carry = 0u;
+      for (uint32_t e0 = 0; e0 < m; e0 += 32u) {
+        const uint32_t e = e0 + lane;
+        const uint32_t len = e < m ? pool_len[pb + e] : 0u;
+        uint32_t incl = len;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= (uint32_t)o) incl += y;
+        }
+        if (e < m) {
+          st[warp][e] = pool_st[pb + e];
+          pre[warp][e] = carry + incl - len;
+        }
+        carry += __shfl_sync(0xffffffffu, incl, 31);
+      }
+      __syncwarp();
+      copy_runs(st[warp], pre[warp], m, carry, srct, out, base, limit, failed);
+      base += carry;
+      __syncwarp();
+    }
+  }
+  if (__any_sync(0xffffffffu, failed) && lane == 0) atomicOr(err, ERRB_CAPACITY);
+}
+
+cudaError_t launch_expand(const SearchCtx& sc) {
+  if (!sc.pool_st) return cudaSuccess;
+  int dev = 0, sms = 148, per = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_expand, XT, 0);
+  if (e != cudaSuccess) return e;
+  if (per < 1) per = 1;
+  k_expand<<<(unsigned)(sms * per), XT, 0, sc.stream>>>(sc.brec, sc.brec_ctr, sc.brec_cap, sc.pool_s, sc.pool_st,
+                                                        sc.pool_len,
+                                                        sc.offsets, sc.heap_out ? sc.tab.dnode : sc.tab.dids, sc.out,
+                                                        sc.capacity, sc.err);
+  count_launches(1);
+  return cudaGetLastError();
 }
 
 // Count / digest with G < 32 lanes per box (G = 1: a thread per box): a warp
@@ -567,16 +864,20 @@ static cudaError_t run_search_grp(SearchCtx& sc) {
   return cudaGetLastError();
 }
 
-template <int DIM, int MODE>
+template <int DIM, int MODE, bool REC = false>
 static cudaError_t run_search(SearchCtx& sc) {
+  if constexpr (MODE == SEARCH_COUNT && !REC) {
+    if (sc.pool_st) return run_search<DIM, MODE, true>(sc);
+  }
   const uint32_t cap = stack_cap(sc.g);
   const size_t smem = (size_t)QW * cap * 5u;
-  cudaError_t e = cudaFuncSetAttribute(k_search<DIM, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e =
+      cudaFuncSetAttribute(k_search<DIM, MODE, REC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int dev = 0, sms = 0, per = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_search<DIM, MODE>, QT, smem);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_search<DIM, MODE, REC>, QT, smem);
   if (e != cudaSuccess) return e;
   if (per < 1) per = 1;
   uint64_t blocks = (uint64_t)sms * per;
@@ -584,7 +885,7 @@ static cudaError_t run_search(SearchCtx& sc) {
   if (blocks > need) blocks = need ? need : 1;
   e = cudaMemsetAsync(sc.qcounter, 0, sizeof(uint32_t), sc.stream);
   if (e != cudaSuccess) return e;
-  k_search<DIM, MODE><<<(unsigned)blocks, QT, smem, sc.stream>>>(sc, cap);
+  k_search<DIM, MODE, REC><<<(unsigned)blocks, QT, smem, sc.stream>>>(sc, cap);
   count_launches(1);
   return cudaGetLastError();
 }
