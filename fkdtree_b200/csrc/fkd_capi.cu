@@ -85,6 +85,8 @@ struct fkd_tree_s {
   DevBuf lfeat, lyhat, lrange, lstats, sdig, dids, dnode, bnd, pool_st, pool_len, pool_s, brec, jctr, rflags;
   // run pool of fkd_search, sized by the previous call's demand
   uint64_t pool_want = 0, pool_s_want = 0, brec_want = 0;
+  bool search_record = true;    // fkd_search records runs in the count pass ("search_record")
+  uint64_t search_pool = 0;     // fixed pool entries ("search_pool"; 0: sized by demand)
   bool sdig_valid = false;
   bool inorder_valid = false;
   // optional per-kernel timing (fkd_set_param "kernel_events"): a ring of
@@ -532,10 +534,11 @@ fkd_status fkd_search(fkd_tree h, const float* mins, const float* maxs, uint64_t
   // call's demand; boxes that do not fit are traversed again by the write pass.
   SearchCtx rec;
   memset(&rec, 0, sizeof rec);
-  bool rec_on = q > 0 && (h->search_lanes == 0 || h->search_lanes == 32);
+  bool rec_on = q > 0 && h->search_record && (h->search_lanes == 0 || h->search_lanes == 32);
   if (rec_on) {
     uint64_t pw = h->pool_want ? h->pool_want : 64 * q + (1u << 22);
     uint64_t sw = h->pool_s_want ? h->pool_s_want : 256 * q + (1u << 22);
+    if (h->search_pool) pw = sw = h->search_pool;
     if (pw > 0xffffffffull) pw = 0xffffffffull;
     if (sw > 0xffffffffull) sw = 0xffffffffull;
     const uint64_t bw = h->brec_want ? h->brec_want : q + (1u << 16);
@@ -586,8 +589,8 @@ fkd_status fkd_search(fkd_tree h, const float* mins, const float* maxs, uint64_t
     memcpy(dem, h->herr + 4, sizeof dem);
     nflag = (uint32_t)dem[3];
     // the next call's pools hold this call's demand with room to spare
-    h->pool_want = std::max<uint64_t>(h->pool_want, dem[0] + dem[0] / 4 + (1u << 22));
-    h->pool_s_want = std::max<uint64_t>(h->pool_s_want, dem[1] + dem[1] / 4 + (1u << 22));
+    if (!h->search_pool) h->pool_want = std::max<uint64_t>(h->pool_want, dem[0] + dem[0] / 4 + (1u << 22));
+    if (!h->search_pool) h->pool_s_want = std::max<uint64_t>(h->pool_s_want, dem[1] + dem[1] / 4 + (1u << 22));
     h->brec_want = std::max<uint64_t>(h->brec_want, dem[2] + dem[2] / 4 + (1u << 16));
   }
   *total = tot;
@@ -678,6 +681,16 @@ fkd_status fkd_set_param(fkd_tree h, const char* name, int64_t value) {
     if (value != 0 && value != 1 && value != 2 && value != 4 && value != 8 && value != 16 && value != 32)
       return fail(FKD_ERR_ARG, "search_lanes must be 0, 1, 2, 4, 8, 16 or 32");
     h->search_lanes = (uint32_t)value;
+    return FKD_OK;
+  }
+  if (strcmp(name, "search_record") == 0) {
+    if (value != 0 && value != 1) return fail(FKD_ERR_ARG, "search_record must be 0 or 1");
+    h->search_record = value != 0;
+    return FKD_OK;
+  }
+  if (strcmp(name, "search_pool") == 0) {
+    if (value < 0 || value > 0xffffffffll) return fail(FKD_ERR_ARG, "search_pool out of range");
+    h->search_pool = (uint64_t)value;
     return FKD_OK;
   }
   if (strcmp(name, "kernel_events") == 0) {

@@ -163,9 +163,15 @@ FKD_API fkd_status fkd_sync(fkd_tree h);
 
 /* Tuning knobs of one tree, same names and ranges as fkd_batch_set_param
  * ("hist_ctas" takes effect at the next build; "search_lanes" applies to
- * fkd_search_count / fkd_search_digest), plus "kernel_events" (0/1): record
- * CUDA events around the kernels of every fkd_build and fkd_search call for
- * fkd_kernel_times.  No reference counterpart. */
+ * fkd_search_count / fkd_search_digest), plus
+ *   "search_record" (0/1, default 1): fkd_search's count pass records every
+ *                   box's result so that the write needs no second traversal
+ *   "search_pool"   entries of the record pools (0, the default: sized by the
+ *                   previous call's demand; boxes that do not fit are traversed
+ *                   again, so any size gives the same results)
+ *   "kernel_events" (0/1): record CUDA events around the kernels of every
+ *                   fkd_build and fkd_search call for fkd_kernel_times.
+ * No reference counterpart. */
 FKD_API fkd_status fkd_set_param(fkd_tree h, const char* name, int64_t value);
 /* Device times (ms) of the kernels of the build / search `back` calls ago
  * (0 = the last; at most 63), measured by CUDA events on the handle's stream:

@@ -163,3 +163,23 @@ def test_search_lanes_per_box(cuda, dim, lanes):
     assert np.array_equal(c2, cb) and np.array_equal(d2, O.digest_of(ib, ob))
     with pytest.raises(F.FKDError):
         t.set_param("search_lanes", 3)
+
+
+@pytest.mark.parametrize("record,pool", [(0, 0), (1, 0), (1, 64), (1, 5000)])
+def test_search_record_paths(cuda, record, pool):
+    """fkd_search with and without the recording count pass, and with record
+    pools so small that some or all boxes fall back to the traversing write
+    pass: the same sets, equal to the recursive search, and the same ordered
+    lists as the reference's level order."""
+    ev = W.clustered_event(n=200_000, n_queries=3000, n_clusters=64, hw_lo=0.001, hw_hi=0.05, seed=12)
+    t = F.FKDTree(ev.coords, ev.ids).build()
+    t.set_param("search_record", record).set_param("search_pool", pool)
+    tab, tid = t.tables()
+    cr, orr, ir, _ = O.search(tab, tid, ev.mins, ev.maxs, variant=O.RECURSIVE)
+    for _ in range(2):  # the second call uses the pools sized by the first
+        offs, got = t.search_boxes(ev.mins, ev.maxs, ordered=False)
+        assert np.array_equal(offs, orr)
+        assert all(np.array_equal(np.sort(a), np.sort(b)) for a, b in zip(slices(offs, got), slices(orr, ir)))
+    offs, got = t.search_boxes(ev.mins, ev.maxs, ordered=True)
+    cl, ol, il, _ = O.search(tab, tid, ev.mins, ev.maxs, variant=O.BRUTE)
+    assert np.array_equal(offs, ol) and np.array_equal(got, il)
