@@ -63,6 +63,8 @@ def parse_args():
     ap.add_argument("--queries", type=int, default=0,
                     help="box count of the 16M-point workload (0: 1,048,576; smaller cases are for profiling)")
     ap.add_argument("--batched-events", type=int, default=4096)
+    ap.add_argument("--level-times", action="store_true",
+                    help="print the device time of every kernel of one build (CUDA activity records) and exit")
     return ap.parse_args()
 
 
@@ -148,30 +150,46 @@ class ClockSampler:
 
 # ------------------------------------------------------- batched events
 
-def batched_report(dev, n_events=4096, steps=3, train_events=2000):
-    """The batched events workload (4,096 events, log-normal sizes median
-    20,000 clipped to [1,000, 200,000], 50-500 clusters each, every point a
-    box of half-width 0.01 on its own event; eval seed 20) three ways:
+def _timed(fn, k):
+    import torch
+    fn()
+    torch.cuda.synchronize()
+    best = float("inf")
+    for _ in range(k):
+        a = time.perf_counter()
+        fn()
+        torch.cuda.synchronize()
+        best = min(best, time.perf_counter() - a)
+    return best
 
-      plain    one fkd_build + fkd_search_digest per event (the plain
-               single-event GPU path), every event, device buffers
-      batched  fkd_batch_run: all builds and searches as one CUDA graph launch,
-               launch knobs from the autotuner
-      learned  the same graph with the learned split (MLP trained on the GPU on
-               splits recorded from 2,000 training events, seed 10)
 
-    Exactness: per-box counts and digests of the batched runs equal the plain
-    path's; the learned tables equal the plain batched tables."""
+def _cpu_events(wb, n_sample):
+    """The oracle (C restatement of FKDTree_CPU build + search per event,
+    OpenMP over events on every host core) on n_sample events spread over the
+    batch, scaled to the whole batch by points."""
+    from fkdtree_b200 import shard as S
+    from oracle import oracle as O
+    threads = O.host_threads()
+    ev = np.linspace(0, wb.n_events - 1, min(n_sample, wb.n_events)).astype(np.int64)
+    sb = S.sub_batch(wb, ev)
+    t0 = time.perf_counter()
+    O.batch(sb, threads=threads)
+    sec = time.perf_counter() - t0
+    scaled = sec * wb.n_points / max(1, sb.n_points)
+    return {"kind": "port", "cores": threads, "value": wb.n_points / scaled / 1e6, "unit": "Mpoints/s",
+            "ms_scaled": 1e3 * scaled,
+            "sample": (f"oracle build + box search of {len(ev)} of {wb.n_events} events ({sb.n_points} points, "
+                       f"{sb.n_queries} boxes) with {threads} threads over events, scaled by points")}
+
+
+def _events_run(wb, mlp, dev, steps, plain_single):
+    """Batched graph run (autotuned) with and without the learned split, the
+    plain single-event path (optional), exactness checks between them."""
     import torch
 
     import fkdtree_b200 as F
     from fkdtree_b200 import _capi
-    from fkdtree_b200 import workloads as W
 
-    t0 = time.perf_counter()
-    wb = W.event_batch(n_events=n_events, seed=20)
-    tr = W.event_batch(n_events=train_events, seed=10, queries=False)
-    gen_s = time.perf_counter() - t0
     L = _capi.lib()
     P = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
     coords = torch.from_numpy(wb.coords).to(dev)
@@ -179,67 +197,115 @@ def batched_report(dev, n_events=4096, steps=3, train_events=2000):
     mins = torch.from_numpy(wb.mins).to(dev)
     maxs = torch.from_numpy(wb.maxs).to(dev)
     nq = wb.n_queries
+    out = {"events": wb.n_events, "points": wb.n_points, "boxes": nq,
+           "dims": sorted(set(int(d) for d in wb.dims))}
+    pc = pd = None
+    if plain_single:
+        pc = torch.empty(nq, dtype=torch.int32, device=dev)
+        pd = torch.empty(nq, dtype=torch.int64, device=dev)
+        hd = {}
+        sh = C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
 
-    def timed(fn, k):
-        fn()
-        torch.cuda.synchronize()
-        best = float("inf")
-        for _ in range(k):
-            a = time.perf_counter()
-            fn()
-            torch.cuda.synchronize()
-            best = min(best, time.perf_counter() - a)
-        return best
+        def plain():
+            for e in range(wb.n_events):
+                d = int(wb.dims[e])
+                if d not in hd:
+                    hh = C.c_void_p()
+                    _capi.check(L.fkd_create(d, _capi.FLAG_ASYNC, sh, C.byref(hh)))
+                    hd[d] = hh
+                hh = hd[d]
+                n = int(wb.pt_off[e + 1] - wb.pt_off[e])
+                q = int(wb.q_off[e + 1] - wb.q_off[e])
+                c0, p0 = int(wb.coord_off[e]), int(wb.pt_off[e])
+                qc0, q0 = int(wb.qcoord_off[e]), int(wb.q_off[e])
+                _capi.check(L.fkd_build(hh, P(coords[c0:c0 + d * n]), P(ids[p0:p0 + n]), n, _capi.MEM_DEVICE))
+                if q:
+                    _capi.check(L.fkd_search_digest(hh, P(mins[qc0:qc0 + d * q]), P(maxs[qc0:qc0 + d * q]), q,
+                                                    P(pc[q0:q0 + q]), P(pd[q0:q0 + q]), _capi.MEM_DEVICE))
+            for hh in hd.values():
+                _capi.check(L.fkd_sync(hh))
 
-    # plain single-event path over every event
-    pc = torch.empty(nq, dtype=torch.int32, device=dev)
-    pd = torch.empty(nq, dtype=torch.int64, device=dev)
-    hd = {}
-    sh = C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
-
-    def plain():
-        for e in range(wb.n_events):
-            d = int(wb.dims[e])
-            if d not in hd:
-                hh = C.c_void_p()
-                _capi.check(L.fkd_create(d, _capi.FLAG_ASYNC, sh, C.byref(hh)))
-                hd[d] = hh
-            hh = hd[d]
-            n = int(wb.pt_off[e + 1] - wb.pt_off[e])
-            q = int(wb.q_off[e + 1] - wb.q_off[e])
-            c0, p0, qc0, q0 = int(wb.coord_off[e]), int(wb.pt_off[e]), int(wb.qcoord_off[e]), int(wb.q_off[e])
-            _capi.check(L.fkd_build(hh, P(coords[c0:c0 + d * n]), P(ids[p0:p0 + n]), n, _capi.MEM_DEVICE))
-            if q:
-                _capi.check(L.fkd_search_digest(hh, P(mins[qc0:qc0 + d * q]), P(maxs[qc0:qc0 + d * q]), q,
-                                                P(pc[q0:q0 + q]), P(pd[q0:q0 + q]), _capi.MEM_DEVICE))
+        plain_s = _timed(plain, 1)
         for hh in hd.values():
-            _capi.check(L.fkd_sync(hh))
+            _capi.check(L.fkd_destroy(hh))
+        out["plain_single_event_ms"] = 1e3 * plain_s
 
-    plain_s = timed(plain, 1)
-    for hh in hd.values():
-        _capi.check(L.fkd_destroy(hh))
-    results = int(pc.to(torch.int64).sum().item())
-
-    # batched, autotuned
     b = F.Batch.of(wb)
     tune = b.autotune(coords, ids, mins, maxs, use_cache=False, reps=1)
     bc = torch.empty(nq, dtype=torch.int32, device=dev)
     bd = torch.empty(nq, dtype=torch.int64, device=dev)
-    batched_s = timed(lambda: b.run(coords, ids, mins, maxs, bc, bd), steps)
-    exact_batched = bool(torch.equal(bc, pc) and torch.equal(bd, pd))
+    batched_s = _timed(lambda: b.run(coords, ids, mins, maxs, bc, bd), steps)
+    out["results"] = int(bc.to(torch.int64).sum().item())
     tab0 = torch.empty(wb.coords.size, dtype=torch.float32, device=dev)
     tid0 = torch.empty(wb.n_points, dtype=torch.int32, device=dev)
     _capi.check(L.fkd_batch_get_tables(b._h, P(tab0), P(tid0), _capi.MEM_DEVICE))
-    build_s = timed(lambda: b.build(coords, ids), steps)
-    digest_s = timed(lambda: b.search_digest(mins, maxs), 1)
+    out["batched_graph_ms"] = 1e3 * batched_s
+    out["batched_build_ms"] = 1e3 * _timed(lambda: b.build(coords, ids), steps)
+    out["batched_digest_ms"] = 1e3 * _timed(lambda: b.search_digest(mins, maxs), 1)
     launches0 = L.fkd_kernel_launches()
     b.build(coords, ids)
     b.search_digest(mins, maxs)
-    batched_launches = L.fkd_kernel_launches() - launches0
+    out["kernels_per_batched_run"] = int(L.fkd_kernel_launches() - launches0)
+    out["autotune"] = {"hist_ctas": tune["hist_ctas"], "search_lanes": tune["search_lanes"],
+                       "build_s": tune["build_s"], "search_s": tune["search_s"]}
+    delta = 0.1
+    b.set_mlp(mlp, delta=delta)
+    lc = torch.empty(nq, dtype=torch.int32, device=dev)
+    ld = torch.empty(nq, dtype=torch.int64, device=dev)
+    learned_s = _timed(lambda: b.run(coords, ids, mins, maxs, lc, ld), steps)
+    st = b.learn_stats(reset=True)
+    tab1 = torch.empty_like(tab0)
+    tid1 = torch.empty_like(tid0)
+    _capi.check(L.fkd_batch_get_tables(b._h, P(tab1), P(tid1), _capi.MEM_DEVICE))
+    out["learned_graph_ms"] = 1e3 * learned_s
+    out["learned_build_ms"] = 1e3 * _timed(lambda: b.build(coords, ids), steps)
+    b.learn_stats(reset=True)
+    b.set_mlp(None)
+    runs = steps + 1
+    hit = st["verified"] / st["brackets"] if st["brackets"] else 0.0
+    out["learned"] = {"delta": delta, "brackets_per_run": st["brackets"] // runs, "hit_rate": hit,
+                      "fallback_rate": 1.0 - hit if st["brackets"] else 0.0,
+                      "fallbacks_per_run": st["fallbacks"] // runs}
+    exact = {"learned_tables_equal_plain_batched": bool(torch.equal(tab0.view(torch.int32), tab1.view(torch.int32))
+                                                        and torch.equal(tid0, tid1)),
+             "learned_counts_digests_equal_plain_batched": bool(torch.equal(lc, bc) and torch.equal(ld, bd))}
+    if plain_single:
+        exact["batched_counts_digests_equal_single_event"] = bool(torch.equal(bc, pc) and torch.equal(bd, pd))
+        out["speedup_batched_vs_plain_single_event"] = plain_s / batched_s
+        out["speedup_learned_batched_vs_plain_single_event"] = plain_s / learned_s
+    out["speedup_learned_vs_plain_batched"] = batched_s / learned_s
+    out["exact"] = exact
+    out["batched_mpoints_per_s"] = wb.n_points / batched_s / 1e6
+    out["learned_mpoints_per_s"] = wb.n_points / learned_s / 1e6
+    out["mboxes_per_s"] = nq / batched_s / 1e6
+    del coords, ids, mins, maxs, bc, bd, lc, ld, tab0, tid0, tab1, tid1, pc, pd
+    b.close()
+    torch.cuda.empty_cache()
+    return out
 
-    # learned split: record on the training events, train on the GPU
+
+def batched_report(dev, n_events=4096, steps=3, train_events=2000, cpu=True):
+    """The batched workloads, each a set of independent events in one CUDA graph
+    launch (fkd_batch_run), launch knobs from the autotuner:
+
+      events4096  4,096 3D events, sizes LogNormal(ln 20000, 1.0) clipped to
+                  [1,000, 200,000], 50-500 clusters each, every point a box of
+                  half-width 0.01 on its own event (eval seed 20); against the
+                  plain single-event GPU path (one fkd_build +
+                  fkd_search_digest per event, every event)
+      mixed1024   1,024 events, ~120M points, half 3D / half 4D (16 discrete
+                  layers), every point a box of half-width 0.005 (seed 5)
+
+    each with and without the learned split (MLP trained on the GPU on splits
+    recorded from 2,000 training events of the events4096 generator, seed 10),
+    and the oracle on the host cores on a sample of events."""
+    import fkdtree_b200 as F
+    from fkdtree_b200 import workloads as W
+
     t0 = time.perf_counter()
+    tr = W.event_batch(n_events=train_events, seed=10, queries=False)
     btr = F.Batch.of(tr)
+    import torch
     trc = torch.from_numpy(tr.coords).to(dev)
     tri = torch.from_numpy(tr.ids.view(np.int32)).to(dev)
     x, t = btr.record(trc, tri)
@@ -248,46 +314,33 @@ def batched_report(dev, n_events=4096, steps=3, train_events=2000):
     t0 = time.perf_counter()
     losses = mlp.train(x, t, epochs=60, batch=256, lr=2e-3)
     train_s = time.perf_counter() - t0
-    del btr, trc, tri
-    delta = 0.1
-    b.set_mlp(mlp, delta=delta)
-    lc = torch.empty(nq, dtype=torch.int32, device=dev)
-    ld = torch.empty(nq, dtype=torch.int64, device=dev)
-    learned_s = timed(lambda: b.run(coords, ids, mins, maxs, lc, ld), steps)
-    st = b.learn_stats(reset=True)
-    tab1 = torch.empty_like(tab0)
-    tid1 = torch.empty_like(tid0)
-    _capi.check(L.fkd_batch_get_tables(b._h, P(tab1), P(tid1), _capi.MEM_DEVICE))
-    exact_learned = bool(torch.equal(lc, pc) and torch.equal(ld, pd) and
-                         torch.equal(tab0.view(torch.int32), tab1.view(torch.int32)) and torch.equal(tid0, tid1))
-    learned_build_s = timed(lambda: b.build(coords, ids), steps)
-    b.learn_stats(reset=True)
-    b.set_mlp(None)
-    runs = steps + 1
-    hit = st["verified"] / st["brackets"] if st["brackets"] else 0.0
-    return {
-        "workload": ("events4096: 4,096 3D events, sizes LogNormal(ln 20000, 1.0) clipped to [1000, 200000], "
-                     "50-500 clusters each, every point a box of half-width 0.01 on its own event, seed 20"),
-        "events": wb.n_events, "points": wb.n_points, "boxes": nq, "results": results, "generate_s": gen_s,
-        "plain_single_event_ms": 1e3 * plain_s,
-        "batched_graph_ms": 1e3 * batched_s,
-        "batched_build_ms": 1e3 * build_s, "batched_digest_ms": 1e3 * digest_s,
-        "learned_graph_ms": 1e3 * learned_s, "learned_build_ms": 1e3 * learned_build_s,
-        "speedup_batched_vs_plain": plain_s / batched_s,
-        "speedup_learned_batched_vs_plain": plain_s / learned_s,
-        "batched_mpoints_per_s": wb.n_points / batched_s / 1e6,
-        "batched_mboxes_per_s": nq / batched_s / 1e6,
-        "kernels_per_batched_run": int(batched_launches),
-        "exact": {"batched_counts_digests_equal_plain": exact_batched,
-                  "learned_counts_digests_tables_equal_plain": exact_learned},
-        "autotune": {"hist_ctas": tune["hist_ctas"], "search_lanes": tune["search_lanes"],
-                     "build_s": tune["build_s"], "search_s": tune["search_s"]},
-        "learned": {"delta": delta, "train_events": train_events, "train_seed": 10, "train_rows": int(x.shape[0]),
-                    "record_s": record_s, "train_s": train_s, "loss_first": float(losses[0]),
-                    "loss_last": float(losses[-1]),
-                    "brackets_per_run": st["brackets"] // runs, "hit_rate": hit, "fallback_rate": 1.0 - hit,
-                    "fallbacks_per_run": st["fallbacks"] // runs},
-    }
+    btr.close()
+    del trc, tri
+    rep = {"training": {"events": train_events, "seed": 10, "rows": int(x.shape[0]), "record_s": record_s,
+                        "train_s": train_s, "loss_first": float(losses[0]), "loss_last": float(losses[-1]),
+                        "kernels": "fkd_mlp_train: k_mlp_grad (bf16 mma.sync, fp32 accumulate) + k_mlp_adam"}}
+    t0 = time.perf_counter()
+    wb = W.event_batch(n_events=n_events, seed=20)
+    gen = time.perf_counter() - t0
+    r = _events_run(wb, mlp, dev, steps, plain_single=True)
+    r["workload"] = ("events4096: 4,096 3D events, LogNormal(ln 20000, 1.0) sizes in [1000, 200000], 50-500 "
+                     "clusters, every point a box of half-width 0.01 on its own event, seed 20")
+    r["generate_s"] = gen
+    if cpu:
+        r["cpu_baseline"] = _cpu_events(wb, 64)
+    rep["events4096"] = r
+    del wb
+    t0 = time.perf_counter()
+    wm = W.mixed_events()
+    gen = time.perf_counter() - t0
+    r = _events_run(wm, mlp, dev, steps, plain_single=False)
+    r["workload"] = ("mixed1024: 1,024 events, ~120M points, LogNormal(ln 80000, 1.0) sizes in [5000, 2000000], "
+                     "half 3D / half 4D (16 discrete layers), every point a box of half-width 0.005, seed 5")
+    r["generate_s"] = gen
+    if cpu:
+        r["cpu_baseline"] = _cpu_events(wm, 16)
+    rep["mixed1024"] = r
+    return rep
 
 
 # ------------------------------------------------------------------ our arm
@@ -435,7 +488,7 @@ def run_ours(args):
     del coords, ids, mins, maxs, offsets, counts, out
     torch.cuda.empty_cache()
     if rank == 0 and world == 1 and not args.no_batched:
-        line["batched"] = batched_report(dev, n_events=args.batched_events)
+        line["batched"] = batched_report(dev, n_events=args.batched_events, cpu=not args.no_cpu)
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(ev, args.cpu_queries)
     if rank == 0:
@@ -559,8 +612,42 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def level_times(args):
+    """Device time of every kernel launch of one build of the workload, in
+    launch order (CUDA activity records through torch.profiler)."""
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+
+    from fkdtree_b200 import _capi
+    ev, cfg = make_workload(args.workload, args.queries or 1)
+    dev = torch.device("cuda", 0)
+    L = _capi.lib()
+    P = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+    coords = torch.from_numpy(ev.coords).to(dev)
+    ids = torch.from_numpy(ev.ids.view(np.int32)).to(dev)
+    h = C.c_void_p()
+    _capi.check(L.fkd_create(ev.dim, 0, None, C.byref(h)))
+    for _ in range(3):
+        _capi.check(L.fkd_build(h, P(coords), P(ids), ev.n, _capi.MEM_DEVICE))
+    torch.cuda.synchronize()
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        _capi.check(L.fkd_build(h, P(coords), P(ids), ev.n, _capi.MEM_DEVICE))
+        torch.cuda.synchronize()
+    seq = []
+    for e in prof.events():
+        if e.device_type == torch.autograd.DeviceType.CUDA:
+            us = e.device_time_total if hasattr(e, "device_time_total") else e.cuda_time_total
+            seq.append([e.name.split("(")[0].replace("void ", ""), round(float(us), 1)])
+    _capi.check(L.fkd_destroy(h))
+    print(json.dumps({"workload": cfg["workload"], "build_kernels_us": seq,
+                      "total_us": round(sum(t for _, t in seq), 1)}), flush=True)
+
+
 def main():
     args = parse_args()
+    if args.level_times:
+        level_times(args)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -301,6 +301,11 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
         } else {
           recfail = true;
         }
+      } else if (lane == 0) {
+        // keep counting what the box would have needed: the next call's pools are sized by it
+        atomicAdd(sc.pool_ctr + 1, (unsigned long long)nsing);
+        atomicAdd(sc.pool_ctr, (unsigned long long)nj);
+        atomicAdd(sc.brec_ctr, 1ull);
       }
       relcur += tot;
       nsing = 0u;

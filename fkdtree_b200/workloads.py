@@ -179,3 +179,12 @@ def event_batch(n_events: int = 4096, median: float = 20_000, sigma_log: float =
         maxs = np.empty(0, dtype=np.float32)
     return Batch(dims, pt_off, coord_off, q_off, qcoord_off, coords, ids, mins, maxs,
                  meta=dict(seed=seed, median=median, sigma_log=sigma_log, half_width=half_width))
+
+
+def mixed_events(seed: int = 5, total: int = 120_000_000, queries: bool = True) -> Batch:
+    """Large mixed-dimension batch: 1,024 events totalling about 120M points,
+    sizes log-normal (median 80,000, sigma_log 1.0) clipped to [5,000,
+    2,000,000], half 3D and half 4D (the fourth coordinate one of 16 discrete
+    layers), every point a box of half-width 0.005 on its own event."""
+    return event_batch(n_events=1024, median=80_000, sigma_log=1.0, size_lo=5_000, size_hi=2_000_000,
+                       half_width=0.005, seed=seed, frac_4d=0.5, total=total, queries=queries)
