@@ -134,6 +134,7 @@ struct fkd_batch_s {
   // tuning knobs (fkd_batch_set_param)
   uint32_t hist_ctas = 0;
   uint32_t search_lanes = 0;
+  int subtree = 0;
   // learned split
   fkd_mlp mlp = nullptr;
   float mlp_delta = 0.f;
@@ -256,6 +257,7 @@ fkd_status enqueue_build(fkd_batch b, const float* coords, const uint32_t* ids) 
     bc.pending = b->passflags.as<uint32_t>();
     bc.bnd = p.bnd.as<uint2>();
     bc.bnd_stride = p.plan.maxseg;
+    bc.subtree = b->subtree;
     bc.stream = b->stream;
     memset(&bc.learn, 0, sizeof bc.learn);
     if (b->mlp || b->rec_x) {
@@ -395,6 +397,12 @@ fkd_status fkd_batch_set_param(fkd_batch b, const char* name, int64_t value) {
     b->hist_ctas = (uint32_t)value;
     drop_graph();
     return batch_plan(b);
+  }
+  if (strcmp(name, "subtree") == 0) {
+    if (value < 0 || value > 2) return capi_fail(FKD_ERR_ARG, "subtree must be 0, 1 or 2");
+    b->subtree = (int)value;
+    drop_graph();
+    return FKD_OK;
   }
   if (strcmp(name, "search_lanes") == 0) {
     if (value != 0 && value != 1 && value != 2 && value != 4 && value != 8 && value != 16 && value != 32)

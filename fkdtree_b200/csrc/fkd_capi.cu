@@ -80,6 +80,7 @@ struct fkd_tree_s {
   uint64_t plan_n = ~0ull;
   uint32_t hist_ctas = 0;    // digit-pass CTAs per level (0: four per SM)
   uint32_t search_lanes = 0; // count / digest lanes per box (0: one warp)
+  int subtree = 0;           // subtree kernel: 0 auto, 1 radix select, 2 presorted lists
   fkd_mlp mlp = nullptr;     // learned split (null: plain radix select)
   float mlp_delta = 0.f;
   DevBuf lfeat, lyhat, lrange, lstats, sdig, dids, dnode, bnd, pool_st, pool_len, pool_s, brec, jctr, rflags;
@@ -343,6 +344,7 @@ fkd_status fkd_build(fkd_tree h, const float* coords, const uint32_t* ids, uint6
   bc.pending = h->passflags.as<uint32_t>();
   bc.bnd = h->plan.levels.empty() ? nullptr : h->bnd.as<uint2>();
   bc.bnd_stride = h->plan.maxseg;
+  bc.subtree = h->subtree;
   bc.stream = h->stream;
   memset(&bc.learn, 0, sizeof bc.learn);
   if (h->mlp && !h->plan.levels.empty()) {
@@ -681,6 +683,11 @@ fkd_status fkd_set_param(fkd_tree h, const char* name, int64_t value) {
     if (value != 0 && value != 1 && value != 2 && value != 4 && value != 8 && value != 16 && value != 32)
       return fail(FKD_ERR_ARG, "search_lanes must be 0, 1, 2, 4, 8, 16 or 32");
     h->search_lanes = (uint32_t)value;
+    return FKD_OK;
+  }
+  if (strcmp(name, "subtree") == 0) {
+    if (value < 0 || value > 2) return fail(FKD_ERR_ARG, "subtree must be 0, 1 or 2");
+    h->subtree = (int)value;
     return FKD_OK;
   }
   if (strcmp(name, "search_record") == 0) {

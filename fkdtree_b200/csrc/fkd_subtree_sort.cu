@@ -1,0 +1,436 @@
+// fkd_subtree_sort.cu -- the shared-memory subtree kernel by presorted lists
+// (dims 1-3).
+//
+// Same contract as k_subtree (fkd_build.cu): one CTA finishes every level
+// below a subtree root of at most SUBN points and writes its nodes.  Instead
+// of a radix select per level, the CTA sorts its points once per dimension
+// and then walks the levels with lists:
+//
+//   1. rank the points by id (a sort of (id, slot) keys): element r is the
+//      point with the r-th smallest id, so (coordinate, r) orders exactly as
+//      the reference comparator's (coordinate, id) (FKDTree_cpu.h:246-252);
+//   2. sort (order bits of coordinate c, r) for every dimension c: list_c;
+//   3. level d, split dimension c = d % dim: every segment [ls, ls + m) of
+//      every list holds the same elements, and list_c holds them in split
+//      order, so the pivot is list_c[ls + rank] -- no select at all; the
+//      elements before it go left, after it right.  list_c is already
+//      partitioned; each other list is partitioned stably (a block scan of
+//      left / right flags), which keeps it sorted inside the children.
+//
+// The children's intervals [ls, ls + rank) and [ls + rank + 1, ls + m) are
+// exactly the heap-tree geometry (fkd_common.cuh), and the pivot slot becomes
+// a gap that no later level touches.  Every level costs one flag pass, one
+// scan and one scatter per other list: no digit passes, few barriers.
+#include "fkd_internal.h"
+
+namespace fkd {
+
+#ifdef FKD_PROF
+// Phase cycle counters of the sorted subtree kernel (profiling builds only).
+__device__ unsigned long long g_prof_sorted[8];
+extern "C" __attribute__((visibility("default"))) void fkd_prof_sorted_read(unsigned long long* out) {
+  cudaMemcpyFromSymbol(out, g_prof_sorted, sizeof(g_prof_sorted));
+}
+extern "C" __attribute__((visibility("default"))) void fkd_prof_sorted_reset() {
+  unsigned long long z[8] = {0};
+  cudaMemcpyToSymbol(g_prof_sorted, z, sizeof(z));
+}
+#define XPROF_T(v) const unsigned long long v = clock64()
+#define XPROF_ADD(slot, a, b) \
+  if (threadIdx.x == 0) atomicAdd(&g_prof_sorted[slot], (b) - (a))
+#else
+#define XPROF_T(v)
+#define XPROF_ADD(slot, a, b)
+#endif
+
+namespace {
+
+#ifndef FKD_SORTED_SUBN
+#define FKD_SORTED_SUBN 2048
+#endif
+constexpr int XN = FKD_SORTED_SUBN;  // slots: the largest subtree (a power of two, 512..4096)
+constexpr int XPPT = 4;              // slots per thread
+constexpr int XST = XN / XPPT;       // threads
+constexpr int XW = XST / 32;         // warps
+static_assert(XN >= 512 && XN <= 4096 && (XN & (XN - 1)) == 0, "sorted subtree size");
+constexpr uint16_t GAP = 0xffffu;  // a slot outside every segment (a pivot of an earlier level)
+constexpr uint8_t SL = 0, SR = 1, SP = 2;
+
+template <int DIM>
+struct XCfg {
+  // recs | eofr | lists (DIM x 2 buffers) | seg (2 buffers) | side | scratch (sort keys, later scans)
+  static constexpr size_t recs = (size_t)(DIM + 1) * XN * 4;
+  static constexpr size_t eofr = (size_t)XN * 2;
+  static constexpr size_t lists = (size_t)DIM * 2 * XN * 2;
+  static constexpr size_t seg = 2ull * XN * 2;
+  static constexpr size_t side = XN;
+  static constexpr size_t scratch = 2ull * XN * 8;
+  static constexpr size_t smem = recs + eofr + lists + seg + side + scratch;
+};
+
+__device__ __forceinline__ unsigned long long umin64(unsigned long long a, unsigned long long b) { return a < b ? a : b; }
+__device__ __forceinline__ unsigned long long umax64(unsigned long long a, unsigned long long b) { return a < b ? b : a; }
+
+// Sorts XN 64-bit keys (ascending) with the whole CTA: bitonic sort of 128
+// keys per warp in registers, then five merge-path rounds through shared
+// memory.  Returns the buffer (a or b) that holds the result.
+__device__ unsigned long long* cta_sort(unsigned long long* a, unsigned long long* b) {
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  unsigned long long v[4];
+  unsigned long long* wbase = a + warp * 128u;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) v[i] = wbase[lane * 4u + i];
+#pragma unroll
+  for (uint32_t k = 2; k <= 128; k <<= 1) {
+#pragma unroll
+    for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+      if (j >= 4) {
+        const uint32_t lm = j >> 2;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const uint32_t idx = lane * 4u + i;
+          const unsigned long long o = __shfl_xor_sync(0xffffffffu, v[i], lm);
+          const bool lower = (idx & j) == 0u;
+          const bool asc = (idx & k) == 0u;
+          v[i] = (lower == asc) ? umin64(v[i], o) : umax64(v[i], o);
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          if ((i & (int)j) == 0) {
+            const uint32_t idx = lane * 4u + i;
+            const bool asc = (idx & k) == 0u;
+            const unsigned long long x = v[i], y = v[i ^ (int)j];
+            if ((x > y) == asc) {
+              v[i] = y;
+              v[i ^ (int)j] = x;
+            }
+          }
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) wbase[lane * 4u + i] = v[i];
+  unsigned long long* src = a;
+  unsigned long long* dst = b;
+  for (uint32_t s = 128; s < (uint32_t)XN; s <<= 1) {
+    __syncthreads();
+    const uint32_t og = threadIdx.x * XPPT;  // first of this thread's outputs
+    const uint32_t pair = og / (2u * s);
+    const uint32_t o = og - pair * 2u * s;
+    const unsigned long long* A = src + pair * 2u * s;
+    const unsigned long long* B = A + s;
+    uint32_t lo = o > s ? o - s : 0u, hi = o < s ? o : s;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (A[mid] <= B[o - 1u - mid])  // ties: A first, as in the sequential merge below
+        lo = mid + 1u;
+      else
+        hi = mid;
+    }
+    uint32_t i = lo, jb = o - lo;
+    unsigned long long* D = dst + pair * 2u * s + o;
+#pragma unroll
+    for (int q = 0; q < XPPT; ++q) {
+      // an exhausted run reads as the padding key ~0 (never past its end)
+      const unsigned long long va = i < s ? A[i] : ~0ull;
+      const unsigned long long vb = jb < s ? B[jb] : ~0ull;
+      const bool takeA = va < vb || (va == vb && i < s);
+      D[q] = takeA ? va : vb;
+      if (takeA)
+        ++i;
+      else
+        ++jb;
+    }
+    unsigned long long* t = src;
+    src = dst;
+    dst = t;
+  }
+  __syncthreads();
+  return src;
+}
+
+// Exclusive scan of XN uint2 values, slots XPPT*tid .. XPPT*tid + XPPT - 1
+// per thread (in: per-slot values; out: written to sc).  Returns the totals.
+__device__ uint2 cta_scan2(const uint2 (&val)[XPPT], uint2* sc, uint2* wtot) {
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  uint32_t ax = 0u, ay = 0u;
+#pragma unroll
+  for (int k = 0; k < XPPT; ++k) {
+    ax += val[k].x;
+    ay += val[k].y;
+  }
+  uint32_t ix = ax, iy = ay;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t yx = __shfl_up_sync(0xffffffffu, ix, o);
+    const uint32_t yy = __shfl_up_sync(0xffffffffu, iy, o);
+    if (lane >= (uint32_t)o) {
+      ix += yx;
+      iy += yy;
+    }
+  }
+  if (lane == 31u) wtot[warp] = make_uint2(ix, iy);
+  __syncthreads();
+  if (warp == 0) {
+    uint2 w = lane < (uint32_t)XW ? wtot[lane] : make_uint2(0u, 0u);
+    uint32_t sx = w.x, sy = w.y;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t yx = __shfl_up_sync(0xffffffffu, sx, o);
+      const uint32_t yy = __shfl_up_sync(0xffffffffu, sy, o);
+      if (lane >= (uint32_t)o) {
+        sx += yx;
+        sy += yy;
+      }
+    }
+    if (lane < (uint32_t)XW) wtot[lane] = make_uint2(sx - w.x, sy - w.y);  // exclusive warp bases
+    if (lane == 31u) wtot[32] = make_uint2(sx, sy);
+  }
+  __syncthreads();
+  const uint2 wb = wtot[warp];
+  uint32_t rx = wb.x + ix - ax, ry = wb.y + iy - ay;
+#pragma unroll
+  for (int k = 0; k < XPPT; ++k) {
+    sc[threadIdx.x * XPPT + k] = make_uint2(rx, ry);
+    rx += val[k].x;
+    ry += val[k].y;
+  }
+  const uint2 tot = wtot[32];
+  return tot;
+}
+
+// Segment (d, t) of the event in subtree-local slots: start, length, rank.
+__device__ __forceinline__ void seg_local(const Geom& g, uint32_t d, uint32_t t, uint32_t base, uint32_t& ls,
+                                          uint32_t& m, uint32_t& k) {
+  const uint32_t sh = g.H - d;
+  const uint32_t W = 1u << sh;
+  const uint32_t tw = t << sh;
+  ls = tw + min(g.M, tw) - base;
+  m = W - 1u + (g.M > tw ? min(g.M - tw, W) : 0u);
+  if (sh == 0u) {
+    k = 0u;
+  } else {
+    const uint32_t Wh = W >> 1;
+    k = Wh - 1u + (g.M > tw ? min(g.M - tw, Wh) : 0u);
+  }
+}
+
+}  // namespace
+
+template <int DIM>
+__global__ void __launch_bounds__(XST, 4096 / XN) k_subtree_sorted(const EvDesc* __restrict__ evs,
+                                                           const uint2* __restrict__ subs, CSoA src_in, CSoA src_b0,
+                                                           CSoA src_b1, Table tab_all, uint32_t* __restrict__ err) {
+  using Cfg = XCfg<DIM>;
+  extern __shared__ __align__(16) unsigned char smem[];
+  uint32_t* recs = (uint32_t*)smem;                                 // [DIM + 1][XN], original slot order
+  uint16_t* eofr = (uint16_t*)(smem + Cfg::recs);                   // id rank -> slot
+  uint16_t* lists = (uint16_t*)(smem + Cfg::recs + Cfg::eofr);      // [DIM][2][XN] id ranks
+  uint16_t* segb = (uint16_t*)(smem + Cfg::recs + Cfg::eofr + Cfg::lists);  // [2][XN]
+  uint8_t* side = smem + Cfg::recs + Cfg::eofr + Cfg::lists + Cfg::seg;
+  unsigned long long* keys = (unsigned long long*)(smem + Cfg::recs + Cfg::eofr + Cfg::lists + Cfg::seg + Cfg::side);
+  uint2* scan = (uint2*)keys;  // after the sorts
+  __shared__ uint2 wtot[33];  // per-warp scan totals (XW <= 32)
+
+  const uint2 sb = subs[blockIdx.x];
+  const EvDesc ev = evs[sb.x];
+  const Geom g = ev.g;
+  const uint32_t d0 = ev.d0;
+  const uint32_t s0 = sb.y;
+  const CSoA src_all = d0 == 0u ? src_in : ((d0 & 1u) ? src_b0 : src_b1);
+  const CSoA src{src_all.base + ev.base, src_all.ids + ev.base, src_all.stride};
+  const Table tab{tab_all.nodes + ev.base, tab_all.ids + ev.base};
+  const uint32_t base = seg_start(g, d0, s0);
+  const uint32_t nloc = seg_len(g, d0, s0);
+  if (nloc > (uint32_t)XN) {
+    if (threadIdx.x == 0) atomicOr(err, ERRB_INTERNAL);
+    return;
+  }
+  // 1. records, and the id keys
+  bool nan = false;
+  for (uint32_t p = threadIdx.x; p < (uint32_t)XN; p += XST) {
+    if (p < nloc) {
+#pragma unroll
+      for (int w = 0; w < DIM; ++w) {
+        const uint32_t v = __ldcs(src.base + (uint64_t)w * src.stride + base + p);
+        nan |= is_nan_bits(v);
+        recs[w * XN + p] = v;
+      }
+      const uint32_t id = __ldcs(src.ids + base + p);
+      recs[DIM * XN + p] = id;
+      keys[p] = ((unsigned long long)id << 12) | p;
+    } else {
+      keys[p] = ~0ull;
+    }
+  }
+  if (nan) atomicOr(err, ERRB_NAN);
+  __syncthreads();
+  XPROF_T(tp0);
+  {
+    const unsigned long long* sk = cta_sort(keys, keys + XN);
+    for (uint32_t r = threadIdx.x; r < nloc; r += XST) eofr[r] = (uint16_t)(sk[r] & 0xfffu);
+    __syncthreads();
+  }
+  XPROF_T(tp1);
+  // 2. one sorted list per dimension: keys (order bits, id rank)
+#pragma unroll 1
+  for (int c = 0; c < DIM; ++c) {
+    for (uint32_t r = threadIdx.x; r < (uint32_t)XN; r += XST)
+      keys[r] = r < nloc ? (((unsigned long long)mono_bits(recs[c * XN + eofr[r]]) << 12) | r) : ~0ull;
+    __syncthreads();
+    const unsigned long long* sk = cta_sort(keys, keys + XN);
+    uint16_t* lc = lists + (size_t)c * 2 * XN;
+    for (uint32_t p = threadIdx.x; p < nloc; p += XST) lc[p] = (uint16_t)(sk[p] & 0xfffu);
+    __syncthreads();
+  }
+  XPROF_T(tp2);
+  // 3. levels
+  int cur[4] = {0, 0, 0, 0};  // which buffer of each list is current
+  int sbuf = 0;
+  for (uint32_t p = threadIdx.x; p < (uint32_t)XN; p += XST) segb[p] = p < nloc ? 0u : GAP;
+  __syncthreads();
+  for (uint32_t d = d0; d <= g.H; ++d) {
+    const uint32_t j = d - d0;
+    const uint32_t t0 = s0 << j;
+    const uint32_t c = d % DIM;
+    const uint16_t* lc = lists + ((size_t)c * 2 + cur[c]) * XN;
+    const uint16_t* sg = segb + (size_t)sbuf * XN;
+    uint16_t* sgn = segb + (size_t)(sbuf ^ 1) * XN;
+    // (a) pivots and sides, from the split dimension's list
+#pragma unroll
+    for (int q = 0; q < XPPT; ++q) {
+      const uint32_t p = threadIdx.x * XPPT + q;
+      const uint16_t u = sg[p];
+      if (u == GAP) {
+        sgn[p] = GAP;
+        continue;
+      }
+      uint32_t ls, m, k;
+      seg_local(g, d, t0 + u, base, ls, m, k);
+      if (p < ls || p >= ls + m) {  // a slot outside its segment: broken invariant
+        atomicOr(err, ERRB_INTERNAL);
+        sgn[p] = GAP;
+        continue;
+      }
+      const uint32_t r = lc[p];
+      const uint32_t pv = ls + k;
+      if (p == pv) {
+        side[r] = SP;
+        sgn[p] = GAP;
+        const uint32_t e = eofr[r];
+        uint32_t rec[DIM + 1];
+#pragma unroll
+        for (int w = 0; w <= DIM; ++w) rec[w] = recs[w * XN + e];
+        uint4 v;
+        v.x = rec[0];
+        v.y = DIM > 1 ? rec[1] : 0u;
+        v.z = DIM > 2 ? rec[2] : 0u;
+        v.w = rec[DIM];
+        const uint32_t node = (1u << d) - 1u + t0 + u;
+        tab.nodes[node] = v;
+        tab.ids[node] = rec[DIM];
+      } else {
+        side[r] = p < pv ? SL : SR;
+        sgn[p] = (uint16_t)(2u * u + (p < pv ? 0u : 1u));
+      }
+    }
+    if (d == g.H || DIM == 1) {
+      // the last level, or a single list: the split list is the whole partition
+      __syncthreads();
+      sbuf ^= 1;
+      continue;
+    }
+    __syncthreads();
+    // (b) stable partition of the other lists: flags (left | right << 16), scan
+    uint2 val[XPPT];
+    uint32_t ra[XPPT], rb[XPPT];
+    const uint32_t o1 = (c + 1u) % DIM, o2 = (c + 2u) % DIM;
+    const uint16_t* l1 = lists + ((size_t)o1 * 2 + cur[o1]) * XN;
+    const uint16_t* l2 = lists + ((size_t)o2 * 2 + cur[o2]) * XN;
+#pragma unroll
+    for (int q = 0; q < XPPT; ++q) {
+      const uint32_t p = threadIdx.x * XPPT + q;
+      const bool live = sg[p] != GAP;
+      ra[q] = live ? l1[p] : 0u;
+      rb[q] = (live && DIM > 2) ? l2[p] : 0u;
+      const uint8_t s1 = live ? side[ra[q]] : SP;
+      const uint8_t s2 = (live && DIM > 2) ? side[rb[q]] : SP;
+      val[q].x = (s1 == SL ? 1u : 0u) | (s1 == SR ? 0x10000u : 0u);
+      val[q].y = (s2 == SL ? 1u : 0u) | (s2 == SR ? 0x10000u : 0u);
+    }
+    cta_scan2(val, scan, wtot);
+    __syncthreads();
+    // (c) scatter into the other buffers
+    uint16_t* n1 = lists + ((size_t)o1 * 2 + (cur[o1] ^ 1)) * XN;
+    uint16_t* n2 = lists + ((size_t)o2 * 2 + (cur[o2] ^ 1)) * XN;
+#pragma unroll
+    for (int q = 0; q < XPPT; ++q) {
+      const uint32_t p = threadIdx.x * XPPT + q;
+      const uint16_t u = sg[p];
+      if (u == GAP) continue;
+      uint32_t ls, m, k;
+      seg_local(g, d, t0 + u, base, ls, m, k);
+      const uint2 at = scan[p], st = scan[ls];
+      // destinations stay inside the segment's child; anything else is a broken invariant
+      uint32_t q1 = 0xffffffffu, q2 = 0xffffffffu;
+      if (val[q].x & 0xffffu)
+        q1 = ls + ((at.x & 0xffffu) - (st.x & 0xffffu));
+      else if (val[q].x)
+        q1 = ls + k + 1u + ((at.x >> 16) - (st.x >> 16));
+      if (DIM > 2) {
+        if (val[q].y & 0xffffu)
+          q2 = ls + ((at.y & 0xffffu) - (st.y & 0xffffu));
+        else if (val[q].y)
+          q2 = ls + k + 1u + ((at.y >> 16) - (st.y >> 16));
+      }
+      if (q1 != 0xffffffffu) {
+        if (q1 < ls + m)
+          n1[q1] = (uint16_t)ra[q];
+        else
+          atomicOr(err, ERRB_INTERNAL);
+      }
+      if (q2 != 0xffffffffu) {
+        if (q2 < ls + m)
+          n2[q2] = (uint16_t)rb[q];
+        else
+          atomicOr(err, ERRB_INTERNAL);
+      }
+    }
+    cur[o1] ^= 1;
+    if (DIM > 2) cur[o2] ^= 1;
+    sbuf ^= 1;
+    __syncthreads();
+  }
+  XPROF_T(tp3);
+  XPROF_ADD(0, tp0, tp1);
+  XPROF_ADD(1, tp1, tp2);
+  XPROF_ADD(2, tp2, tp3);
+}
+
+int sorted_sub_capacity() { return XN; }
+
+template <int DIM>
+static cudaError_t run_sorted(const EvDesc* evs, const uint2* subs, uint32_t nsub, CSoA in, CSoA b0, CSoA b1,
+                              Table tab, uint32_t* err, cudaStream_t stream) {
+  const size_t smem = XCfg<DIM>::smem;
+  cudaError_t e = cudaFuncSetAttribute(k_subtree_sorted<DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  k_subtree_sorted<DIM><<<nsub, XST, smem, stream>>>(evs, subs, in, b0, b1, tab, err);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_subtree_sorted(const EvDesc* evs, const uint2* subs, uint32_t nsub, CSoA in, CSoA b0, CSoA b1,
+                                  Table tab, uint32_t* err, int dim, cudaStream_t stream) {
+  if (nsub == 0) return cudaSuccess;
+  switch (dim) {
+    case 1: return run_sorted<1>(evs, subs, nsub, in, b0, b1, tab, err, stream);
+    case 2: return run_sorted<2>(evs, subs, nsub, in, b0, b1, tab, err, stream);
+    case 3: return run_sorted<3>(evs, subs, nsub, in, b0, b1, tab, err, stream);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace fkd

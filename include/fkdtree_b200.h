@@ -202,6 +202,8 @@ FKD_API fkd_status fkd_batch_destroy(fkd_batch b);
  *   "hist_ctas"    digit-pass CTAs per level (0 = four per SM); re-plans the batch
  *   "search_lanes" lanes per box of the count / digest search: 1, 2, 4, 8, 16
  *                  or 32 (0 = 32, one warp per box)
+ *   "subtree"      shared-memory subtree kernel: 0 auto (presorted lists for
+ *                  dims 1-3, radix select for dim 4), 1 radix select, 2 lists
  * No reference counterpart (the reference has one fixed launch shape). */
 FKD_API fkd_status fkd_batch_set_param(fkd_batch b, const char* name, int64_t value);
 /* Builds every event; the tables equal one FKDTree_CPU::build per event. */

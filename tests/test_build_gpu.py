@@ -114,3 +114,25 @@ def test_large_clustered_build_properties(cuda):
         else:
             assert np.all((chv > pv) | ((chv == pv) & (tid[ch] > tid[p])))
     assert_same((tab, tid), O.build(ev.coords, ev.ids))
+
+
+@pytest.mark.parametrize("subtree", [1, 2])
+@pytest.mark.parametrize("dim,kind", [(1, "uniform"), (2, "uniform"), (3, "uniform"), (3, "grid"), (2, "grid"),
+                                      (3, "signed_zero"), (3, "sparse_ids")])
+def test_subtree_kernels_agree(cuda, subtree, dim, kind):
+    """Both shared-memory subtree kernels (radix select, presorted lists) give
+    the oracle's tables, on ties, signed zeros, and ids far apart."""
+    rng = np.random.default_rng(31 + dim)
+    n = 50_000
+    c = rng.random((dim, n), dtype=np.float32)
+    ids = rng.permutation(n).astype(np.uint32)
+    if kind == "grid":
+        c = rng.integers(0, 3, (dim, n)).astype(np.float32)
+    elif kind == "signed_zero":
+        c[:, : n // 3] = np.where(rng.random((dim, n // 3)) < 0.5, np.float32(-0.0), np.float32(0.0))
+    elif kind == "sparse_ids":
+        ids = rng.choice(np.iinfo(np.uint32).max, n, replace=False).astype(np.uint32)
+    t = F.FKDTree(c, ids).set_param("subtree", subtree).build()
+    got = t.tables()
+    t.close()
+    assert_same(got, O.build(c, ids), f"subtree={subtree} dim={dim} {kind}")
