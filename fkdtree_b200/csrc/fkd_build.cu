@@ -489,6 +489,119 @@ __global__ void __launch_bounds__(GT, 4) k_partition(uint32_t d, const EvDesc* _
   }
 }
 
+// ------------------------------------------------------- small-segment select
+//
+// For levels whose segments all hold at most SEL_MAX points, one CTA selects
+// a whole segment: its split coordinate is loaded into shared memory once and
+// every digit pass (value bits, then id bits for points that tie on the
+// value) runs there -- one launch per level instead of a digit pass launch
+// per 11 bits with a global histogram flush each.  Same digits and the same
+// final SegSel as the k_hist passes, so k_partition is unchanged.
+constexpr int SEL_MAX = 32768;
+constexpr int SELT = 512;  // threads
+constexpr int SELB = 4;    // bins per thread (2,048 bins)
+
+template <int DIM>
+__global__ void __launch_bounds__(SELT) k_select_small(uint32_t d, const EvDesc* __restrict__ evs,
+                                                       const uint2* __restrict__ segs, CSoA src,
+                                                       SegSel* __restrict__ sel, uint32_t* __restrict__ err) {
+  extern __shared__ uint32_t vals[];  // mono bits of the segment's split coordinate
+  __shared__ uint32_t hist[SELT * SELB];
+  __shared__ uint32_t wsum[SELT / 32];
+  __shared__ unsigned long long s_prefix;
+  __shared__ uint32_t s_bits, s_krem, s_cnt;
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint32_t s = blockIdx.x;
+  if (sel[s].done) return;
+  const uint2 sd = segs[s];
+  const Geom eg = evs[sd.x].g;
+  const uint32_t start = evs[sd.x].base + seg_start(eg, d, sd.y);
+  const uint32_t len = seg_len(eg, d, sd.y);
+  if (len > (uint32_t)SEL_MAX) {
+    if (threadIdx.x == 0) atomicOr(err, ERRB_INTERNAL);
+    return;
+  }
+  const uint32_t c = d % DIM;
+  const uint32_t* X = src.base + (uint64_t)c * src.stride + start;
+  for (uint32_t p = threadIdx.x; p < len; p += SELT) vals[p] = mono_bits(__ldcs(X + p));
+  if (threadIdx.x == 0) {
+    s_prefix = sel[s].prefix;
+    s_bits = sel[s].bits;
+    s_krem = sel[s].krem;
+    s_cnt = sel[s].cnt;
+  }
+  __syncthreads();
+  for (int guard = 0; guard < 8; ++guard) {
+    const uint32_t bits = s_bits, cnt = s_cnt, krem = s_krem;
+    const unsigned long long prefix = s_prefix;
+    if (bits >= 64u || cnt <= 1u) break;
+    const uint32_t w = (32u - (bits & 31u)) < 11u ? (32u - (bits & 31u)) : 11u;
+    const uint32_t nb = 1u << w;
+    for (uint32_t i = threadIdx.x; i < nb; i += SELT) hist[i] = 0u;
+    __syncthreads();
+    if (bits < 32u) {
+      const uint32_t vpre = (uint32_t)prefix;
+      for (uint32_t p = threadIdx.x; p < len; p += SELT) {
+        const uint32_t v = vals[p];
+        if (bits == 0u || (v >> (32u - bits)) == vpre) atomicAdd(&hist[(v >> (32u - bits - w)) & (nb - 1u)], 1u);
+      }
+    } else {
+      // the value is fixed: the id digits of the points holding it
+      const uint32_t vpre = (uint32_t)(prefix >> (bits - 32u));
+      const uint32_t ib = bits - 32u;
+      const uint32_t ipre = ib ? (uint32_t)(prefix & ((1ull << ib) - 1ull)) : 0u;
+      for (uint32_t p = threadIdx.x; p < len; p += SELT) {
+        if (vals[p] != vpre) continue;
+        const uint32_t id = __ldcs(src.ids + start + p);
+        if (ib != 0u && (id >> (32u - ib)) != ipre) continue;
+        atomicAdd(&hist[(id >> (32u - ib - w)) & (nb - 1u)], 1u);
+      }
+    }
+    __syncthreads();
+    // the digit holding rank krem: block scan of SELB bins per thread
+    uint32_t h[SELB], mine = 0u;
+#pragma unroll
+    for (int k = 0; k < SELB; ++k) {
+      const uint32_t b = threadIdx.x * SELB + k;
+      h[k] = b < nb ? hist[b] : 0u;
+      mine += h[k];
+    }
+    uint32_t incl = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= (uint32_t)o) incl += y;
+    }
+    if (lane == 31u) wsum[warp] = incl;
+    __syncthreads();
+    uint32_t cum = incl - mine;
+    for (uint32_t k = 0; k < warp; ++k) cum += wsum[k];
+    if (krem >= cum && krem < cum + mine) {
+#pragma unroll
+      for (int k = 0; k < SELB; ++k) {
+        const uint32_t b = threadIdx.x * SELB + k;
+        if (b < nb && krem >= cum && krem < cum + h[k]) {
+          s_prefix = (bits == 0u ? 0ull : (prefix << w)) | b;
+          s_bits = bits + w;
+          s_krem = krem - cum;
+          s_cnt = h[k];
+        }
+        cum += h[k];
+      }
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    SegSel* p = &sel[s];
+    p->prefix = s_prefix;
+    p->bits = s_bits;
+    p->krem = s_krem;
+    p->cnt = s_cnt;
+    p->done = 1u;
+    if (s_cnt == 0u) atomicOr(err, ERRB_INTERNAL);
+  }
+}
+
 // ---------------------------------------------------------------- subtree
 
 constexpr int ST = 1024;         // threads of the subtree kernel
@@ -937,18 +1050,26 @@ static cudaError_t run_build(BuildCtx& bc) {
                                                             bnd_out, lp.child);
     count_launches(1);
     const LearnCtx& lc = bc.learn;
-    if (lc.params || lc.rec_x) {
+    // levels of small segments: one CTA selects a whole segment (no learned bracket there)
+    const bool small = lp.maxlen <= (uint32_t)SEL_MAX && bc.small_select;
+    if (lc.rec_x || (lc.params && !small)) {
       cudaError_t e = launch_features(d, bc.evs, lp.segs, lp.nseg, src, DIM, lc.feat, lc.range, bc.stream);
       if (e != cudaSuccess) return e;
     }
-    if (lc.params) {
+    if (small) {
+      const size_t sm = (size_t)lp.maxlen * sizeof(uint32_t);
+      cudaError_t e = cudaFuncSetAttribute(k_select_small<DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      if (e != cudaSuccess) return e;
+      k_select_small<DIM><<<lp.nseg, SELT, sm, bc.stream>>>(d, bc.evs, lp.segs, src, bc.sel, bc.err);
+      count_launches(1);
+    } else if (lc.params) {
       cudaError_t e = mlp_infer(lc.params, lc.feat, lp.nseg, lc.yhat, bc.stream);
       if (e == cudaSuccess)
         e = launch_bracket(d, bc.evs, lp.segs, lp.nseg, lc.yhat, lc.range, lc.delta, bc.sel, lc.stats, bc.stream);
       if (e != cudaSuccess) return e;
     }
     // the plain select needs at most 6 passes; a failed prediction costs one more
-    const int passes = lc.params ? RPASSES : RPASSES - 1;
+    const int passes = small ? 0 : (lc.params ? RPASSES : RPASSES - 1);
     for (int pass = 0; pass < passes; ++pass) {
       k_hist<DIM><<<lp.nhtile, GT, 0, bc.stream>>>(d, bc.evs, lp.segs, lp.htiles, lp.hts, src, bc.sel, bc.ghist,
                                                     bc.pending + pass, bc.pending + pass + 1, bc.err,

@@ -81,6 +81,7 @@ struct fkd_tree_s {
   uint32_t hist_ctas = 0;    // digit-pass CTAs per level (0: four per SM)
   uint32_t search_lanes = 0; // count / digest lanes per box (0: one warp)
   int subtree = 0;           // subtree kernel: 0 auto, 1 radix select, 2 presorted lists
+  bool small_select = true;  // one CTA per segment on levels of small segments
   fkd_mlp mlp = nullptr;     // learned split (null: plain radix select)
   float mlp_delta = 0.f;
   DevBuf lfeat, lyhat, lrange, lstats, sdig, dids, dnode, bnd, pool_st, pool_len, pool_s, brec, jctr, rflags;
@@ -345,6 +346,7 @@ fkd_status fkd_build(fkd_tree h, const float* coords, const uint32_t* ids, uint6
   bc.bnd = h->plan.levels.empty() ? nullptr : h->bnd.as<uint2>();
   bc.bnd_stride = h->plan.maxseg;
   bc.subtree = h->subtree;
+  bc.small_select = h->small_select;
   bc.stream = h->stream;
   memset(&bc.learn, 0, sizeof bc.learn);
   if (h->mlp && !h->plan.levels.empty()) {
@@ -683,6 +685,11 @@ fkd_status fkd_set_param(fkd_tree h, const char* name, int64_t value) {
     if (value != 0 && value != 1 && value != 2 && value != 4 && value != 8 && value != 16 && value != 32)
       return fail(FKD_ERR_ARG, "search_lanes must be 0, 1, 2, 4, 8, 16 or 32");
     h->search_lanes = (uint32_t)value;
+    return FKD_OK;
+  }
+  if (strcmp(name, "small_select") == 0) {
+    if (value != 0 && value != 1) return fail(FKD_ERR_ARG, "small_select must be 0 or 1");
+    h->small_select = value != 0;
     return FKD_OK;
   }
   if (strcmp(name, "subtree") == 0) {

@@ -71,6 +71,7 @@ struct LevelPlan {
   const uint2* ptiles;  // partition CTA -> (segment, tile)
   uint32_t nptile;
   const uint32_t* child;  // per segment: its left child's index in the next level (~0u: not a global segment)
+  uint32_t maxlen;        // longest segment of the level
 };
 
 struct BuildCtx {
@@ -93,6 +94,7 @@ struct BuildCtx {
   LearnCtx learn;
   cudaEvent_t ev_sub = nullptr;  // optional: recorded right before the subtree kernel
   int subtree = 0;               // shared-memory subtree kernel: 0 auto, 1 radix select, 2 presorted lists
+  bool small_select = true;      // levels of small segments select with one CTA per segment
 };
 
 // Number of levels split by the global kernels (the first level whose

@@ -50,6 +50,7 @@ void plan_build(const uint32_t* n_ev, const uint32_t* base_ev, uint32_t nev, int
         lv.segs.push_back(make_uint2(e, t));
         lv.child.push_back(d.d0 > L + 1 ? first[L + 1][e] + 2u * t : ~0u);
         total += seg_len(d.g, L, t);
+        lv.maxlen = std::max<uint32_t>(lv.maxlen, seg_len(d.g, L, t));
       }
     }
     out.maxseg = std::max<uint32_t>(out.maxseg, (uint32_t)lv.segs.size());
@@ -121,6 +122,7 @@ cudaError_t PlanDev::upload(const PlanHost& h, cudaStream_t stream) {
     lp.ptiles = (const uint2*)(d + at[4 * L + 2]);
     lp.nptile = (uint32_t)h.levels[L].ptiles.size();
     lp.child = (const uint32_t*)(d + at[4 * L + 3]);
+    lp.maxlen = h.levels[L].maxlen;
   }
   maxseg = h.maxseg;
   return cudaSuccess;

@@ -12,6 +12,7 @@ struct PlanLevel {
   std::vector<uint2> segs, htiles, ptiles;
   std::vector<uint32_t> child;  // per segment: index of its left child in the next level's list (~0u: none)
   uint32_t hts = HIST_STEP;
+  uint32_t maxlen = 0;  // longest segment of the level
 };
 
 struct PlanHost {

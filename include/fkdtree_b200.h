@@ -164,6 +164,8 @@ FKD_API fkd_status fkd_sync(fkd_tree h);
 /* Tuning knobs of one tree, same names and ranges as fkd_batch_set_param
  * ("hist_ctas" takes effect at the next build; "search_lanes" applies to
  * fkd_search_count / fkd_search_digest), plus
+ *   "small_select"  (0/1, default 1): global levels whose segments are small
+ *                   select each segment with one CTA in shared memory
  *   "search_record" (0/1, default 1): fkd_search's count pass records every
  *                   box's result so that the write needs no second traversal
  *   "search_pool"   entries of the record pools (0, the default: sized by the
