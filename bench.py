@@ -45,6 +45,13 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "build Mpoints/s + box queries/s, learned/batched vs plain GPU, exact results"
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of the recording
+# count pass + k_expand per result id, from one ncu --set full capture of the
+# same search with 65,536 boxes (2.84e8 results: 2.72 GB), scaled to a full
+# search by its results:
+#   ncu --set full --clock-control none -k regex:k_expand -s 4 -c 1 python bench.py --steps 1 --warmup 4 \
+#       --queries 65536 --no-e2e --no-cpu --no-batched   (and the same for k_search<3,0,1>)
+SEARCH_DRAM_BYTES_PER_RESULT = 9.57
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 
@@ -470,7 +477,10 @@ def run_ours(args):
               key=lambda k: kern[k]["ms"])
     roof = {"bound": "hbm", "kernel": dom, "achieved": kern[dom]["gbs"], "peak": peak, "unit": "GB/s",
             "frac": kern[dom]["gbs"] / peak, "peak_kind": f"{peak_kind} (copy bandwidth, MEASURED_PEAKS.json)",
-            "traffic": None, "algorithmic_bytes_per_launch": kern[dom]["algorithmic_bytes"],
+            "traffic": (SEARCH_DRAM_BYTES_PER_RESULT * results
+                        if dom.startswith("search") and args.workload == "clustered16m" else None),
+            "traffic_note": "ncu DRAM bytes of a 65,536-box capture, scaled by results",
+            "algorithmic_bytes_per_launch": kern[dom]["algorithmic_bytes"],
             "launch_ms": kern[dom]["ms"],
             "build_frac": bb / kms[2] / 1e6 / peak if kms[2] > 0 else None}
 

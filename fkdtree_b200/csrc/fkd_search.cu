@@ -360,10 +360,17 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
       __syncwarp();
       top = base;
       bool emit = false, pushL = false, pushR = false, contL = false, contR = false;
-      uint32_t maskL = 0u, maskR = 0u, idv = 0u;
+      uint32_t maskL = 0u, maskR = 0u, idv = 0u, cnext = 0u;
       if (have) {
-        const uint32_t dep = floor_log2_u32(i + 1u);
-        const uint32_t c = dep % DIM;
+        // 3D: the node's split dimension rides in the top bits of its mask byte
+        uint32_t c;
+        if (DIM == 3) {
+          c = mask >> 6;
+          mask &= 0x3fu;
+        } else {
+          c = floor_log2_u32(i + 1u) % DIM;
+        }
+        cnext = c + 1u == (uint32_t)DIM ? 0u : c + 1u;
         const uint4 nd = __ldg(tab.nodes + i);
         const float x0 = __uint_as_float(nd.x), x1 = __uint_as_float(nd.y), x2 = __uint_as_float(nd.z),
                     x3 = __uint_as_float(nd.w);
@@ -505,14 +512,15 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
         break;
       }
       uint32_t p = (uint32_t)top + __popc(bpl & lt) + __popc(bpr & lt);
+      const uint32_t ctag = DIM == 3 ? cnext << 6 : 0u;
       if (pushL) {
         stk_node[p] = 2u * i + 1u;
-        stk_mask[p] = (uint8_t)maskL;
+        stk_mask[p] = (uint8_t)(maskL | ctag);
         ++p;
       }
       if (pushR) {
         stk_node[p] = 2u * i + 2u;
-        stk_mask[p] = (uint8_t)maskR;
+        stk_mask[p] = (uint8_t)(maskR | ctag);
       }
       top += (int)tot;
       __syncwarp();
