@@ -55,7 +55,7 @@ extern "C" __attribute__((visibility("default"))) void fkd_prof_reset() {
 // ---------------------------------------------------------------- global
 
 constexpr int GT = 256;            // threads of the global-level kernels
-constexpr int PIPT = 4;            // records per thread (partition)
+constexpr int PIPT = FKD_PART_PIPT;  // records per thread (partition)
 constexpr int PTILE = GT * PIPT;
 static_assert(PTILE == (int)PART_TILE, "partition tile");
 constexpr int GWARPS = GT / 32;
@@ -309,7 +309,7 @@ __device__ __forceinline__ uint32_t pick_coord(const uint32_t* rec, uint32_t c) 
 // Streams every record of depth-d segments once: records below the pivot go
 // to [start, start + rank), the pivot to the table, the rest above it.
 template <int DIM>
-__global__ void __launch_bounds__(GT, 4) k_partition(uint32_t d, const EvDesc* __restrict__ evs,
+__global__ void __launch_bounds__(GT, PIPT <= 4 ? 4 : 3) k_partition(uint32_t d, const EvDesc* __restrict__ evs,
                                                      const uint2* __restrict__ segs, const uint2* __restrict__ tiles,
                                                      CSoA src, SoA dst, SegSel* __restrict__ sel, Table tab,
                                                      uint32_t* __restrict__ err, uint2* __restrict__ bnd_out,

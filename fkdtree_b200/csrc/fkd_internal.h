@@ -103,7 +103,10 @@ uint32_t build_global_levels(uint32_t n, int dim);
 int sub_capacity(int dim);
 int sorted_sub_capacity();  // largest subtree of the presorted-list kernel (dims 1-3)
 constexpr uint32_t HIST_BINS = 2048;  // global digit histogram per segment
-constexpr uint32_t PART_TILE = 1024;  // records per partition CTA
+#ifndef FKD_PART_PIPT
+#define FKD_PART_PIPT 4
+#endif
+constexpr uint32_t PART_TILE = 256 * FKD_PART_PIPT;  // records per partition CTA
 constexpr uint32_t HIST_STEP = 2048;  // digit-pass tile granularity
 cudaError_t launch_build(BuildCtx& bc, int dim);
 // fkd_subtree_sort.cu: the subtree kernel by presorted lists (dims 1-3)

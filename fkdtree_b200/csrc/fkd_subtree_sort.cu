@@ -46,7 +46,7 @@ extern "C" __attribute__((visibility("default"))) void fkd_prof_sorted_reset() {
 namespace {
 
 #ifndef FKD_SORTED_SUBN
-#define FKD_SORTED_SUBN 2048
+#define FKD_SORTED_SUBN 1024
 #endif
 constexpr int XN = FKD_SORTED_SUBN;  // slots: the largest subtree (a power of two, 512..4096)
 constexpr int XPPT = 4;              // slots per thread
