@@ -352,8 +352,10 @@ __global__ void __launch_bounds__(GT, PIPT <= 4 ? 4 : 3) k_partition(uint32_t d,
     const uint32_t e = t0 + k * GT + threadIdx.x;
     uint32_t cls = 3u;  // 0 below, 1 equal, 2 above, 3 none
     if (e < t1) {
+      if (d == 0u) {  // deeper levels move the records level 0 checked
 #pragma unroll
-      for (int w = 0; w < DIM; ++w) nan |= is_nan_bits(rec[k][w]);
+        for (int w = 0; w < DIM; ++w) nan |= is_nan_bits(rec[k][w]);
+      }
       const uint64_t key = order_key(pick_coord<DIM>(rec[k], c), rec[k][DIM]);
       if (bits == 0u) {
         cls = 1u;
