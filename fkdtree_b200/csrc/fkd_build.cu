@@ -173,37 +173,56 @@ __global__ void __launch_bounds__(GT, 4) k_hist(uint32_t d, const EvDesc* __rest
   const uint32_t vpre = (uint32_t)(prefix >> (bits > 32u ? bits - 32u : 0u));  // value part of the prefix
   const uint32_t vbits = bits < 32u ? bits : 32u;
   uint32_t nbelow = 0u;  // verify pass: points below the predicted block
-  constexpr int HIPT = 8;  // records per thread per step
-  for (uint32_t t0 = start + t * ts; t0 < tend; t0 += GT * HIPT) {
-    const uint32_t t1 = min(tend, t0 + (uint32_t)(GT * HIPT));
-    uint32_t vb[HIPT];
-#pragma unroll
-    for (int k = 0; k < HIPT; ++k) {
-      const uint32_t e = t0 + k * GT + threadIdx.x;
-      vb[k] = e < t1 ? __ldcs(X + e) : 0u;
-    }
-#pragma unroll
-    for (int k = 0; k < HIPT; ++k) {
-      const uint32_t e = t0 + k * GT + threadIdx.x;
-      if (e < t1) {
-        const uint32_t mv = mono_bits(vb[k]);
-        if (verify && vbits != 0u && (mv >> (32u - vbits)) < vpre) ++nbelow;
-        // value bits first; the id is read only by points whose value matches
-        if (vbits == 0u || (mv >> (32u - vbits)) == vpre) {
-          uint32_t dig;
-          if (!need_id) {
-            dig = (mv >> (32u - bits - w)) & (nb - 1u);
-          } else {
-            const uint32_t id = __ldcs(src.ids + e);
-            const uint32_t ib = bits - 32u;  // id bits already fixed
-            if (ib != 0u && (id >> (32u - ib)) != (uint32_t)(prefix & ((1ull << ib) - 1u))) continue;
-            dig = (id >> (32u - ib - w)) & (nb - 1u);
-          }
-          atomicAdd(&myhist[dig], 1u);
-        }
+  // one value of the tile: the next digit of the points matching the prefix
+  auto count = [&](uint32_t raw, uint32_t e) {
+    const uint32_t mv = mono_bits(raw);
+    if (verify && vbits != 0u && (mv >> (32u - vbits)) < vpre) ++nbelow;
+    // value bits first; the id is read only by points whose value matches
+    if (vbits == 0u || (mv >> (32u - vbits)) == vpre) {
+      uint32_t dig;
+      if (!need_id) {
+        dig = (mv >> (32u - bits - w)) & (nb - 1u);
+      } else {
+        const uint32_t id = __ldcs(src.ids + e);
+        const uint32_t ib = bits - 32u;  // id bits already fixed
+        if (ib != 0u && (id >> (32u - ib)) != (uint32_t)(prefix & ((1ull << ib) - 1u))) return;
+        dig = (id >> (32u - ib - w)) & (nb - 1u);
       }
+      atomicAdd(&myhist[dig], 1u);
+    }
+  };
+  // the tile [tb, tend): a scalar head up to a 16-byte boundary, 16-byte
+  // loads (two per thread in flight), a scalar tail
+  const uint32_t tb = start + t * ts;
+  const uint32_t tlen = tend > tb ? tend - tb : 0u;
+  uint32_t head = (uint32_t)(((16u - ((uint32_t)(uintptr_t)(X + tb) & 15u)) & 15u) >> 2);
+  if (head > tlen) head = tlen;
+  if (threadIdx.x < head) count(__ldcs(X + tb + threadIdx.x), tb + threadIdx.x);
+  const uint32_t vb0 = tb + head;
+  const uint32_t nv = (tlen - head) >> 2;
+  const uint4* X4 = reinterpret_cast<const uint4*>(X + vb0);
+  for (uint32_t v0 = 0; v0 < nv; v0 += 2u * GT) {
+    const uint32_t va = v0 + threadIdx.x, vb = va + GT;
+    uint4 qa = make_uint4(0u, 0u, 0u, 0u), qb = qa;
+    if (va < nv) qa = __ldcs(X4 + va);
+    if (vb < nv) qb = __ldcs(X4 + vb);
+    if (va < nv) {
+      const uint32_t e = vb0 + 4u * va;
+      count(qa.x, e);
+      count(qa.y, e + 1u);
+      count(qa.z, e + 2u);
+      count(qa.w, e + 3u);
+    }
+    if (vb < nv) {
+      const uint32_t e = vb0 + 4u * vb;
+      count(qb.x, e);
+      count(qb.y, e + 1u);
+      count(qb.z, e + 2u);
+      count(qb.w, e + 3u);
     }
   }
+  const uint32_t tail0 = vb0 + 4u * nv;
+  if (tail0 + threadIdx.x < tend) count(__ldcs(X + tail0 + threadIdx.x), tail0 + threadIdx.x);
   if (verify) {
     for (int o = 16; o > 0; o >>= 1) nbelow += __shfl_xor_sync(0xffffffffu, nbelow, o);
     if (lane == 0 && nbelow) atomicAdd(&sel[s].below, nbelow);
