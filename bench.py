@@ -254,7 +254,8 @@ def _events_run(wb, mlp, dev, steps, plain_single):
     b.search_digest(mins, maxs)
     out["kernels_per_batched_run"] = int(L.fkd_kernel_launches() - launches0)
     out["autotune"] = {"hist_ctas": tune["hist_ctas"], "search_lanes": tune["search_lanes"],
-                       "build_s": tune["build_s"], "search_s": tune["search_s"]}
+                       "search_big_n": tune["search_big_n"], "search_lanes_big": tune["search_lanes_big"],
+                       "build_s": tune["build_s"], "search_s": tune["search_s"], "split_s": tune["split_s"]}
     delta = 0.1
     b.set_mlp(mlp, delta=delta)
     lc = torch.empty(nq, dtype=torch.int32, device=dev)

@@ -8,6 +8,10 @@ expose (include/fkdtree_b200.h):
                     (the tile count of the segmented radix select);
 * ``search_lanes``  lanes that share one box in the count / digest search
                     (32 = a warp per box; 1 = a thread per box).
+* ``search_big_n``, ``search_lanes_big``  a size split of the digest search:
+                    events of at least big_n points search in a launch of
+                    their own with their own lanes per box (large events fill
+                    a warp per box, small ones do not).
 
 The build and the search are independent, so each knob is swept on its own
 phase: every candidate is timed (best of ``reps`` runs after one warm-up),
@@ -30,6 +34,9 @@ import numpy as np
 
 SEARCH_LANES = (32, 16, 8, 4, 2, 1)
 HIST_CTAS_PER_SM = (1, 2, 4, 8)
+# size split of the digest search: events of at least big_n points get their
+# own launch with big_lanes lanes per box ((0, 0): no split)
+SPLITS = ((0, 0), (32768, 32), (65536, 32), (131072, 32), (65536, 16))
 
 
 def cache_path() -> str:
@@ -118,11 +125,13 @@ def _sms() -> int:
 
 def tune_batch(batch, coords, ids, mins, maxs, *, device: Optional[str] = None, use_cache: bool = True,
                cache_file: Optional[str] = None, reps: int = 2, lanes: Sequence[int] = SEARCH_LANES,
+               splits: Sequence[Tuple[int, int]] = SPLITS,
                hist_ctas: Optional[Sequence[int]] = None, sync: Optional[Callable[[], None]] = None,
                clock: Callable[[], float] = time.perf_counter) -> dict:
     """Chooses hist_ctas (build) and search_lanes (digest search) for
     `batch` (a fkdtree_b200.Batch) on its own inputs, applies them and returns
-    {"hist_ctas", "search_lanes", "cached", "key", "build_s", "search_s"}.
+    {"hist_ctas", "search_lanes", "search_big_n", "search_lanes_big", "cached",
+    "key", "build_s", "search_s", "split_s"}.
     Inputs may be host arrays or CUDA tensors (device tensors keep the copies
     out of the timing)."""
     if sync is None:
@@ -140,6 +149,8 @@ def tune_batch(batch, coords, ids, mins, maxs, *, device: Optional[str] = None, 
     if hit is not None and "hist_ctas" in hit and "search_lanes" in hit:
         batch.set_param("hist_ctas", int(hit["hist_ctas"]))
         batch.set_param("search_lanes", int(hit["search_lanes"]))
+        batch.set_param("search_lanes_big", int(hit.get("search_lanes_big", 0)))
+        batch.set_param("search_big_n", int(hit.get("search_big_n", 0)))
         return dict(hit, cached=True, key=key)
     if hist_ctas is None:
         hist_ctas = [k * _sms() for k in HIST_CTAS_PER_SM]
@@ -150,9 +161,19 @@ def tune_batch(batch, coords, ids, mins, maxs, *, device: Optional[str] = None, 
     ln, search_table = sweep(lanes, lambda v: batch.set_param("search_lanes", int(v)),
                              lambda: batch.search_digest(mins, maxs), sync, reps=reps, clock=clock)
     batch.set_param("search_lanes", int(ln))
-    result = {"hist_ctas": int(hc), "search_lanes": int(ln),
+
+    def apply_split(v):
+        batch.set_param("search_lanes_big", int(v[1]))
+        batch.set_param("search_big_n", int(v[0]))
+
+    sp, split_table = sweep(splits, apply_split, lambda: batch.search_digest(mins, maxs), sync, reps=reps,
+                            clock=clock)
+    apply_split(sp)
+    result = {"hist_ctas": int(hc), "search_lanes": int(ln), "search_big_n": int(sp[0]),
+              "search_lanes_big": int(sp[1]),
               "build_s": {str(k): v for k, v in build_table},
-              "search_s": {str(k): v for k, v in search_table}}
+              "search_s": {str(k): v for k, v in search_table},
+              "split_s": {f"{k[0]}:{k[1]}": v for k, v in split_table}}
     if use_cache:
         entries = load_cache(cache_file)
         entries[key] = result

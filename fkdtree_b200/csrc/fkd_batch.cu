@@ -115,6 +115,11 @@ struct Part {
   PlanDev plan;
   Buf io, chunks, work0, work1, nodes, ids, sel, ghist, lfeat, lyhat, lrange, sdig, bnd;
   uint32_t nchunks = 0;
+  std::vector<uint32_t> ev_n;  // points of every (local) event
+  // digest search split by event size (knob search_big_n): [0] smaller events, [1] the others
+  Buf evsel[2], evsel_q[2];
+  uint32_t nsel[2] = {0, 0};
+  uint64_t selq[2] = {0, 0};
 };
 
 }  // namespace
@@ -134,6 +139,8 @@ struct fkd_batch_s {
   // tuning knobs (fkd_batch_set_param)
   uint32_t hist_ctas = 0;
   uint32_t search_lanes = 0;
+  uint32_t search_lanes_big = 0;  // lanes per box for events of at least search_big_n points (0: search_lanes)
+  uint32_t search_big_n = 0;      // 0: one launch for every event
   int subtree = 0;
   // learned split
   fkd_mlp mlp = nullptr;
@@ -180,6 +187,7 @@ fkd_status batch_plan(fkd_batch b) {
       base += n;
     }
     p.npts = base;
+    p.ev_n = n_ev;
     PlanHost ph;
     plan_build(n_ev.data(), base_ev.data(), (uint32_t)n_ev.size(), p.dim, hist_ctas, ph);
     for (uint32_t le = 0; le < p.events.size(); ++le) {
@@ -281,6 +289,36 @@ fkd_status enqueue_build(fkd_batch b, const float* coords, const uint32_t* ids) 
   return FKD_OK;
 }
 
+// The event subsets of a size-split digest search: events with boxes, below
+// search_big_n points in [0], the others in [1] (uploaded once per knob value).
+fkd_status batch_search_sets(fkd_batch b) {
+  for (auto& pp : b->parts) {
+    Part& p = *pp;
+    std::vector<uint32_t> sel[2];
+    std::vector<uint64_t> q[2];
+    q[0].push_back(0);
+    q[1].push_back(0);
+    for (uint32_t le = 0; le < p.ev_n.size(); ++le) {
+      const uint32_t e = p.events[le];
+      const uint64_t nq = b->q_off[e + 1] - b->q_off[e];
+      if (nq == 0) continue;
+      const int k = (b->search_big_n && p.ev_n[le] >= b->search_big_n) ? 1 : 0;
+      sel[k].push_back(le);
+      q[k].push_back(q[k].back() + nq);
+    }
+    for (int k = 0; k < 2; ++k) {
+      p.nsel[k] = (uint32_t)sel[k].size();
+      p.selq[k] = q[k].back();
+      if (sel[k].empty()) continue;
+      BCUDA(p.evsel[k].ensure(sel[k].size() * sizeof(uint32_t)));
+      BCUDA(p.evsel_q[k].ensure(q[k].size() * sizeof(uint64_t)));
+      BCUDA(cudaMemcpy(p.evsel[k].p, sel[k].data(), sel[k].size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+      BCUDA(cudaMemcpy(p.evsel_q[k].p, q[k].data(), q[k].size() * sizeof(uint64_t), cudaMemcpyHostToDevice));
+    }
+  }
+  return FKD_OK;
+}
+
 fkd_status enqueue_digest(fkd_batch b, const float* mins, const float* maxs, uint32_t* counts, uint64_t* digests) {
   for (auto& pp : b->parts) {
     Part& p = *pp;
@@ -301,7 +339,21 @@ fkd_status enqueue_digest(fkd_batch b, const float* mins, const float* maxs, uin
     sc.capacity = ~0ull;
     sc.lanes = b->search_lanes;
     sc.stream = b->stream;
-    BCUDA(launch_search(sc, p.dim, SEARCH_DIGEST));
+    if (b->search_big_n == 0) {
+      BCUDA(launch_search(sc, p.dim, SEARCH_DIGEST));
+      continue;
+    }
+    // small and large events with their own lanes per box
+    for (int k = 0; k < 2; ++k) {
+      if (p.nsel[k] == 0) continue;
+      SearchCtx s2 = sc;
+      s2.boxes.q = p.selq[k];
+      s2.evsel = p.evsel[k].as<uint32_t>();
+      s2.evsel_q = p.evsel_q[k].as<uint64_t>();
+      s2.nsel = p.nsel[k];
+      if (k == 1 && b->search_lanes_big) s2.lanes = b->search_lanes_big;
+      BCUDA(launch_search(s2, p.dim, SEARCH_DIGEST));
+    }
   }
   return FKD_OK;
 }
@@ -403,6 +455,19 @@ fkd_status fkd_batch_set_param(fkd_batch b, const char* name, int64_t value) {
     b->subtree = (int)value;
     drop_graph();
     return FKD_OK;
+  }
+  if (strcmp(name, "search_lanes_big") == 0) {
+    if (value != 0 && value != 1 && value != 2 && value != 4 && value != 8 && value != 16 && value != 32)
+      return capi_fail(FKD_ERR_ARG, "search_lanes_big must be 0, 1, 2, 4, 8, 16 or 32");
+    b->search_lanes_big = (uint32_t)value;
+    drop_graph();
+    return FKD_OK;
+  }
+  if (strcmp(name, "search_big_n") == 0) {
+    if (value < 0 || value > 0x7fffffffll) return capi_fail(FKD_ERR_ARG, "search_big_n out of range");
+    b->search_big_n = (uint32_t)value;
+    drop_graph();
+    return batch_search_sets(b);
   }
   if (strcmp(name, "search_lanes") == 0) {
     if (value != 0 && value != 1 && value != 2 && value != 4 && value != 8 && value != 16 && value != 32)

@@ -82,6 +82,7 @@ struct fkd_tree_s {
   uint32_t search_lanes = 0; // count / digest lanes per box (0: one warp)
   int subtree = 0;           // subtree kernel: 0 auto, 1 radix select, 2 presorted lists
   bool small_select = true;  // one CTA per segment on levels of small segments
+  bool box_order = true;     // search boxes in the spatial order of their centres
   fkd_mlp mlp = nullptr;     // learned split (null: plain radix select)
   float mlp_delta = 0.f;
   DevBuf lfeat, lyhat, lrange, lstats, sdig, dids, dnode, bnd, pool_st, pool_len, pool_s, brec, jctr, rflags;
@@ -198,6 +199,10 @@ fkd_status check_search_args(fkd_tree h, const float* mins, const float* maxs, u
 
 // Spatial processing order of the boxes (fkd_search.cu: launch_box_order).
 fkd_status box_order(fkd_tree h, const Boxes& b, const uint32_t** order) {
+  if (!h->box_order) {
+    *order = nullptr;
+    return FKD_OK;
+  }
   FKD_CUDA(h->qorder.ensure(box_order_words(b.q) * sizeof(uint32_t)));
   uint32_t* o = nullptr;
   FKD_CUDA(launch_box_order(make_geom((uint32_t)h->n), table_of(h), b, h->dim, h->qorder.as<uint32_t>(), &o,
@@ -685,6 +690,11 @@ fkd_status fkd_set_param(fkd_tree h, const char* name, int64_t value) {
     if (value != 0 && value != 1 && value != 2 && value != 4 && value != 8 && value != 16 && value != 32)
       return fail(FKD_ERR_ARG, "search_lanes must be 0, 1, 2, 4, 8, 16 or 32");
     h->search_lanes = (uint32_t)value;
+    return FKD_OK;
+  }
+  if (strcmp(name, "box_order") == 0) {
+    if (value != 0 && value != 1) return fail(FKD_ERR_ARG, "box_order must be 0 or 1");
+    h->box_order = value != 0;
     return FKD_OK;
   }
   if (strcmp(name, "small_select") == 0) {

@@ -153,6 +153,9 @@ struct SearchCtx {
   uint32_t* err;
   int heap_out;            // write heap indices instead of ids
   uint32_t lanes;          // count / digest: lanes per box (1, 2, 4, 8, 16; 0 or 32: one warp per box)
+  const uint32_t* evsel;   // batched search over a subset of the events (null: all boxes in order)
+  const uint64_t* evsel_q; // exclusive prefix of the subset's box counts (nsel + 1 entries)
+  uint32_t nsel;
   // count pass with a run pool: every box's result recorded as runs of the
   // in-order table, in chunks that k_expand writes out (null pool: no record)
   uint32_t* pool_st;             // in-order start of every run

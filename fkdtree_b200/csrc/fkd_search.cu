@@ -67,6 +67,22 @@ __host__ __device__ inline uint32_t stack_cap(const Geom& g) {
   return c;
 }
 
+// Batched search over a subset of the events (sc.evsel, in increasing
+// order, with sc.evsel_q the exclusive prefix of their box counts): the
+// qi-th box of the subset, and its event.
+__device__ __forceinline__ uint32_t select_box(const SearchCtx& sc, uint32_t qi, uint32_t& ev) {
+  uint32_t lo = 0u, hi = sc.nsel;  // evsel_q[lo] <= qi < evsel_q[hi]
+  while (hi - lo > 1u) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (sc.evsel_q[mid] <= (uint64_t)qi)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  ev = sc.evsel[lo];
+  return (uint32_t)(sc.evs[ev].qbase + ((uint64_t)qi - sc.evsel_q[lo]));
+}
+
 // Copies the concatenation of nj runs of the in-order table srct -- run k
 // starts at srct[st[k]] and lands at out[base + pre[k]], pre being the
 // exclusive prefix of the run lengths and total their sum -- with one warp.
@@ -138,7 +154,8 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
     if (lane == 0) qi = atomicAdd(sc.qcounter, 1u);
     qi = __shfl_sync(0xffffffffu, qi, 0);
     if ((uint64_t)qi >= sc.boxes.q) break;
-    const uint32_t qj = sc.order ? sc.order[qi] : qi;
+    uint32_t qj = sc.order ? sc.order[qi] : qi;
+    if (sc.evsel) qj = select_box(sc, qi, cur_ev);
     uint64_t oj = qj;  // output slot of this box
     Geom g = sc.g;
     Table tab = sc.tab;
@@ -726,7 +743,8 @@ __global__ void __launch_bounds__(QT) k_search_grp(SearchCtx sc, uint32_t cap) {
         exhausted = true;
         break;
       }
-      const uint32_t qj = sc.order ? sc.order[qi] : qi;
+      uint32_t qj = sc.order ? sc.order[qi] : qi;
+      if (sc.evsel) qj = select_box(sc, qi, cur_ev);
       oj = qj;
       g = sc.g;
       tab = sc.tab;

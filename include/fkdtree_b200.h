@@ -164,6 +164,8 @@ FKD_API fkd_status fkd_sync(fkd_tree h);
 /* Tuning knobs of one tree, same names and ranges as fkd_batch_set_param
  * ("hist_ctas" takes effect at the next build; "search_lanes" applies to
  * fkd_search_count / fkd_search_digest), plus
+ *   "box_order"     (0/1, default 1): searches visit the boxes in the spatial
+ *                   order of their centres (tree cell), not in input order
  *   "small_select"  (0/1, default 1): global levels whose segments are small
  *                   select each segment with one CTA in shared memory
  *   "search_record" (0/1, default 1): fkd_search's count pass records every
@@ -204,6 +206,9 @@ FKD_API fkd_status fkd_batch_destroy(fkd_batch b);
  *   "hist_ctas"    digit-pass CTAs per level (0 = four per SM); re-plans the batch
  *   "search_lanes" lanes per box of the count / digest search: 1, 2, 4, 8, 16
  *                  or 32 (0 = 32, one warp per box)
+ *   "search_big_n", "search_lanes_big"  digest search: events of at least
+ *                  search_big_n points search with search_lanes_big lanes per
+ *                  box in a launch of their own (0: one launch for all)
  *   "subtree"      shared-memory subtree kernel: 0 auto (presorted lists for
  *                  dims 1-3, radix select for dim 4), 1 radix select, 2 lists
  * No reference counterpart (the reference has one fixed launch shape). */

@@ -20,12 +20,17 @@ def check_batch(wb, gpu_tab, gpu_tid, counts, digests):
     assert np.array_equal(np.asarray(digests).astype(np.uint64), od), "digests differ"
 
 
-@pytest.mark.parametrize("frac_4d,lanes", [(0.0, 0), (0.5, 0), (0.5, 1), (0.0, 2), (0.5, 4), (0.0, 8), (0.5, 16)])
-def test_batch_matches_per_event_oracle(cuda, frac_4d, lanes):
+@pytest.mark.parametrize("frac_4d,lanes,big_n,lanes_big", [(0.0, 0, 0, 0), (0.5, 0, 0, 0), (0.5, 1, 0, 0),
+                                                           (0.0, 2, 0, 0), (0.5, 4, 0, 0), (0.0, 8, 0, 0),
+                                                           (0.5, 16, 0, 0), (0.0, 2, 6000, 32), (0.5, 1, 3000, 8),
+                                                           (0.5, 4, 100_000, 32)])
+def test_batch_matches_per_event_oracle(cuda, frac_4d, lanes, big_n, lanes_big):
     wb = W.event_batch(n_events=64, median=6000, size_lo=1, size_hi=60_000, clusters_lo=5, clusters_hi=50,
                        half_width=0.01, seed=21, frac_4d=frac_4d)
     b = F.Batch.of(wb)
     b.set_param("search_lanes", lanes)
+    b.set_param("search_lanes_big", lanes_big)
+    b.set_param("search_big_n", big_n)
     b.build(wb.coords, wb.ids)
     tab, tid = b.tables()
     c, d = b.search_digest(wb.mins, wb.maxs)
