@@ -171,21 +171,28 @@ def _timed(fn, k):
 
 
 def _cpu_events(wb, n_sample):
-    """The oracle (C restatement of FKDTree_CPU build + search per event,
-    OpenMP over events on every host core) on n_sample events spread over the
-    batch, scaled to the whole batch by points."""
+    """The reference CPU path on n_sample events spread over the batch, scaled
+    to the whole batch by points: the unmodified FKDTree_CPU (oracle/_ref) with
+    OpenMP over events, each a serial build and a serial
+    search_in_the_box_recursive of its boxes -- or, without oracle/_ref, the C
+    restatement the same way."""
     from fkdtree_b200 import shard as S
     from oracle import oracle as O
     threads = O.host_threads()
     ev = np.linspace(0, wb.n_events - 1, min(n_sample, wb.n_events)).astype(np.int64)
     sb = S.sub_batch(wb, ev)
+    kind = "reference" if O.ref_available() else "port"
     t0 = time.perf_counter()
-    O.batch(sb, threads=threads)
+    if kind == "reference":
+        O.ref_batch(sb, threads=threads)
+    else:
+        O.batch(sb, threads=threads)
     sec = time.perf_counter() - t0
     scaled = sec * wb.n_points / max(1, sb.n_points)
-    return {"kind": "port", "cores": threads, "value": wb.n_points / scaled / 1e6, "unit": "Mpoints/s",
+    what = "FKDTree_CPU build + search_in_the_box_recursive" if kind == "reference" else "restated build + search"
+    return {"kind": kind, "cores": threads, "value": wb.n_points / scaled / 1e6, "unit": "Mpoints/s",
             "ms_scaled": 1e3 * scaled,
-            "sample": (f"oracle build + box search of {len(ev)} of {wb.n_events} events ({sb.n_points} points, "
+            "sample": (f"{what} of {len(ev)} of {wb.n_events} events ({sb.n_points} points, "
                        f"{sb.n_queries} boxes) with {threads} threads over events, scaled by points")}
 
 

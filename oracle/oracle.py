@@ -84,6 +84,9 @@ def ref_lib():
         L.fkdref_search.argtypes = [C.c_void_p, C.c_int, C.c_uint64, _f32p, _f32p, C.c_void_p, C.c_void_p, C.c_void_p,
                                     C.c_int, C.POINTER(C.c_double)]
         L.fkdref_max_threads.restype = C.c_int
+        L.fkdref_batch.argtypes = [C.c_uint32, _u32p, _u64p, _u64p, _f32p, _u32p, _u64p, _u64p, _f32p, _f32p, _u32p,
+                                   _u64p, C.c_int]
+        L.fkdref_batch.restype = C.c_double
         _ref = L
     return _ref
 
@@ -174,6 +177,19 @@ def batch(b, threads: int = 0):
     if rc != 0:
         raise RuntimeError("fkd_oracle_batch failed")
     return tab, tid, counts, dig
+
+
+def ref_batch(b, threads: int = 0):
+    """The unmodified reference over every event of a workloads.Batch (OpenMP
+    over events, each a serial FKDTree_CPU build + search_in_the_box_recursive
+    of its boxes): returns (counts, digests, seconds)."""
+    counts = np.empty(b.n_queries, dtype=np.uint32)
+    dig = np.empty(b.n_queries, dtype=np.uint64)
+    sec = ref_lib().fkdref_batch(b.n_events, _soa(b.dims, np.uint32), _soa(b.pt_off, np.uint64),
+                                 _soa(b.coord_off, np.uint64), _soa(b.coords, np.float32), _soa(b.ids, np.uint32),
+                                 _soa(b.q_off, np.uint64), _soa(b.qcoord_off, np.uint64), _soa(b.mins, np.float32),
+                                 _soa(b.maxs, np.float32), counts, dig, threads)
+    return counts, dig, float(sec)
 
 
 def mix64(ids: np.ndarray) -> np.ndarray:

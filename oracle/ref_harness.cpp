@@ -37,7 +37,16 @@ struct HandleBase {
   virtual void tables(float* tab_soa, uint32_t* ids) = 0;
   virtual void search(int variant, uint64_t nq, const float* mins, const float* maxs, uint32_t* counts,
                       const uint64_t* offsets, uint32_t* out, int threads, double* seconds) = 0;
+  // serial search_in_the_box_recursive of every box: count and digest of its ids
+  virtual void digest(uint64_t nq, const float* mins, const float* maxs, uint32_t* counts, uint64_t* digests) = 0;
 };
+
+inline uint64_t mix_id(uint32_t id) {
+  uint64_t z = (uint64_t)id + 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
 
 template <int D>
 struct Handle : HandleBase {
@@ -82,6 +91,22 @@ struct Handle : HandleBase {
         tree->search_in_the_box_recursive(lo, hi, r);
         return r;
       }
+    }
+  }
+
+  void digest(uint64_t nq, const float* mins, const float* maxs, uint32_t* counts, uint64_t* digests) override {
+    FKDPoint<float, D> lo, hi;
+    for (uint64_t j = 0; j < nq; ++j) {
+      for (int c = 0; c < D; ++c) {
+        lo.setDimension(c, mins[(size_t)c * nq + j]);
+        hi.setDimension(c, maxs[(size_t)c * nq + j]);
+      }
+      std::vector<unsigned int> r;
+      tree->search_in_the_box_recursive(lo, hi, r);
+      uint64_t dg = 0;
+      for (unsigned int id : r) dg += mix_id(id);
+      counts[j] = (uint32_t)r.size();
+      digests[j] = dg;
     }
   }
 
@@ -138,5 +163,43 @@ void fkdref_search(void* h, int variant, uint64_t nq, const float* mins_soa, con
 }
 
 int fkdref_max_threads(void) { return omp_get_max_threads(); }
+
+// Batched events, the reference way (OpenMP over events; each event a serial
+// FKDTree_CPU build and a serial search_in_the_box_recursive of its boxes):
+// per box the result count and the digest (wrap-around sum over the result
+// ids of the splitmix64 finaliser of id + 0x9E3779B97F4A7C15, the digest the
+// GPU library reports).  Event e owns points [pt_off[e], pt_off[e+1]) with
+// coordinates SoA at coords[coord_off[e] + c*n + i] and boxes [q_off[e],
+// q_off[e+1]) with bounds SoA at mins/maxs[qcoord_off[e] + c*q + j].
+// Returns the elapsed seconds.
+double fkdref_batch(uint32_t nev, const uint32_t* dims, const uint64_t* pt_off, const uint64_t* coord_off,
+                    const float* coords, const uint32_t* ids, const uint64_t* q_off, const uint64_t* qcoord_off,
+                    const float* mins, const float* maxs, uint32_t* counts, uint64_t* digests, int threads) {
+  if (threads > 0) omp_set_num_threads(threads);
+  auto t0 = std::chrono::steady_clock::now();
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int64_t e = 0; e < (int64_t)nev; ++e) {
+    const uint32_t n = (uint32_t)(pt_off[e + 1] - pt_off[e]);
+    const uint64_t q = q_off[e + 1] - q_off[e];
+    if (n == 0) {
+      for (uint64_t j = 0; j < q; ++j) {
+        counts[q_off[e] + j] = 0;
+        digests[q_off[e] + j] = 0;
+      }
+      continue;
+    }
+    std::unique_ptr<HandleBase> h;
+    switch (dims[e]) {
+      case 1: h.reset(new Handle<1>(n, coords + coord_off[e], ids + pt_off[e])); break;
+      case 2: h.reset(new Handle<2>(n, coords + coord_off[e], ids + pt_off[e])); break;
+      case 3: h.reset(new Handle<3>(n, coords + coord_off[e], ids + pt_off[e])); break;
+      default: h.reset(new Handle<4>(n, coords + coord_off[e], ids + pt_off[e])); break;
+    }
+    h->build();
+    h->digest(q, mins + qcoord_off[e], maxs + qcoord_off[e], counts + q_off[e], digests + q_off[e]);
+  }
+  auto t1 = std::chrono::steady_clock::now();
+  return std::chrono::duration<double>(t1 - t0).count();
+}
 
 }  // extern "C"

@@ -93,3 +93,16 @@ def test_oracle_matches_reference_on_random_inputs():
             t2 = r.tables()
             r.close()
             assert np.array_equal(t1[0].view(np.uint32), t2[0].view(np.uint32)) and np.array_equal(t1[1], t2[1])
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built")
+def test_reference_batch_matches_restated_batch():
+    """The unmodified reference over a batch of events (OpenMP over events,
+    recursive search) gives the same per-box counts and digests as the C
+    restatement -- the batched CPU baseline and the GPU parity target agree."""
+    from fkdtree_b200 import workloads as W
+    wb = W.event_batch(n_events=24, median=2000, size_lo=1, size_hi=12_000, clusters_lo=5, clusters_hi=30,
+                       half_width=0.02, seed=8, frac_4d=0.3)
+    c1, d1, _ = O.ref_batch(wb, threads=2)
+    _, _, c2, d2 = O.batch(wb)
+    assert np.array_equal(c1, c2) and np.array_equal(d1, d2)
