@@ -330,9 +330,23 @@ def batched_report(dev, n_events=4096, steps=3, train_events=2000, cpu=True):
     losses = mlp.train(x, t, epochs=60, batch=256, lr=2e-3)
     train_s = time.perf_counter() - t0
     btr.close()
+    # (the MLP is tiny: its training is launch- and latency-bound, not a roofline concern)
     del trc, tri
-    rep = {"training": {"events": train_events, "seed": 10, "rows": int(x.shape[0]), "record_s": record_s,
-                        "train_s": train_s, "loss_first": float(losses[0]), "loss_last": float(losses[-1]),
+    # 40 -> 64 -> 64 -> 1: 2 * (40*64 + 64*64 + 64) FLOPs per node forward, about 3x that per
+    # training sample (forward, input and weight gradients)
+    fwd = 2 * (40 * 64 + 64 * 64 + 64)
+    epochs = 60
+    train_flops = 3 * fwd * int(x.shape[0]) * epochs
+    try:
+        with open(PEAKS_FILE) as f:
+            bf16 = float(json.load(f)["bf16_tflops_sustained"])
+    except Exception:
+        bf16 = 1400.0
+    rep = {"training": {"events": train_events, "seed": 10, "rows": int(x.shape[0]), "epochs": epochs,
+                        "record_s": record_s, "train_s": train_s, "loss_first": float(losses[0]),
+                        "loss_last": float(losses[-1]), "flops_per_node_forward": fwd,
+                        "train_tflops": train_flops / train_s / 1e12,
+                        "train_frac_of_bf16_sustained": train_flops / train_s / 1e12 / bf16,
                         "kernels": "fkd_mlp_train: k_mlp_grad (bf16 mma.sync, fp32 accumulate) + k_mlp_adam"}}
     t0 = time.perf_counter()
     wb = W.event_batch(n_events=n_events, seed=20)
