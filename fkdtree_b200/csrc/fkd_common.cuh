@@ -63,10 +63,19 @@ FKD_HD uint32_t seg_start(const Geom& g, uint32_t d, uint32_t t) {
 // Split rank of node (d, t), d < H: the size of its left subtree.
 FKD_HD uint32_t seg_rank(const Geom& g, uint32_t d, uint32_t t) { return seg_len(g, d + 1, 2u * t); }
 
-// Subtree size of heap node i.
+// Subtree size of heap node i.  Device code uses 32-bit arithmetic: a tree
+// holds fewer than 2^31 points, so t * 2^(H-d) <= 2^H < 2^31 and no term
+// overflows.
 FKD_HD uint32_t subtree_size(const Geom& g, uint32_t i) {
   const uint32_t d = floor_log2_u32(i + 1u);
+#ifdef __CUDA_ARCH__
+  const uint32_t sh = g.H - d;
+  const uint32_t W = 1u << sh;
+  const uint32_t tw = (i + 1u - (1u << d)) << sh;
+  return W - 1u + (g.M > tw ? min(g.M - tw, W) : 0u);
+#else
   return seg_len(g, d, i + 1u - (1u << d));
+#endif
 }
 
 // Order key of the reference comparator (FKDTree_cpu.h:246-252): the float
