@@ -48,34 +48,38 @@ inline Geom make_geom(uint32_t n) {
   return g;
 }
 
+// (Device code uses 32-bit arithmetic: a tree holds fewer than 2^31 points,
+// so t * W <= 2^H < 2^31 and no term overflows; host code keeps 64 bits.)
 FKD_HD uint32_t seg_len(const Geom& g, uint32_t d, uint32_t t) {
+#ifdef __CUDA_ARCH__
+  const uint32_t W = 1u << (g.H - d);
+  const uint32_t tw = t * W;
+  return W - 1u + (g.M > tw ? min(g.M - tw, W) : 0u);
+#else
   const uint64_t W = 1ull << (g.H - d);
   const uint64_t tw = (uint64_t)t * W;
   const uint64_t last = (uint64_t)g.M > tw ? (((uint64_t)g.M - tw) < W ? ((uint64_t)g.M - tw) : W) : 0ull;
   return (uint32_t)(W - 1ull + last);
+#endif
 }
 
 FKD_HD uint32_t seg_start(const Geom& g, uint32_t d, uint32_t t) {
+#ifdef __CUDA_ARCH__
+  const uint32_t tw = t << (g.H - d);
+  return tw + min(g.M, tw);
+#else
   const uint64_t tw = (uint64_t)t << (g.H - d);
   return (uint32_t)(tw + ((uint64_t)g.M < tw ? (uint64_t)g.M : tw));
+#endif
 }
 
 // Split rank of node (d, t), d < H: the size of its left subtree.
 FKD_HD uint32_t seg_rank(const Geom& g, uint32_t d, uint32_t t) { return seg_len(g, d + 1, 2u * t); }
 
-// Subtree size of heap node i.  Device code uses 32-bit arithmetic: a tree
-// holds fewer than 2^31 points, so t * 2^(H-d) <= 2^H < 2^31 and no term
-// overflows.
+// Subtree size of heap node i.
 FKD_HD uint32_t subtree_size(const Geom& g, uint32_t i) {
   const uint32_t d = floor_log2_u32(i + 1u);
-#ifdef __CUDA_ARCH__
-  const uint32_t sh = g.H - d;
-  const uint32_t W = 1u << sh;
-  const uint32_t tw = (i + 1u - (1u << d)) << sh;
-  return W - 1u + (g.M > tw ? min(g.M - tw, W) : 0u);
-#else
   return seg_len(g, d, i + 1u - (1u << d));
-#endif
 }
 
 // Order key of the reference comparator (FKDTree_cpu.h:246-252): the float
