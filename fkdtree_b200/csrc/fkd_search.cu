@@ -13,8 +13,8 @@
 // FQueue replacement): the warp pops up to 32 nodes, each lane tests one node
 // with a single 16-byte load, and the children are pushed back in lane order.
 // Popping the top 32 of a depth-sorted stack keeps it depth-sorted and leaves
-// at most 64 entries per depth, so 64*(H+1) entries can never overflow; the
-// bound is still checked and reported (FKD_ERR_CAPACITY) rather than trusted.
+// at most min(64, 2^d) entries at depth d (stack_cap); the bound is still
+// checked and reported (FKD_ERR_CAPACITY) rather than trusted.
 //
 // Every node also carries a 2*dim-bit mask saying which sides of its cell
 // (the closed slab its ancestors' split values bound it by) already lie
@@ -25,8 +25,15 @@
 // the interval the build gave it.
 //
 // Two passes ("count then write"): SEARCH_COUNT fills counts, a prefix sum
-// turns them into offsets, SEARCH_WRITE writes every box's ids to its slice.
-// SEARCH_DIGEST replaces the write by a per-box order-independent digest.
+// turns them into offsets, and the ids go to every box's slice.  In
+// fkd_search the count pass also records each box's result (single in-order
+// positions and in-order runs, k_search<count, REC>) and k_expand writes the
+// ids from that record, so the tree is traversed once; SEARCH_WRITE, the
+// traversing write pass, serves fkd_search_write called alone and the boxes a
+// full record pool missed.  SEARCH_DIGEST replaces the write by a per-box
+// order-independent digest (contained subtrees add one precomputed subtree
+// digest).  Count and digest also run with 1-16 lanes per box
+// (k_search_grp), several boxes per warp.
 #include <math.h>
 
 #include "fkd_internal.h"
