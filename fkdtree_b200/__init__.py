@@ -89,10 +89,41 @@ class FKDTree:
         self._h = h
         self._tables = None
 
+    @classmethod
+    def from_points(cls, points, dim: int, stream=None, flags: int = 0) -> "FKDTree":
+        """A tree over points in the reference's FKDPoint<float, dim> layout
+        (FKDPoint.h:102-103): n records of dim float32 coordinates then the
+        uint32 id -- a numpy array or CUDA tensor of n * (dim + 1) 32-bit words
+        (e.g. shape (n, dim + 1) float32 with the ids' bits in the last
+        column).  build() passes them to fkd_build_points as they are."""
+        self = cls.__new__(cls)
+        self._lib = lib()
+        self.device = _is_torch(points)
+        if self.device:
+            points = points.contiguous()
+            words = points.numel() * points.element_size() // 4
+        else:
+            points = np.ascontiguousarray(points)
+            words = points.nbytes // 4
+        self.dim = int(dim)
+        if words % (self.dim + 1):
+            raise ValueError("points must hold n * (dim + 1) 32-bit words")
+        self.n = words // (self.dim + 1)
+        self._coords = self._ids = None
+        self._points = points
+        h = C.c_void_p()
+        check(self._lib.fkd_create(self.dim, flags, _stream_handle(stream), C.byref(h)))
+        self._h = h
+        self._tables = None
+        return self
+
     # -- FKDTree_CPU::build (FKDTree_cpu.h:221-277)
     def build(self) -> "FKDTree":
         mem = MEM_DEVICE if self.device else MEM_HOST
-        check(self._lib.fkd_build(self._h, _ptr(self._coords), _ptr(self._ids), self.n, mem))
+        if getattr(self, "_points", None) is not None:
+            check(self._lib.fkd_build_points(self._h, _ptr(self._points), self.n, mem))
+        else:
+            check(self._lib.fkd_build(self._h, _ptr(self._coords), _ptr(self._ids), self.n, mem))
         self._tables = None
         return self
 
@@ -191,6 +222,70 @@ class FKDTree:
         (FKDTree_opencl.h:123-164); the CPU backend's stub returns nothing
         (FKDTree_cpu.h:215-219)."""
         return self.count_boxes(minPoints, maxPoints)
+
+    # -- radius and k-nearest-neighbour search (fkd_nn.cu; no reference counterpart)
+    def _centres(self, centres):
+        if _is_torch(centres):
+            return centres.contiguous(), MEM_DEVICE, int(centres.shape[-1])
+        centres = _host_f32(centres).reshape(self.dim, -1)
+        return centres, MEM_HOST, int(centres.shape[1])
+
+    def _radii(self, radii, q, mem, like):
+        if mem == MEM_DEVICE:
+            import torch
+            r = radii if _is_torch(radii) else torch.as_tensor(np.asarray(radii, dtype=np.float32))
+            r = r.to(device=like.device, dtype=torch.float32)
+            return r.expand(q).contiguous() if r.dim() == 0 or r.numel() == 1 else r.contiguous()
+        r = _host_f32(radii).reshape(-1)
+        return np.full(q, r[0], dtype=np.float32) if r.size == 1 else r
+
+    def count_radius(self, centres, radii):
+        """Points within radii[j] (inclusive) of every centre (dim, q); radii
+        is (q,) or one value."""
+        ctr, mem, q = self._centres(centres)
+        rad = self._radii(radii, q, mem, ctr)
+        if mem == MEM_DEVICE:
+            import torch
+            counts = torch.empty(q, dtype=torch.int32, device=ctr.device)
+        else:
+            counts = np.empty(q, dtype=np.uint32)
+        check(self._lib.fkd_search_radius_count(self._h, _ptr(ctr), _ptr(rad), q, _ptr(counts), mem))
+        return counts
+
+    def search_radius(self, centres, radii, capacity: int | None = None):
+        """Returns (offsets (q+1,), ids): the ids of query j, in ascending heap
+        index, are ids[offsets[j]:offsets[j+1]]."""
+        ctr, mem, q = self._centres(centres)
+        rad = self._radii(radii, q, mem, ctr)
+        if capacity is None:
+            counts = self.count_radius(ctr, rad)
+            capacity = int(counts.sum().item()) if mem == MEM_DEVICE else int(counts.sum(dtype=np.uint64))
+        total = C.c_uint64(0)
+        if mem == MEM_DEVICE:
+            import torch
+            offsets = torch.empty(q + 1, dtype=torch.int64, device=ctr.device)
+            out = torch.empty(max(capacity, 1), dtype=torch.int32, device=ctr.device)
+        else:
+            offsets = np.empty(q + 1, dtype=np.uint64)
+            out = np.empty(max(capacity, 1), dtype=np.uint32)
+        check(self._lib.fkd_search_radius(self._h, _ptr(ctr), _ptr(rad), q, _ptr(offsets), _ptr(out), capacity,
+                                          C.byref(total), mem))
+        return offsets, out[:total.value]
+
+    def knn(self, centres, k: int):
+        """The k nearest points of every centre (dim, q), ascending in
+        (squared distance, id): returns (ids (q, k), d2 (q, k)); missing
+        neighbours are id 0xffffffff with d2 = inf."""
+        ctr, mem, q = self._centres(centres)
+        if mem == MEM_DEVICE:
+            import torch
+            ids = torch.empty((q, k), dtype=torch.int32, device=ctr.device)
+            d2 = torch.empty((q, k), dtype=torch.float32, device=ctr.device)
+        else:
+            ids = np.empty((q, k), dtype=np.uint32)
+            d2 = np.empty((q, k), dtype=np.float32)
+        check(self._lib.fkd_search_knn(self._h, _ptr(ctr), q, int(k), _ptr(ids), _ptr(d2), mem))
+        return ids, d2
 
     def set_param(self, name: str, value: int) -> "FKDTree":
         """Tuning knob ("hist_ctas", "search_lanes"; fkd_set_param)."""

@@ -37,6 +37,11 @@ SIGNATURES = {
     "fkd_search_write": ([_vp, _vp, _vp, _u64, _vp, _vp, _int, _int], _int),
     "fkd_search": ([_vp, _vp, _vp, _u64, _vp, _vp, _u64, C.POINTER(_u64), _int, _int], _int),
     "fkd_search_digest": ([_vp, _vp, _vp, _u64, _vp, _vp, _int], _int),
+    "fkd_build_points": ([_vp, _vp, _u64, _int], _int),
+    "fkd_search_radius_count": ([_vp, _vp, _vp, _u64, _vp, _int], _int),
+    "fkd_search_radius": ([_vp, _vp, _vp, _u64, _vp, _vp, _u64, C.POINTER(_u64), _int], _int),
+    "fkd_search_knn": ([_vp, _vp, _u64, _u32, _vp, _vp, _int], _int),
+    "fkd_knn_max_k": ([], _u32),
     "fkd_sync": ([_vp], _int),
     "fkd_batch_create": ([_u32, _vp, _vp, _vp, _u32, _vp, C.POINTER(_vp)], _int),
     "fkd_batch_destroy": ([_vp], _int),

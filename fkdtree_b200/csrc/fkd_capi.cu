@@ -289,11 +289,27 @@ fkd_status fkd_set_stream(fkd_tree h, void* stream) {
   return FKD_OK;
 }
 
-fkd_status fkd_build(fkd_tree h, const float* coords, const uint32_t* ids, uint64_t n, int mem) {
+}  // extern "C"
+
+namespace {
+
+// Points in the reference's FKDPoint<float, dim> layout (FKDPoint.h:102-103:
+// dim coordinates then the id, (dim + 1) words per point) to the SoA records
+// of the build (coordinate c of point i at soa[c*n + i], ids at soa[dim*n + i]).
+__global__ void k_points_to_soa(const uint32_t* __restrict__ pts, uint64_t n, int dim, uint32_t* __restrict__ soa) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t* p = pts + i * (uint64_t)(dim + 1);
+  for (int w = 0; w <= dim; ++w) soa[(uint64_t)w * n + i] = __ldg(p + w);
+}
+
+// fkd_build (coords + ids SoA) and fkd_build_points (AoS points) share this.
+fkd_status build_impl(fkd_tree h, const float* coords, const uint32_t* ids, const void* points, uint64_t n,
+                             int mem) {
   if (!h) return fail(FKD_ERR_ARG, "null handle");
   if (mem != FKD_MEM_HOST && mem != FKD_MEM_DEVICE) return fail(FKD_ERR_ARG, "mem must be FKD_MEM_HOST or FKD_MEM_DEVICE");
   if (n >= (1ull << 31)) return fail(FKD_ERR_ARG, "at most 2^31-1 points per tree");
-  if (n && (!coords || !ids)) return fail(FKD_ERR_ARG, "null coords or ids");
+  if (n && !points && (!coords || !ids)) return fail(FKD_ERR_ARG, "null coords or ids");
   h->built = false;
   h->sdig_valid = false;
   h->inorder_valid = false;
@@ -326,7 +342,19 @@ fkd_status fkd_build(fkd_tree h, const float* coords, const uint32_t* ids, uint6
   }
   FKD_CUDA(cudaMemsetAsync(h->err.p, 0, sizeof(uint32_t), h->stream));
   BuildCtx bc;
-  if (mem == FKD_MEM_HOST) {
+  if (points) {
+    uint32_t* w1 = h->work1.as<uint32_t>();
+    const uint32_t* src = (const uint32_t*)points;
+    if (mem == FKD_MEM_HOST) {
+      FKD_CUDA(h->tmp.ensure(rec_bytes));
+      FKD_CUDA(cudaMemcpyAsync(h->tmp.p, points, rec_bytes, cudaMemcpyHostToDevice, h->stream));
+      src = h->tmp.as<uint32_t>();
+    }
+    k_points_to_soa<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(src, n, dim, w1);
+    count_launches(1);
+    FKD_CUDA(cudaGetLastError());
+    bc.input = CSoA{w1, w1 + (size_t)dim * n, n};
+  } else if (mem == FKD_MEM_HOST) {
     uint32_t* w1 = h->work1.as<uint32_t>();
     FKD_CUDA(cudaMemcpyAsync(w1, coords, (size_t)dim * n * sizeof(float), cudaMemcpyHostToDevice, h->stream));
     FKD_CUDA(cudaMemcpyAsync(w1 + (size_t)dim * n, ids, n * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
@@ -378,9 +406,22 @@ fkd_status fkd_build(fkd_tree h, const float* coords, const uint32_t* ids, uint6
     ++h->kev_builds;
   }
   h->built = true;
-  fkd_status s = finish(h, "fkd_build", mem);
+  fkd_status s = finish(h, points ? "fkd_build_points" : "fkd_build", mem);
   if (s != FKD_OK) h->built = false;
   return s;
+}
+
+}  // namespace
+
+extern "C" {
+
+fkd_status fkd_build(fkd_tree h, const float* coords, const uint32_t* ids, uint64_t n, int mem) {
+  return build_impl(h, coords, ids, nullptr, n, mem);
+}
+
+fkd_status fkd_build_points(fkd_tree h, const void* points, uint64_t n, int mem) {
+  if (n && !points) return fail(FKD_ERR_ARG, "null points");
+  return build_impl(h, nullptr, nullptr, points, n, mem);
 }
 
 fkd_status fkd_size(fkd_tree h, uint64_t* n) {
@@ -676,6 +717,167 @@ fkd_status fkd_search_digest(fkd_tree h, const float* mins, const float* maxs, u
     FKD_CUDA(cudaMemcpyAsync(digests, dd, q * sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
   }
   return finish(h, "fkd_search_digest", mem);
+}
+
+}  // extern "C"
+
+namespace {
+
+fkd_status check_nn_args(fkd_tree h, const float* centers, uint64_t q, int mem) {
+  if (!h) return fail(FKD_ERR_ARG, "null handle");
+  if (!h->built) return fail(FKD_ERR_STATE, "search before build");
+  if (mem != FKD_MEM_HOST && mem != FKD_MEM_DEVICE) return fail(FKD_ERR_ARG, "mem must be FKD_MEM_HOST or FKD_MEM_DEVICE");
+  if (q > 0xffffffffull) return fail(FKD_ERR_ARG, "at most 2^32-1 queries per call");
+  if (q && !centers) return fail(FKD_ERR_ARG, "null centers");
+  return FKD_OK;
+}
+
+// Stages host centres (dim*q SoA) and radii (q, optional) or aliases device ones.
+fkd_status stage_centres(fkd_tree h, const float* centers, const float* radii, uint64_t q, int mem,
+                         const float** dctr, const float** drad) {
+  if (mem == FKD_MEM_DEVICE) {
+    *dctr = centers;
+    if (drad) *drad = radii;
+    return FKD_OK;
+  }
+  const size_t cb = (size_t)h->dim * q * sizeof(float);
+  FKD_CUDA(h->qlo.ensure(cb ? cb : 4));
+  FKD_CUDA(cudaMemcpyAsync(h->qlo.p, centers, cb, cudaMemcpyHostToDevice, h->stream));
+  *dctr = h->qlo.as<float>();
+  if (drad) {
+    FKD_CUDA(h->qhi.ensure(q * sizeof(float)));
+    FKD_CUDA(cudaMemcpyAsync(h->qhi.p, radii, q * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    *drad = h->qhi.as<float>();
+  }
+  return FKD_OK;
+}
+
+// Spatial order of the query centres (the box order of zero-size boxes).
+fkd_status centre_order(fkd_tree h, const float* dctr, uint64_t q, const uint32_t** order) {
+  Boxes b;
+  b.lo = dctr;
+  b.hi = dctr;
+  b.stride = q;
+  b.q = q;
+  return box_order(h, b, order);
+}
+
+}  // namespace
+
+extern "C" {
+
+fkd_status fkd_search_radius_count(fkd_tree h, const float* centers, const float* radii, uint64_t q,
+                                   uint32_t* counts, int mem) {
+  fkd_status s = check_nn_args(h, centers, q, mem);
+  if (s != FKD_OK) return s;
+  if (q && (!radii || !counts)) return fail(FKD_ERR_ARG, "null radii or counts");
+  if (q == 0) return FKD_OK;
+  const float *dctr = nullptr, *drad = nullptr;
+  if ((s = stage_centres(h, centers, radii, q, mem, &dctr, &drad)) != FKD_OK) return s;
+  uint32_t* dc = counts;
+  if (mem == FKD_MEM_HOST) {
+    FKD_CUDA(h->counts.ensure(q * sizeof(uint32_t)));
+    dc = h->counts.as<uint32_t>();
+  }
+  FKD_CUDA(cudaMemsetAsync(h->err.p, 0, sizeof(uint32_t), h->stream));
+  const uint32_t* order = nullptr;
+  if ((s = centre_order(h, dctr, q, &order)) != FKD_OK) return s;
+  FKD_CUDA(launch_radius(make_geom((uint32_t)h->n), table_of(h), dctr, drad, q, order, dc, nullptr, nullptr,
+                         h->err.as<uint32_t>(), h->dim, h->stream));
+  if (mem == FKD_MEM_HOST)
+    FKD_CUDA(cudaMemcpyAsync(counts, dc, q * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+  return finish(h, "fkd_search_radius_count", mem);
+}
+
+fkd_status fkd_search_radius(fkd_tree h, const float* centers, const float* radii, uint64_t q, uint64_t* offsets_out,
+                             uint32_t* ids_out, uint64_t capacity, uint64_t* total, int mem) {
+  fkd_status s = check_nn_args(h, centers, q, mem);
+  if (s != FKD_OK) return s;
+  if (!offsets_out || !total) return fail(FKD_ERR_ARG, "null offsets_out or total");
+  if (q && !radii) return fail(FKD_ERR_ARG, "null radii");
+  const float *dctr = nullptr, *drad = nullptr;
+  if ((s = stage_centres(h, centers, radii, q, mem, &dctr, &drad)) != FKD_OK) return s;
+  FKD_CUDA(h->counts.ensure(q ? q * sizeof(uint32_t) : 4));
+  FKD_CUDA(h->partials.ensure(scan_partials_words(q) * sizeof(unsigned long long)));
+  uint64_t* doff = offsets_out;
+  if (mem == FKD_MEM_HOST) {
+    FKD_CUDA(h->offsets.ensure((q + 1) * sizeof(uint64_t)));
+    doff = h->offsets.as<uint64_t>();
+  }
+  FKD_CUDA(cudaMemsetAsync(h->err.p, 0, sizeof(uint32_t), h->stream));
+  const uint32_t* order = nullptr;
+  if (q && (s = centre_order(h, dctr, q, &order)) != FKD_OK) return s;
+  const Geom g = make_geom((uint32_t)h->n);
+  const Table tab = table_of(h);
+  FKD_CUDA(launch_radius(g, tab, dctr, drad, q, order, h->counts.as<uint32_t>(), nullptr, nullptr,
+                         h->err.as<uint32_t>(), h->dim, h->stream));
+  FKD_CUDA(launch_scan_counts(h->counts.as<uint32_t>(), q, doff, h->partials.as<unsigned long long>(), h->stream));
+  FKD_CUDA(cudaMemcpyAsync(h->herr + 2, doff + q, sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
+  FKD_CUDA(cudaStreamSynchronize(h->stream));
+  uint64_t tot = 0;
+  memcpy(&tot, h->herr + 2, sizeof(uint64_t));
+  *total = tot;
+  if ((s = check_err_word(h, "fkd_search_radius (count)")) != FKD_OK) return s;
+  if (mem == FKD_MEM_HOST)
+    FKD_CUDA(cudaMemcpyAsync(offsets_out, doff, (q + 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
+  if (tot > capacity) {
+    FKD_CUDA(cudaStreamSynchronize(h->stream));
+    char buf[128];
+    snprintf(buf, sizeof buf, "fkd_search_radius: %llu results exceed the capacity of %llu ids",
+             (unsigned long long)tot, (unsigned long long)capacity);
+    return fail(FKD_ERR_CAPACITY, buf);
+  }
+  if (tot && !ids_out) return fail(FKD_ERR_ARG, "null ids_out");
+  if (tot == 0) {
+    FKD_CUDA(cudaStreamSynchronize(h->stream));
+    return FKD_OK;
+  }
+  uint32_t* dout = ids_out;
+  if (mem == FKD_MEM_HOST) {
+    FKD_CUDA(h->out.ensure(tot * sizeof(uint32_t)));
+    dout = h->out.as<uint32_t>();
+  }
+  FKD_CUDA(launch_radius(g, tab, dctr, drad, q, order, nullptr, doff, dout, h->err.as<uint32_t>(), h->dim,
+                         h->stream));
+  FKD_CUDA(h->tmp.ensure(tot * sizeof(uint32_t)));
+  FKD_CUDA(launch_order_results(g, tab, doff, q, dout, h->tmp.as<uint32_t>(), h->err.as<uint32_t>(), h->stream));
+  if (mem == FKD_MEM_HOST)
+    FKD_CUDA(cudaMemcpyAsync(ids_out, dout, tot * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+  return finish(h, "fkd_search_radius", mem);
+}
+
+uint32_t fkd_knn_max_k(void) { return KNN_MAX; }
+
+fkd_status fkd_search_knn(fkd_tree h, const float* centers, uint64_t q, uint32_t k, uint32_t* ids_out,
+                          float* dist2_out, int mem) {
+  fkd_status s = check_nn_args(h, centers, q, mem);
+  if (s != FKD_OK) return s;
+  if (k < 1 || k > KNN_MAX) return fail(FKD_ERR_ARG, "k must be 1..fkd_knn_max_k()");
+  if (q && !ids_out) return fail(FKD_ERR_ARG, "null ids_out");
+  if (q == 0) return FKD_OK;
+  const float* dctr = nullptr;
+  if ((s = stage_centres(h, centers, nullptr, q, mem, &dctr, nullptr)) != FKD_OK) return s;
+  const uint64_t cells = q * (uint64_t)k;
+  uint32_t* di = ids_out;
+  float* dd = dist2_out;
+  if (mem == FKD_MEM_HOST) {
+    FKD_CUDA(h->out.ensure(cells * sizeof(uint32_t)));
+    di = h->out.as<uint32_t>();
+    if (dist2_out) {
+      FKD_CUDA(h->tmp.ensure(cells * sizeof(float)));
+      dd = h->tmp.as<float>();
+    }
+  }
+  FKD_CUDA(cudaMemsetAsync(h->err.p, 0, sizeof(uint32_t), h->stream));
+  const uint32_t* order = nullptr;
+  if ((s = centre_order(h, dctr, q, &order)) != FKD_OK) return s;
+  FKD_CUDA(launch_knn(make_geom((uint32_t)h->n), table_of(h), dctr, q, order, k, di, dd, h->err.as<uint32_t>(),
+                      h->dim, h->stream));
+  if (mem == FKD_MEM_HOST) {
+    FKD_CUDA(cudaMemcpyAsync(ids_out, di, cells * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+    if (dist2_out) FKD_CUDA(cudaMemcpyAsync(dist2_out, dd, cells * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+  }
+  return finish(h, "fkd_search_knn", mem);
 }
 
 fkd_status fkd_set_param(fkd_tree h, const char* name, int64_t value) {

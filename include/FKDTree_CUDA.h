@@ -19,6 +19,8 @@
 //   * search_in_the_box_multiple returns per-box counts, the OpenCL backend's
 //     meaning (FKDTree_opencl.h:123-164) -- the CPU backend's is a stub;
 //   * search_in_the_box_batch is the bulk form (one GPU launch for all boxes);
+//   * search_in_the_ball / nearest_neighbours add radius and kNN queries on the
+//     same tree (no reference counterpart; fkd_search_radius, fkd_search_knn);
 //   * getDimensionVector / getIdVector download the tables lazily after a
 //     build, like FKDTree_OpenCL (FKDTree_opencl.h:194-206);
 //   * failures throw std::runtime_error carrying fkd_last_error(); the
@@ -45,12 +47,12 @@ class FKDTree_CUDA : public FKDTree<TYPE, numberOfDimensions> {
  public:
   typedef FKDPoint<TYPE, numberOfDimensions> Point;
 
+  // The points are kept as given (the reference copies them into its own SoA
+  // arrays, FKDTree_cpu.h:19-23); build() uploads them in FKDPoint layout.
   explicit FKDTree_CUDA(const std::vector<Point>& points, void* stream = nullptr)
-      : n_(points.size()), coords_(numberOfDimensions * points.size()), ids_(points.size()), synced_(false) {
-    for (size_t i = 0; i < n_; ++i) {
-      for (unsigned int c = 0; c < numberOfDimensions; ++c) coords_[c * n_ + i] = points[i][c];
-      ids_[i] = points[i].getId();
-    }
+      : n_(points.size()), points_(points), synced_(false) {
+    static_assert(sizeof(Point) == (numberOfDimensions + 1) * sizeof(float),
+                  "FKDPoint<float, dim> is dim floats followed by the id (FKDPoint.h:102-103)");
     check(fkd_create((int)numberOfDimensions, 0u, stream, &h_));
   }
 
@@ -59,8 +61,39 @@ class FKDTree_CUDA : public FKDTree<TYPE, numberOfDimensions> {
   FKDTree_CUDA& operator=(const FKDTree_CUDA&) = delete;
 
   void build() override {
-    check(fkd_build(h_, coords_.data(), ids_.data(), n_, FKD_MEM_HOST));
+    check(fkd_build_points(h_, points_.data(), n_, FKD_MEM_HOST));
     synced_ = false;
+  }
+
+  // Ids of the points within `radius` of `centre` (squared float32 distance
+  // <= radius * radius), ascending heap order.  No reference counterpart.
+  std::vector<unsigned int> search_in_the_ball(const Point& centre, float radius) {
+    float c[numberOfDimensions];
+    for (unsigned int d = 0; d < numberOfDimensions; ++d) c[d] = centre[d];
+    unsigned int count = 0;
+    check(fkd_search_radius_count(h_, c, &radius, 1, &count, FKD_MEM_HOST));
+    std::vector<unsigned int> out(count);
+    uint64_t offsets[2] = {0, 0};
+    uint64_t total = 0;
+    check(fkd_search_radius(h_, c, &radius, 1, offsets, out.data(), count, &total, FKD_MEM_HOST));
+    return out;
+  }
+
+  // The k nearest points of `centre`, ascending in (squared distance, id);
+  // fewer than k when the tree is smaller.  No reference counterpart.
+  std::vector<unsigned int> nearest_neighbours(const Point& centre, unsigned int k,
+                                               std::vector<float>* dist2 = nullptr) {
+    float c[numberOfDimensions];
+    for (unsigned int d = 0; d < numberOfDimensions; ++d) c[d] = centre[d];
+    std::vector<unsigned int> ids(k);
+    std::vector<float> d2(k);
+    check(fkd_search_knn(h_, c, 1, k, ids.data(), d2.data(), FKD_MEM_HOST));
+    size_t m = 0;
+    while (m < k && ids[m] != 0xffffffffu) ++m;
+    ids.resize(m);
+    d2.resize(m);
+    if (dist2) *dist2 = d2;
+    return ids;
   }
 
   std::vector<unsigned int> search_in_the_box(const Point& minPoint, const Point& maxPoint) override {
@@ -161,8 +194,7 @@ class FKDTree_CUDA : public FKDTree<TYPE, numberOfDimensions> {
   }
 
   size_t n_;
-  std::vector<float> coords_;
-  std::vector<unsigned int> ids_;
+  std::vector<Point> points_;
   fkd_tree h_ = nullptr;
   bool synced_;
   std::vector<std::vector<TYPE>> dims_;

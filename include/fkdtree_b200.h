@@ -98,6 +98,13 @@ FKD_API fkd_status fkd_set_stream(fkd_tree h, void* stream);
  * call). */
 FKD_API fkd_status fkd_build(fkd_tree h, const float* coords, const uint32_t* ids, uint64_t n, int mem);
 
+/* Same as fkd_build, from points in the reference's FKDPoint<float, dim>
+ * layout (FKDPoint.h:102-103, the element type of the std::vector the
+ * FKDTree_CPU constructor takes, FKDTree_cpu.h:19-23): per point dim floats
+ * then the uint32 id, (dim + 1) * 4 bytes, n points back to back.  Saves the
+ * caller the conversion to SoA; the tree is the same. */
+FKD_API fkd_status fkd_build_points(fkd_tree h, const void* points, uint64_t n, int mem);
+
 /* Builds one small tree without allocating any memory (no counterpart in the
  * reference).  For callers that may not call cudaMalloc / cudaFree while
  * they work -- code inside a framework that owns all device memory through
@@ -156,6 +163,34 @@ FKD_API fkd_status fkd_search(fkd_tree h, const float* mins, const float* maxs, 
  * for test_correct_search (FKDTree.h:54-86) at scale. */
 FKD_API fkd_status fkd_search_digest(fkd_tree h, const float* mins, const float* maxs, uint64_t q, uint32_t* counts,
                              uint64_t* digests, int mem);
+
+/* ------------------------------------------------ radius and kNN search
+ * No reference counterpart (the reference answers boxes only); both walk the
+ * same tree with the reference's split rule (FKDTree_cpu.h:240-269) and
+ * prune by the distance to the split plane, exactly (no point is missed).
+ * centers: dim*q floats SoA like the boxes.  Distances are squared Euclidean
+ * in float32, evaluated as (((0 + (p0-c0)^2) + (p1-c1)^2) + ...) with every
+ * operation rounded separately (no fused multiply-add). */
+
+/* Number of points within distance radii[j] of centre j: those with
+ * d2 <= radii[j]*radii[j] (rounded to float).  A negative or NaN radius, or a
+ * centre with a NaN coordinate, matches nothing. */
+FKD_API fkd_status fkd_search_radius_count(fkd_tree h, const float* centers, const float* radii, uint64_t q,
+                                           uint32_t* counts, int mem);
+/* Ids of those points, query j in ids_out[offsets_out[j] .. offsets_out[j+1])
+ * in ascending heap-index order; offsets_out receives q+1 entries, *total the
+ * number of results; FKD_ERR_CAPACITY (no ids written) when total > capacity. */
+FKD_API fkd_status fkd_search_radius(fkd_tree h, const float* centers, const float* radii, uint64_t q,
+                                     uint64_t* offsets_out, uint32_t* ids_out, uint64_t capacity, uint64_t* total,
+                                     int mem);
+/* The k nearest points of every centre (1 <= k <= fkd_knn_max_k()), ascending
+ * in (d2, id): ids_out[j*k + m] and, unless dist2_out is NULL,
+ * dist2_out[j*k + m] = d2.  Ties of d2 go to the smaller id, so the answer
+ * depends on the point set only.  Points with a NaN d2 never qualify; rows
+ * with fewer than k neighbours end in id 0xffffffff, d2 = +inf. */
+FKD_API fkd_status fkd_search_knn(fkd_tree h, const float* centers, uint64_t q, uint32_t k, uint32_t* ids_out,
+                                  float* dist2_out, int mem);
+FKD_API uint32_t fkd_knn_max_k(void);
 
 /* Waits for the handle's stream and reports any device-side error latched by
  * earlier asynchronous calls. */

@@ -2,6 +2,7 @@
 // behind the reference's FKDTree<T, dim> interface.  Built by oracle/Makefile
 // (target `dropin`, against the reference headers) into oracle/_ref/test_dropin;
 // run on a GPU by tests/test_dropin_gpu.py.  Prints "DROPIN OK" on success.
+#include <algorithm>
 #include <cstdio>
 #include <memory>
 #include <random>
@@ -9,6 +10,18 @@
 
 #include "FKDTree_CUDA.h"
 #include "FKDTree_cpu.h"
+
+// squared distance as the library evaluates it: each operation rounded on its
+// own, coordinates in order (the Makefile compiles this with -ffp-contract=off)
+template <int D>
+static float dist2(const FKDPoint<float, D>& p, const FKDPoint<float, D>& c) {
+  float acc = 0.f;
+  for (int d = 0; d < D; ++d) {
+    const float t = p[d] - c[d];
+    acc = acc + t * t;
+  }
+  return acc;
+}
 
 template <unsigned D>
 static int run(unsigned n, unsigned seed, float hw) {
@@ -63,7 +76,38 @@ static int run(unsigned n, unsigned seed, float hw) {
       return 1;
     }
   }
-  std::printf("dim %u n %u: %u boxes identical\n", D, n, q);
+  // radius and kNN queries against the reference's box search and a brute force
+  std::vector<unsigned> heap_of(n);  // id -> heap index
+  for (unsigned i = 0; i < n; ++i) heap_of[cpu.getIdVector()[i]] = i;
+  for (unsigned j = 0; j < 200 && j < n; ++j) {
+    const float r = hw * (1.f + (float)(j % 3));
+    FKDPoint<float, D> blo, bhi;
+    for (unsigned c = 0; c < D; ++c) {
+      blo.setDimension(c, pts[j][c] - r * 1.001f - 1e-6f);
+      bhi.setDimension(c, pts[j][c] + r * 1.001f + 1e-6f);
+    }
+    std::vector<unsigned> box, want;
+    cpu.search_in_the_box_recursive(blo, bhi, box);  // no frontier bound
+    for (unsigned id : box)
+      if (dist2(pts[id], pts[j]) <= r * r) want.push_back(id);
+    std::sort(want.begin(), want.end(), [&](unsigned a, unsigned b) { return heap_of[a] < heap_of[b]; });
+    if (cu->search_in_the_ball(pts[j], r) != want) {
+      std::printf("ball %u: results differ\n", j);
+      return 1;
+    }
+    std::vector<std::pair<float, unsigned>> all;
+    for (unsigned i = 0; i < n; ++i) all.emplace_back(dist2(pts[i], pts[j]), pts[i].getId());
+    const unsigned k = 1 + j % 20;
+    std::partial_sort(all.begin(), all.begin() + k, all.end());
+    std::vector<float> d2;
+    std::vector<unsigned> nn = cu->nearest_neighbours(pts[j], k, &d2);
+    for (unsigned m = 0; m < k; ++m)
+      if (nn.size() != k || nn[m] != all[m].second || d2[m] != all[m].first) {
+        std::printf("knn %u: results differ at %u\n", j, m);
+        return 1;
+      }
+  }
+  std::printf("dim %u n %u: %u boxes identical, 200 balls and kNN rows identical\n", D, n, q);
   return 0;
 }
 
