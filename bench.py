@@ -67,6 +67,7 @@ def parse_args():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-queries", type=int, default=8192, help="box sample of the CPU baseline")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched / learned events report")
+    ap.add_argument("--no-nn", action="store_true", help="skip the radius / kNN search report")
     ap.add_argument("--queries", type=int, default=0,
                     help="box count of the 16M-point workload (0: 1,048,576; smaller cases are for profiling)")
     ap.add_argument("--batched-events", type=int, default=4096)
@@ -516,6 +517,8 @@ def run_ours(args):
 
     if not args.no_e2e:
         line["e2e"] = run_e2e(args, L, h, ev, results, stream, world, barrier, dev)
+    if rank == 0 and world == 1 and not args.no_nn:
+        line["radius_knn"] = nn_report(L, h, ev, dev, stream, out)
     _capi.check(L.fkd_destroy(h))
     del coords, ids, mins, maxs, offsets, counts, out
     torch.cuda.empty_cache()
@@ -527,6 +530,73 @@ def run_ours(args):
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def nn_report(L, h, ev, dev, stream, out, reps=3, k=16):
+    """Radius and kNN search on the built tree (fkd_nn.cu; no reference
+    counterpart): every box's inscribed ball (centre, smallest half-width) and
+    the k nearest points of every box centre, device buffers, CUDA events on
+    the library's stream, best of `reps` after one warm-up call."""
+    import torch
+
+    from fkdtree_b200 import _capi
+    P = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+    n, q, dim = ev.n, ev.q, ev.dim
+    ctr = torch.from_numpy(((ev.mins + ev.maxs) * np.float32(0.5)).astype(np.float32)).to(dev)
+    rad = torch.from_numpy(((ev.maxs - ev.mins) * np.float32(0.5)).min(axis=0).astype(np.float32)).to(dev)
+    offs = torch.empty(q + 1, dtype=torch.int64, device=dev)
+    kids = torch.empty((q, k), dtype=torch.int32, device=dev)
+    kd2 = torch.empty((q, k), dtype=torch.float32, device=dev)
+    total = C.c_uint64(0)
+
+    cnt = torch.empty(q, dtype=torch.int32, device=dev)
+
+    def radius(ordered=0):
+        _capi.check(L.fkd_search_radius(h, P(ctr), P(rad), q, P(offs), P(out), out.numel(), C.byref(total),
+                                        ordered, _capi.MEM_DEVICE))
+
+    def radius_count():
+        _capi.check(L.fkd_search_radius_count(h, P(ctr), P(rad), q, P(cnt), _capi.MEM_DEVICE))
+
+    def knn():
+        _capi.check(L.fkd_search_knn(h, P(ctr), q, k, P(kids), P(kd2), _capi.MEM_DEVICE))
+
+    def best_ms(fn):
+        fn()
+        _capi.check(L.fkd_sync(h))
+        best = float("inf")
+        for _ in range(reps):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            torch.cuda.synchronize()
+            best = min(best, a.elapsed_time(b))
+        _capi.check(L.fkd_sync(h))
+        return best
+
+    peak, _ = hbm_peak()
+    c_ms = best_ms(radius_count)
+    o_ms = best_ms(lambda: radius(1))
+    r_ms = best_ms(radius)
+    res = int(total.value)
+    r_bytes = n * (4 * dim + 4) + q * (4 * dim + 4 + 8 + 4) + 4 * res
+    k_ms = best_ms(knn)
+    k_bytes = n * (4 * dim + 4) + q * (4 * dim) + q * k * 8
+    return {
+        "radius": {"queries": q, "results": res, "ms": r_ms, "count_pass_ms": c_ms, "ordered_ms": o_ms,
+                   "mqueries_per_s": q / r_ms / 1e3,
+                   "algorithmic_bytes": r_bytes, "gbs": r_bytes / r_ms / 1e6, "frac_of_hbm": r_bytes / r_ms / 1e6 / peak,
+                   "bytes_rule": "tree once + centre, radius, count, offset per query + 4 B per result id",
+                   "kernels": ["k_radius (count)", "k_scan_*", "k_radius (write)"],
+                   "note": "ms: depth-first order (like the box search line's unordered write); ordered_ms adds "
+                           "the sort to ascending heap index (k_order)"},
+        "knn": {"queries": q, "k": k, "ms": k_ms, "mqueries_per_s": q / k_ms / 1e3,
+                "algorithmic_bytes": k_bytes, "gbs": k_bytes / k_ms / 1e6, "frac_of_hbm": k_bytes / k_ms / 1e6 / peak,
+                "bytes_rule": "tree once + centre per query + (id, d2) per neighbour", "kernels": ["k_knn"]},
+        "workload": "the bench tree; centres = box centres, radius = smallest box half-width, k = 16",
+    }
 
 
 def run_e2e(args, L, h, ev, results, stream, world, barrier, dev):

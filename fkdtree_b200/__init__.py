@@ -252,9 +252,10 @@ class FKDTree:
         check(self._lib.fkd_search_radius_count(self._h, _ptr(ctr), _ptr(rad), q, _ptr(counts), mem))
         return counts
 
-    def search_radius(self, centres, radii, capacity: int | None = None):
-        """Returns (offsets (q+1,), ids): the ids of query j, in ascending heap
-        index, are ids[offsets[j]:offsets[j+1]]."""
+    def search_radius(self, centres, radii, ordered: bool = True, capacity: int | None = None):
+        """Returns (offsets (q+1,), ids): the ids of query j are
+        ids[offsets[j]:offsets[j+1]], in ascending heap index when ``ordered``
+        (else in the walk's depth-first order)."""
         ctr, mem, q = self._centres(centres)
         rad = self._radii(radii, q, mem, ctr)
         if capacity is None:
@@ -269,7 +270,7 @@ class FKDTree:
             offsets = np.empty(q + 1, dtype=np.uint64)
             out = np.empty(max(capacity, 1), dtype=np.uint32)
         check(self._lib.fkd_search_radius(self._h, _ptr(ctr), _ptr(rad), q, _ptr(offsets), _ptr(out), capacity,
-                                          C.byref(total), mem))
+                                          C.byref(total), int(ordered), mem))
         return offsets, out[:total.value]
 
     def knn(self, centres, k: int):

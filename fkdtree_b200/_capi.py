@@ -39,7 +39,7 @@ SIGNATURES = {
     "fkd_search_digest": ([_vp, _vp, _vp, _u64, _vp, _vp, _int], _int),
     "fkd_build_points": ([_vp, _vp, _u64, _int], _int),
     "fkd_search_radius_count": ([_vp, _vp, _vp, _u64, _vp, _int], _int),
-    "fkd_search_radius": ([_vp, _vp, _vp, _u64, _vp, _vp, _u64, C.POINTER(_u64), _int], _int),
+    "fkd_search_radius": ([_vp, _vp, _vp, _u64, _vp, _vp, _u64, C.POINTER(_u64), _int, _int], _int),
     "fkd_search_knn": ([_vp, _vp, _u64, _u32, _vp, _vp, _int], _int),
     "fkd_knn_max_k": ([], _u32),
     "fkd_sync": ([_vp], _int),

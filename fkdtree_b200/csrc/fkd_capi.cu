@@ -782,7 +782,7 @@ fkd_status fkd_search_radius_count(fkd_tree h, const float* centers, const float
   FKD_CUDA(cudaMemsetAsync(h->err.p, 0, sizeof(uint32_t), h->stream));
   const uint32_t* order = nullptr;
   if ((s = centre_order(h, dctr, q, &order)) != FKD_OK) return s;
-  FKD_CUDA(launch_radius(make_geom((uint32_t)h->n), table_of(h), dctr, drad, q, order, dc, nullptr, nullptr,
+  FKD_CUDA(launch_radius(make_geom((uint32_t)h->n), table_of(h), dctr, drad, q, order, dc, nullptr, nullptr, 0,
                          h->err.as<uint32_t>(), h->dim, h->stream));
   if (mem == FKD_MEM_HOST)
     FKD_CUDA(cudaMemcpyAsync(counts, dc, q * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
@@ -790,7 +790,7 @@ fkd_status fkd_search_radius_count(fkd_tree h, const float* centers, const float
 }
 
 fkd_status fkd_search_radius(fkd_tree h, const float* centers, const float* radii, uint64_t q, uint64_t* offsets_out,
-                             uint32_t* ids_out, uint64_t capacity, uint64_t* total, int mem) {
+                             uint32_t* ids_out, uint64_t capacity, uint64_t* total, int ordered, int mem) {
   fkd_status s = check_nn_args(h, centers, q, mem);
   if (s != FKD_OK) return s;
   if (!offsets_out || !total) return fail(FKD_ERR_ARG, "null offsets_out or total");
@@ -809,7 +809,7 @@ fkd_status fkd_search_radius(fkd_tree h, const float* centers, const float* radi
   if (q && (s = centre_order(h, dctr, q, &order)) != FKD_OK) return s;
   const Geom g = make_geom((uint32_t)h->n);
   const Table tab = table_of(h);
-  FKD_CUDA(launch_radius(g, tab, dctr, drad, q, order, h->counts.as<uint32_t>(), nullptr, nullptr,
+  FKD_CUDA(launch_radius(g, tab, dctr, drad, q, order, h->counts.as<uint32_t>(), nullptr, nullptr, 0,
                          h->err.as<uint32_t>(), h->dim, h->stream));
   FKD_CUDA(launch_scan_counts(h->counts.as<uint32_t>(), q, doff, h->partials.as<unsigned long long>(), h->stream));
   FKD_CUDA(cudaMemcpyAsync(h->herr + 2, doff + q, sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
@@ -837,10 +837,13 @@ fkd_status fkd_search_radius(fkd_tree h, const float* centers, const float* radi
     FKD_CUDA(h->out.ensure(tot * sizeof(uint32_t)));
     dout = h->out.as<uint32_t>();
   }
-  FKD_CUDA(launch_radius(g, tab, dctr, drad, q, order, nullptr, doff, dout, h->err.as<uint32_t>(), h->dim,
-                         h->stream));
-  FKD_CUDA(h->tmp.ensure(tot * sizeof(uint32_t)));
-  FKD_CUDA(launch_order_results(g, tab, doff, q, dout, h->tmp.as<uint32_t>(), h->err.as<uint32_t>(), h->stream));
+  // ordered: the write pass emits heap indices that k_order sorts and maps to ids
+  FKD_CUDA(launch_radius(g, tab, dctr, drad, q, order, nullptr, doff, dout, ordered ? 1 : 0, h->err.as<uint32_t>(),
+                         h->dim, h->stream));
+  if (ordered) {
+    FKD_CUDA(h->tmp.ensure(tot * sizeof(uint32_t)));
+    FKD_CUDA(launch_order_results(g, tab, doff, q, dout, h->tmp.as<uint32_t>(), h->err.as<uint32_t>(), h->stream));
+  }
   if (mem == FKD_MEM_HOST)
     FKD_CUDA(cudaMemcpyAsync(ids_out, dout, tot * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
   return finish(h, "fkd_search_radius", mem);

@@ -190,11 +190,12 @@ cudaError_t launch_box_order(const Geom& g, const Table& tab, const Boxes& b, in
                              uint32_t** order_out, cudaStream_t stream);
 // fkd_nn.cu: radius and k-nearest-neighbour search (one thread per query;
 // ctr is the SoA centre array of stride q).  launch_radius counts into
-// `counts` when `out` is null, else writes heap indices at `offsets`.
+// `counts` when `out` is null, else writes heap indices (heap_out) or ids at
+// `offsets`.
 constexpr uint32_t KNN_MAX = 64;
 cudaError_t launch_radius(const Geom& g, const Table& tab, const float* ctr, const float* rad, uint64_t q,
                           const uint32_t* order, uint32_t* counts, const uint64_t* offsets, uint32_t* out,
-                          uint32_t* err, int dim, cudaStream_t stream);
+                          int heap_out, uint32_t* err, int dim, cudaStream_t stream);
 cudaError_t launch_knn(const Geom& g, const Table& tab, const float* ctr, uint64_t q, const uint32_t* order,
                        uint32_t k, uint32_t* ids, float* d2, uint32_t* err, int dim, cudaStream_t stream);
 // Exclusive prefix sum of q uint32 counts into q+1 uint64 offsets.

@@ -24,10 +24,10 @@
 //
 // Radius: point p qualifies for query (c, r) when d2 <= fl(r*r) and r >= 0.
 //   A negative or NaN radius, or a centre with a NaN coordinate, qualifies
-//   nothing.  A count pass, a write pass of heap indices, then every query's
-//   slice is sorted by heap index and mapped to ids (launch_order_results):
-//   within a query the ids come in ascending heap-index order, the order of
-//   the ordered box search.
+//   nothing.  A count pass, then a write pass: of ids in the walk's
+//   depth-first order, or (ordered) of heap indices that launch_order_results
+//   sorts and maps to ids -- ascending heap-index order, the order of the
+//   ordered box search.
 // kNN: the k points smallest in (d2, id) order, ascending.  Ties of d2 go to
 //   the smaller id, so the answer depends on the point set only, not on the
 //   tree.  Points whose d2 is NaN never qualify; a centre with a NaN
@@ -78,13 +78,14 @@ __device__ __forceinline__ bool load_centre(const float* __restrict__ ctr, uint6
 }
 
 // Radius search; out == nullptr: count pass (counts[j]); otherwise write pass
-// of heap indices into out[offsets[j] ..).
+// into out[offsets[j] ..) of heap indices (heap_out) or ids.
 template <int DIM>
 __global__ void __launch_bounds__(NNT) k_radius(Geom g, const uint4* __restrict__ nodes,
-                                                const float* __restrict__ ctr, const float* __restrict__ rad,
-                                                uint64_t q, const uint32_t* __restrict__ order,
-                                                uint32_t* __restrict__ counts, const uint64_t* __restrict__ offsets,
-                                                uint32_t* __restrict__ out, uint32_t* __restrict__ err) {
+                                                const uint32_t* __restrict__ ids, const float* __restrict__ ctr,
+                                                const float* __restrict__ rad, uint64_t q,
+                                                const uint32_t* __restrict__ order, uint32_t* __restrict__ counts,
+                                                const uint64_t* __restrict__ offsets, uint32_t* __restrict__ out,
+                                                int heap_out, uint32_t* __restrict__ err) {
   const uint64_t t = (uint64_t)blockIdx.x * NNT + threadIdx.x;
   if (t >= q) return;
   const uint64_t j = order ? (uint64_t)order[t] : t;
@@ -113,7 +114,7 @@ __global__ void __launch_bounds__(NNT) k_radius(Geom g, const uint4* __restrict_
         if (node_dist2<DIM>(nd, qc) <= r2) {
           if (write) {
             if (cnt < room)
-              out[base + cnt] = i;
+              out[base + cnt] = heap_out ? i : (DIM <= 3 ? nd.w : __ldg(ids + i));
             else
               atomicOr(err, ERRB_INTERNAL);
           }
@@ -251,10 +252,11 @@ __global__ void __launch_bounds__(NNT) k_knn(Geom g, const uint4* __restrict__ n
 
 template <int DIM>
 cudaError_t radius_dim(const Geom& g, const Table& tab, const float* ctr, const float* rad, uint64_t q,
-                       const uint32_t* order, uint32_t* counts, const uint64_t* offsets, uint32_t* out, uint32_t* err,
-                       cudaStream_t stream) {
+                       const uint32_t* order, uint32_t* counts, const uint64_t* offsets, uint32_t* out, int heap_out,
+                       uint32_t* err, cudaStream_t stream) {
   const uint64_t blocks = (q + NNT - 1) / NNT;
-  k_radius<DIM><<<(unsigned)blocks, NNT, 0, stream>>>(g, tab.nodes, ctr, rad, q, order, counts, offsets, out, err);
+  k_radius<DIM><<<(unsigned)blocks, NNT, 0, stream>>>(g, tab.nodes, tab.ids, ctr, rad, q, order, counts, offsets,
+                                                      out, heap_out, err);
   count_launches(1);
   return cudaGetLastError();
 }
@@ -272,13 +274,13 @@ cudaError_t knn_dim(const Geom& g, const Table& tab, const float* ctr, uint64_t 
 
 cudaError_t launch_radius(const Geom& g, const Table& tab, const float* ctr, const float* rad, uint64_t q,
                           const uint32_t* order, uint32_t* counts, const uint64_t* offsets, uint32_t* out,
-                          uint32_t* err, int dim, cudaStream_t stream) {
+                          int heap_out, uint32_t* err, int dim, cudaStream_t stream) {
   if (q == 0) return cudaSuccess;
   switch (dim) {
-    case 1: return radius_dim<1>(g, tab, ctr, rad, q, order, counts, offsets, out, err, stream);
-    case 2: return radius_dim<2>(g, tab, ctr, rad, q, order, counts, offsets, out, err, stream);
-    case 3: return radius_dim<3>(g, tab, ctr, rad, q, order, counts, offsets, out, err, stream);
-    default: return radius_dim<4>(g, tab, ctr, rad, q, order, counts, offsets, out, err, stream);
+    case 1: return radius_dim<1>(g, tab, ctr, rad, q, order, counts, offsets, out, heap_out, err, stream);
+    case 2: return radius_dim<2>(g, tab, ctr, rad, q, order, counts, offsets, out, heap_out, err, stream);
+    case 3: return radius_dim<3>(g, tab, ctr, rad, q, order, counts, offsets, out, heap_out, err, stream);
+    default: return radius_dim<4>(g, tab, ctr, rad, q, order, counts, offsets, out, heap_out, err, stream);
   }
 }
 

@@ -75,7 +75,7 @@ class FKDTree_CUDA : public FKDTree<TYPE, numberOfDimensions> {
     std::vector<unsigned int> out(count);
     uint64_t offsets[2] = {0, 0};
     uint64_t total = 0;
-    check(fkd_search_radius(h_, c, &radius, 1, offsets, out.data(), count, &total, FKD_MEM_HOST));
+    check(fkd_search_radius(h_, c, &radius, 1, offsets, out.data(), count, &total, 1, FKD_MEM_HOST));
     return out;
   }
 

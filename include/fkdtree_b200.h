@@ -177,12 +177,14 @@ FKD_API fkd_status fkd_search_digest(fkd_tree h, const float* mins, const float*
  * centre with a NaN coordinate, matches nothing. */
 FKD_API fkd_status fkd_search_radius_count(fkd_tree h, const float* centers, const float* radii, uint64_t q,
                                            uint32_t* counts, int mem);
-/* Ids of those points, query j in ids_out[offsets_out[j] .. offsets_out[j+1])
- * in ascending heap-index order; offsets_out receives q+1 entries, *total the
- * number of results; FKD_ERR_CAPACITY (no ids written) when total > capacity. */
+/* Ids of those points, query j in ids_out[offsets_out[j] .. offsets_out[j+1]):
+ * in ascending heap-index order when `ordered` is nonzero, otherwise in the
+ * walk's depth-first order (deterministic; the same set).  offsets_out
+ * receives q+1 entries, *total the number of results; FKD_ERR_CAPACITY (no
+ * ids written) when total > capacity. */
 FKD_API fkd_status fkd_search_radius(fkd_tree h, const float* centers, const float* radii, uint64_t q,
                                      uint64_t* offsets_out, uint32_t* ids_out, uint64_t capacity, uint64_t* total,
-                                     int mem);
+                                     int ordered, int mem);
 /* The k nearest points of every centre (1 <= k <= fkd_knn_max_k()), ascending
  * in (d2, id): ids_out[j*k + m] and, unless dist2_out is NULL,
  * dist2_out[j*k + m] = d2.  Ties of d2 go to the smaller id, so the answer

@@ -80,6 +80,9 @@ def knn(coords: np.ndarray, ids: np.ndarray, centres: np.ndarray, k: int):
             continue
         d2 = dist2(coords, c)
         ok = np.nonzero(~np.isnan(d2))[0]
+        if ok.size > k:  # keep the candidates up to the k-th smallest d2 (ties included)
+            kth = np.partition(d2[ok], k - 1)[k - 1]
+            ok = ok[d2[ok] <= kth]
         sel = ok[np.lexsort((ids[ok], d2[ok]))][:k]
         out_i[j, :sel.size] = ids[sel]
         out_d[j, :sel.size] = d2[sel]

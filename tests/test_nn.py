@@ -65,7 +65,7 @@ def test_abi_arg_checks_without_gpu():
     assert L.fkd_build_points(None, None, 0, 0) == 1
     assert L.fkd_search_radius_count(None, None, None, 0, None, 0) == 1
     tot = C.c_uint64(0)
-    assert L.fkd_search_radius(None, None, None, 0, None, None, 0, C.byref(tot), 0) == 1
+    assert L.fkd_search_radius(None, None, None, 0, None, None, 0, C.byref(tot), 1, 0) == 1
     assert L.fkd_search_knn(None, None, 0, 1, None, None, 0) == 1
 
 
@@ -150,6 +150,10 @@ def test_radius_matches_checker(cuda, n, dim, grid):
     off, got = t.search_radius(ctr, rad)
     assert np.array_equal(off, woff)
     assert np.array_equal(got, wids)
+    off, got = t.search_radius(ctr, rad, ordered=False)  # depth-first order: the same sets
+    assert np.array_equal(off, woff)
+    for a, b in zip(slices(off, got), slices(woff, wids)):
+        assert np.array_equal(np.sort(a), np.sort(b))
 
 
 @pytest.mark.gpu
