@@ -653,9 +653,10 @@ def ref_step(oracle_mod, ev, nq_sample, threads):
     r = oracle_mod.RefTree(ev.coords, ev.ids)
     tb = r.build()
     sel = np.linspace(0, ev.q - 1, nq_sample).astype(np.int64)
-    _, _, _, ts = r.search(ev.mins[:, sel], ev.maxs[:, sel], variant=oracle_mod.RECURSIVE, want_ids=True,
-                           threads=threads)
+    counts, _, _, ts = r.search(ev.mins[:, sel], ev.maxs[:, sel], variant=oracle_mod.RECURSIVE, want_ids=True,
+                                threads=threads)
     r.close()
+    ref_step.last_counts = counts
     return tb, ts * ev.q / nq_sample
 
 
@@ -666,11 +667,24 @@ def cpu_baseline(ev, nq_sample):
                 "sample": "reference CPU build unavailable (oracle/_ref not built)"}
     threads = O.host_threads()
     tb, ts = ref_step(O, ev, nq_sample, threads)
-    return {"value": ev.n / (tb + ts) / 1e6, "unit": "Mpoints/s", "kind": "reference", "cores": threads,
-            "build_s": tb, "search_s": ts,
-            "sample": (f"FKDTree_CPU::build of all {ev.n} points (serial, as in the reference) + "
-                       f"search_in_the_box_recursive on {nq_sample} of {ev.q} boxes with {threads} OpenMP threads, "
-                       "search time scaled to all boxes")}
+    out = {"value": ev.n / (tb + ts) / 1e6, "unit": "Mpoints/s", "kind": "reference", "cores": threads,
+           "build_s": tb, "search_s": ts,
+           "sample": (f"FKDTree_CPU::build of all {ev.n} points (serial, as in the reference) + "
+                      f"search_in_the_box_recursive on {nq_sample} of {ev.q} boxes with {threads} OpenMP threads, "
+                      "search time scaled to all boxes")}
+    if ev.dim == 3:
+        # the reference's other CPU tree, an extra column (main.cpp:558-612)
+        sel = np.linspace(0, ev.q - 1, nq_sample).astype(np.int64)
+        vc, vb, vs = O.ref_cmssw(ev.coords, ev.mins[:, sel], ev.maxs[:, sel])
+        vs_all = vs * ev.q / nq_sample
+        out["cmssw_vanilla"] = {
+            "value": ev.n / (vb + vs_all) / 1e6, "unit": "Mpoints/s", "kind": "reference", "cores": 1,
+            "build_s": vb, "search_s": vs_all,
+            "counts_equal_fkdtree": float(np.mean(vc == ref_step.last_counts)),
+            "sample": (f"KDTreeLinkerAlgo<unsigned, 3> (KDTreeLinkerAlgoT.h) build of all {ev.n} points + serial "
+                       f"search of {nq_sample} of {ev.q} boxes, as main.cpp runs it; search time scaled to all "
+                       "boxes")}
+    return out
 
 
 def run_reference(args):

@@ -87,6 +87,8 @@ def ref_lib():
         L.fkdref_batch.argtypes = [C.c_uint32, _u32p, _u64p, _u64p, _f32p, _u32p, _u64p, _u64p, _f32p, _f32p, _u32p,
                                    _u64p, C.c_int]
         L.fkdref_batch.restype = C.c_double
+        L.fkdref_cmssw.argtypes = [C.c_uint32, _f32p, C.c_uint64, _f32p, _f32p, _u32p, C.POINTER(C.c_double)]
+        L.fkdref_cmssw.restype = C.c_double
         _ref = L
     return _ref
 
@@ -190,6 +192,25 @@ def ref_batch(b, threads: int = 0):
                                  _soa(b.q_off, np.uint64), _soa(b.qcoord_off, np.uint64), _soa(b.mins, np.float32),
                                  _soa(b.maxs, np.float32), counts, dig, threads)
     return counts, dig, float(sec)
+
+
+def ref_cmssw(coords, mins, maxs):
+    """The reference's vanilla CMSSW tree (KDTreeLinkerAlgoT.h) over 3D points,
+    built and searched serially as main.cpp:558-612 does: returns (counts,
+    build_seconds, search_seconds).  Its search tests boxes with strict
+    inequalities for inner regions (KDTreeLinkerAlgoT.h:186-207), so points
+    lying exactly on a box face may be missed; counts equal FKDTree's
+    otherwise."""
+    coords = _soa(coords, np.float32)
+    mins = _soa(mins, np.float32)
+    maxs = _soa(maxs, np.float32)
+    if coords.shape[0] != 3:
+        raise ValueError("the vanilla CMSSW comparison is 3D (main.cpp:564)")
+    q = mins.shape[1]
+    counts = np.empty(q, dtype=np.uint32)
+    ts = C.c_double(0.0)
+    tb = ref_lib().fkdref_cmssw(coords.shape[1], coords, q, mins, maxs, counts, C.byref(ts))
+    return counts, float(tb), float(ts.value)
 
 
 def mix64(ids: np.ndarray) -> np.ndarray:

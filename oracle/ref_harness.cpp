@@ -11,7 +11,11 @@
 //   * the CPU baseline timed by bench.py: the reference build (serial by
 //     design, FKDTree_cpu.h:221-277) and its searches under an OpenMP
 //     parallel-for over boxes, the reference driver's `-p <threads>` loop
-//     (main.cpp:369-381) with OpenMP standing in for TBB as in test.cpp:71-76.
+//     (main.cpp:369-381) with OpenMP standing in for TBB as in test.cpp:71-76;
+//   * the reference's other CPU tree, the "vanilla" CMSSW KDTreeLinkerAlgo
+//     (KDTreeLinkerAlgoT.h), built and searched the way main.cpp:558-612
+//     does it (serially: its search keeps the result list in a member), as an
+//     extra baseline column.
 //
 // It is compiled WITHOUT -DNDEBUG, so a FQueue overflow (FQueue.h:158) aborts
 // loudly rather than corrupting results; callers only run the level-order,
@@ -26,6 +30,7 @@
 #include <vector>
 
 #include "FKDTree_cpu.h"
+#include "KDTreeLinkerAlgoT.h"
 
 namespace {
 
@@ -199,6 +204,42 @@ double fkdref_batch(uint32_t nev, const uint32_t* dims, const uint64_t* pt_off, 
     h->digest(q, mins + qcoord_off[e], maxs + qcoord_off[e], counts + q_off[e], digests + q_off[e]);
   }
   auto t1 = std::chrono::steady_clock::now();
+  return std::chrono::duration<double>(t1 - t0).count();
+}
+
+// The vanilla CMSSW tree over n 3D points (coords_soa[c*n + i], data = i),
+// region = the points' bounding box, as main.cpp:558-590 builds it; then one
+// serial search per box (main.cpp:596-605).  counts[j] receives the number of
+// points found for box j.  Returns the build seconds (filling the node list
+// included, as main.cpp times it); *search_seconds the search loop.
+double fkdref_cmssw(uint32_t n, const float* coords_soa, uint64_t nq, const float* mins, const float* maxs,
+                    uint32_t* counts, double* search_seconds) {
+  auto t0 = std::chrono::steady_clock::now();
+  KDTreeLinkerAlgo<unsigned, 3> tree;
+  std::vector<KDTreeNodeInfoT<unsigned, 3>> nodes;
+  nodes.reserve(n);
+  float lo[3] = {0.f, 0.f, 0.f}, hi[3] = {0.f, 0.f, 0.f};
+  for (uint32_t i = 0; i < n; ++i) {
+    const float x = coords_soa[i], y = coords_soa[(size_t)n + i], z = coords_soa[2 * (size_t)n + i];
+    nodes.emplace_back(i, x, y, z);
+    const float p[3] = {x, y, z};
+    for (int c = 0; c < 3; ++c) {
+      if (i == 0 || p[c] < lo[c]) lo[c] = p[c];
+      if (i == 0 || p[c] > hi[c]) hi[c] = p[c];
+    }
+  }
+  KDTreeCube bounds(lo[0], hi[0], lo[1], hi[1], lo[2], hi[2]);
+  tree.build(nodes, bounds);
+  auto t1 = std::chrono::steady_clock::now();
+  std::vector<KDTreeNodeInfoT<unsigned, 3>> found;
+  for (uint64_t j = 0; j < nq; ++j) {
+    KDTreeCube box(mins[j], maxs[j], mins[nq + j], maxs[nq + j], mins[2 * nq + j], maxs[2 * nq + j]);
+    tree.search(box, found);
+    counts[j] = (uint32_t)found.size();
+    found.clear();
+  }
+  auto t2 = std::chrono::steady_clock::now();
+  *search_seconds = std::chrono::duration<double>(t2 - t1).count();
   return std::chrono::duration<double>(t1 - t0).count();
 }
 

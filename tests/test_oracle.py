@@ -106,3 +106,18 @@ def test_reference_batch_matches_restated_batch():
     c1, d1, _ = O.ref_batch(wb, threads=2)
     _, _, c2, d2 = O.batch(wb)
     assert np.array_equal(c1, c2) and np.array_equal(d1, d2)
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built")
+def test_vanilla_cmssw_tree_counts_match_reference():
+    """The reference's vanilla CMSSW tree (the extra CPU baseline column)
+    finds the same number of points per box as FKDTree_CPU on boxes whose
+    faces hold no point (it tests inner regions with strict inequalities)."""
+    ev = W.clustered_event(n=50_000, n_queries=500, n_clusters=64, seed=12)
+    counts, tb, ts = O.ref_cmssw(ev.coords, ev.mins, ev.maxs)
+    r = O.RefTree(ev.coords, ev.ids)
+    r.build()
+    want, _, _, _ = r.search(ev.mins, ev.maxs, variant=O.RECURSIVE, want_ids=False)
+    r.close()
+    assert np.array_equal(counts, want)
+    assert tb > 0 and ts > 0
