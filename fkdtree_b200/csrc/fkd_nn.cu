@@ -25,20 +25,25 @@
 // Radius: point p qualifies for query (c, r) when d2 <= fl(r*r) and r >= 0.
 //   A negative or NaN radius, or a centre with a NaN coordinate, qualifies
 //   nothing.  A count pass, then a write pass: of ids in the walk's
-//   depth-first order, or (ordered) of heap indices that launch_order_results
-//   sorts and maps to ids -- ascending heap-index order, the order of the
-//   ordered box search.
+//   depth-first order, or (ordered) of heap indices that
+//   launch_order_results sorts and maps to ids -- ascending heap-index order,
+//   the order of the ordered box search.
 // kNN: the k points smallest in (d2, id) order, ascending.  Ties of d2 go to
 //   the smaller id, so the answer depends on the point set only, not on the
 //   tree.  Points whose d2 is NaN never qualify; a centre with a NaN
 //   coordinate has no neighbours.  Rows with fewer than k neighbours end in
 //   id 0xffffffff with d2 = +inf.
 //
-// One thread per query; queries run in the spatial order of launch_box_order
-// (neighbouring threads walk neighbouring parts of the tree and share its
-// nodes in L1/L2).  The walk is depth-first with an explicit stack of pending
-// far children: the entries' depths strictly increase from the bottom of the
-// stack to its top, so it never holds more than H + 1 <= 32 entries.
+// Queries run in the spatial order of launch_box_order (neighbouring warps
+// walk neighbouring parts of the tree and share its nodes in L1/L2).  The
+// radius search runs a warp per query (below); kNN a thread per query, a
+// depth-first walk with an explicit stack of pending far children whose
+// depths strictly increase from the bottom of the stack to its top, so it
+// never holds more than H + 1 <= 32 entries.  (Stopping the radius walk at
+// subtrees whose whole cell lies inside the ball, as the box search does for
+// boxes, was measured slower: kd cells are rarely inside a ball -- 11% fewer
+// visits on clustered points -- and carrying the cell doubled the cost of a
+// visit.)
 #include <math.h>
 
 #include "fkd_internal.h"
@@ -77,79 +82,108 @@ __device__ __forceinline__ bool load_centre(const float* __restrict__ ctr, uint6
   return ok;
 }
 
-// Radius search; out == nullptr: count pass (counts[j]); otherwise write pass
-// into out[offsets[j] ..) of heap indices (heap_out) or ids.
-template <int DIM>
+// ---------------------------------------------------------------- radius
+//
+// A warp per query.  The warp keeps the query's pending nodes in a
+// shared-memory stack and takes up to 32 of them per round from its top, one
+// per lane: each lane tests its node's point and its two children, the hits
+// leave as one coalesced store at consecutive positions (ballot prefix), and
+// the children are pushed back in lane order.  Lane k takes the k-th of the
+// popped entries from below, so the stack stays sorted by depth (children of
+// shallower nodes go lower); then a depth's entries can only come from the
+// one round that popped its parents, so no depth holds more than
+// min(64, 2^d) entries and the stack never exceeds 1 + sum_{d=1..H} min(64,
+// 2^d) words (a check latches an error instead of overflowing).  The result
+// order within a query is this walk's order (deterministic).
+
+// Stack words per warp for a tree of depth H.
+inline uint32_t radius_stack_words(uint32_t H) {
+  uint32_t w = 1u;
+  for (uint32_t d = 1; d <= H; ++d) w += d < 6u ? (1u << d) : 64u;
+  return w;
+}
+
+template <int DIM, int MODE>  // MODE 0: counts, 1: ids, 2: heap indices
 __global__ void __launch_bounds__(NNT) k_radius(Geom g, const uint4* __restrict__ nodes,
                                                 const uint32_t* __restrict__ ids, const float* __restrict__ ctr,
                                                 const float* __restrict__ rad, uint64_t q,
                                                 const uint32_t* __restrict__ order, uint32_t* __restrict__ counts,
                                                 const uint64_t* __restrict__ offsets, uint32_t* __restrict__ out,
-                                                int heap_out, uint32_t* __restrict__ err) {
-  const uint64_t t = (uint64_t)blockIdx.x * NNT + threadIdx.x;
+                                                uint32_t cap, uint32_t* __restrict__ err) {
+  extern __shared__ uint32_t nn_stack[];
+  const uint32_t lane = threadIdx.x & 31u, wp = threadIdx.x >> 5;
+  const uint32_t lt = (1u << lane) - 1u;
+  uint32_t* stk = nn_stack + (size_t)wp * cap;
+  const uint64_t t = (uint64_t)blockIdx.x * (NNT / 32) + wp;  // warp-uniform
   if (t >= q) return;
   const uint64_t j = order ? (uint64_t)order[t] : t;
   if (j >= q) {
-    atomicOr(err, ERRB_INTERNAL);
+    if (lane == 0u) atomicOr(err, ERRB_INTERNAL);
     return;
   }
   float qc[4];
   const bool centre_ok = load_centre<DIM>(ctr, q, j, qc);
   const float r = rad[j];
-  const bool write = out != nullptr;
   uint64_t base = 0ull, room = 0ull;
-  if (write) {
+  if (MODE != 0) {
     base = offsets[j];
     room = offsets[j + 1] - base;
   }
-  uint32_t cnt = 0u;
+  uint64_t found = 0ull;
   if (centre_ok && r >= 0.f && g.n > 0u) {
     const float r2 = __fmul_rn(r, r);
-    uint32_t stack[NN_STACK];
-    int sp = 0;
-    uint32_t i = 0u;
-    for (;;) {
-      for (;;) {
+    if (lane == 0u) stk[0] = 0u;
+    uint32_t sp = 1u;
+    __syncwarp();
+    while (sp > 0u) {
+      const uint32_t cnt = sp < 32u ? sp : 32u;
+      const uint32_t b0 = sp - cnt;
+      const bool act = lane < cnt;
+      const uint32_t i = act ? stk[b0 + lane] : 0u;
+      __syncwarp();  // every entry read before the pushes overwrite them
+      bool hit = false, go_l = false, go_r = false;
+      uint32_t v = 0u;
+      const uint32_t l = 2u * i + 1u;
+      if (act) {
         const uint4 nd = __ldg(nodes + i);
-        if (node_dist2<DIM>(nd, qc) <= r2) {
-          if (write) {
-            if (cnt < room)
-              out[base + cnt] = heap_out ? i : (DIM <= 3 ? nd.w : __ldg(ids + i));
-            else
-              atomicOr(err, ERRB_INTERNAL);
-          }
-          ++cnt;
-        }
+        hit = node_dist2<DIM>(nd, qc) <= r2;
+        if (MODE == 1) v = DIM <= 3 ? nd.w : (hit ? __ldg(ids + i) : 0u);
+        if (MODE == 2) v = i;
         const uint32_t a = floor_log2_u32(i + 1u) % (uint32_t)DIM;
         const float diff = __fsub_rn(qc[a], node_coord<DIM>(nd, a));
         const float pd = __fmul_rn(diff, diff);
-        const uint32_t l = 2u * i + 1u;
         // the left side holds coordinates <= s: beyond reach when q_a > s and
         // the plane is farther than r; the right side mirrors it
-        const bool go_l = l < g.n && !(diff > 0.f && pd > r2);
-        const bool go_r = l + 1u < g.n && !(diff < 0.f && pd > r2);
-        if (go_l) {
-          if (go_r) {
-            if (sp < NN_STACK)
-              stack[sp++] = l + 1u;
-            else
-              atomicOr(err, ERRB_INTERNAL);
-          }
-          i = l;
-        } else if (go_r) {
-          i = l + 1u;
-        } else {
-          break;
-        }
+        go_l = l < g.n && !(diff > 0.f && pd > r2);
+        go_r = l + 1u < g.n && !(diff < 0.f && pd > r2);
       }
-      if (sp == 0) break;
-      i = stack[--sp];
+      const uint32_t hm = __ballot_sync(0xffffffffu, hit);
+      if (MODE != 0 && hit) {
+        const uint64_t pos = found + __popc(hm & lt);
+        if (pos < room)
+          out[base + pos] = v;
+        else
+          atomicOr(err, ERRB_INTERNAL);
+      }
+      found += __popc(hm);
+      const uint32_t ml = __ballot_sync(0xffffffffu, go_l), mr = __ballot_sync(0xffffffffu, go_r);
+      const uint32_t np = b0 + __popc(ml) + __popc(mr);
+      if (np > cap) {  // not reachable by the bound above
+        if (lane == 0u) atomicOr(err, ERRB_INTERNAL);
+        break;
+      }
+      uint32_t p = b0 + __popc(ml & lt) + __popc(mr & lt);
+      if (go_l) stk[p++] = l;
+      if (go_r) stk[p] = l + 1u;
+      sp = np;
+      __syncwarp();
     }
   }
-  if (write) {
-    if ((uint64_t)cnt != room) atomicOr(err, ERRB_INTERNAL);
-  } else {
-    counts[j] = cnt;
+  if (lane == 0u) {
+    if (MODE == 0)
+      counts[j] = (uint32_t)found;
+    else if (found != room)
+      atomicOr(err, ERRB_INTERNAL);
   }
 }
 
@@ -250,15 +284,26 @@ __global__ void __launch_bounds__(NNT) k_knn(Geom g, const uint4* __restrict__ n
   }
 }
 
+template <int DIM, int MODE>
+cudaError_t radius_mode(const Geom& g, const Table& tab, const float* ctr, const float* rad, uint64_t q,
+                        const uint32_t* order, uint32_t* counts, const uint64_t* offsets, uint32_t* out, uint32_t* err,
+                        cudaStream_t stream) {
+  const uint32_t cap = radius_stack_words(g.H);
+  const size_t smem = (size_t)(NNT / 32) * cap * sizeof(uint32_t);
+  const uint64_t blocks = (q + NNT / 32 - 1) / (NNT / 32);
+  k_radius<DIM, MODE><<<(unsigned)blocks, NNT, smem, stream>>>(g, tab.nodes, tab.ids, ctr, rad, q, order, counts,
+                                                               offsets, out, cap, err);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
 template <int DIM>
 cudaError_t radius_dim(const Geom& g, const Table& tab, const float* ctr, const float* rad, uint64_t q,
                        const uint32_t* order, uint32_t* counts, const uint64_t* offsets, uint32_t* out, int heap_out,
                        uint32_t* err, cudaStream_t stream) {
-  const uint64_t blocks = (q + NNT - 1) / NNT;
-  k_radius<DIM><<<(unsigned)blocks, NNT, 0, stream>>>(g, tab.nodes, tab.ids, ctr, rad, q, order, counts, offsets,
-                                                      out, heap_out, err);
-  count_launches(1);
-  return cudaGetLastError();
+  if (!out) return radius_mode<DIM, 0>(g, tab, ctr, rad, q, order, counts, offsets, out, err, stream);
+  if (heap_out) return radius_mode<DIM, 2>(g, tab, ctr, rad, q, order, counts, offsets, out, err, stream);
+  return radius_mode<DIM, 1>(g, tab, ctr, rad, q, order, counts, offsets, out, err, stream);
 }
 
 template <int DIM>
