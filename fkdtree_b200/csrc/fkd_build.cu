@@ -130,9 +130,12 @@ __global__ void k_sel_init(uint32_t d, const EvDesc* __restrict__ evs, const uin
 // counter), then adds them to the segment's global histogram once.  The last
 // CTA of a segment picks the digit holding the pivot rank.
 constexpr int HCOPIES = 4;
+#ifndef FKD_HIST_MINB
+#define FKD_HIST_MINB 4
+#endif
 
 template <int DIM>
-__global__ void __launch_bounds__(GT, 4) k_hist(uint32_t d, const EvDesc* __restrict__ evs,
+__global__ void __launch_bounds__(GT, FKD_HIST_MINB) k_hist(uint32_t d, const EvDesc* __restrict__ evs,
                                                 const uint2* __restrict__ segs, const uint2* __restrict__ tiles,
                                                 uint32_t ts, CSoA src, SegSel* __restrict__ sel,
                                                 uint32_t* __restrict__ ghist, const uint32_t* __restrict__ pending_now,
@@ -325,10 +328,17 @@ __device__ __forceinline__ uint32_t pick_coord(const uint32_t* rec, uint32_t c) 
   return v;
 }
 
+// resident CTAs per SM the partition is compiled for: 8 (32 registers, a few
+// spilled words) keeps 2,048 threads per SM loading; measured on the 16M
+// clustered build: 4 / 5 / 6 / 8 CTAs -> 5.92 / 5.72 / 5.69 / 5.61 ms
+#ifndef FKD_PART_MINB
+#define FKD_PART_MINB (PIPT <= 4 ? 8 : 3)
+#endif
+
 // Streams every record of depth-d segments once: records below the pivot go
 // to [start, start + rank), the pivot to the table, the rest above it.
 template <int DIM>
-__global__ void __launch_bounds__(GT, PIPT <= 4 ? 4 : 3) k_partition(uint32_t d, const EvDesc* __restrict__ evs,
+__global__ void __launch_bounds__(GT, FKD_PART_MINB) k_partition(uint32_t d, const EvDesc* __restrict__ evs,
                                                      const uint2* __restrict__ segs, const uint2* __restrict__ tiles,
                                                      CSoA src, SoA dst, SegSel* __restrict__ sel, Table tab,
                                                      uint32_t* __restrict__ err, uint2* __restrict__ bnd_out,
