@@ -188,8 +188,8 @@ cudaError_t launch_order_results(const Geom& g, const Table& tab, const uint64_t
 size_t box_order_words(uint64_t q);
 cudaError_t launch_box_order(const Geom& g, const Table& tab, const Boxes& b, int dim, uint32_t* scratch,
                              uint32_t** order_out, cudaStream_t stream);
-// fkd_nn.cu: radius and k-nearest-neighbour search (one thread per query;
-// ctr is the SoA centre array of stride q).  launch_radius counts into
+// fkd_nn.cu: radius search (a warp per query) and k-nearest-neighbour search
+// (a thread per query); ctr is the SoA centre array of stride q.  launch_radius counts into
 // `counts` when `out` is null, else writes heap indices (heap_out) or ids at
 // `offsets`.
 constexpr uint32_t KNN_MAX = 64;
