@@ -742,11 +742,11 @@ fkd_status stage_centres(fkd_tree h, const float* centers, const float* radii, u
   }
   const size_t cb = (size_t)h->dim * q * sizeof(float);
   FKD_CUDA(h->qlo.ensure(cb ? cb : 4));
-  FKD_CUDA(cudaMemcpyAsync(h->qlo.p, centers, cb, cudaMemcpyHostToDevice, h->stream));
+  if (cb) FKD_CUDA(cudaMemcpyAsync(h->qlo.p, centers, cb, cudaMemcpyHostToDevice, h->stream));
   *dctr = h->qlo.as<float>();
   if (drad) {
-    FKD_CUDA(h->qhi.ensure(q * sizeof(float)));
-    FKD_CUDA(cudaMemcpyAsync(h->qhi.p, radii, q * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    FKD_CUDA(h->qhi.ensure(q ? q * sizeof(float) : 4));
+    if (q) FKD_CUDA(cudaMemcpyAsync(h->qhi.p, radii, q * sizeof(float), cudaMemcpyHostToDevice, h->stream));
     *drad = h->qhi.as<float>();
   }
   return FKD_OK;

@@ -281,3 +281,15 @@ def test_build_points_from_device(cuda):
     tab, tid = a.tables()
     assert np.array_equal(tab.view(np.uint32), want[0].view(np.uint32))
     assert np.array_equal(tid, want[1])
+
+
+@pytest.mark.gpu
+def test_zero_queries(cuda):
+    coords, ids = _cloud(1000, 3, seed=2)
+    t = F.FKDTree(coords, ids).build()
+    none = np.zeros((3, 0), dtype=np.float32)
+    off, got = t.search_radius(none, np.zeros(0, dtype=np.float32))
+    assert off.shape == (1,) and off[0] == 0 and got.size == 0
+    assert t.count_radius(none, np.zeros(0, dtype=np.float32)).size == 0
+    gi, gd = t.knn(none, 4)
+    assert gi.shape == (0, 4) and gd.shape == (0, 4)
