@@ -302,7 +302,12 @@ static void search_bfs(const qctx_t* q, fifo_t* f, emit_t* e) {
   }
 }
 
-/* FKDTree_cpu.h:25-70: level order with arithmetic child selection. */
+/* FKDTree_cpu.h:25-70: level order with arithmetic child selection.  Where
+ * a node with only a left child misses the box and the walk turns right
+ * (FKDTree_cpu.h:56-60), the reference pushes index n, one past the tables,
+ * and reads theDimensions[c][n] at the next depth (undefined behaviour; it
+ * emits nothing unless that stray value happens to lie in the box).  Here a
+ * child index at or past n is never pushed. */
 static void search_branchless(const qctx_t* q, fifo_t* f, emit_t* e) {
   f->head = f->tail = 0;
   fifo_push(f, 0);
@@ -321,6 +326,7 @@ static void search_branchless(const qctx_t* q, fifo_t* f, emit_t* e) {
       } else {
         nsons = maxsons < 1 ? maxsons : 1;
         first += (q->tab[(size_t)c * q->n + i] < q->lo[c]);
+        if (first >= q->n) nsons = 0;
       }
       for (int s = 0; s < nsons; ++s) fifo_push(f, first + (uint32_t)s);
     }

@@ -21,8 +21,10 @@ from pathlib import Path
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-ORACLE_SO = HERE / "_build" / "libfkdoracle.so"
-REF_SO = HERE / "_ref" / "libfkdref.so"
+# FKD_ORACLE_SO / FKD_REF_SO select other builds of the same sources (the
+# sanitised ones of `make -C oracle sanitize`)
+ORACLE_SO = Path(os.environ.get("FKD_ORACLE_SO") or HERE / "_build" / "libfkdoracle.so")
+REF_SO = Path(os.environ.get("FKD_REF_SO") or HERE / "_ref" / "libfkdref.so")
 
 LEVEL_ORDER, BFS, BRANCHLESS, RECURSIVE, BRUTE = 0, 1, 2, 3, 4
 FQUEUE_SLOTS = 1024  # FQueue.h:232 -- the reference frontier ring
