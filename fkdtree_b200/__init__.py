@@ -464,6 +464,20 @@ class MLP:
         check(self._lib.fkd_mlp_grad(self._h, _ptr(x), _ptr(t), x.shape[0], _ptr(g), C.byref(loss), MEM_HOST))
         return g, float(loss.value)
 
+    def save(self, path, storage: str = "f32") -> None:
+        """Writes the parameters to a versioned weights file
+        (fkdtree_b200.mlp_file; "f32" exact, "bf16" half the size)."""
+        from . import mlp_file
+        mlp_file.save_params(path, self.params, storage)
+
+    @classmethod
+    def load(cls, path) -> "MLP":
+        """A network with the parameters of a weights file written by save()."""
+        from . import mlp_file
+        m = cls()
+        m.params = mlp_file.load_params(path)
+        return m
+
     def train(self, x, t, epochs: int = 30, batch: int = 256, lr: float = 2e-3, seed: int = 0) -> np.ndarray:
         x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, self.IN)
         t = np.ascontiguousarray(t, dtype=np.float32)
