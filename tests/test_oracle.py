@@ -121,3 +121,39 @@ def test_vanilla_cmssw_tree_counts_match_reference():
     r.close()
     assert np.array_equal(counts, want)
     assert tb > 0 and ts > 0
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference build not present")
+@pytest.mark.parametrize("dim", [1, 2, 3, 4])
+def test_oracle_matches_reference_at_edge_sizes_and_values(dim):
+    """Sizes around powers of two (incomplete last levels, single-child
+    nodes) and degenerate values -- all-equal coordinates, an integer grid,
+    signed zeros and infinities -- built by the restatement and by the
+    unmodified reference: identical tables; every search variant of the
+    restatement equals brute force on them."""
+    rng = np.random.default_rng(dim)
+    sizes = [1, 2, 3, 4, 7, 8, 9, 15, 16, 17, 31, 32, 33, 1023, 1024, 1025, 4095, 4096, 4097]
+    kinds = ["uniform", "equal", "grid", "signed_zero_inf"]
+    for n in sizes:
+        for kind in kinds:
+            c = rng.random((dim, n), dtype=np.float32)
+            if kind == "equal":
+                c[:] = np.float32(0.25)
+            elif kind == "grid":
+                c = np.round(c * 4).astype(np.float32)
+            elif kind == "signed_zero_inf":
+                c = np.where(c < 0.3, np.float32(-0.0), np.where(c > 0.9, np.float32(np.inf), c)).astype(np.float32)
+                c[:, ::5] = np.float32(0.0)
+            ids = rng.permutation(n).astype(np.uint32)
+            t1 = O.build(c, ids)
+            r = O.RefTree(c, ids)
+            r.build()
+            t2 = r.tables()
+            r.close()
+            assert np.array_equal(t1[0].view(np.uint32), t2[0].view(np.uint32)), (n, kind)
+            assert np.array_equal(t1[1], t2[1]), (n, kind)
+            lo = (c[:, : min(n, 40)] - np.float32(0.3)).astype(np.float32)
+            hi = (c[:, : min(n, 40)] + np.float32(0.3)).astype(np.float32)
+            want = O.search(t1[0], t1[1], lo, hi, variant=O.BRUTE)[0]
+            for v in (O.LEVEL_ORDER, O.BFS, O.BRANCHLESS, O.RECURSIVE):
+                assert np.array_equal(O.search(t1[0], t1[1], lo, hi, variant=v)[0], want), (n, kind, v)
