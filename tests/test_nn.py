@@ -70,7 +70,7 @@ def test_abi_arg_checks_without_gpu():
 
 
 @pytest.mark.skipif(not O.ref_available(), reason="reference harness not built")
-@pytest.mark.parametrize("dim", [2, 3, 4])
+@pytest.mark.parametrize("dim", [1, 2, 3, 4])
 def test_radius_checker_matches_reference_box_search(dim):
     coords, ids = _cloud(6000, dim, seed=dim)
     ref = O.RefTree(coords, ids)
