@@ -25,6 +25,7 @@ SIGNATURES = {
     "fkd_version": ([], C.c_char_p),
     "fkd_last_error": ([], C.c_char_p),
     "fkd_kernel_launches": ([], C.c_uint64),
+    "fkd_debug_fail_alloc": ([C.c_int32], None),
     "fkd_create": ([_int, _u32, _vp, C.POINTER(_vp)], _int),
     "fkd_destroy": ([_vp], _int),
     "fkd_set_stream": ([_vp, _vp], _int),

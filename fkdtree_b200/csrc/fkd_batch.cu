@@ -50,7 +50,7 @@ struct Buf {
     p = nullptr;
     bytes = 0;
     if (want == 0) want = 16;
-    cudaError_t e = cudaMalloc(&p, want);
+    cudaError_t e = device_alloc(&p, want);
     if (e == cudaSuccess) bytes = want;
     return e;
   }

@@ -21,6 +21,23 @@ fkd_status capi_status_from_err(uint32_t e, const char* what);
 static unsigned long long g_launches = 0;
 void count_launches(uint64_t k) { __atomic_fetch_add(&g_launches, (unsigned long long)k, __ATOMIC_RELAXED); }
 uint64_t launches_total() { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
+
+// Allocation failure injection (fkd_debug_fail_alloc): >= 0 counts down the
+// device allocations left before one fails; -1 (the default) is off.
+static int g_fail_alloc = -1;
+cudaError_t device_alloc(void** p, size_t bytes) {
+  int v = __atomic_load_n(&g_fail_alloc, __ATOMIC_RELAXED);
+  while (v >= 0) {
+    if (__atomic_compare_exchange_n(&g_fail_alloc, &v, v - 1, false, __ATOMIC_RELAXED, __ATOMIC_RELAXED)) {
+      if (v == 0) {
+        *p = nullptr;
+        return cudaErrorMemoryAllocation;
+      }
+      break;
+    }
+  }
+  return cudaMalloc(p, bytes);
+}
 }  // namespace fkd
 
 namespace {
@@ -49,7 +66,7 @@ struct DevBuf {
     p = nullptr;
     bytes = 0;
     if (want == 0) return cudaSuccess;
-    cudaError_t e = cudaMalloc(&p, want);
+    cudaError_t e = device_alloc(&p, want);
     if (e == cudaSuccess) bytes = want;
     return e;
   }
@@ -249,6 +266,8 @@ const char* fkd_version(void) { return "fkdtree_b200 0.1 (sm_100a)"; }
 uint64_t fkd_kernel_launches(void) { return launches_total(); }
 
 const char* fkd_last_error(void) { return g_last_error.c_str(); }
+
+void fkd_debug_fail_alloc(int32_t after) { __atomic_store_n(&fkd::g_fail_alloc, after < 0 ? -1 : after, __ATOMIC_RELAXED); }
 
 fkd_status fkd_create(int dim, uint32_t flags, void* stream, fkd_tree* out) {
   if (!out) return fail(FKD_ERR_ARG, "null output handle pointer");

@@ -11,6 +11,8 @@ namespace fkd {
 // benchmarks: how many of the library's own kernels ran in a timed region).
 void count_launches(uint64_t k);
 uint64_t launches_total();
+// cudaMalloc with the allocation-failure injection of fkd_debug_fail_alloc
+cudaError_t device_alloc(void** p, size_t bytes);
 
 // Per-segment state of the global-level radix select (one per node of the
 // level being split).

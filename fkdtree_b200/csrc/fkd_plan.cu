@@ -100,7 +100,7 @@ cudaError_t PlanDev::upload(const PlanHost& h, cudaStream_t stream) {
     if (dev) cudaFree(dev);
     dev = nullptr;
     cap = 0;
-    cudaError_t e = cudaMalloc(&dev, bytes);
+    cudaError_t e = device_alloc(&dev, bytes);
     if (e != cudaSuccess) return e;
     cap = bytes;
   }

@@ -82,6 +82,13 @@ FKD_API uint64_t fkd_kernel_launches(void);
 /* Description of the last failure on the calling thread ("" if none). */
 FKD_API const char* fkd_last_error(void);
 
+/* Test hook (no reference counterpart): the device allocation `after`
+ * allocations from now -- by any tree or batch handle of this process --
+ * fails as if the device were out of memory, so callers can test their
+ * FKD_ERR_NOMEM paths; -1 turns it off (the default).  The failing call
+ * returns FKD_ERR_NOMEM and the handle stays usable. */
+FKD_API void fkd_debug_fail_alloc(int32_t after);
+
 /* Creates an empty tree for points of `dim` coordinates (1..4) on the current
  * CUDA device.  Replaces the FKDTree_CPU constructor (FKDTree_cpu.h:19-23);
  * the points are passed to fkd_build instead.  `stream` is a cudaStream_t
