@@ -157,3 +157,32 @@ def test_oracle_matches_reference_at_edge_sizes_and_values(dim):
             want = O.search(t1[0], t1[1], lo, hi, variant=O.BRUTE)[0]
             for v in (O.LEVEL_ORDER, O.BFS, O.BRANCHLESS, O.RECURSIVE):
                 assert np.array_equal(O.search(t1[0], t1[1], lo, hi, variant=v)[0], want), (n, kind, v)
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference build not present")
+def test_fixtures_reproduce_from_the_reference():
+    """The committed fixtures are what tests/golden/make_golden.py gets from
+    the unmodified reference today: same generator, same tables, same lists."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("make_golden", GOLDEN / "make_golden.py")
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    checked = 0
+    for name, coords, ids, boxes in mg.cases():
+        if not (name.startswith("tiny3d") or name in ("layers4d_n3000", "grid2d_n2000", "zeros_inf3d_n600")):
+            continue
+        f = load(name)
+        assert np.array_equal(f["coords"].view(np.uint32), coords.view(np.uint32)) and np.array_equal(f["ids"], ids)
+        r = O.RefTree(coords, ids)
+        r.build()
+        tab, tid = r.tables()
+        assert np.array_equal(tab.view(np.uint32), f["tab"].view(np.uint32)) and np.array_equal(tid, f["tab_ids"])
+        rc, ro, ri, _ = r.search(f["mins"], f["maxs"], variant=O.RECURSIVE)
+        assert np.array_equal(ro, f["rec_offsets"]) and np.array_equal(ri, f["rec_ids"])
+        sel = f.get("lvl_sel")
+        lo, hi = (f["mins"], f["maxs"]) if sel is None else (f["mins"][:, sel], f["maxs"][:, sel])
+        _, lo_off, lo_ids, _ = r.search(lo, hi, variant=O.LEVEL_ORDER)
+        assert np.array_equal(lo_off, f["lvl_offsets"]) and np.array_equal(lo_ids, f["lvl_ids"])
+        r.close()
+        checked += 1
+    assert checked == 22
