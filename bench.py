@@ -171,7 +171,7 @@ def _timed(fn, k):
     return best
 
 
-def _cpu_events(wb, n_sample):
+def _cpu_events(wb, n_sample, gpu_counts=None, gpu_digests=None):
     """The reference CPU path on n_sample events spread over the batch, scaled
     to the whole batch by points: the unmodified FKDTree_CPU (oracle/_ref) with
     OpenMP over events, each a serial build and a serial
@@ -185,19 +185,27 @@ def _cpu_events(wb, n_sample):
     kind = "reference" if O.ref_available() else "port"
     t0 = time.perf_counter()
     if kind == "reference":
-        O.ref_batch(sb, threads=threads)
+        rc, rd, _ = O.ref_batch(sb, threads=threads)
     else:
-        O.batch(sb, threads=threads)
+        _, _, rc, rd = O.batch(sb, threads=threads)
     sec = time.perf_counter() - t0
     scaled = sec * wb.n_points / max(1, sb.n_points)
     what = "FKDTree_CPU build + search_in_the_box_recursive" if kind == "reference" else "restated build + search"
-    return {"kind": kind, "cores": threads, "value": wb.n_points / scaled / 1e6, "unit": "Mpoints/s",
-            "ms_scaled": 1e3 * scaled,
-            "sample": (f"{what} of {len(ev)} of {wb.n_events} events ({sb.n_points} points, "
-                       f"{sb.n_queries} boxes) with {threads} threads over events, scaled by points")}
+    out = {"kind": kind, "cores": threads, "value": wb.n_points / scaled / 1e6, "unit": "Mpoints/s",
+           "ms_scaled": 1e3 * scaled, "events_run_fraction": len(ev) / wb.n_events,
+           "points_run_fraction": sb.n_points / wb.n_points,
+           "sample": (f"{what} of {len(ev)} of {wb.n_events} events ({sb.n_points} points, "
+                      f"{sb.n_queries} boxes) with {threads} threads over events, measured, then scaled to the "
+                      "whole batch by points")}
+    if gpu_counts is not None:
+        # the same events' boxes in the GPU run, re-indexed into the sample's order
+        bi = S.box_index(wb, ev)
+        out["sample_counts_digests_equal_" + kind] = bool(np.array_equal(gpu_counts[bi].view(np.uint32), rc)
+                                                         and np.array_equal(gpu_digests[bi].view(np.uint64), rd))
+    return out
 
 
-def _events_run(wb, mlp, dev, steps, plain_single):
+def _events_run(wb, mlp, dev, steps, plain_single, cpu_sample=0):
     """Batched graph run (autotuned) with and without the learned split, the
     plain single-event path (optional), exactness checks between them."""
     import torch
@@ -290,6 +298,10 @@ def _events_run(wb, mlp, dev, steps, plain_single):
         out["speedup_batched_vs_plain_single_event"] = plain_s / batched_s
         out["speedup_learned_batched_vs_plain_single_event"] = plain_s / learned_s
     out["speedup_learned_vs_plain_batched"] = batched_s / learned_s
+    if cpu_sample:
+        out["cpu_baseline"] = _cpu_events(wb, cpu_sample, bc.cpu().numpy(), bd.cpu().numpy())
+        k = [x for x in out["cpu_baseline"] if x.startswith("sample_counts_digests_equal_")][0]
+        exact[k] = out["cpu_baseline"][k]
     out["exact"] = exact
     out["batched_mpoints_per_s"] = wb.n_points / batched_s / 1e6
     out["learned_mpoints_per_s"] = wb.n_points / learned_s / 1e6
@@ -352,23 +364,19 @@ def batched_report(dev, n_events=4096, steps=3, train_events=2000, cpu=True):
     t0 = time.perf_counter()
     wb = W.event_batch(n_events=n_events, seed=20)
     gen = time.perf_counter() - t0
-    r = _events_run(wb, mlp, dev, steps, plain_single=True)
+    r = _events_run(wb, mlp, dev, steps, plain_single=True, cpu_sample=64 if cpu else 0)
     r["workload"] = ("events4096: 4,096 3D events, LogNormal(ln 20000, 1.0) sizes in [1000, 200000], 50-500 "
                      "clusters, every point a box of half-width 0.01 on its own event, seed 20")
     r["generate_s"] = gen
-    if cpu:
-        r["cpu_baseline"] = _cpu_events(wb, 64)
     rep["events4096"] = r
     del wb
     t0 = time.perf_counter()
     wm = W.mixed_events()
     gen = time.perf_counter() - t0
-    r = _events_run(wm, mlp, dev, steps, plain_single=False)
+    r = _events_run(wm, mlp, dev, steps, plain_single=False, cpu_sample=16 if cpu else 0)
     r["workload"] = ("mixed1024: 1,024 events, ~120M points, LogNormal(ln 80000, 1.0) sizes in [5000, 2000000], "
                      "half 3D / half 4D (16 discrete layers), every point a box of half-width 0.005, seed 5")
     r["generate_s"] = gen
-    if cpu:
-        r["cpu_baseline"] = _cpu_events(wm, 16)
     rep["mixed1024"] = r
     return rep
 
@@ -515,17 +523,33 @@ def run_ours(args):
             "phases": phases, "kernels": kern, "roofline": roof, "gpu_launches": int(launches)}
     line["clocks"] = clk.summary()
 
+    host = None
     if not args.no_e2e:
-        line["e2e"] = run_e2e(args, L, h, ev, results, stream, world, barrier, dev)
+        line["e2e"], host = run_e2e(args, L, h, ev, results, stream, world, barrier, dev)
+    check = rank == 0 and world == 1 and not args.no_cpu
+    if check:
+        # the device-timed output itself: offsets and a checksum of all ids
+        if host is None:
+            host = {"offsets": offsets.cpu().numpy().view(np.uint64), "ids": out[:results].cpu().numpy().view(np.uint32)}
+            tab = np.empty((dim, n), dtype=np.float32)
+            tid = np.empty(n, dtype=np.uint32)
+            _capi.check(L.fkd_get_tables(h, tab.ctypes.data_as(C.c_void_p), tid.ctypes.data_as(C.c_void_p),
+                                         _capi.MEM_HOST))
+            host["tab"], host["tid"] = tab, tid
+        host["device_offsets_equal"] = bool(np.array_equal(offsets.cpu().numpy().view(np.uint64), host["offsets"]))
+        host["device_checksum"] = device_checksum(out[:results])
     if rank == 0 and world == 1 and not args.no_nn:
         line["radius_knn"] = nn_report(L, h, ev, dev, stream, out)
     _capi.check(L.fkd_destroy(h))
     del coords, ids, mins, maxs, offsets, counts, out
     torch.cuda.empty_cache()
+    if rank == 0 and world == 1:
+        line["c1"] = c1_report(dev, cpu=not args.no_cpu)
     if rank == 0 and world == 1 and not args.no_batched:
         line["batched"] = batched_report(dev, n_events=args.batched_events, cpu=not args.no_cpu)
-    if rank == 0 and world == 1 and not args.no_cpu:
-        line["cpu_baseline"] = cpu_baseline(ev, args.cpu_queries)
+    if check:
+        line["cpu_baseline"], line["exact"] = reference_check(ev, host, args.cpu_queries)
+        del host
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -640,51 +664,203 @@ def run_e2e(args, L, h, ev, results, stream, world, barrier, dev):
     assert total.value == results
     h2d = n * 4 * dim + n * 4 + 2 * q * 4 * dim
     d2h = n * 4 * dim + n * 4 + (q + 1) * 8 + 4 * results
-    return {"value": world * n / (sec / k) / 1e6, "unit": "Mpoints/s", "steps": k, "ms_per_step": 1e3 * sec / k,
+    line = {"value": world * n / (sec / k) / 1e6, "unit": "Mpoints/s", "steps": k, "ms_per_step": 1e3 * sec / k,
             "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
             "path": "fkd_build + fkd_get_tables + fkd_search, FKD_MEM_HOST (pinned)"}
+    host = {"tab": tab_h.numpy(), "tid": tid_h.numpy().view(np.uint32), "offsets": offs_h.numpy().view(np.uint64),
+            "ids": out_h.numpy().view(np.uint32)[:results]}
+    return line, host
 
 
 # ------------------------------------------------------------ reference arm
 
-def ref_step(oracle_mod, ev, nq_sample, threads):
-    """Reference FKDTree_CPU build of all points (serial) + recursive search of
-    a box sample on all threads; returns (build_s, search_s_extrapolated)."""
+def ref_step(oracle_mod, ev, threads):
+    """One reference step, measured in full: FKDTree_CPU construction + build
+    of all points (serial by design) and search_in_the_box_recursive of every
+    box on all threads (main.cpp:201-212, :369-381).  Returns (tree,
+    build_s, search_s, counts); the caller closes the tree."""
     r = oracle_mod.RefTree(ev.coords, ev.ids)
     tb = r.build()
-    sel = np.linspace(0, ev.q - 1, nq_sample).astype(np.int64)
-    counts, _, _, ts = r.search(ev.mins[:, sel], ev.maxs[:, sel], variant=oracle_mod.RECURSIVE, want_ids=True,
-                                threads=threads)
-    r.close()
-    ref_step.last_counts = counts
-    return tb, ts * ev.q / nq_sample
+    counts, _, _, ts = r.search(ev.mins, ev.maxs, variant=oracle_mod.RECURSIVE, want_ids=False, threads=threads)
+    return r, tb, ts, counts
 
 
-def cpu_baseline(ev, nq_sample):
+MIX_C = (0x9E3779B97F4A7C15, 0xBF58476D1CE4E5B9, 0x94D049BB133111EB)
+
+
+def device_checksum(ids_dev, chunk=1 << 27):
+    """Wrap-around sum over all ids of the digest finaliser (the per-box digest
+    summed over boxes), computed on the GPU from the search's own output
+    buffer: checks the device-timed result against the reference's digests
+    without copying it to the host."""
+    import torch
+
+    def s64(v):
+        return v - (1 << 64) if v >= (1 << 63) else v
+
+    def lsr(z, k):
+        return (z >> k) & ((1 << (64 - k)) - 1)
+
+    tot = torch.zeros((), dtype=torch.int64, device=ids_dev.device)
+    for a in range(0, ids_dev.numel(), chunk):
+        z = ids_dev[a:a + chunk].to(torch.int64) & 0xFFFFFFFF
+        z = z + s64(MIX_C[0])
+        z = (z ^ lsr(z, 30)) * s64(MIX_C[1])
+        z = (z ^ lsr(z, 27)) * s64(MIX_C[2])
+        z = z ^ lsr(z, 31)
+        tot += z.sum()
+    return int(tot.item()) & ((1 << 64) - 1)
+
+
+def reference_check(ev, host, nq_sample):
+    """The unmodified reference (oracle/_ref) on the bench workload, in full:
+    its build and recursive search are timed (the cpu_baseline) and its output
+    is compared with the GPU's -- tables bit for bit, every box's count and
+    digest against the written result ids (copied out through the C ABI), a
+    checksum of the device-timed output buffer, and full sorted id sets on a
+    sample of boxes."""
     from oracle import oracle as O
     if not O.ref_available():
-        return {"value": None, "unit": "Mpoints/s", "kind": "reference", "cores": 0,
-                "sample": "reference CPU build unavailable (oracle/_ref not built)"}
+        return ({"value": None, "unit": "Mpoints/s", "kind": "reference", "cores": 0,
+                 "sample": "reference CPU build unavailable (oracle/_ref not built)"}, {"checked": False})
     threads = O.host_threads()
-    tb, ts = ref_step(O, ev, nq_sample, threads)
+    r, tb, ts, counts = ref_step(O, ev, threads)
     out = {"value": ev.n / (tb + ts) / 1e6, "unit": "Mpoints/s", "kind": "reference", "cores": threads,
            "build_s": tb, "search_s": ts,
-           "sample": (f"FKDTree_CPU::build of all {ev.n} points (serial, as in the reference) + "
-                      f"search_in_the_box_recursive on {nq_sample} of {ev.q} boxes with {threads} OpenMP threads, "
-                      "search time scaled to all boxes")}
+           "sample": (f"the whole workload, measured: FKDTree_CPU::build of all {ev.n} points (serial, as in the "
+                      f"reference) + search_in_the_box_recursive of all {ev.q} boxes with {threads} OpenMP threads")}
+    tab, tid = r.tables()
+    exact = {"c2_tables_equal_reference": bool(np.array_equal(tab.view(np.uint32), host["tab"].view(np.uint32))
+                                               and np.array_equal(tid, host["tid"]))}
+    rc, rd, tsd = r.search_digest(ev.mins, ev.maxs, threads=threads)
+    gcounts = np.diff(host["offsets"]).astype(np.uint32)
+    gd = O.digest_lists(host["offsets"], host["ids"], threads=threads)
+    exact["c2_counts_equal_reference"] = bool(np.array_equal(gcounts, counts) and np.array_equal(rc, counts))
+    exact["c2_digests_equal_reference"] = bool(np.array_equal(gd, rd))
+    if "device_checksum" in host:
+        want = int(np.sum(rd, dtype=np.uint64))
+        exact["c2_device_output_checksum_equal_reference"] = bool(host["device_checksum"] == want
+                                                                  and host["device_offsets_equal"])
+    sel = np.linspace(0, ev.q - 1, min(nq_sample, ev.q)).astype(np.int64)
+    sc, so, sids, _ = r.search(ev.mins[:, sel], ev.maxs[:, sel], variant=O.RECURSIVE, want_ids=True,
+                               threads=threads)
+    ok = True
+    go = host["offsets"]
+    for k, j in enumerate(sel):
+        a = np.sort(host["ids"][int(go[j]):int(go[j + 1])])
+        b = np.sort(sids[int(so[k]):int(so[k + 1])])
+        if not np.array_equal(a, b):
+            ok = False
+            break
+    exact["c2_sample_sets_equal_reference"] = ok
+    exact["what"] = (f"{ev.n} points, {ev.q} boxes, {int(counts.sum(dtype=np.uint64))} result ids; sets on "
+                     f"{len(sel)} sampled boxes; reference digest pass {tsd:.2f} s")
+    r.close()
     if ev.dim == 3:
         # the reference's other CPU tree, an extra column (main.cpp:558-612)
-        sel = np.linspace(0, ev.q - 1, nq_sample).astype(np.int64)
         vc, vb, vs = O.ref_cmssw(ev.coords, ev.mins[:, sel], ev.maxs[:, sel])
-        vs_all = vs * ev.q / nq_sample
+        vs_all = vs * ev.q / len(sel)
         out["cmssw_vanilla"] = {
             "value": ev.n / (vb + vs_all) / 1e6, "unit": "Mpoints/s", "kind": "reference", "cores": 1,
             "build_s": vb, "search_s": vs_all,
-            "counts_equal_fkdtree": float(np.mean(vc == ref_step.last_counts)),
+            "counts_equal_fkdtree": float(np.mean(vc == counts[sel])),
             "sample": (f"KDTreeLinkerAlgo<unsigned, 3> (KDTreeLinkerAlgoT.h) build of all {ev.n} points + serial "
-                       f"search of {nq_sample} of {ev.q} boxes, as main.cpp runs it; search time scaled to all "
+                       f"search of {len(sel)} of {ev.q} boxes, as main.cpp runs it; search time scaled to all "
                        "boxes")}
-    return out
+    return out, exact
+
+
+def c1_report(dev=None, cpu=True, reps=5):
+    """The small single-event case: 100,000 U[0,1)^3 points (seed 0), one box of
+    half-width 0.01 per point -- the reference's own CPU path (FKDTree_CPU
+    build, level-order search_in_the_box and search_in_the_box_recursive of
+    every box on all host threads, main.cpp:201-212, :369-381) and, with a
+    device, the GPU (build + ordered search = the reference's level-order
+    lists, device buffers, CUDA events), with exactness flags."""
+    from fkdtree_b200 import workloads as W
+    ev = W.uniform_event(n=100_000, half_width=0.01, seed=0)
+    rep = {"workload": "uniform3d_100k: 100,000 U[0,1)^3 points, seed 0, one box of half-width 0.01 per point",
+           "n_points": ev.n, "n_boxes": ev.q}
+    gpu = None
+    if dev is not None:
+        import torch
+
+        from fkdtree_b200 import _capi
+        L = _capi.lib()
+        P = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+        stream = torch.cuda.current_stream(dev)
+        h = C.c_void_p()
+        _capi.check(L.fkd_create(3, _capi.FLAG_ASYNC, C.c_void_p(stream.cuda_stream), C.byref(h)))
+        coords = torch.from_numpy(ev.coords).to(dev)
+        ids = torch.from_numpy(ev.ids.view(np.int32)).to(dev)
+        mins = torch.from_numpy(ev.mins).to(dev)
+        maxs = torch.from_numpy(ev.maxs).to(dev)
+        cnt = torch.empty(ev.q, dtype=torch.int32, device=dev)
+        _capi.check(L.fkd_build(h, P(coords), P(ids), ev.n, _capi.MEM_DEVICE))
+        _capi.check(L.fkd_search_count(h, P(mins), P(maxs), ev.q, P(cnt), _capi.MEM_DEVICE))
+        _capi.check(L.fkd_sync(h))
+        res = int(cnt.to(torch.int64).sum().item())
+        offs = torch.empty(ev.q + 1, dtype=torch.int64, device=dev)
+        out = torch.empty(max(res, 1), dtype=torch.int32, device=dev)
+        total = C.c_uint64(0)
+        times = {"build": [], "search_ordered": [], "search": []}
+        for it in range(reps + 2):
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+            e[0].record(stream)
+            _capi.check(L.fkd_build(h, P(coords), P(ids), ev.n, _capi.MEM_DEVICE))
+            e[1].record(stream)
+            _capi.check(L.fkd_search(h, P(mins), P(maxs), ev.q, P(offs), P(out), res, C.byref(total), 0,
+                                     _capi.MEM_DEVICE))
+            e[2].record(stream)
+            _capi.check(L.fkd_search(h, P(mins), P(maxs), ev.q, P(offs), P(out), res, C.byref(total), 1,
+                                     _capi.MEM_DEVICE))
+            e[3].record(stream)
+            torch.cuda.synchronize()
+            if it >= 2:
+                times["build"].append(e[0].elapsed_time(e[1]))
+                times["search"].append(e[1].elapsed_time(e[2]))
+                times["search_ordered"].append(e[2].elapsed_time(e[3]))
+        _capi.check(L.fkd_sync(h))
+        tab = np.empty((3, ev.n), dtype=np.float32)
+        tid = np.empty(ev.n, dtype=np.uint32)
+        _capi.check(L.fkd_get_tables(h, tab.ctypes.data_as(C.c_void_p), tid.ctypes.data_as(C.c_void_p),
+                                     _capi.MEM_HOST))
+        gpu = {"tab": tab, "tid": tid, "offsets": offs.cpu().numpy().view(np.uint64),
+               "ids": out[:res].cpu().numpy().view(np.uint32)}
+        _capi.check(L.fkd_destroy(h))
+        ms = {k: float(np.median(v)) for k, v in times.items()}
+        rep["gpu"] = {"build_ms": ms["build"], "search_ms": ms["search"], "search_ordered_ms": ms["search_ordered"],
+                      "value": ev.n / (ms["build"] + ms["search_ordered"]) / 1e3, "unit": "Mpoints/s",
+                      "mboxes_per_s": ev.q / ms["search_ordered"] / 1e3, "results": res,
+                      "timing": f"median of {reps} after 2 warm-up, CUDA events, device buffers; value = points / "
+                                "(build + ordered search)"}
+    if cpu:
+        from oracle import oracle as O
+        if O.ref_available():
+            threads = O.host_threads()
+            r = O.RefTree(ev.coords, ev.ids)
+            tb = r.build()
+            lc, lo, lids, tl = r.search(ev.mins, ev.maxs, variant=O.LEVEL_ORDER, want_ids=True, threads=threads)
+            rc, ro, rids, tr = r.search(ev.mins, ev.maxs, variant=O.RECURSIVE, want_ids=True, threads=threads)
+            rtab, rtid = r.tables()
+            r.close()
+            rep["reference"] = {"build_ms": 1e3 * tb, "search_level_order_ms": 1e3 * tl,
+                                "search_recursive_ms": 1e3 * tr, "cores": threads, "kind": "reference",
+                                "value": ev.n / (tb + tl) / 1e6, "unit": "Mpoints/s",
+                                "what": "FKDTree_CPU build (serial) + search_in_the_box (level order) of every box "
+                                        f"on {threads} OpenMP threads; value = points / (build + level-order search)"}
+            if gpu is not None:
+                rep["exact"] = {
+                    "tables_equal_reference": bool(np.array_equal(rtab.view(np.uint32), gpu["tab"].view(np.uint32))
+                                                   and np.array_equal(rtid, gpu["tid"])),
+                    "ordered_lists_equal_reference_level_order": bool(np.array_equal(lo, gpu["offsets"])
+                                                                      and np.array_equal(lids, gpu["ids"])),
+                    "sets_equal_reference_recursive": bool(
+                        np.array_equal(ro, gpu["offsets"])
+                        and np.array_equal(O.digest_lists(ro, rids), O.digest_lists(gpu["offsets"], gpu["ids"]))),
+                }
+                rep["speedup_gpu_vs_reference"] = rep["gpu"]["value"] / rep["reference"]["value"]
+    return rep
 
 
 def run_reference(args):
@@ -697,17 +873,19 @@ def run_reference(args):
         return
     ev, cfg = make_workload(args.workload, args.queries)
     threads = O.host_threads()
-    nq = min(args.cpu_queries, ev.q)
-    # warm-up steps on a 1/16 sample of the points keep the run bounded
+    # warm-up steps on a 1/16 sample of the points and boxes keep the run bounded
     from fkdtree_b200 import workloads as W
+    m = max(1, ev.q // 16)
     sub = W.Event(ev.dim, np.ascontiguousarray(ev.coords[:, : ev.n // 16]), ev.ids[: ev.n // 16].copy(),
-                  ev.mins, ev.maxs)
+                  np.ascontiguousarray(ev.mins[:, :m]), np.ascontiguousarray(ev.maxs[:, :m]))
     for _ in range(args.warmup):
-        ref_step(O, sub, min(512, nq), threads)
+        r, _, _, _ = ref_step(O, sub, threads)
+        r.close()
     tot_b = tot_s = 0.0
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        tb, ts = ref_step(O, ev, nq, threads)
+        r, tb, ts, _ = ref_step(O, ev, threads)
+        r.close()
         tot_b += tb
         tot_s += ts
     wall = time.perf_counter() - t0
@@ -718,13 +896,14 @@ def run_reference(args):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator, fkdtree_b200/workloads.py)",
             "config": dict(cfg, parallelism="cpu"), "impl": "reference",
             "cpu_baseline": {"value": value, "unit": "Mpoints/s", "kind": "reference", "cores": threads,
-                             "sample": (f"per step: FKDTree_CPU::build of all {ev.n} points (serial) + "
-                                        f"search_in_the_box_recursive on {nq} of {ev.q} boxes with {threads} "
-                                        "OpenMP threads, search time scaled to all boxes; warm-up steps on 1/16 "
-                                        "of the points"),
+                             "sample": (f"per step, the whole workload, measured: FKDTree_CPU::build of all {ev.n} "
+                                        f"points (serial) + search_in_the_box_recursive of all {ev.q} boxes with "
+                                        f"{threads} OpenMP threads; warm-up steps on 1/16 of the points and boxes"),
                              "build_s_per_step": tot_b / args.steps, "search_s_per_step": tot_s / args.steps,
                              "wall_s": wall},
             "e2e": {"value": value, "unit": "Mpoints/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if args.workload == "clustered16m":
+        line["c1"] = c1_report(None, cpu=True)
     print(json.dumps(line), flush=True)
 
 

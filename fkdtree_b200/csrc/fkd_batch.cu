@@ -136,6 +136,7 @@ struct fkd_batch_s {
   Buf err, qctr, passflags, stage_coords, stage_ids, stage_lo, stage_hi, stage_counts, stage_dig;
   uint32_t* herr = nullptr;
   bool built = false;
+  bool planned = false;  // false after a failed (re-)plan: builds are refused until one succeeds
   // tuning knobs (fkd_batch_set_param)
   uint32_t hist_ctas = 0;
   uint32_t search_lanes = 0;
@@ -167,6 +168,8 @@ struct fkd_batch_s {
 namespace {
 
 fkd_status batch_plan(fkd_batch b) {
+  b->planned = false;
+  b->built = false;
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
   const uint32_t hist_ctas = b->hist_ctas ? b->hist_ctas : 4u * (uint32_t)sms;
@@ -222,6 +225,7 @@ fkd_status batch_plan(fkd_batch b) {
   }
   BCUDA(b->lstats.ensure(64));
   BCUDA(cudaStreamSynchronize(b->stream));
+  b->planned = true;
   return FKD_OK;
 }
 
@@ -484,6 +488,7 @@ fkd_status fkd_batch_build(fkd_batch b, const float* coords, const uint32_t* ids
   if (mem != FKD_MEM_HOST && mem != FKD_MEM_DEVICE) return capi_fail(FKD_ERR_ARG, "bad mem");
   const uint64_t nc = coords_total(b), np = b->pt_off[b->nev];
   if (np && (!coords || !ids)) return capi_fail(FKD_ERR_ARG, "null coords or ids");
+  if (!b->planned) return capi_fail(FKD_ERR_STATE, "the batch has no build plan (a re-plan failed); set hist_ctas again");
   b->built = false;
   if (mem == FKD_MEM_HOST && np) {
     BCUDA(b->stage_coords.ensure(nc * 4));
@@ -579,6 +584,7 @@ fkd_status fkd_batch_run(fkd_batch b, const float* coords, const uint32_t* ids, 
   const uint64_t q = b->q_off[b->nev], np = b->pt_off[b->nev];
   if ((np && (!coords || !ids)) || (q && (!mins || !maxs || !counts || !digests)))
     return capi_fail(FKD_ERR_ARG, "null device buffer");
+  if (!b->planned) return capi_fail(FKD_ERR_STATE, "the batch has no build plan (a re-plan failed); set hist_ctas again");
   const void* key[6] = {coords, ids, mins, maxs, counts, digests};
   if (!b->gexec || memcmp(key, b->gkey, sizeof key) != 0) {
     if (b->gexec) cudaGraphExecDestroy(b->gexec);

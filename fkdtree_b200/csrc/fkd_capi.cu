@@ -344,6 +344,8 @@ fkd_status build_impl(fkd_tree h, const float* coords, const uint32_t* ids, cons
     PlanHost ph;
     const uint32_t n32 = (uint32_t)n, base0 = 0u;
     plan_build(&n32, &base0, 1, dim, h->hist_ctas ? h->hist_ctas : 4u * (uint32_t)sms, ph);
+    // a failed upload leaves no plan: the next build must plan again
+    h->plan_n = ~0ull;
     FKD_CUDA(h->plan.upload(ph, h->stream));
     h->plan_n = n;
   }

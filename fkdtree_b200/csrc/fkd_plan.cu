@@ -73,7 +73,19 @@ void plan_build(const uint32_t* n_ev, const uint32_t* base_ev, uint32_t nev, int
   }
 }
 
+// Forgets the uploaded plan: after a failed upload nothing may point into a
+// freed or half-written device copy.
+void PlanDev::clear() {
+  evs = nullptr;
+  nev = 0;
+  subs = nullptr;
+  nsub = 0;
+  levels.clear();
+  maxseg = 1;
+}
+
 cudaError_t PlanDev::upload(const PlanHost& h, cudaStream_t stream) {
+  clear();
   // every array starts on a 16-byte boundary (uint2 / EvDesc loads need 8)
   size_t words = h.evs.size() * (sizeof(EvDesc) / 4) + 2 * h.subs.size() + 8;
   for (const PlanLevel& lv : h.levels)

@@ -34,7 +34,9 @@ struct PlanDev {
   uint32_t nsub = 0;
   std::vector<LevelPlan> levels;
   uint32_t maxseg = 1;
+  // On failure the plan is left empty (clear()); the caller must re-upload.
   cudaError_t upload(const PlanHost& h, cudaStream_t stream);
+  void clear();
   ~PlanDev();
 };
 

@@ -122,7 +122,9 @@ FKD_API fkd_status fkd_build_points(fkd_tree h, const void* points, uint64_t n, 
  * fixed scratch array of its own (one per device, kept until exit), so n is
  * limited to fkd_build_noalloc_max_points(dim) (4096, or 3072 for dim 4);
  * larger n is rejected with FKD_ERR_ARG.  The first call on a device looks up
- * the scratch address -- make it before any stream capture.  Calls share the
+ * the scratch address and keeps it for the life of the process -- make it
+ * before any stream capture; a cudaDeviceReset after that first call is not
+ * supported (the kept address would belong to the destroyed context).  Calls share the
  * scratch: calls whose GPU work overlaps (other streams or threads on the same
  * device) race and must be serialised by the caller.  Synchronises `stream`
  * before returning, to report device-side errors. */

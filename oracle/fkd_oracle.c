@@ -466,6 +466,26 @@ int fkd_oracle_search_digest(int dim, uint32_t n, const float* tab_soa, const ui
   return 0;
 }
 
+/* Per-box digests of result lists already written out: box j's ids are
+ * ids[offsets[j] .. offsets[j+1]).  Checks a search's output id for id
+ * against fkd_oracle_search_digest / the reference's digests without
+ * holding a second copy of the lists. */
+int fkd_oracle_digest_lists(uint64_t nq, const uint64_t* offsets, const uint32_t* ids, uint64_t* digests,
+                            int threads) {
+#ifdef _OPENMP
+  if (threads > 0) omp_set_num_threads(threads);
+#else
+  (void)threads;
+#endif
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int64_t j = 0; j < (int64_t)nq; ++j) {
+    uint64_t d = 0;
+    for (uint64_t k = offsets[j]; k < offsets[j + 1]; ++k) d += fkd_mix64(ids[k]);
+    digests[j] = d;
+  }
+  return 0;
+}
+
 /* Batched events: event e owns points [pt_off[e], pt_off[e+1]) of the
  * concatenated input and boxes [q_off[e], q_off[e+1]); each event is built and
  * searched independently (one OpenMP task per event, serial inside, the

@@ -63,6 +63,8 @@ def lib():
         L.fkd_oracle_batch.argtypes = [C.c_uint32, _u32p, _u64p, _u64p, _f32p, _u32p, _u64p, _u64p, _f32p, _f32p,
                                        _f32p, _u32p, _u32p, _u64p, C.c_int]
         L.fkd_oracle_batch.restype = C.c_int
+        L.fkd_oracle_digest_lists.argtypes = [C.c_uint64, _u64p, _u32p, _u64p, C.c_int]
+        L.fkd_oracle_digest_lists.restype = C.c_int
         _c = L
     return _c
 
@@ -89,6 +91,8 @@ def ref_lib():
         L.fkdref_batch.argtypes = [C.c_uint32, _u32p, _u64p, _u64p, _f32p, _u32p, _u64p, _u64p, _f32p, _f32p, _u32p,
                                    _u64p, C.c_int]
         L.fkdref_batch.restype = C.c_double
+        L.fkdref_search_digest.argtypes = [C.c_void_p, C.c_uint64, _f32p, _f32p, _u32p, _u64p, C.c_int]
+        L.fkdref_search_digest.restype = C.c_double
         L.fkdref_cmssw.argtypes = [C.c_uint32, _f32p, C.c_uint64, _f32p, _f32p, _u32p, C.POINTER(C.c_double)]
         L.fkdref_cmssw.restype = C.c_double
         _ref = L
@@ -165,6 +169,17 @@ def search_digest(tab, tab_ids, mins, maxs, threads: int = 0):
     if rc != 0:
         raise RuntimeError("fkd_oracle_search_digest failed")
     return counts, dig
+
+
+def digest_lists(offsets: np.ndarray, ids: np.ndarray, threads: int = 0) -> np.ndarray:
+    """Per-box digest of result lists laid out as ids[offsets[j]:offsets[j+1]]
+    (the C twin of digest_of, multi-threaded, for billions of ids)."""
+    offsets = _soa(offsets, np.uint64)
+    ids = _soa(ids, np.uint32)
+    q = offsets.shape[0] - 1
+    dig = np.empty(q, dtype=np.uint64)
+    lib().fkd_oracle_digest_lists(q, offsets, ids, dig, threads)
+    return dig
 
 
 def batch(b, threads: int = 0):
@@ -277,6 +292,18 @@ class RefTree:
             self.L.fkdref_search(self.h, variant, q, mins, maxs, None, _ptr(offsets), _ptr(ids), threads,
                                  C.byref(secs))
         return counts, offsets, ids, secs.value
+
+    def search_digest(self, mins, maxs, threads: int = 0):
+        """search_in_the_box_recursive of every box on `threads` OpenMP
+        threads, each list reduced to (count, digest): returns (counts,
+        digests, seconds)."""
+        mins = _soa(mins, np.float32)
+        maxs = _soa(maxs, np.float32)
+        q = mins.shape[1]
+        counts = np.empty(q, dtype=np.uint32)
+        dig = np.empty(q, dtype=np.uint64)
+        sec = self.L.fkdref_search_digest(self.h, q, mins, maxs, counts, dig, threads)
+        return counts, dig, float(sec)
 
     def close(self):
         if self.h:

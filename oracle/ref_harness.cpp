@@ -42,8 +42,10 @@ struct HandleBase {
   virtual void tables(float* tab_soa, uint32_t* ids) = 0;
   virtual void search(int variant, uint64_t nq, const float* mins, const float* maxs, uint32_t* counts,
                       const uint64_t* offsets, uint32_t* out, int threads, double* seconds) = 0;
-  // serial search_in_the_box_recursive of every box: count and digest of its ids
-  virtual void digest(uint64_t nq, const float* mins, const float* maxs, uint32_t* counts, uint64_t* digests) = 0;
+  // search_in_the_box_recursive of boxes [j0, j1) (bounds SoA with row
+  // stride `stride`): count and digest of its ids, serially
+  virtual void digest(uint64_t j0, uint64_t j1, uint64_t stride, const float* mins, const float* maxs,
+                      uint32_t* counts, uint64_t* digests) = 0;
 };
 
 inline uint64_t mix_id(uint32_t id) {
@@ -99,12 +101,13 @@ struct Handle : HandleBase {
     }
   }
 
-  void digest(uint64_t nq, const float* mins, const float* maxs, uint32_t* counts, uint64_t* digests) override {
+  void digest(uint64_t j0, uint64_t j1, uint64_t stride, const float* mins, const float* maxs, uint32_t* counts,
+              uint64_t* digests) override {
     FKDPoint<float, D> lo, hi;
-    for (uint64_t j = 0; j < nq; ++j) {
+    for (uint64_t j = j0; j < j1; ++j) {
       for (int c = 0; c < D; ++c) {
-        lo.setDimension(c, mins[(size_t)c * nq + j]);
-        hi.setDimension(c, maxs[(size_t)c * nq + j]);
+        lo.setDimension(c, mins[(size_t)c * stride + j]);
+        hi.setDimension(c, maxs[(size_t)c * stride + j]);
       }
       std::vector<unsigned int> r;
       tree->search_in_the_box_recursive(lo, hi, r);
@@ -169,6 +172,24 @@ void fkdref_search(void* h, int variant, uint64_t nq, const float* mins_soa, con
 
 int fkdref_max_threads(void) { return omp_get_max_threads(); }
 
+// search_in_the_box_recursive of every box under an OpenMP parallel-for over
+// boxes (main.cpp:351-359's loop), reducing each box's id list to its count
+// and digest (the one fkdref_batch reports).  Returns the elapsed seconds.
+double fkdref_search_digest(void* h, uint64_t nq, const float* mins_soa, const float* maxs_soa, uint32_t* counts,
+                            uint64_t* digests, int threads) {
+  HandleBase* b = static_cast<HandleBase*>(h);
+  if (threads > 0) omp_set_num_threads(threads);
+  const int64_t chunk = 64;
+  auto t0 = std::chrono::steady_clock::now();
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int64_t j = 0; j < (int64_t)nq; j += chunk) {
+    const uint64_t j1 = (uint64_t)j + chunk < nq ? (uint64_t)j + chunk : nq;
+    b->digest((uint64_t)j, j1, nq, mins_soa, maxs_soa, counts, digests);
+  }
+  auto t1 = std::chrono::steady_clock::now();
+  return std::chrono::duration<double>(t1 - t0).count();
+}
+
 // Batched events, the reference way (OpenMP over events; each event a serial
 // FKDTree_CPU build and a serial search_in_the_box_recursive of its boxes):
 // per box the result count and the digest (wrap-around sum over the result
@@ -201,7 +222,7 @@ double fkdref_batch(uint32_t nev, const uint32_t* dims, const uint64_t* pt_off, 
       default: h.reset(new Handle<4>(n, coords + coord_off[e], ids + pt_off[e])); break;
     }
     h->build();
-    h->digest(q, mins + qcoord_off[e], maxs + qcoord_off[e], counts + q_off[e], digests + q_off[e]);
+    h->digest(0, q, q, mins + qcoord_off[e], maxs + qcoord_off[e], counts + q_off[e], digests + q_off[e]);
   }
   auto t1 = std::chrono::steady_clock::now();
   return std::chrono::duration<double>(t1 - t0).count();

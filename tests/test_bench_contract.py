@@ -39,3 +39,66 @@ def test_clock_summary_reasons():
     assert s.summary()["reasons"] == ["hw_slowdown"]
     s.out = ""
     assert s.summary()["reasons"] == ["unsampled"]
+
+
+def test_device_checksum_matches_digest_sum():
+    """The on-device checksum of a search's output equals the sum over boxes of
+    the per-box digests (torch CPU tensors stand in for the device buffer)."""
+    import numpy as np
+    import torch
+
+    from oracle import oracle as O
+    rng = np.random.default_rng(3)
+    ids = rng.integers(0, 2**32, size=100_003, dtype=np.uint64).astype(np.uint32)
+    offs = np.array([0, 10, 10, 5000, 100_003], dtype=np.uint64)
+    want = int(np.sum(O.digest_lists(offs, ids), dtype=np.uint64))
+    got = bench.device_checksum(torch.from_numpy(ids.view(np.int32)), chunk=4096)
+    assert got == want
+
+
+def _fake_gpu_output(ev, tab, tid):
+    """The host dict reference_check reads, filled from the C restatement."""
+    import numpy as np
+
+    from oracle import oracle as O
+    _, offs, ids, _ = O.search(tab, tid, ev.mins, ev.maxs, variant=O.RECURSIVE)
+    return {"tab": tab, "tid": tid, "offsets": offs, "ids": ids}
+
+
+def test_reference_check_flags():
+    """reference_check's exactness flags on a small clustered event: true for the
+    restatement's output, false once one result id is changed."""
+    import numpy as np
+    import pytest
+
+    from fkdtree_b200 import workloads as W
+    from oracle import oracle as O
+    if not O.ref_available():
+        pytest.skip("oracle/_ref not built")
+    ev = W.clustered_event(n=50_000, n_queries=2_000, n_clusters=32)
+    tab, tid = O.build(ev.coords, ev.ids)
+    host = _fake_gpu_output(ev, tab, tid)
+    cpu, exact = bench.reference_check(ev, host, 64)
+    assert cpu["kind"] == "reference" and cpu["value"] > 0 and cpu["search_s"] > 0
+    assert exact["c2_tables_equal_reference"] and exact["c2_counts_equal_reference"]
+    assert exact["c2_digests_equal_reference"] and exact["c2_sample_sets_equal_reference"]
+    k = int(np.argmax(np.diff(host["offsets"]) > 0))
+    host["ids"] = host["ids"].copy()
+    host["ids"][int(host["offsets"][k])] ^= 1
+    _, bad = bench.reference_check(ev, host, ev.q)
+    assert bad["c2_tables_equal_reference"] and bad["c2_counts_equal_reference"]
+    assert not bad["c2_digests_equal_reference"] and not bad["c2_sample_sets_equal_reference"]
+
+
+def test_c1_reference_block():
+    """The config-1 block's reference part runs on the CPU alone."""
+    import pytest
+
+    from oracle import oracle as O
+    if not O.ref_available():
+        pytest.skip("oracle/_ref not built")
+    rep = bench.c1_report(None, cpu=True)
+    assert rep["n_points"] == 100_000 and rep["n_boxes"] == 100_000
+    r = rep["reference"]
+    assert r["kind"] == "reference" and r["value"] > 0 and r["build_ms"] > 0
+    assert "gpu" not in rep and "exact" not in rep

@@ -49,3 +49,31 @@ def test_search_reports_nomem_then_recovers(cuda, inject):
     tab, tid = t.tables()
     _, o, want, _ = O.search(tab, tid, ev.mins[:, :500], ev.maxs[:, :500], variant=O.LEVEL_ORDER)
     assert np.array_equal(offs, o) and np.array_equal(ids, want)
+
+
+def test_failed_replan_is_not_reused(cuda, inject):
+    """A build of size B whose plan upload fails must not leave the handle
+    believing it still holds a plan: building size A again afterwards plans
+    again and gives the reference's tables."""
+    import ctypes as C
+    L = _capi.lib()
+    a = W.uniform_event(n=30_000, seed=6)
+    b = W.uniform_event(n=200_000, seed=7)
+    t = F.FKDTree(a.coords, a.ids)
+
+    def build(ev):
+        return L.fkd_build(t._h, ev.coords.ctypes.data_as(C.c_void_p), ev.ids.ctypes.data_as(C.c_void_p),
+                           ev.n, F.MEM_HOST)
+
+    assert build(a) == 0
+    inject(0)  # the larger plan's upload is the first allocation of this build
+    assert build(b) == NOMEM
+    inject(-1)
+    assert build(a) == 0
+    tab = np.empty((3, a.n), dtype=np.float32)
+    tid = np.empty(a.n, dtype=np.uint32)
+    assert L.fkd_get_tables(t._h, tab.ctypes.data_as(C.c_void_p), tid.ctypes.data_as(C.c_void_p), F.MEM_HOST) == 0
+    want = O.build(a.coords, a.ids)
+    assert np.array_equal(tab.view(np.uint32), want[0].view(np.uint32)) and np.array_equal(tid, want[1])
+    assert build(b) == 0
+    t.close()
