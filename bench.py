@@ -312,6 +312,35 @@ def _events_run(wb, mlp, dev, steps, plain_single, cpu_sample=0):
     return out
 
 
+def sharded_events(rank, world, dev, n_events=4096, reps=3):
+    """The events4096 batch split over the ranks (one GPU each) by points
+    (shard.assign_events); every rank builds and digest-searches its own share
+    as one batch graph (shard.run_share), no collective on the data path.  The
+    job's time is the slowest rank's CUDA-event time (max over ranks);
+    value = all ranks' points / that time."""
+    import torch
+    import torch.distributed as dist
+
+    from fkdtree_b200 import shard as S
+    from fkdtree_b200 import workloads as W
+    wb = W.event_batch(n_events=n_events, seed=20)
+    share = S.assign_events(np.diff(wb.pt_off.astype(np.int64)), world)[rank]
+    counts, _, _, ms = S.run_share(wb, share, dev, reps=reps)
+    pts = int(sum(int(wb.pt_off[e + 1] - wb.pt_off[e]) for e in share))
+    t = torch.tensor([ms, float(pts), float(counts.to(torch.int64).sum().item())], device=dev, dtype=torch.float64)
+    mx = t.clone()
+    dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+    sm = t.clone()
+    dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+    del counts
+    torch.cuda.empty_cache()
+    return {"workload": f"events{n_events}: seed 20, every point a box of half-width 0.01 on its own event",
+            "ranks": world, "points": int(sm[1].item()), "results": int(sm[2].item()),
+            "slowest_rank_ms": float(mx[0].item()), "value": float(sm[1].item()) / float(mx[0].item()) / 1e3,
+            "unit": "Mpoints/s", "scaling": "strong (the batch is fixed; ranks split its events)",
+            "assignment": "largest event first onto the rank with the fewest points (shard.assign_events)"}
+
+
 def batched_report(dev, n_events=4096, steps=3, train_events=2000, cpu=True):
     """The batched workloads, each a set of independent events in one CUDA graph
     launch (fkd_batch_run), launch knobs from the autotuner:
@@ -543,6 +572,8 @@ def run_ours(args):
     _capi.check(L.fkd_destroy(h))
     del coords, ids, mins, maxs, offsets, counts, out
     torch.cuda.empty_cache()
+    if world > 1 and not args.no_batched:
+        line["sharded_events"] = sharded_events(rank, world, dev, args.batched_events)
     if rank == 0 and world == 1:
         line["c1"] = c1_report(dev, cpu=not args.no_cpu)
     if rank == 0 and world == 1 and not args.no_batched:
@@ -770,6 +801,44 @@ def reference_check(ev, host, nq_sample):
     return out, exact
 
 
+def single_box_latency(L, h, ev, boxes=2000, threads=8):
+    """The per-box path (search_in_the_box on one box, as main.cpp:351-359
+    calls it): fkd_search with one box and host buffers, timed by the wall
+    clock over `boxes` calls from one thread, then from `threads` host threads
+    sharing the tree (ctypes releases the GIL inside each call).  Python's
+    call overhead (a few microseconds) is included."""
+    import threading
+
+    from fkdtree_b200 import _capi
+
+    def run(idx):
+        buf = np.empty(1 << 16, dtype=np.uint32)
+        offs = np.zeros(2, dtype=np.uint64)
+        tot = C.c_uint64(0)
+        lo = np.ascontiguousarray(ev.mins[:, idx].T)
+        hi = np.ascontiguousarray(ev.maxs[:, idx].T)
+        for k in range(len(idx)):
+            _capi.check(L.fkd_search(h, lo[k].ctypes.data_as(C.c_void_p), hi[k].ctypes.data_as(C.c_void_p), 1,
+                                     offs.ctypes.data_as(C.c_void_p), buf.ctypes.data_as(C.c_void_p), buf.size,
+                                     C.byref(tot), 1, _capi.MEM_HOST))
+
+    run(np.arange(50))
+    t0 = time.perf_counter()
+    run(np.arange(boxes))
+    one = time.perf_counter() - t0
+    parts = [np.arange(t, threads * boxes, threads) % ev.q for t in range(threads)]
+    th = [threading.Thread(target=run, args=(p,)) for p in parts]
+    t0 = time.perf_counter()
+    for x in th:
+        x.start()
+    for x in th:
+        x.join()
+    many = time.perf_counter() - t0
+    return {"us_per_box_one_thread": 1e6 * one / boxes, "boxes_per_s_one_thread": boxes / one,
+            "threads": threads, "boxes_per_s_threads": threads * boxes / many,
+            "what": "fkd_search(q=1, host buffers, ordered) per box through ctypes; wall clock"}
+
+
 def c1_report(dev=None, cpu=True, reps=5):
     """The small single-event case: 100,000 U[0,1)^3 points (seed 0), one box of
     half-width 0.01 per point -- the reference's own CPU path (FKDTree_CPU
@@ -827,13 +896,15 @@ def c1_report(dev=None, cpu=True, reps=5):
                                      _capi.MEM_HOST))
         gpu = {"tab": tab, "tid": tid, "offsets": offs.cpu().numpy().view(np.uint64),
                "ids": out[:res].cpu().numpy().view(np.uint32)}
+        single = single_box_latency(L, h, ev)
         _capi.check(L.fkd_destroy(h))
         ms = {k: float(np.median(v)) for k, v in times.items()}
         rep["gpu"] = {"build_ms": ms["build"], "search_ms": ms["search"], "search_ordered_ms": ms["search_ordered"],
                       "value": ev.n / (ms["build"] + ms["search_ordered"]) / 1e3, "unit": "Mpoints/s",
                       "mboxes_per_s": ev.q / ms["search_ordered"] / 1e3, "results": res,
                       "timing": f"median of {reps} after 2 warm-up, CUDA events, device buffers; value = points / "
-                                "(build + ordered search)"}
+                                "(build + ordered search)",
+                      "single_box": single}
     if cpu:
         from oracle import oracle as O
         if O.ref_available():

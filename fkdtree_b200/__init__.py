@@ -19,6 +19,7 @@ Batch entry points (``search_boxes``, ``count_boxes``, ``digest_boxes``) take
 from __future__ import annotations
 
 import ctypes as C
+import threading
 
 import numpy as np
 
@@ -46,6 +47,9 @@ def _ptr(x):
 
 def _host_f32(a) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=np.float32)
+
+
+_THREAD_BUFS = threading.local()
 
 
 def _stream_handle(stream):
@@ -200,10 +204,24 @@ class FKDTree:
 
     # -- single-box searches, the reference's per-query API
     def _one(self, minPoint, maxPoint, ordered=True) -> np.ndarray:
+        """One box in one library call: the ids land in a per-thread buffer
+        sized by the largest box seen so far (a larger box takes a second call
+        with the total fkd_search reports).  Safe from several threads at once."""
         lo = _host_f32(minPoint).reshape(self.dim, 1)
         hi = _host_f32(maxPoint).reshape(self.dim, 1)
-        _, ids = self.search_boxes(lo, hi, ordered=ordered)
-        return ids
+        tl = _THREAD_BUFS.__dict__
+        buf = tl.get("buf")
+        if buf is None:
+            buf = tl["buf"] = np.empty(256, dtype=np.uint32)
+        offs = np.zeros(2, dtype=np.uint64)
+        total = C.c_uint64(0)
+        args = (self._h, _ptr(lo), _ptr(hi), 1, _ptr(offs))
+        st = self._lib.fkd_search(*args, _ptr(buf), buf.size, C.byref(total), int(ordered), MEM_HOST)
+        if st == _capi.ERR_CAPACITY and total.value > buf.size:
+            buf = tl["buf"] = np.empty(total.value + total.value // 2, dtype=np.uint32)
+            st = self._lib.fkd_search(*args, _ptr(buf), buf.size, C.byref(total), int(ordered), MEM_HOST)
+        check(st)
+        return buf[:total.value].copy()
 
     def search_in_the_box(self, minPoint, maxPoint) -> np.ndarray:  # FKDTree_cpu.h:123-169
         return self._one(minPoint, maxPoint)

@@ -17,6 +17,7 @@ STATUS = {
     6: "FKD_ERR_CAPACITY", 7: "FKD_ERR_INTERNAL", 8: "FKD_ERR_TIMEOUT",
 }
 MEM_HOST, MEM_DEVICE = 0, 1
+ERR_CAPACITY = 6
 FLAG_ASYNC = 1
 
 # Every entry point include/fkdtree_b200.h declares, with its ctypes signature.

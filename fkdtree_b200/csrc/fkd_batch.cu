@@ -113,7 +113,7 @@ struct Part {
   uint64_t npts = 0, nq = 0;
   uint32_t maxn = 0;  // largest event (sizes the search stack)
   PlanDev plan;
-  Buf io, chunks, work0, work1, nodes, ids, sel, ghist, lfeat, lyhat, lrange, sdig, bnd;
+  Buf io, chunks, work0, work1, nodes, ids, sel, ghist, lfeat, lyhat, lrange, sdig, bnd, tiebuf;
   uint32_t nchunks = 0;
   std::vector<uint32_t> ev_n;  // points of every (local) event
   // digest search split by event size (knob search_big_n): [0] smaller events, [1] the others
@@ -143,6 +143,7 @@ struct fkd_batch_s {
   uint32_t search_lanes_big = 0;  // lanes per box for events of at least search_big_n points (0: search_lanes)
   uint32_t search_big_n = 0;      // 0: one launch for every event
   int subtree = 0;
+  bool tie_fix = true;  // ties on a pivot value resolved in the partition
   // learned split
   fkd_mlp mlp = nullptr;
   float mlp_delta = 0.f;
@@ -217,6 +218,7 @@ fkd_status batch_plan(fkd_batch b) {
     BCUDA(p.ids.ensure(p.npts * 4));
     BCUDA(p.sel.ensure(sizeof(SegSel) * (size_t)p.plan.maxseg));
     BCUDA(p.bnd.ensure(2 * sizeof(uint2) * (size_t)p.plan.maxseg));
+    BCUDA(p.tiebuf.ensure((size_t)p.plan.maxseg * TIE_CAP * (p.dim + 1) * 4));
     BCUDA(p.ghist.ensure((size_t)p.plan.maxseg * HIST_BINS * 4));
     BCUDA(p.sdig.ensure(p.npts * sizeof(unsigned long long)));
     BCUDA(p.lfeat.ensure((size_t)p.plan.maxseg * FKD_MLP_FEATURES * 4));
@@ -269,6 +271,7 @@ fkd_status enqueue_build(fkd_batch b, const float* coords, const uint32_t* ids) 
     bc.pending = b->passflags.as<uint32_t>();
     bc.bnd = p.bnd.as<uint2>();
     bc.bnd_stride = p.plan.maxseg;
+    bc.tiebuf = b->tie_fix ? p.tiebuf.as<uint32_t>() : nullptr;
     bc.subtree = b->subtree;
     bc.stream = b->stream;
     memset(&bc.learn, 0, sizeof bc.learn);
@@ -457,6 +460,12 @@ fkd_status fkd_batch_set_param(fkd_batch b, const char* name, int64_t value) {
   if (strcmp(name, "subtree") == 0) {
     if (value < 0 || value > 2) return capi_fail(FKD_ERR_ARG, "subtree must be 0, 1 or 2");
     b->subtree = (int)value;
+    drop_graph();
+    return FKD_OK;
+  }
+  if (strcmp(name, "tie_fix") == 0) {
+    if (value != 0 && value != 1) return capi_fail(FKD_ERR_ARG, "tie_fix must be 0 or 1");
+    b->tie_fix = value != 0;
     drop_graph();
     return FKD_OK;
   }

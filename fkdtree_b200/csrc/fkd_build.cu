@@ -115,6 +115,7 @@ __global__ void k_sel_init(uint32_t d, const EvDesc* __restrict__ evs, const uin
   st.verify = 0u;
   st.below = 0u;
   st.kfull = st.krem;
+  st.tie = 0u;
   sel[s] = st;
   if (bnd_out && child[s] != ~0u) {
     bnd_out[child[s]] = make_uint2(0xffffffffu, 0u);
@@ -140,7 +141,7 @@ __global__ void __launch_bounds__(GT, FKD_HIST_MINB) k_hist(uint32_t d, const Ev
                                                 uint32_t ts, CSoA src, SegSel* __restrict__ sel,
                                                 uint32_t* __restrict__ ghist, const uint32_t* __restrict__ pending_now,
                                                 uint32_t* __restrict__ pending_next, uint32_t* __restrict__ err,
-                                                unsigned long long* __restrict__ lstats) {
+                                                unsigned long long* __restrict__ lstats, uint32_t ties) {
   __shared__ uint32_t hist[HCOPIES * RBINS];
   __shared__ uint32_t wsum[GWARPS];
   __shared__ uint32_t s_last;
@@ -309,6 +310,12 @@ __global__ void __launch_bounds__(GT, FKD_HIST_MINB) k_hist(uint32_t d, const Ev
       p->krem = krem - cum;
       p->cnt = h[k];
       p->done = (h[k] == 1u || nbits == 64u) ? 1u : 0u;
+      if (!p->done && ties && nbits == 32u && h[k] <= TIE_CAP) {
+        // the pivot value is known and only a few points carry it: the
+        // partition orders them by id (k_tie_fix) instead of id digit passes
+        p->done = 1u;
+        p->tie = 1u;
+      }
       if (!p->done) *pending_next = 1u;
     }
     cum += h[k];
@@ -342,7 +349,8 @@ __global__ void __launch_bounds__(GT, FKD_PART_MINB) k_partition(uint32_t d, con
                                                      const uint2* __restrict__ segs, const uint2* __restrict__ tiles,
                                                      CSoA src, SoA dst, SegSel* __restrict__ sel, Table tab,
                                                      uint32_t* __restrict__ err, uint2* __restrict__ bnd_out,
-                                                     const uint32_t* __restrict__ child) {
+                                                     const uint32_t* __restrict__ child,
+                                                     uint32_t* __restrict__ tiebuf) {
   __shared__ uint32_t sL[PIPT * GWARPS], sR[PIPT * GWARPS];
   __shared__ uint32_t s_base[2];
   const uint2 tl = tiles[blockIdx.x];
@@ -361,6 +369,7 @@ __global__ void __launch_bounds__(GT, FKD_PART_MINB) k_partition(uint32_t d, con
   const uint32_t bits = sel[s].bits;
   const unsigned long long prefix = sel[s].prefix;
   const uint32_t cnt = sel[s].cnt;
+  const bool tie = sel[s].tie != 0u;
   const uint32_t c = d % DIM;
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
 
@@ -454,6 +463,16 @@ __global__ void __launch_bounds__(GT, FKD_PART_MINB) k_partition(uint32_t d, con
     } else if ((br[k] >> lane) & 1u) {
       pos = baseR + sR[k * GWARPS + warp] + __popc(br[k] & lt);
       lim = endR;
+    } else if (((eqmask >> k) & 1u) && tie) {
+      // ties on the pivot value: parked for k_tie_fix, which orders them by id
+      const uint32_t slot = atomicAdd(&sel[s].curE, 1u);
+      if (slot < TIE_CAP && tiebuf) {
+        uint32_t* tb = tiebuf + ((size_t)s * TIE_CAP + slot) * (DIM + 1);
+#pragma unroll
+        for (int w = 0; w <= DIM; ++w) tb[w] = rec[k][w];
+      } else {
+        atomicOr(err, ERRB_INTERNAL);
+      }
     } else if ((eqmask >> k) & 1u) {
       const uint32_t krem = sel[s].krem;
       uint32_t ticket = 0u;
@@ -516,6 +535,80 @@ __global__ void __launch_bounds__(GT, FKD_PART_MINB) k_partition(uint32_t d, con
         atomicMin(&bnd_out[ch + 1u].x, sb[2]);
         atomicMax(&bnd_out[ch + 1u].y, sb[3]);
       }
+    }
+  }
+}
+
+// Segments whose pivot value is carried by 2..TIE_CAP points (SegSel::tie):
+// the partition parked those records; one warp per segment orders them by id
+// -- the reference comparator's tie-break (FKDTree_cpu.h:248-251) -- writes
+// the one of rank krem to the table and the others to the ends of the
+// children's intervals the partition left free: the krem smaller ones to the
+// last krem slots of the left interval, the larger ones to the last slots of
+// the right interval.  It also widens the children's split-coordinate bounds.
+template <int DIM>
+__global__ void k_tie_fix(uint32_t d, const EvDesc* __restrict__ evs, const uint2* __restrict__ segs, uint32_t nseg,
+                          const SegSel* __restrict__ sel, const uint32_t* __restrict__ tiebuf, SoA dst, Table tab,
+                          uint32_t* __restrict__ err, uint2* __restrict__ bnd_out, const uint32_t* __restrict__ child) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t s = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (s >= nseg) return;
+  const SegSel st = sel[s];
+  if (!st.tie) return;
+  const uint32_t m = st.cnt;
+  if (m > TIE_CAP || st.curE != m) {
+    if (lane == 0) atomicOr(err, ERRB_INTERNAL);
+    return;
+  }
+  const uint2 sd = segs[s];
+  const Geom eg = evs[sd.x].g;
+  const uint32_t ebase = evs[sd.x].base;
+  const uint32_t len = seg_len(eg, d, sd.y);
+  const uint32_t start = ebase + seg_start(eg, d, sd.y);
+  const uint32_t rank = seg_rank(eg, d, sd.y);
+  const uint32_t node = ebase + (1u << d) - 1u + sd.y;
+  const uint32_t endL = start + rank, endR = start + len;
+  uint32_t rec[DIM + 1];
+  const bool have = lane < m;
+#pragma unroll
+  for (int w = 0; w <= DIM; ++w) rec[w] = have ? tiebuf[((size_t)s * TIE_CAP + lane) * (DIM + 1) + w] : 0u;
+  // rank by id (lane order breaks repeated ids, which the reference leaves undefined)
+  const uint32_t myid = rec[DIM];
+  uint32_t r = 0u;
+  for (uint32_t o = 0; o < m; ++o) {
+    const uint32_t oid = __shfl_sync(0xffffffffu, myid, o);
+    r += (oid < myid || (oid == myid && o < lane)) ? 1u : 0u;
+  }
+  const uint32_t krem = st.krem;
+  const uint32_t cnext = (d + 1u) % DIM;
+  const uint32_t ch = bnd_out ? child[s] : ~0u;
+  uint32_t pos = 0xffffffffu, lim = 0u;
+  bool left = false;
+  if (have) {
+    if (r == krem) {
+      write_node(tab, node, rec, DIM);
+    } else if (r < krem) {
+      pos = endL - krem + r;
+      lim = endL;
+      left = true;
+    } else {
+      pos = endR - (m - 1u - krem) + (r - krem - 1u);
+      lim = endR;
+    }
+  }
+  if (pos != 0xffffffffu) {
+    if (pos < lim && pos >= start) {
+#pragma unroll
+      for (int w = 0; w < DIM; ++w) dst.base[(uint64_t)w * dst.stride + pos] = rec[w];
+      dst.ids[pos] = rec[DIM];
+      if (ch != ~0u) {
+        const uint32_t mv = mono_bits(pick_coord<DIM>(rec, cnext));
+        uint2* b = &bnd_out[left ? ch : ch + 1u];
+        atomicMin(&b->x, mv);
+        atomicMax(&b->y, mv);
+      }
+    } else {
+      atomicOr(err, ERRB_INTERNAL);
     }
   }
 }
@@ -1104,13 +1197,18 @@ static cudaError_t run_build(BuildCtx& bc) {
     for (int pass = 0; pass < passes; ++pass) {
       k_hist<DIM><<<lp.nhtile, GT, 0, bc.stream>>>(d, bc.evs, lp.segs, lp.htiles, lp.hts, src, bc.sel, bc.ghist,
                                                     bc.pending + pass, bc.pending + pass + 1, bc.err,
-                                                    lc.params ? lc.stats : nullptr);
+                                                    lc.params ? lc.stats : nullptr, bc.tiebuf ? 1u : 0u);
       count_launches(1);
     }
     SoA dst = bufs[nb];
     k_partition<DIM><<<lp.nptile, GT, 0, bc.stream>>>(d, bc.evs, lp.segs, lp.ptiles, src, dst, bc.sel, bc.tab,
-                                                        bc.err, bnd_out, lp.child);
+                                                        bc.err, bnd_out, lp.child, bc.tiebuf);
     count_launches(1);
+    if (bc.tiebuf && !small) {
+      k_tie_fix<DIM><<<(lp.nseg + 7) / 8, 256, 0, bc.stream>>>(d, bc.evs, lp.segs, lp.nseg, bc.sel, bc.tiebuf, dst,
+                                                              bc.tab, bc.err, bnd_out, lp.child);
+      count_launches(1);
+    }
     if (lc.rec_x) {
       cudaError_t e = launch_record(d, bc.evs, lp.segs, lp.nseg, DIM, bc.tab, lc.feat, lc.range, lc.rec_x, lc.rec_t,
                                     lc.rec_n, lc.rec_cap, bc.stream);

@@ -4,6 +4,8 @@
 #include <string.h>
 
 #include <algorithm>
+#include <memory>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -83,6 +85,30 @@ struct DevBuf {
 
 }  // namespace
 
+// Per-call scratch of the searches.  Every search call leases one slot from
+// its handle's pool for its duration, so searches on one built tree may run
+// from several host threads at once (the reference's TBB loop over one tree,
+// main.cpp:351-359): each has its own staging buffers, error word and -- for
+// host-memory calls -- its own stream; the tree tables are only read.
+struct SearchSlot {
+  DevBuf qlo, qhi, counts, offsets, partials, out, tmp, digests, qorder;
+  DevBuf pool_st, pool_len, pool_s, brec, jctr, rflags, err, qctr;
+  uint32_t* herr = nullptr;      // pinned: [0] error word, [2..3] total, [4..11] pool demand
+  cudaStream_t own = nullptr;    // stream of host-memory calls
+  cudaEvent_t done = nullptr;    // the slot's last work (waited on by its next lease)
+  // run pool of fkd_search, sized by the previous call's demand
+  uint64_t pool_want = 0, pool_s_want = 0, brec_want = 0;
+  ~SearchSlot() {
+    DevBuf* all[] = {&qlo, &qhi, &counts, &offsets, &partials, &out, &tmp, &digests, &qorder,
+                     &pool_st, &pool_len, &pool_s, &brec, &jctr, &rflags, &err, &qctr};
+    if (own) cudaStreamSynchronize(own);
+    for (DevBuf* b : all) b->release();
+    if (herr) cudaFreeHost(herr);
+    if (done) cudaEventDestroy(done);
+    if (own) cudaStreamDestroy(own);
+  }
+};
+
 struct fkd_tree_s {
   int dim = 3;
   uint32_t flags = 0;
@@ -90,8 +116,7 @@ struct fkd_tree_s {
   int device = 0;
   uint64_t n = 0;
   bool built = false;
-  DevBuf nodes, ids, work0, work1, sel, ghist, err, qctr, passflags;
-  DevBuf qlo, qhi, counts, offsets, partials, out, tmp, digests, qorder;
+  DevBuf nodes, ids, work0, work1, sel, ghist, err, qctr, passflags, tmp;
   uint32_t* herr = nullptr;  // pinned mirror of err
   PlanDev plan;              // build plan of the last size built
   uint64_t plan_n = ~0ull;
@@ -102,13 +127,23 @@ struct fkd_tree_s {
   bool box_order = true;     // search boxes in the spatial order of their centres
   fkd_mlp mlp = nullptr;     // learned split (null: plain radix select)
   float mlp_delta = 0.f;
-  DevBuf lfeat, lyhat, lrange, lstats, sdig, dids, dnode, bnd, pool_st, pool_len, pool_s, brec, jctr, rflags;
-  // run pool of fkd_search, sized by the previous call's demand
-  uint64_t pool_want = 0, pool_s_want = 0, brec_want = 0;
+  DevBuf lfeat, lyhat, lrange, lstats, sdig, dids, dnode, ipts, bnd, tiebuf;
+  bool tie_fix = true;          // ties on a pivot value resolved in the partition ("tie_fix")
+  uint32_t search_bucket = 4;   // leaf-bucket height of the searches ("search_bucket"; 0: walk every level)
   bool search_record = true;    // fkd_search records runs in the count pass ("search_record")
   uint64_t search_pool = 0;     // fixed pool entries ("search_pool"; 0: sized by demand)
+  // tables derived from the tree on first use (in-order ids / heap indices /
+  // nodes, subtree digests), built once under tree_mu; the events mark them ready
   bool sdig_valid = false;
   bool inorder_valid = false;
+  bool ipts_valid = false;
+  std::mutex tree_mu;
+  cudaEvent_t built_ev = nullptr, inorder_ev = nullptr, sdig_ev = nullptr;
+  // search slots (SearchSlot): all of them, and the ones not leased
+  std::mutex slot_mu;
+  std::vector<std::unique_ptr<SearchSlot>> slots;
+  std::vector<SearchSlot*> free_slots;
+  std::mutex tab_mu;  // fkd_get_tables stages through work0
   // optional per-kernel timing (fkd_set_param "kernel_events"): a ring of
   // KEV_RING event sets, one per build / search call
   static constexpr uint32_t KEV_RING = 64;
@@ -117,13 +152,14 @@ struct fkd_tree_s {
   uint64_t kev_builds = 0, kev_searches = 0;
 
   ~fkd_tree_s() {
-    DevBuf* all[] = {&nodes, &ids, &work0, &work1, &sel, &ghist, &err, &qctr, &passflags,
-                     &qlo, &qhi, &counts, &offsets, &partials, &out, &tmp, &digests, &qorder,
-                     &lfeat, &lyhat, &lrange, &lstats, &sdig, &dids, &dnode, &bnd, &pool_st, &pool_len, &pool_s,
-                     &brec, &jctr, &rflags};
+    slots.clear();
+    DevBuf* all[] = {&nodes, &ids, &work0, &work1, &sel, &ghist, &err, &qctr, &passflags, &tmp,
+                     &lfeat, &lyhat, &lrange, &lstats, &sdig, &dids, &dnode, &ipts, &bnd, &tiebuf};
     for (DevBuf* b : all) b->release();
     if (herr) cudaFreeHost(herr);
     for (cudaEvent_t e : kev) cudaEventDestroy(e);
+    for (cudaEvent_t e : {built_ev, inorder_ev, sdig_ev})
+      if (e) cudaEventDestroy(e);
   }
   cudaEvent_t kev_at(uint64_t call, int k) { return kev[(size_t)(call % KEV_RING) * 7 + k]; }
 };
@@ -149,8 +185,10 @@ fkd_status status_from_err(uint32_t e, const char* what) {
   return fail(FKD_ERR_INTERNAL, buf);
 }
 
+// Reads the handle's (build) error word and clears it.
 fkd_status check_err_word(fkd_tree h, const char* what) {
   FKD_CUDA(cudaMemcpyAsync(h->herr, h->err.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+  FKD_CUDA(cudaMemsetAsync(h->err.p, 0, sizeof(uint32_t), h->stream));
   FKD_CUDA(cudaStreamSynchronize(h->stream));
   return status_from_err(*h->herr, what);
 }
@@ -162,6 +200,81 @@ fkd_status finish(fkd_tree h, const char* what, int mem) {
 
 Table table_of(fkd_tree h) { return Table{h->nodes.as<uint4>(), h->ids.as<uint32_t>()}; }
 
+// Makes the calling thread's current device the handle's for one call.
+struct DeviceScope {
+  int prev = -1;
+  explicit DeviceScope(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess || prev == dev) prev = -1;
+    else cudaSetDevice(dev);
+  }
+  ~DeviceScope() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+// One search call's slot and stream.  Device-memory calls run on the
+// handle's stream (stream-ordered with the caller's work); host-memory calls
+// are synchronous and run on the slot's own stream, so concurrent ones
+// overlap on the GPU.  Every lease first waits for the slot's previous work
+// and for the last build; release records the slot's completion event and
+// returns it to the pool.
+struct Lease {
+  fkd_tree h = nullptr;
+  SearchSlot* s = nullptr;
+  cudaStream_t st = nullptr;
+  ~Lease() {
+    if (!s) return;
+    cudaEventRecord(s->done, st);
+    std::lock_guard<std::mutex> g(h->slot_mu);
+    h->free_slots.push_back(s);
+  }
+};
+
+fkd_status lease_slot(fkd_tree h, int mem, Lease* L) {
+  SearchSlot* s = nullptr;
+  {
+    std::lock_guard<std::mutex> g(h->slot_mu);
+    if (!h->free_slots.empty()) {
+      s = h->free_slots.back();
+      h->free_slots.pop_back();
+    }
+  }
+  if (!s) {
+    std::unique_ptr<SearchSlot> ns(new (std::nothrow) SearchSlot());
+    if (!ns) return fail(FKD_ERR_NOMEM, "host allocation failed");
+    FKD_CUDA(cudaStreamCreateWithFlags(&ns->own, cudaStreamNonBlocking));
+    FKD_CUDA(cudaEventCreateWithFlags(&ns->done, cudaEventDisableTiming));
+    FKD_CUDA(ns->err.ensure(sizeof(uint32_t) * 4));
+    FKD_CUDA(ns->qctr.ensure(sizeof(uint32_t) * 4));
+    FKD_CUDA(cudaMallocHost((void**)&ns->herr, sizeof(uint32_t) * 16));
+    FKD_CUDA(cudaMemsetAsync(ns->err.p, 0, sizeof(uint32_t) * 4, ns->own));
+    FKD_CUDA(cudaEventRecord(ns->done, ns->own));
+    s = ns.get();
+    std::lock_guard<std::mutex> g(h->slot_mu);
+    h->slots.push_back(std::move(ns));
+  }
+  L->h = h;
+  L->s = s;
+  L->st = mem == FKD_MEM_DEVICE ? h->stream : s->own;
+  FKD_CUDA(cudaStreamWaitEvent(L->st, s->done, 0));
+  if (L->st != h->stream) FKD_CUDA(cudaStreamWaitEvent(L->st, h->built_ev, 0));
+  return FKD_OK;
+}
+
+// Reads the slot's error word and clears it (an error latched by an earlier
+// asynchronous call that used the slot is reported here too).
+fkd_status check_slot_err(const Lease& L, const char* what) {
+  FKD_CUDA(cudaMemcpyAsync(L.s->herr, L.s->err.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, L.st));
+  FKD_CUDA(cudaMemsetAsync(L.s->err.p, 0, sizeof(uint32_t), L.st));
+  FKD_CUDA(cudaStreamSynchronize(L.st));
+  return status_from_err(*L.s->herr, what);
+}
+
+fkd_status finish_search(fkd_tree h, const Lease& L, const char* what, int mem) {
+  if (mem == FKD_MEM_DEVICE && (h->flags & FKD_FLAG_ASYNC)) return FKD_OK;
+  return check_slot_err(L, what);
+}
+
 __global__ void k_tables_out(uint32_t n, int dim, const uint4* __restrict__ nodes, float* __restrict__ tab) {
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -171,7 +284,8 @@ __global__ void k_tables_out(uint32_t n, int dim, const uint4* __restrict__ node
 }
 
 // Stages host boxes (or aliases device boxes).
-fkd_status stage_boxes(fkd_tree h, const float* mins, const float* maxs, uint64_t q, int mem, Boxes* b) {
+fkd_status stage_boxes(fkd_tree h, const Lease& L, const float* mins, const float* maxs, uint64_t q, int mem,
+                       Boxes* b) {
   b->q = q;
   b->stride = q;
   if (mem == FKD_MEM_DEVICE) {
@@ -179,27 +293,34 @@ fkd_status stage_boxes(fkd_tree h, const float* mins, const float* maxs, uint64_
     b->hi = maxs;
     return FKD_OK;
   }
+  SearchSlot* s = L.s;
   const size_t bytes = (size_t)h->dim * q * sizeof(float);
-  FKD_CUDA(h->qlo.ensure(bytes ? bytes : 4));
-  FKD_CUDA(h->qhi.ensure(bytes ? bytes : 4));
+  FKD_CUDA(s->qlo.ensure(bytes ? bytes : 4));
+  FKD_CUDA(s->qhi.ensure(bytes ? bytes : 4));
   if (bytes) {
-    FKD_CUDA(cudaMemcpyAsync(h->qlo.p, mins, bytes, cudaMemcpyHostToDevice, h->stream));
-    FKD_CUDA(cudaMemcpyAsync(h->qhi.p, maxs, bytes, cudaMemcpyHostToDevice, h->stream));
+    FKD_CUDA(cudaMemcpyAsync(s->qlo.p, mins, bytes, cudaMemcpyHostToDevice, L.st));
+    FKD_CUDA(cudaMemcpyAsync(s->qhi.p, maxs, bytes, cudaMemcpyHostToDevice, L.st));
   }
-  b->lo = h->qlo.as<float>();
-  b->hi = h->qhi.as<float>();
+  b->lo = s->qlo.as<float>();
+  b->hi = s->qhi.as<float>();
   return FKD_OK;
 }
 
-SearchCtx search_ctx(fkd_tree h, const Boxes& b) {
+SearchCtx search_ctx(fkd_tree h, const Lease& L, const Boxes& b) {
   SearchCtx sc;
   memset(&sc, 0, sizeof sc);
   sc.g = make_geom((uint32_t)h->n);
   sc.tab = table_of(h);
+  if (h->search_bucket && h->ipts_valid) {
+    sc.tab.ipts = h->ipts.as<uint4>();
+    sc.tab.dids = h->dids.as<uint32_t>();
+    sc.tab.dnode = h->dnode.as<uint32_t>();
+    sc.bucket = h->search_bucket;
+  }
   sc.boxes = b;
-  sc.qcounter = h->qctr.as<uint32_t>();
-  sc.err = h->err.as<uint32_t>();
-  sc.stream = h->stream;
+  sc.qcounter = L.s->qctr.as<uint32_t>();
+  sc.err = L.s->err.as<uint32_t>();
+  sc.stream = L.st;
   sc.capacity = ~0ull;
   sc.lanes = h->search_lanes;
   return sc;
@@ -214,25 +335,27 @@ fkd_status check_search_args(fkd_tree h, const float* mins, const float* maxs, u
   return FKD_OK;
 }
 
+// Boxes below this count are searched in the caller's order: a spatial order
+// only pays when many boxes share the tree's cache lines.
+constexpr uint64_t BOX_ORDER_MIN = 4096;
+
 // Spatial processing order of the boxes (fkd_search.cu: launch_box_order).
-fkd_status box_order(fkd_tree h, const Boxes& b, const uint32_t** order) {
-  if (!h->box_order) {
-    *order = nullptr;
-    return FKD_OK;
-  }
-  FKD_CUDA(h->qorder.ensure(box_order_words(b.q) * sizeof(uint32_t)));
+fkd_status box_order(fkd_tree h, const Lease& L, const Boxes& b, const uint32_t** order) {
+  *order = nullptr;
+  if (!h->box_order || b.q < BOX_ORDER_MIN) return FKD_OK;
+  FKD_CUDA(L.s->qorder.ensure(box_order_words(b.q) * sizeof(uint32_t)));
   uint32_t* o = nullptr;
-  FKD_CUDA(launch_box_order(make_geom((uint32_t)h->n), table_of(h), b, h->dim, h->qorder.as<uint32_t>(), &o,
-                            h->stream));
+  FKD_CUDA(launch_box_order(make_geom((uint32_t)h->n), table_of(h), b, h->dim, L.s->qorder.as<uint32_t>(), &o,
+                            L.st));
   *order = o;
   return FKD_OK;
 }
 
 // count pass into dcounts (device)
 // rec (optional): the run pool fields of a recording count pass
-fkd_status count_pass(fkd_tree h, const Boxes& b, uint32_t* dcounts, const uint32_t* order,
+fkd_status count_pass(fkd_tree h, const Lease& L, const Boxes& b, uint32_t* dcounts, const uint32_t* order,
                       const SearchCtx* rec = nullptr) {
-  SearchCtx sc = search_ctx(h, b);
+  SearchCtx sc = search_ctx(h, L, b);
   sc.counts = dcounts;
   sc.order = order;
   if (rec) {
@@ -249,6 +372,57 @@ fkd_status count_pass(fkd_tree h, const Boxes& b, uint32_t* dcounts, const uint3
     sc.flag_ctr = rec->flag_ctr;
   }
   FKD_CUDA(launch_search(sc, h->dim, SEARCH_COUNT));
+  return FKD_OK;
+}
+
+// In-order id / heap-index tables of the current tree -- and, with leaf
+// buckets on, the in-order copy of the nodes -- built once per tree by the
+// first search that needs them; every caller's stream then waits for them.
+fkd_status ensure_inorder(fkd_tree h, cudaStream_t st) {
+  if (h->n == 0) return FKD_OK;
+  {
+    std::lock_guard<std::mutex> g(h->tree_mu);
+    const bool want_ipts = h->search_bucket != 0;
+    if (!h->inorder_valid || (want_ipts && !h->ipts_valid)) {
+      FKD_CUDA(h->dids.ensure(h->n * sizeof(uint32_t)));
+      FKD_CUDA(h->dnode.ensure(h->n * sizeof(uint32_t)));
+      Table t = table_of(h);
+      t.dids = h->dids.as<uint32_t>();
+      t.dnode = h->dnode.as<uint32_t>();
+      if (want_ipts) {
+        FKD_CUDA(h->ipts.ensure(h->n * sizeof(uint4)));
+        t.ipts = h->ipts.as<uint4>();
+      }
+      FKD_CUDA(launch_inorder(make_geom((uint32_t)h->n), t, st));
+      FKD_CUDA(cudaEventRecord(h->inorder_ev, st));
+      h->inorder_valid = true;
+      h->ipts_valid = want_ipts;
+    }
+  }
+  FKD_CUDA(cudaStreamWaitEvent(st, h->inorder_ev, 0));
+  return FKD_OK;
+}
+
+// The leaf-bucket scan's in-order tables, when it is on.
+fkd_status ensure_buckets(fkd_tree h, cudaStream_t st) {
+  return h->search_bucket ? ensure_inorder(h, st) : FKD_OK;
+}
+
+// Subtree digests of the current tree (digest search), built once per tree.
+fkd_status ensure_sdig(fkd_tree h, cudaStream_t st) {
+  if (h->n == 0) return FKD_OK;
+  {
+    std::lock_guard<std::mutex> g(h->tree_mu);
+    if (!h->sdig_valid) {
+      FKD_CUDA(h->sdig.ensure(h->n * sizeof(unsigned long long)));
+      Table t = table_of(h);
+      t.sdig = h->sdig.as<unsigned long long>();
+      FKD_CUDA(launch_subtree_digests(h->plan.evs, 1, (uint32_t)h->n, t, st));
+      FKD_CUDA(cudaEventRecord(h->sdig_ev, st));
+      h->sdig_valid = true;
+    }
+  }
+  FKD_CUDA(cudaStreamWaitEvent(st, h->sdig_ev, 0));
   return FKD_OK;
 }
 
@@ -283,7 +457,10 @@ fkd_status fkd_create(int dim, uint32_t flags, void* stream, fkd_tree* out) {
   if (e == cudaSuccess) e = h->qctr.ensure(sizeof(uint32_t) * 4);
   if (e == cudaSuccess) e = h->passflags.ensure(sizeof(uint32_t) * 64);
   if (e == cudaSuccess) e = cudaMallocHost((void**)&h->herr, sizeof(uint32_t) * 16);
+  for (cudaEvent_t* ev : {&h->built_ev, &h->inorder_ev, &h->sdig_ev})
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaMemsetAsync(h->err.p, 0, sizeof(uint32_t), h->stream);
+  if (e == cudaSuccess) e = cudaEventRecord(h->built_ev, h->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess) {
     delete h;
@@ -297,6 +474,7 @@ fkd_status fkd_create(int dim, uint32_t flags, void* stream, fkd_tree* out) {
 
 fkd_status fkd_destroy(fkd_tree h) {
   if (!h) return FKD_OK;
+  DeviceScope ds(h->device);
   cudaStreamSynchronize(h->stream);
   delete h;
   return FKD_OK;
@@ -329,12 +507,18 @@ fkd_status build_impl(fkd_tree h, const float* coords, const uint32_t* ids, cons
   if (mem != FKD_MEM_HOST && mem != FKD_MEM_DEVICE) return fail(FKD_ERR_ARG, "mem must be FKD_MEM_HOST or FKD_MEM_DEVICE");
   if (n >= (1ull << 31)) return fail(FKD_ERR_ARG, "at most 2^31-1 points per tree");
   if (n && !points && (!coords || !ids)) return fail(FKD_ERR_ARG, "null coords or ids");
+  DeviceScope ds(h->device);
   h->built = false;
-  h->sdig_valid = false;
-  h->inorder_valid = false;
+  {
+    std::lock_guard<std::mutex> g(h->tree_mu);
+    h->sdig_valid = false;
+    h->inorder_valid = false;
+    h->ipts_valid = false;
+  }
   h->n = n;
   if (n == 0) {
     h->built = true;
+    FKD_CUDA(cudaEventRecord(h->built_ev, h->stream));
     return FKD_OK;
   }
   const int dim = h->dim;
@@ -357,6 +541,7 @@ fkd_status build_impl(fkd_tree h, const float* coords, const uint32_t* ids, cons
     FKD_CUDA(h->work0.ensure(rec_bytes));
     FKD_CUDA(h->sel.ensure(sizeof(SegSel) * (size_t)h->plan.maxseg));
     FKD_CUDA(h->bnd.ensure(2 * sizeof(uint2) * (size_t)h->plan.maxseg));
+    if (h->tie_fix) FKD_CUDA(h->tiebuf.ensure((size_t)h->plan.maxseg * TIE_CAP * (dim + 1) * sizeof(uint32_t)));
     const size_t gw = (size_t)h->plan.maxseg * HIST_BINS;
     FKD_CUDA(h->ghist.ensure(gw * sizeof(uint32_t)));
     FKD_CUDA(cudaMemsetAsync(h->ghist.p, 0, gw * sizeof(uint32_t), h->stream));
@@ -398,6 +583,7 @@ fkd_status build_impl(fkd_tree h, const float* coords, const uint32_t* ids, cons
   bc.err = h->err.as<uint32_t>();
   bc.pending = h->passflags.as<uint32_t>();
   bc.bnd = h->plan.levels.empty() ? nullptr : h->bnd.as<uint2>();
+  bc.tiebuf = (h->tie_fix && !h->plan.levels.empty()) ? h->tiebuf.as<uint32_t>() : nullptr;
   bc.bnd_stride = h->plan.maxseg;
   bc.subtree = h->subtree;
   bc.small_select = h->small_select;
@@ -426,6 +612,7 @@ fkd_status build_impl(fkd_tree h, const float* coords, const uint32_t* ids, cons
     FKD_CUDA(cudaEventRecord(h->kev_at(h->kev_builds, 6), h->stream));
     ++h->kev_builds;
   }
+  FKD_CUDA(cudaEventRecord(h->built_ev, h->stream));
   h->built = true;
   fkd_status s = finish(h, points ? "fkd_build_points" : "fkd_build", mem);
   if (s != FKD_OK) h->built = false;
@@ -457,6 +644,8 @@ fkd_status fkd_get_tables(fkd_tree h, float* tab, uint32_t* tab_ids, int mem) {
   if (mem != FKD_MEM_HOST && mem != FKD_MEM_DEVICE) return fail(FKD_ERR_ARG, "mem must be FKD_MEM_HOST or FKD_MEM_DEVICE");
   const uint64_t n = h->n;
   if (n == 0) return FKD_OK;
+  DeviceScope ds(h->device);
+  std::lock_guard<std::mutex> g(h->tab_mu);
   if (tab) {
     float* dst = tab;
     if (mem == FKD_MEM_HOST) {
@@ -481,44 +670,38 @@ fkd_status fkd_search_count(fkd_tree h, const float* mins, const float* maxs, ui
   if (s != FKD_OK) return s;
   if (q && !counts) return fail(FKD_ERR_ARG, "null counts");
   if (q == 0) return FKD_OK;
+  DeviceScope ds(h->device);
+  Lease L;
+  if ((s = lease_slot(h, mem, &L)) != FKD_OK) return s;
   Boxes b;
-  if ((s = stage_boxes(h, mins, maxs, q, mem, &b)) != FKD_OK) return s;
+  if ((s = stage_boxes(h, L, mins, maxs, q, mem, &b)) != FKD_OK) return s;
   uint32_t* dc = counts;
   if (mem == FKD_MEM_HOST) {
-    FKD_CUDA(h->counts.ensure(q * sizeof(uint32_t)));
-    dc = h->counts.as<uint32_t>();
+    FKD_CUDA(L.s->counts.ensure(q * sizeof(uint32_t)));
+    dc = L.s->counts.as<uint32_t>();
   }
-  FKD_CUDA(cudaMemsetAsync(h->err.p, 0, sizeof(uint32_t), h->stream));
+  if ((s = ensure_buckets(h, L.st)) != FKD_OK) return s;
   const uint32_t* order = nullptr;
-  if ((s = box_order(h, b, &order)) != FKD_OK) return s;
-  if ((s = count_pass(h, b, dc, order)) != FKD_OK) return s;
+  if ((s = box_order(h, L, b, &order)) != FKD_OK) return s;
+  if ((s = count_pass(h, L, b, dc, order)) != FKD_OK) return s;
   if (mem == FKD_MEM_HOST)
-    FKD_CUDA(cudaMemcpyAsync(counts, dc, q * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
-  return finish(h, "fkd_search_count", mem);
+    FKD_CUDA(cudaMemcpyAsync(counts, dc, q * sizeof(uint32_t), cudaMemcpyDeviceToHost, L.st));
+  return finish_search(h, L, "fkd_search_count", mem);
 }
 
-// In-order id / heap-index tables of the current tree (built once per tree,
-// before the first write pass).
-static fkd_status ensure_inorder(fkd_tree h) {
-  if (h->inorder_valid || h->n == 0) return FKD_OK;
-  FKD_CUDA(h->dids.ensure(h->n * sizeof(uint32_t)));
-  FKD_CUDA(h->dnode.ensure(h->n * sizeof(uint32_t)));
-  Table t = table_of(h);
-  t.dids = h->dids.as<uint32_t>();
-  t.dnode = h->dnode.as<uint32_t>();
-  FKD_CUDA(launch_inorder(make_geom((uint32_t)h->n), t, h->stream));
-  h->inorder_valid = true;
-  return FKD_OK;
-}
+}  // extern "C"
+
+namespace {
 
 // rec: the run pool the count pass filled (null: traverse every box); with
 // it, k_expand writes the recorded runs and the traversal only revisits the
 // nflag boxes whose runs did not fit.
-static fkd_status write_pass(fkd_tree h, const Boxes& b, const uint64_t* doffsets, uint32_t* dout, uint64_t total,
-                             int ordered, const uint32_t* order, const SearchCtx* rec = nullptr, uint32_t nflag = 0) {
-  fkd_status s0 = ensure_inorder(h);
+fkd_status write_pass(fkd_tree h, const Lease& L, const Boxes& b, const uint64_t* doffsets, uint32_t* dout,
+                      uint64_t total, int ordered, const uint32_t* order, const SearchCtx* rec = nullptr,
+                      uint32_t nflag = 0) {
+  fkd_status s0 = ensure_inorder(h, L.st);
   if (s0 != FKD_OK) return s0;
-  SearchCtx sc = search_ctx(h, b);
+  SearchCtx sc = search_ctx(h, L, b);
   sc.tab.dids = h->dids.as<uint32_t>();
   sc.tab.dnode = h->dnode.as<uint32_t>();
   sc.order = order;
@@ -540,11 +723,15 @@ static fkd_status write_pass(fkd_tree h, const Boxes& b, const uint64_t* doffset
   }
   if (sc.boxes.q) FKD_CUDA(launch_search(sc, h->dim, SEARCH_WRITE));
   if (ordered) {
-    FKD_CUDA(h->tmp.ensure(total ? total * sizeof(uint32_t) : 4));
-    FKD_CUDA(launch_order_results(sc.g, sc.tab, doffsets, b.q, dout, h->tmp.as<uint32_t>(), sc.err, h->stream));
+    FKD_CUDA(L.s->tmp.ensure(total ? total * sizeof(uint32_t) : 4));
+    FKD_CUDA(launch_order_results(sc.g, sc.tab, doffsets, b.q, dout, L.s->tmp.as<uint32_t>(), sc.err, L.st));
   }
   return FKD_OK;
 }
+
+}  // namespace
+
+extern "C" {
 
 fkd_status fkd_search_write(fkd_tree h, const float* mins, const float* maxs, uint64_t q, const uint64_t* offsets,
                             uint32_t* ids_out, int ordered, int mem) {
@@ -552,32 +739,35 @@ fkd_status fkd_search_write(fkd_tree h, const float* mins, const float* maxs, ui
   if (s != FKD_OK) return s;
   if (!offsets) return fail(FKD_ERR_ARG, "null offsets");
   if (q == 0) return FKD_OK;
+  DeviceScope ds(h->device);
+  Lease L;
+  if ((s = lease_slot(h, mem, &L)) != FKD_OK) return s;
+  SearchSlot* sl = L.s;
   Boxes b;
-  if ((s = stage_boxes(h, mins, maxs, q, mem, &b)) != FKD_OK) return s;
+  if ((s = stage_boxes(h, L, mins, maxs, q, mem, &b)) != FKD_OK) return s;
   const uint64_t* doff = offsets;
   uint32_t* dout = ids_out;
   uint64_t total = 0;
   if (mem == FKD_MEM_HOST) {
     total = offsets[q];
     if (total && !ids_out) return fail(FKD_ERR_ARG, "null ids_out");
-    FKD_CUDA(h->offsets.ensure((q + 1) * sizeof(uint64_t)));
-    FKD_CUDA(cudaMemcpyAsync(h->offsets.p, offsets, (q + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, h->stream));
-    doff = h->offsets.as<uint64_t>();
-    FKD_CUDA(h->out.ensure(total ? total * sizeof(uint32_t) : 4));
-    dout = h->out.as<uint32_t>();
+    FKD_CUDA(sl->offsets.ensure((q + 1) * sizeof(uint64_t)));
+    FKD_CUDA(cudaMemcpyAsync(sl->offsets.p, offsets, (q + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, L.st));
+    doff = sl->offsets.as<uint64_t>();
+    FKD_CUDA(sl->out.ensure(total ? total * sizeof(uint32_t) : 4));
+    dout = sl->out.as<uint32_t>();
   } else {
-    FKD_CUDA(cudaMemcpyAsync(h->herr + 2, offsets + q, sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
-    FKD_CUDA(cudaStreamSynchronize(h->stream));
-    memcpy(&total, h->herr + 2, sizeof(uint64_t));
+    FKD_CUDA(cudaMemcpyAsync(sl->herr + 2, offsets + q, sizeof(uint64_t), cudaMemcpyDeviceToHost, L.st));
+    FKD_CUDA(cudaStreamSynchronize(L.st));
+    memcpy(&total, sl->herr + 2, sizeof(uint64_t));
     if (total && !ids_out) return fail(FKD_ERR_ARG, "null ids_out");
   }
-  FKD_CUDA(cudaMemsetAsync(h->err.p, 0, sizeof(uint32_t), h->stream));
   const uint32_t* order = nullptr;
-  if ((s = box_order(h, b, &order)) != FKD_OK) return s;
-  if ((s = write_pass(h, b, doff, dout, total, ordered, order)) != FKD_OK) return s;
+  if ((s = box_order(h, L, b, &order)) != FKD_OK) return s;
+  if ((s = write_pass(h, L, b, doff, dout, total, ordered, order)) != FKD_OK) return s;
   if (mem == FKD_MEM_HOST && total)
-    FKD_CUDA(cudaMemcpyAsync(ids_out, dout, total * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
-  return finish(h, "fkd_search_write", mem);
+    FKD_CUDA(cudaMemcpyAsync(ids_out, dout, total * sizeof(uint32_t), cudaMemcpyDeviceToHost, L.st));
+  return finish_search(h, L, "fkd_search_write", mem);
 }
 
 fkd_status fkd_search(fkd_tree h, const float* mins, const float* maxs, uint64_t q, uint64_t* offsets_out,
@@ -585,21 +775,27 @@ fkd_status fkd_search(fkd_tree h, const float* mins, const float* maxs, uint64_t
   fkd_status s = check_search_args(h, mins, maxs, q, mem);
   if (s != FKD_OK) return s;
   if (!offsets_out || !total) return fail(FKD_ERR_ARG, "null offsets_out or total");
+  DeviceScope ds(h->device);
+  Lease L;
+  if ((s = lease_slot(h, mem, &L)) != FKD_OK) return s;
+  SearchSlot* sl = L.s;
+  const cudaStream_t st = L.st;
   Boxes b;
-  if ((s = stage_boxes(h, mins, maxs, q, mem, &b)) != FKD_OK) return s;
-  FKD_CUDA(h->counts.ensure(q ? q * sizeof(uint32_t) : 4));
-  FKD_CUDA(h->partials.ensure(scan_partials_words(q) * sizeof(unsigned long long)));
+  if ((s = stage_boxes(h, L, mins, maxs, q, mem, &b)) != FKD_OK) return s;
+  FKD_CUDA(sl->counts.ensure(q ? q * sizeof(uint32_t) : 4));
+  FKD_CUDA(sl->partials.ensure(scan_partials_words(q) * sizeof(unsigned long long)));
   uint64_t* doff = offsets_out;
   if (mem == FKD_MEM_HOST) {
-    FKD_CUDA(h->offsets.ensure((q + 1) * sizeof(uint64_t)));
-    doff = h->offsets.as<uint64_t>();
+    FKD_CUDA(sl->offsets.ensure((q + 1) * sizeof(uint64_t)));
+    doff = sl->offsets.as<uint64_t>();
   }
-  FKD_CUDA(cudaMemsetAsync(h->err.p, 0, sizeof(uint32_t), h->stream));
   const uint32_t* order = nullptr;
-  if (q && (s = box_order(h, b, &order)) != FKD_OK) return s;
-  if ((s = ensure_inorder(h)) != FKD_OK) return s;
-  const bool kt = !h->kev.empty();
-  if (kt) FKD_CUDA(cudaEventRecord(h->kev_at(h->kev_searches, 0), h->stream));
+  if (q && (s = box_order(h, L, b, &order)) != FKD_OK) return s;
+  if ((s = ensure_inorder(h, st)) != FKD_OK) return s;
+  // per-kernel events only for calls on the handle's stream (a benchmark's
+  // single-threaded loop); the ring is not shared between threads
+  const bool kt = !h->kev.empty() && st == h->stream;
+  if (kt) FKD_CUDA(cudaEventRecord(h->kev_at(h->kev_searches, 0), st));
   // The count pass records every box's result as runs of the in-order table
   // (fkd_search.cu: k_search, k_expand) into a pool sized by the previous
   // call's demand; boxes that do not fit are traversed again by the write pass.
@@ -607,69 +803,69 @@ fkd_status fkd_search(fkd_tree h, const float* mins, const float* maxs, uint64_t
   memset(&rec, 0, sizeof rec);
   bool rec_on = q > 0 && h->search_record && (h->search_lanes == 0 || h->search_lanes == 32);
   if (rec_on) {
-    uint64_t pw = h->pool_want ? h->pool_want : 64 * q + (1u << 22);
-    uint64_t sw = h->pool_s_want ? h->pool_s_want : 256 * q + (1u << 22);
+    uint64_t pw = sl->pool_want ? sl->pool_want : 64 * q + (1u << 22);
+    uint64_t sw = sl->pool_s_want ? sl->pool_s_want : 256 * q + (1u << 22);
     if (h->search_pool) pw = sw = h->search_pool;
     if (pw > 0xffffffffull) pw = 0xffffffffull;
     if (sw > 0xffffffffull) sw = 0xffffffffull;
-    const uint64_t bw = h->brec_want ? h->brec_want : q + (1u << 16);
-    cudaError_t ae = h->pool_st.ensure(pw * sizeof(uint32_t));
-    if (ae == cudaSuccess) ae = h->pool_len.ensure(pw * sizeof(uint32_t));
-    if (ae == cudaSuccess) ae = h->pool_s.ensure(sw * sizeof(uint32_t));
-    if (ae == cudaSuccess) ae = h->brec.ensure(2 * bw * sizeof(uint4));
-    if (ae == cudaSuccess) ae = h->rflags.ensure(q * sizeof(uint32_t));
-    if (ae == cudaSuccess) ae = h->jctr.ensure(4 * sizeof(unsigned long long));
+    const uint64_t bw = sl->brec_want ? sl->brec_want : q + (1u << 16);
+    cudaError_t ae = sl->pool_st.ensure(pw * sizeof(uint32_t));
+    if (ae == cudaSuccess) ae = sl->pool_len.ensure(pw * sizeof(uint32_t));
+    if (ae == cudaSuccess) ae = sl->pool_s.ensure(sw * sizeof(uint32_t));
+    if (ae == cudaSuccess) ae = sl->brec.ensure(2 * bw * sizeof(uint4));
+    if (ae == cudaSuccess) ae = sl->rflags.ensure(q * sizeof(uint32_t));
+    if (ae == cudaSuccess) ae = sl->jctr.ensure(4 * sizeof(unsigned long long));
     if (ae != cudaSuccess) {
       // no room for the pool: traverse twice
       (void)cudaGetLastError();
-      h->pool_st.release();
-      h->pool_len.release();
-      h->pool_s.release();
-      h->brec.release();
-      h->pool_want = h->pool_s_want = h->brec_want = 0;
+      sl->pool_st.release();
+      sl->pool_len.release();
+      sl->pool_s.release();
+      sl->brec.release();
+      sl->pool_want = sl->pool_s_want = sl->brec_want = 0;
       rec_on = false;
     } else {
-      FKD_CUDA(cudaMemsetAsync(h->jctr.p, 0, 4 * sizeof(unsigned long long), h->stream));
+      FKD_CUDA(cudaMemsetAsync(sl->jctr.p, 0, 4 * sizeof(unsigned long long), st));
       // chunk records are reserved in blocks; the unused tail of a block must read as empty
-      FKD_CUDA(cudaMemsetAsync(h->brec.p, 0, h->brec.bytes, h->stream));
-      unsigned long long* ctr = h->jctr.as<unsigned long long>();
-      rec.pool_st = h->pool_st.as<uint32_t>();
-      rec.pool_len = h->pool_len.as<uint32_t>();
-      rec.pool_s = h->pool_s.as<uint32_t>();
+      FKD_CUDA(cudaMemsetAsync(sl->brec.p, 0, sl->brec.bytes, st));
+      unsigned long long* ctr = sl->jctr.as<unsigned long long>();
+      rec.pool_st = sl->pool_st.as<uint32_t>();
+      rec.pool_len = sl->pool_len.as<uint32_t>();
+      rec.pool_s = sl->pool_s.as<uint32_t>();
       rec.pool_ctr = ctr;  // [0] runs, [1] singles
-      rec.pool_cap = h->pool_st.bytes / sizeof(uint32_t);
-      rec.pool_cap_s = h->pool_s.bytes / sizeof(uint32_t);
-      rec.brec = h->brec.as<uint4>();
+      rec.pool_cap = sl->pool_st.bytes / sizeof(uint32_t);
+      rec.pool_cap_s = sl->pool_s.bytes / sizeof(uint32_t);
+      rec.brec = sl->brec.as<uint4>();
       rec.brec_ctr = ctr + 2;
-      rec.brec_cap = h->brec.bytes / (2 * sizeof(uint4));
-      rec.flags = h->rflags.as<uint32_t>();
+      rec.brec_cap = sl->brec.bytes / (2 * sizeof(uint4));
+      rec.flags = sl->rflags.as<uint32_t>();
       rec.flag_ctr = (uint32_t*)(ctr + 3);
     }
   }
-  if (q && (s = count_pass(h, b, h->counts.as<uint32_t>(), order, rec_on ? &rec : nullptr)) != FKD_OK) return s;
-  if (kt) FKD_CUDA(cudaEventRecord(h->kev_at(h->kev_searches, 1), h->stream));
-  FKD_CUDA(launch_scan_counts(h->counts.as<uint32_t>(), q, doff, h->partials.as<unsigned long long>(), h->stream));
-  FKD_CUDA(cudaMemcpyAsync(h->herr + 2, doff + q, sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
-  if (rec_on) FKD_CUDA(cudaMemcpyAsync(h->herr + 4, h->jctr.p, 4 * sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
-  FKD_CUDA(cudaStreamSynchronize(h->stream));
+  if (q && (s = count_pass(h, L, b, sl->counts.as<uint32_t>(), order, rec_on ? &rec : nullptr)) != FKD_OK) return s;
+  if (kt) FKD_CUDA(cudaEventRecord(h->kev_at(h->kev_searches, 1), st));
+  FKD_CUDA(launch_scan_counts(sl->counts.as<uint32_t>(), q, doff, sl->partials.as<unsigned long long>(), st));
+  FKD_CUDA(cudaMemcpyAsync(sl->herr + 2, doff + q, sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+  if (rec_on) FKD_CUDA(cudaMemcpyAsync(sl->herr + 4, sl->jctr.p, 4 * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+  FKD_CUDA(cudaStreamSynchronize(st));
   uint64_t tot = 0;
-  memcpy(&tot, h->herr + 2, sizeof(uint64_t));
+  memcpy(&tot, sl->herr + 2, sizeof(uint64_t));
   uint32_t nflag = 0;
   if (rec_on) {
     uint64_t dem[4];
-    memcpy(dem, h->herr + 4, sizeof dem);
+    memcpy(dem, sl->herr + 4, sizeof dem);
     nflag = (uint32_t)dem[3];
     // the next call's pools hold this call's demand with room to spare
-    if (!h->search_pool) h->pool_want = std::max<uint64_t>(h->pool_want, dem[0] + dem[0] / 4 + (1u << 22));
-    if (!h->search_pool) h->pool_s_want = std::max<uint64_t>(h->pool_s_want, dem[1] + dem[1] / 4 + (1u << 22));
-    h->brec_want = std::max<uint64_t>(h->brec_want, dem[2] + dem[2] / 4 + (1u << 16));
+    if (!h->search_pool) sl->pool_want = std::max<uint64_t>(sl->pool_want, dem[0] + dem[0] / 4 + (1u << 22));
+    if (!h->search_pool) sl->pool_s_want = std::max<uint64_t>(sl->pool_s_want, dem[1] + dem[1] / 4 + (1u << 22));
+    sl->brec_want = std::max<uint64_t>(sl->brec_want, dem[2] + dem[2] / 4 + (1u << 16));
   }
   *total = tot;
-  if ((s = check_err_word(h, "fkd_search (count)")) != FKD_OK) return s;
+  if ((s = check_slot_err(L, "fkd_search (count)")) != FKD_OK) return s;
   if (mem == FKD_MEM_HOST)
-    FKD_CUDA(cudaMemcpyAsync(offsets_out, doff, (q + 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
+    FKD_CUDA(cudaMemcpyAsync(offsets_out, doff, (q + 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
   if (tot > capacity) {
-    FKD_CUDA(cudaStreamSynchronize(h->stream));
+    FKD_CUDA(cudaStreamSynchronize(st));
     char buf[128];
     snprintf(buf, sizeof buf, "fkd_search: %llu results exceed the capacity of %llu ids", (unsigned long long)tot,
              (unsigned long long)capacity);
@@ -678,27 +874,27 @@ fkd_status fkd_search(fkd_tree h, const float* mins, const float* maxs, uint64_t
   if (tot && !ids_out) return fail(FKD_ERR_ARG, "null ids_out");
   if (tot == 0) {
     if (kt) {
-      FKD_CUDA(cudaEventRecord(h->kev_at(h->kev_searches, 2), h->stream));
-      FKD_CUDA(cudaEventRecord(h->kev_at(h->kev_searches, 3), h->stream));
+      FKD_CUDA(cudaEventRecord(h->kev_at(h->kev_searches, 2), st));
+      FKD_CUDA(cudaEventRecord(h->kev_at(h->kev_searches, 3), st));
       ++h->kev_searches;
     }
-    FKD_CUDA(cudaStreamSynchronize(h->stream));
+    FKD_CUDA(cudaStreamSynchronize(st));
     return FKD_OK;
   }
   uint32_t* dout = ids_out;
   if (mem == FKD_MEM_HOST) {
-    FKD_CUDA(h->out.ensure(tot * sizeof(uint32_t)));
-    dout = h->out.as<uint32_t>();
+    FKD_CUDA(sl->out.ensure(tot * sizeof(uint32_t)));
+    dout = sl->out.as<uint32_t>();
   }
-  if (kt) FKD_CUDA(cudaEventRecord(h->kev_at(h->kev_searches, 2), h->stream));
-  if ((s = write_pass(h, b, doff, dout, tot, ordered, order, rec_on ? &rec : nullptr, nflag)) != FKD_OK) return s;
+  if (kt) FKD_CUDA(cudaEventRecord(h->kev_at(h->kev_searches, 2), st));
+  if ((s = write_pass(h, L, b, doff, dout, tot, ordered, order, rec_on ? &rec : nullptr, nflag)) != FKD_OK) return s;
   if (kt) {
-    FKD_CUDA(cudaEventRecord(h->kev_at(h->kev_searches, 3), h->stream));
+    FKD_CUDA(cudaEventRecord(h->kev_at(h->kev_searches, 3), st));
     ++h->kev_searches;
   }
   if (mem == FKD_MEM_HOST)
-    FKD_CUDA(cudaMemcpyAsync(ids_out, dout, tot * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
-  return finish(h, "fkd_search", mem);
+    FKD_CUDA(cudaMemcpyAsync(ids_out, dout, tot * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  return finish_search(h, L, "fkd_search", mem);
 }
 
 fkd_status fkd_search_digest(fkd_tree h, const float* mins, const float* maxs, uint64_t q, uint32_t* counts,
@@ -707,37 +903,34 @@ fkd_status fkd_search_digest(fkd_tree h, const float* mins, const float* maxs, u
   if (s != FKD_OK) return s;
   if (q && (!counts || !digests)) return fail(FKD_ERR_ARG, "null counts or digests");
   if (q == 0) return FKD_OK;
+  DeviceScope ds(h->device);
+  Lease L;
+  if ((s = lease_slot(h, mem, &L)) != FKD_OK) return s;
   Boxes b;
-  if ((s = stage_boxes(h, mins, maxs, q, mem, &b)) != FKD_OK) return s;
+  if ((s = stage_boxes(h, L, mins, maxs, q, mem, &b)) != FKD_OK) return s;
   uint32_t* dc = counts;
   uint64_t* dd = digests;
   if (mem == FKD_MEM_HOST) {
-    FKD_CUDA(h->counts.ensure(q * sizeof(uint32_t)));
-    FKD_CUDA(h->digests.ensure(q * sizeof(uint64_t)));
-    dc = h->counts.as<uint32_t>();
-    dd = h->digests.as<uint64_t>();
+    FKD_CUDA(L.s->counts.ensure(q * sizeof(uint32_t)));
+    FKD_CUDA(L.s->digests.ensure(q * sizeof(uint64_t)));
+    dc = L.s->counts.as<uint32_t>();
+    dd = L.s->digests.as<uint64_t>();
   }
-  FKD_CUDA(cudaMemsetAsync(h->err.p, 0, sizeof(uint32_t), h->stream));
-  if (!h->sdig_valid && h->n) {
-    FKD_CUDA(h->sdig.ensure(h->n * sizeof(unsigned long long)));
-    Table t = table_of(h);
-    t.sdig = h->sdig.as<unsigned long long>();
-    FKD_CUDA(launch_subtree_digests(h->plan.evs, 1, (uint32_t)h->n, t, h->stream));
-    h->sdig_valid = true;
-  }
+  if ((s = ensure_sdig(h, L.st)) != FKD_OK) return s;
+  if ((s = ensure_buckets(h, L.st)) != FKD_OK) return s;
   const uint32_t* order = nullptr;
-  if ((s = box_order(h, b, &order)) != FKD_OK) return s;
-  SearchCtx sc = search_ctx(h, b);
+  if ((s = box_order(h, L, b, &order)) != FKD_OK) return s;
+  SearchCtx sc = search_ctx(h, L, b);
   sc.tab.sdig = h->sdig.as<unsigned long long>();
   sc.order = order;
   sc.counts = dc;
   sc.digests = (unsigned long long*)dd;
   FKD_CUDA(launch_search(sc, h->dim, SEARCH_DIGEST));
   if (mem == FKD_MEM_HOST) {
-    FKD_CUDA(cudaMemcpyAsync(counts, dc, q * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
-    FKD_CUDA(cudaMemcpyAsync(digests, dd, q * sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
+    FKD_CUDA(cudaMemcpyAsync(counts, dc, q * sizeof(uint32_t), cudaMemcpyDeviceToHost, L.st));
+    FKD_CUDA(cudaMemcpyAsync(digests, dd, q * sizeof(uint64_t), cudaMemcpyDeviceToHost, L.st));
   }
-  return finish(h, "fkd_search_digest", mem);
+  return finish_search(h, L, "fkd_search_digest", mem);
 }
 
 }  // extern "C"
@@ -754,33 +947,34 @@ fkd_status check_nn_args(fkd_tree h, const float* centers, uint64_t q, int mem) 
 }
 
 // Stages host centres (dim*q SoA) and radii (q, optional) or aliases device ones.
-fkd_status stage_centres(fkd_tree h, const float* centers, const float* radii, uint64_t q, int mem,
+fkd_status stage_centres(fkd_tree h, const Lease& L, const float* centers, const float* radii, uint64_t q, int mem,
                          const float** dctr, const float** drad) {
   if (mem == FKD_MEM_DEVICE) {
     *dctr = centers;
     if (drad) *drad = radii;
     return FKD_OK;
   }
+  SearchSlot* s = L.s;
   const size_t cb = (size_t)h->dim * q * sizeof(float);
-  FKD_CUDA(h->qlo.ensure(cb ? cb : 4));
-  if (cb) FKD_CUDA(cudaMemcpyAsync(h->qlo.p, centers, cb, cudaMemcpyHostToDevice, h->stream));
-  *dctr = h->qlo.as<float>();
+  FKD_CUDA(s->qlo.ensure(cb ? cb : 4));
+  if (cb) FKD_CUDA(cudaMemcpyAsync(s->qlo.p, centers, cb, cudaMemcpyHostToDevice, L.st));
+  *dctr = s->qlo.as<float>();
   if (drad) {
-    FKD_CUDA(h->qhi.ensure(q ? q * sizeof(float) : 4));
-    if (q) FKD_CUDA(cudaMemcpyAsync(h->qhi.p, radii, q * sizeof(float), cudaMemcpyHostToDevice, h->stream));
-    *drad = h->qhi.as<float>();
+    FKD_CUDA(s->qhi.ensure(q ? q * sizeof(float) : 4));
+    if (q) FKD_CUDA(cudaMemcpyAsync(s->qhi.p, radii, q * sizeof(float), cudaMemcpyHostToDevice, L.st));
+    *drad = s->qhi.as<float>();
   }
   return FKD_OK;
 }
 
 // Spatial order of the query centres (the box order of zero-size boxes).
-fkd_status centre_order(fkd_tree h, const float* dctr, uint64_t q, const uint32_t** order) {
+fkd_status centre_order(fkd_tree h, const Lease& L, const float* dctr, uint64_t q, const uint32_t** order) {
   Boxes b;
   b.lo = dctr;
   b.hi = dctr;
   b.stride = q;
   b.q = q;
-  return box_order(h, b, order);
+  return box_order(h, L, b, order);
 }
 
 }  // namespace
@@ -793,21 +987,23 @@ fkd_status fkd_search_radius_count(fkd_tree h, const float* centers, const float
   if (s != FKD_OK) return s;
   if (q && (!radii || !counts)) return fail(FKD_ERR_ARG, "null radii or counts");
   if (q == 0) return FKD_OK;
+  DeviceScope ds(h->device);
+  Lease L;
+  if ((s = lease_slot(h, mem, &L)) != FKD_OK) return s;
   const float *dctr = nullptr, *drad = nullptr;
-  if ((s = stage_centres(h, centers, radii, q, mem, &dctr, &drad)) != FKD_OK) return s;
+  if ((s = stage_centres(h, L, centers, radii, q, mem, &dctr, &drad)) != FKD_OK) return s;
   uint32_t* dc = counts;
   if (mem == FKD_MEM_HOST) {
-    FKD_CUDA(h->counts.ensure(q * sizeof(uint32_t)));
-    dc = h->counts.as<uint32_t>();
+    FKD_CUDA(L.s->counts.ensure(q * sizeof(uint32_t)));
+    dc = L.s->counts.as<uint32_t>();
   }
-  FKD_CUDA(cudaMemsetAsync(h->err.p, 0, sizeof(uint32_t), h->stream));
   const uint32_t* order = nullptr;
-  if ((s = centre_order(h, dctr, q, &order)) != FKD_OK) return s;
+  if ((s = centre_order(h, L, dctr, q, &order)) != FKD_OK) return s;
   FKD_CUDA(launch_radius(make_geom((uint32_t)h->n), table_of(h), dctr, drad, q, order, dc, nullptr, nullptr, 0,
-                         h->err.as<uint32_t>(), h->dim, h->stream));
+                         L.s->err.as<uint32_t>(), h->dim, L.st));
   if (mem == FKD_MEM_HOST)
-    FKD_CUDA(cudaMemcpyAsync(counts, dc, q * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
-  return finish(h, "fkd_search_radius_count", mem);
+    FKD_CUDA(cudaMemcpyAsync(counts, dc, q * sizeof(uint32_t), cudaMemcpyDeviceToHost, L.st));
+  return finish_search(h, L, "fkd_search_radius_count", mem);
 }
 
 fkd_status fkd_search_radius(fkd_tree h, const float* centers, const float* radii, uint64_t q, uint64_t* offsets_out,
@@ -816,33 +1012,38 @@ fkd_status fkd_search_radius(fkd_tree h, const float* centers, const float* radi
   if (s != FKD_OK) return s;
   if (!offsets_out || !total) return fail(FKD_ERR_ARG, "null offsets_out or total");
   if (q && !radii) return fail(FKD_ERR_ARG, "null radii");
+  DeviceScope ds(h->device);
+  Lease L;
+  if ((s = lease_slot(h, mem, &L)) != FKD_OK) return s;
+  SearchSlot* sl = L.s;
+  const cudaStream_t st = L.st;
   const float *dctr = nullptr, *drad = nullptr;
-  if ((s = stage_centres(h, centers, radii, q, mem, &dctr, &drad)) != FKD_OK) return s;
-  FKD_CUDA(h->counts.ensure(q ? q * sizeof(uint32_t) : 4));
-  FKD_CUDA(h->partials.ensure(scan_partials_words(q) * sizeof(unsigned long long)));
+  if ((s = stage_centres(h, L, centers, radii, q, mem, &dctr, &drad)) != FKD_OK) return s;
+  FKD_CUDA(sl->counts.ensure(q ? q * sizeof(uint32_t) : 4));
+  FKD_CUDA(sl->partials.ensure(scan_partials_words(q) * sizeof(unsigned long long)));
   uint64_t* doff = offsets_out;
   if (mem == FKD_MEM_HOST) {
-    FKD_CUDA(h->offsets.ensure((q + 1) * sizeof(uint64_t)));
-    doff = h->offsets.as<uint64_t>();
+    FKD_CUDA(sl->offsets.ensure((q + 1) * sizeof(uint64_t)));
+    doff = sl->offsets.as<uint64_t>();
   }
-  FKD_CUDA(cudaMemsetAsync(h->err.p, 0, sizeof(uint32_t), h->stream));
   const uint32_t* order = nullptr;
-  if (q && (s = centre_order(h, dctr, q, &order)) != FKD_OK) return s;
+  if (q && (s = centre_order(h, L, dctr, q, &order)) != FKD_OK) return s;
   const Geom g = make_geom((uint32_t)h->n);
   const Table tab = table_of(h);
-  FKD_CUDA(launch_radius(g, tab, dctr, drad, q, order, h->counts.as<uint32_t>(), nullptr, nullptr, 0,
-                         h->err.as<uint32_t>(), h->dim, h->stream));
-  FKD_CUDA(launch_scan_counts(h->counts.as<uint32_t>(), q, doff, h->partials.as<unsigned long long>(), h->stream));
-  FKD_CUDA(cudaMemcpyAsync(h->herr + 2, doff + q, sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
-  FKD_CUDA(cudaStreamSynchronize(h->stream));
+  uint32_t* err = sl->err.as<uint32_t>();
+  FKD_CUDA(launch_radius(g, tab, dctr, drad, q, order, sl->counts.as<uint32_t>(), nullptr, nullptr, 0, err, h->dim,
+                         st));
+  FKD_CUDA(launch_scan_counts(sl->counts.as<uint32_t>(), q, doff, sl->partials.as<unsigned long long>(), st));
+  FKD_CUDA(cudaMemcpyAsync(sl->herr + 2, doff + q, sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+  FKD_CUDA(cudaStreamSynchronize(st));
   uint64_t tot = 0;
-  memcpy(&tot, h->herr + 2, sizeof(uint64_t));
+  memcpy(&tot, sl->herr + 2, sizeof(uint64_t));
   *total = tot;
-  if ((s = check_err_word(h, "fkd_search_radius (count)")) != FKD_OK) return s;
+  if ((s = check_slot_err(L, "fkd_search_radius (count)")) != FKD_OK) return s;
   if (mem == FKD_MEM_HOST)
-    FKD_CUDA(cudaMemcpyAsync(offsets_out, doff, (q + 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
+    FKD_CUDA(cudaMemcpyAsync(offsets_out, doff, (q + 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
   if (tot > capacity) {
-    FKD_CUDA(cudaStreamSynchronize(h->stream));
+    FKD_CUDA(cudaStreamSynchronize(st));
     char buf[128];
     snprintf(buf, sizeof buf, "fkd_search_radius: %llu results exceed the capacity of %llu ids",
              (unsigned long long)tot, (unsigned long long)capacity);
@@ -850,24 +1051,23 @@ fkd_status fkd_search_radius(fkd_tree h, const float* centers, const float* radi
   }
   if (tot && !ids_out) return fail(FKD_ERR_ARG, "null ids_out");
   if (tot == 0) {
-    FKD_CUDA(cudaStreamSynchronize(h->stream));
+    FKD_CUDA(cudaStreamSynchronize(st));
     return FKD_OK;
   }
   uint32_t* dout = ids_out;
   if (mem == FKD_MEM_HOST) {
-    FKD_CUDA(h->out.ensure(tot * sizeof(uint32_t)));
-    dout = h->out.as<uint32_t>();
+    FKD_CUDA(sl->out.ensure(tot * sizeof(uint32_t)));
+    dout = sl->out.as<uint32_t>();
   }
   // ordered: the write pass emits heap indices that k_order sorts and maps to ids
-  FKD_CUDA(launch_radius(g, tab, dctr, drad, q, order, nullptr, doff, dout, ordered ? 1 : 0, h->err.as<uint32_t>(),
-                         h->dim, h->stream));
+  FKD_CUDA(launch_radius(g, tab, dctr, drad, q, order, nullptr, doff, dout, ordered ? 1 : 0, err, h->dim, st));
   if (ordered) {
-    FKD_CUDA(h->tmp.ensure(tot * sizeof(uint32_t)));
-    FKD_CUDA(launch_order_results(g, tab, doff, q, dout, h->tmp.as<uint32_t>(), h->err.as<uint32_t>(), h->stream));
+    FKD_CUDA(sl->tmp.ensure(tot * sizeof(uint32_t)));
+    FKD_CUDA(launch_order_results(g, tab, doff, q, dout, sl->tmp.as<uint32_t>(), err, st));
   }
   if (mem == FKD_MEM_HOST)
-    FKD_CUDA(cudaMemcpyAsync(ids_out, dout, tot * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
-  return finish(h, "fkd_search_radius", mem);
+    FKD_CUDA(cudaMemcpyAsync(ids_out, dout, tot * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  return finish_search(h, L, "fkd_search_radius", mem);
 }
 
 uint32_t fkd_knn_max_k(void) { return KNN_MAX; }
@@ -879,29 +1079,32 @@ fkd_status fkd_search_knn(fkd_tree h, const float* centers, uint64_t q, uint32_t
   if (k < 1 || k > KNN_MAX) return fail(FKD_ERR_ARG, "k must be 1..fkd_knn_max_k()");
   if (q && !ids_out) return fail(FKD_ERR_ARG, "null ids_out");
   if (q == 0) return FKD_OK;
+  DeviceScope ds(h->device);
+  Lease L;
+  if ((s = lease_slot(h, mem, &L)) != FKD_OK) return s;
+  SearchSlot* sl = L.s;
   const float* dctr = nullptr;
-  if ((s = stage_centres(h, centers, nullptr, q, mem, &dctr, nullptr)) != FKD_OK) return s;
+  if ((s = stage_centres(h, L, centers, nullptr, q, mem, &dctr, nullptr)) != FKD_OK) return s;
   const uint64_t cells = q * (uint64_t)k;
   uint32_t* di = ids_out;
   float* dd = dist2_out;
   if (mem == FKD_MEM_HOST) {
-    FKD_CUDA(h->out.ensure(cells * sizeof(uint32_t)));
-    di = h->out.as<uint32_t>();
+    FKD_CUDA(sl->out.ensure(cells * sizeof(uint32_t)));
+    di = sl->out.as<uint32_t>();
     if (dist2_out) {
-      FKD_CUDA(h->tmp.ensure(cells * sizeof(float)));
-      dd = h->tmp.as<float>();
+      FKD_CUDA(sl->tmp.ensure(cells * sizeof(float)));
+      dd = sl->tmp.as<float>();
     }
   }
-  FKD_CUDA(cudaMemsetAsync(h->err.p, 0, sizeof(uint32_t), h->stream));
   const uint32_t* order = nullptr;
-  if ((s = centre_order(h, dctr, q, &order)) != FKD_OK) return s;
-  FKD_CUDA(launch_knn(make_geom((uint32_t)h->n), table_of(h), dctr, q, order, k, di, dd, h->err.as<uint32_t>(),
-                      h->dim, h->stream));
+  if ((s = centre_order(h, L, dctr, q, &order)) != FKD_OK) return s;
+  FKD_CUDA(launch_knn(make_geom((uint32_t)h->n), table_of(h), dctr, q, order, k, di, dd, sl->err.as<uint32_t>(),
+                      h->dim, L.st));
   if (mem == FKD_MEM_HOST) {
-    FKD_CUDA(cudaMemcpyAsync(ids_out, di, cells * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
-    if (dist2_out) FKD_CUDA(cudaMemcpyAsync(dist2_out, dd, cells * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    FKD_CUDA(cudaMemcpyAsync(ids_out, di, cells * sizeof(uint32_t), cudaMemcpyDeviceToHost, L.st));
+    if (dist2_out) FKD_CUDA(cudaMemcpyAsync(dist2_out, dd, cells * sizeof(float), cudaMemcpyDeviceToHost, L.st));
   }
-  return finish(h, "fkd_search_knn", mem);
+  return finish_search(h, L, "fkd_search_knn", mem);
 }
 
 fkd_status fkd_set_param(fkd_tree h, const char* name, int64_t value) {
@@ -931,6 +1134,16 @@ fkd_status fkd_set_param(fkd_tree h, const char* name, int64_t value) {
   if (strcmp(name, "subtree") == 0) {
     if (value < 0 || value > 2) return fail(FKD_ERR_ARG, "subtree must be 0, 1 or 2");
     h->subtree = (int)value;
+    return FKD_OK;
+  }
+  if (strcmp(name, "tie_fix") == 0) {
+    if (value != 0 && value != 1) return fail(FKD_ERR_ARG, "tie_fix must be 0 or 1");
+    h->tie_fix = value != 0;
+    return FKD_OK;
+  }
+  if (strcmp(name, "search_bucket") == 0) {
+    if (value < 0 || value > (int64_t)BUCKET_MAX) return fail(FKD_ERR_ARG, "search_bucket must be 0..6");
+    h->search_bucket = (uint32_t)value;
     return FKD_OK;
   }
   if (strcmp(name, "search_record") == 0) {
@@ -1013,7 +1226,23 @@ fkd_status fkd_learn_stats(fkd_tree h, uint64_t* stats, int reset) {
 
 fkd_status fkd_sync(fkd_tree h) {
   if (!h) return fail(FKD_ERR_ARG, "null handle");
-  return check_err_word(h, "fkd_sync");
+  DeviceScope ds(h->device);
+  fkd_status s = check_err_word(h, "fkd_sync");
+  if (s != FKD_OK) return s;
+  // asynchronous searches latch into the error word of the slot they leased
+  std::vector<SearchSlot*> all;
+  {
+    std::lock_guard<std::mutex> g(h->slot_mu);
+    for (auto& p : h->slots) all.push_back(p.get());
+  }
+  for (SearchSlot* sl : all) {
+    FKD_CUDA(cudaStreamWaitEvent(h->stream, sl->done, 0));
+    FKD_CUDA(cudaMemcpyAsync(h->herr + 1, sl->err.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+    FKD_CUDA(cudaMemsetAsync(sl->err.p, 0, sizeof(uint32_t), h->stream));
+    FKD_CUDA(cudaStreamSynchronize(h->stream));
+    if ((s = status_from_err(h->herr[1], "fkd_sync")) != FKD_OK) return s;
+  }
+  return FKD_OK;
 }
 
 }  // extern "C"

@@ -136,6 +136,10 @@ struct Table {
   // the write pass
   uint32_t* dids = nullptr;
   uint32_t* dnode = nullptr;
+  // optional: the nodes in in-order position (ipts[p] = nodes[dnode[p]]), so
+  // a subtree's points are one contiguous range -- the searches scan the
+  // bottom subtrees ("leaf buckets") with coalesced loads instead of walking them
+  uint4* ipts = nullptr;
 };
 
 }  // namespace fkd

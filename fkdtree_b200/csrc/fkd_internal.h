@@ -29,7 +29,12 @@ struct SegSel {
   uint32_t kfull;             // the pivot rank within the segment (fallback restart)
   uint32_t bits0;             // the common prefix every key of the segment shares (restart point)
   unsigned long long prefix0;
+  uint32_t tie;               // 1: the pivot value is known and cnt <= TIE_CAP points carry it; the
+                              //    partition parks them and k_tie_fix orders them by id (no id passes)
 };
+// Points sharing a level's pivot value that the partition resolves by id
+// itself; more ties than this fall back to digit passes over the id bits.
+constexpr uint32_t TIE_CAP = 32;
 
 constexpr int FKD_MLP_FEATURES = 40;  // node summary width (== FKD_MLP_IN of the C ABI)
 
@@ -87,6 +92,8 @@ struct BuildCtx {
   SegSel* sel;    // >= max segments of a level
   uint32_t* ghist;
   uint32_t* pending;  // one word per digit pass (+1): does that pass have work
+  uint32_t* tiebuf = nullptr;  // >= max segments * TIE_CAP * (dim + 1) words: records tying on the pivot
+                               // value (null: ties resolved by id digit passes)
   uint2* bnd = nullptr;    // 2 x bnd_stride: per-segment (min, max) of the split coordinate's
                            // order bits, written by the previous level's partition (null: unused)
   uint32_t bnd_stride = 0; // >= max segments of a level
@@ -172,14 +179,20 @@ struct SearchCtx {
   uint64_t brec_cap;
   uint32_t* flags;               // boxes whose runs did not fit (the write pass traverses them)
   uint32_t* flag_ctr;            // (zeroed by the caller)
+  // leaf buckets (needs tab.ipts): visited subtrees of height <= bucket are
+  // scanned in in-order layout instead of walked (0: walk every level)
+  uint32_t bucket;
   cudaStream_t stream;
 };
 
 cudaError_t launch_search(SearchCtx& sc, int dim, int mode);
 // Writes the results of the runs a recording count pass stored (no-op without a pool).
 cudaError_t launch_expand(const SearchCtx& sc);
-// Fills tab.dids / tab.dnode (in-order tables); required by SEARCH_WRITE.
+// Fills tab.dids / tab.dnode (in-order tables; required by SEARCH_WRITE) and,
+// when tab.ipts is set, the in-order node copy the leaf-bucket scan reads.
 cudaError_t launch_inorder(const Geom& g, Table tab, cudaStream_t stream);
+// Largest leaf-bucket height the searches accept (subtrees of up to 2^(h+1)-1 points).
+constexpr uint32_t BUCKET_MAX = 6;
 // Fills tab.sdig (subtree digests) for every event; required by SEARCH_DIGEST.
 cudaError_t launch_subtree_digests(const EvDesc* evs, uint32_t nev, uint32_t max_n, Table tab, cudaStream_t stream);
 // Sorts every box's result slice by heap index and maps it to ids.

@@ -52,6 +52,7 @@ constexpr uint32_t SBLK = 4096;  // recording count pass: singles reserved per w
 constexpr uint32_t RBLK = 2048;  // runs reserved per warp at a time
 constexpr uint32_t CBLK = 64;    // chunk records reserved per warp at a time
 constexpr uint32_t RCAP = 4096;  // results per chunk record before a new one starts
+constexpr int BQ = 128;          // leaf buckets queued per warp (one step adds at most 64)
 
 __device__ __forceinline__ uint32_t lanemask_lt_s() {
   uint32_t m;
@@ -71,9 +72,12 @@ __device__ __forceinline__ unsigned long long warp_sum64(unsigned long long v) {
 
 // Popping the top 32 of a depth-sorted stack leaves at most 64 entries per
 // depth, and depth d has only 2^d nodes: sum over d of min(64, 2^d), plus one.
-__host__ __device__ inline uint32_t stack_cap(const Geom& g) {
+// With leaf buckets of height b (and the in-order nodes to scan them) no node
+// deeper than H - b - 1 is ever pushed.
+__host__ __device__ inline uint32_t stack_cap(const Geom& g, uint32_t bucket = 0u) {
+  const uint32_t dmax = bucket ? (g.H > bucket ? g.H - bucket - 1u : 0u) : g.H;
   uint32_t c = 1u;
-  for (uint32_t d = 0; d <= g.H; ++d) c += d < 6u ? (1u << d) : 64u;
+  for (uint32_t d = 0; d <= dmax; ++d) c += d < 6u ? (1u << d) : 64u;
   return c;
 }
 
@@ -150,6 +154,8 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
   __shared__ uint32_t jst[QW][JN];   // in-order start of each buffered subtree (write pass, recording count)
   __shared__ uint32_t jlen[QW][JN];  // its size
   __shared__ uint32_t jpre[QW][JN];  // write pass: exclusive prefix of the sizes; recording count: single positions
+  __shared__ uint32_t bq_st[QW][BQ];   // leaf buckets: in-order start of each queued subtree
+  __shared__ uint32_t bq_len[QW][BQ];  // its size (the scan overwrites it with the exclusive prefix)
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   uint32_t* stk_node = (uint32_t*)smem_raw + (size_t)warp * cap;
   uint8_t* stk_mask = (uint8_t*)((uint32_t*)smem_raw + (size_t)QW * cap) + (size_t)warp * cap;
@@ -179,6 +185,9 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
       tab.nodes = sc.tab.nodes + ev.base;
       tab.ids = sc.tab.ids + ev.base;
       tab.sdig = sc.tab.sdig ? sc.tab.sdig + ev.base : nullptr;
+      tab.ipts = sc.tab.ipts ? sc.tab.ipts + ev.base : nullptr;
+      tab.dids = sc.tab.dids ? sc.tab.dids + ev.base : nullptr;
+      tab.dnode = sc.tab.dnode ? sc.tab.dnode + ev.base : nullptr;
       blo = sc.boxes.lo + ev.qcbase;
       bhi = sc.boxes.hi + ev.qcbase;
       bstride = ev.nq;
@@ -186,6 +195,8 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
       oj = ev.qout + bj;
     }
     const uint32_t n = g.n;
+    // children at depth >= bdep are leaf buckets: subtrees of height <= sc.bucket, scanned in in-order layout
+    const uint32_t bdep = (tab.ipts && sc.bucket) ? (g.H > sc.bucket ? g.H - sc.bucket : 0u) : 0xffffffffu;
     float lo[4] = {0.f, 0.f, 0.f, 0.f}, hi[4] = {0.f, 0.f, 0.f, 0.f};
     uint32_t mask0 = 0u;
 #pragma unroll
@@ -339,6 +350,109 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
       __syncwarp();
     };
 
+    // Scans the queued leaf buckets: bucket k is the in-order range
+    // [bq_st[k], bq_st[k] + bq_len[k]) of a subtree the walk would enter;
+    // the ranges are concatenated and every lane tests one point per step
+    // (16-byte loads of consecutive in-order nodes) -- the same points the
+    // walk would have found, since the walk only skips subtrees that lie
+    // outside the box.  Recording: consecutive in-box positions become one
+    // run, isolated ones singles.
+    uint32_t nb = 0;  // queued buckets (warp-uniform)
+    auto scan_buckets = [&](uint32_t nbk) {
+      uint32_t carry = 0u;
+      for (uint32_t e0 = 0; e0 < nbk; e0 += 32u) {
+        const uint32_t e = e0 + lane;
+        const uint32_t len = e < nbk ? bq_len[warp][e] : 0u;
+        uint32_t incl = len;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= (uint32_t)o) incl += y;
+        }
+        if (e < nbk) bq_len[warp][e] = carry + incl - len;
+        carry += __shfl_sync(0xffffffffu, incl, 31);
+      }
+      __syncwarp();
+      const uint32_t total = carry;
+      uint32_t jb = 0u;  // the bucket holding slot w0 (warp-uniform)
+      for (uint32_t w0 = 0; w0 < total; w0 += 32u) {
+        const uint32_t k = jb + lane;
+        const bool kv = k < nbk;
+        const uint32_t pk = kv ? bq_len[warp][k] : total;
+        const uint32_t sk = kv ? bq_st[warp][k] : 0u;
+        // buckets after jb start after w0 (every bucket holds at least one point)
+        const uint32_t B =
+            __reduce_or_sync(0xffffffffu, (lane > 0u && kv && pk < w0 + 32u) ? (1u << (pk - w0)) : 0u);
+        const uint32_t jl = __popc(B & (0xffffffffu >> (31u - lane)));
+        const uint32_t mp = __shfl_sync(0xffffffffu, pk, jl);
+        const uint32_t ms = __shfl_sync(0xffffffffu, sk, jl);
+        uint32_t nbn = jb + __popc(B);
+        if (nbn + 1u < nbk && bq_len[warp][nbn + 1u] == w0 + 32u) ++nbn;
+        jb = nbn;
+        const bool ok = w0 + lane < total;
+        const uint32_t pos = ms + (w0 + lane - mp);
+        bool hit = false;
+        uint4 pt = make_uint4(0u, 0u, 0u, 0u);
+        if (ok) {
+          pt = __ldg(tab.ipts + pos);
+          bool in = true;
+          if (DIM > 0) in &= (__uint_as_float(pt.x) <= hi[0] && __uint_as_float(pt.x) >= lo[0]);
+          if (DIM > 1) in &= (__uint_as_float(pt.y) <= hi[1] && __uint_as_float(pt.y) >= lo[1]);
+          if (DIM > 2) in &= (__uint_as_float(pt.z) <= hi[2] && __uint_as_float(pt.z) >= lo[2]);
+          if (DIM > 3) in &= (__uint_as_float(pt.w) <= hi[3] && __uint_as_float(pt.w) >= lo[3]);
+          hit = in;
+        }
+        if (MODE == SEARCH_COUNT && !record) {
+          acc += hit ? 1u : 0u;
+        } else if (MODE == SEARCH_DIGEST) {
+          if (hit) {
+            acc += mix64(DIM <= 3 ? pt.w : __ldg(tab.dids + pos));
+            acc2 += 1u;
+          }
+        } else if (MODE == SEARCH_WRITE) {
+          uint32_t idv = 0u, node = 0u;
+          if (hit) {
+            if (sc.heap_out)
+              node = __ldg(tab.dnode + pos);
+            else
+              idv = DIM <= 3 ? pt.w : __ldg(tab.dids + pos);
+          }
+          emit_ballot(hit, node, idv);
+        } else {
+          acc += hit ? 1u : 0u;
+          if (njobs > (uint32_t)(JN - 16) || nsing > (uint32_t)(JN - 32)) {
+            __syncwarp();
+            flush_runs(njobs);
+            njobs = 0;
+          }
+          const uint32_t hb = __ballot_sync(0xffffffffu, hit);
+          const uint32_t ppos = __shfl_up_sync(0xffffffffu, pos, 1);
+          const bool cont = hit && lane > 0u && ((hb >> (lane - 1u)) & 1u) && ppos + 1u == pos;
+          const uint32_t cb = __ballot_sync(0xffffffffu, cont);
+          const bool start = hit && !cont;
+          const uint32_t after = lane < 31u ? (cb >> (lane + 1u)) : 0u;
+          const uint32_t rl = (uint32_t)__ffs(~after);  // 1 + the continuations that follow
+          const bool single = start && rl == 1u;
+          const bool isrun = start && rl > 1u;
+          const uint32_t bs = __ballot_sync(0xffffffffu, single), br = __ballot_sync(0xffffffffu, isrun);
+          if (isrun) {
+            const uint32_t jp = njobs + __popc(br & lt);
+            jst[warp][jp] = pos;
+            jlen[warp][jp] = rl;
+          }
+          if (single) jpre[warp][nsing + __popc(bs & lt)] = pos;
+          njobs += __popc(br);
+          nsing += __popc(bs);
+        }
+      }
+      if (record && (njobs > (uint32_t)(JN - 64) || nsing > (uint32_t)(JN - 32))) {
+        __syncwarp();
+        flush_runs(njobs);
+        njobs = 0;
+      }
+      __syncwarp();
+    };
+
     int top = 0;
     if (n > 0) {
       if (mask0 == FULL) {
@@ -387,6 +501,7 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
       __syncwarp();
       top = base;
       bool emit = false, pushL = false, pushR = false, contL = false, contR = false;
+      bool bucketL = false, bucketR = false;
       uint32_t maskL = 0u, maskR = 0u, idv = 0u, cnext = 0u;
       if (have) {
         // 3D: the node's split dimension rides in the top bits of its mask byte
@@ -424,6 +539,15 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
         contR = visitR && maskR == FULL;
         pushL = visitL && !contL;
         pushR = visitR && !contR;
+        if (pushL || pushR) {
+          // children at the bucket depth are scanned, not walked
+          const uint32_t dep = 31u - (uint32_t)__clz(i + 1u);
+          if (dep + 1u >= bdep) {
+            bucketL = pushL;
+            bucketR = pushR;
+            pushL = pushR = false;
+          }
+        }
       }
       if (MODE == SEARCH_COUNT) {
         if (!record) {
@@ -550,7 +674,36 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
         stk_mask[p] = (uint8_t)(maskR | ctag);
       }
       top += (int)tot;
+      // queue the leaf buckets
+      const uint32_t bbl = __ballot_sync(0xffffffffu, bucketL), bbr = __ballot_sync(0xffffffffu, bucketR);
+      if (bbl | bbr) {
+        uint32_t q = nb + __popc(bbl & lt) + __popc(bbr & lt);
+        if (bucketL || bucketR) {
+          const uint32_t dc = floor_log2_u32(i + 1u) + 1u;
+          const uint32_t tl = 2u * (i + 1u - (1u << (dc - 1u)));
+          if (bucketL) {
+            bq_st[warp][q] = seg_start(g, dc, tl);
+            bq_len[warp][q] = seg_len(g, dc, tl);
+            ++q;
+          }
+          if (bucketR) {
+            bq_st[warp][q] = seg_start(g, dc, tl + 1u);
+            bq_len[warp][q] = seg_len(g, dc, tl + 1u);
+          }
+        }
+        nb += __popc(bbl) + __popc(bbr);
+        if (nb > (uint32_t)(BQ - 64)) {
+          __syncwarp();
+          scan_buckets(nb);
+          nb = 0;
+        }
+      }
       __syncwarp();
+    }
+    if (nb) {
+      __syncwarp();
+      scan_buckets(nb);
+      nb = 0;
     }
 
     if (MODE == SEARCH_WRITE && njobs) {
@@ -913,7 +1066,7 @@ static cudaError_t run_search(SearchCtx& sc) {
   if constexpr (MODE == SEARCH_COUNT && !REC) {
     if (sc.pool_st) return run_search<DIM, MODE, true>(sc);
   }
-  const uint32_t cap = stack_cap(sc.g);
+  const uint32_t cap = stack_cap(sc.g, sc.tab.ipts ? sc.bucket : 0u);
   const size_t smem = (size_t)QW * cap * 5u;
   cudaError_t e =
       cudaFuncSetAttribute(k_search<DIM, MODE, REC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -978,14 +1131,15 @@ cudaError_t launch_search(SearchCtx& sc, int dim, int mode) {
 // dids / dnode list the ids / heap indices in that order, so every subtree
 // is one contiguous range of them.
 
-__global__ void k_inorder(Geom g, const uint32_t* __restrict__ ids, uint32_t* __restrict__ dids,
-                          uint32_t* __restrict__ dnode) {
+__global__ void k_inorder(Geom g, const uint32_t* __restrict__ ids, const uint4* __restrict__ nodes,
+                          uint32_t* __restrict__ dids, uint32_t* __restrict__ dnode, uint4* __restrict__ ipts) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x) {
     const uint32_t d = floor_log2_u32(i + 1u);
     const uint32_t t = i + 1u - (1u << d);
     const uint32_t p = seg_start(g, d, t) + (d < g.H ? seg_rank(g, d, t) : 0u);
     dids[p] = ids[i];
     dnode[p] = i;
+    if (ipts) ipts[p] = nodes[i];
   }
 }
 
@@ -997,7 +1151,7 @@ cudaError_t launch_inorder(const Geom& g, Table tab, cudaStream_t stream) {
   uint32_t blocks = (g.n + 255u) / 256u;
   const uint32_t cap = (uint32_t)sms * 8u;
   if (blocks > cap) blocks = cap;
-  k_inorder<<<blocks, 256, 0, stream>>>(g, tab.ids, tab.dids, tab.dnode);
+  k_inorder<<<blocks, 256, 0, stream>>>(g, tab.ids, tab.nodes, tab.dids, tab.dnode, tab.ipts);
   count_launches(1);
   return cudaGetLastError();
 }

@@ -63,3 +63,43 @@ def box_index(wb: Batch, events: Sequence[int]) -> np.ndarray:
     scatters per-shard counts / digests back into the full batch's order."""
     parts = [np.arange(int(wb.q_off[e]), int(wb.q_off[e + 1]), dtype=np.int64) for e in events]
     return np.concatenate(parts) if parts else np.zeros(0, dtype=np.int64)
+
+
+def run_share(wb: Batch, events: Sequence[int], device, reps: int = 1, stream=None):
+    """Builds and digest-searches one rank's share of the events on its own GPU
+    through the batch C ABI (fkd_batch_run: gather, build and per-box count +
+    digest in one CUDA graph), `reps` times after one warm-up run.  Returns
+    (counts, digests, box_index, ms): counts / digests (CUDA tensors, the
+    share's boxes in its order), box_index the global box index of each
+    (box_index()), ms the CUDA-event time of the last run on the share's
+    stream.  No collective: events are independent trees."""
+    import torch
+
+    from . import Batch as _Batch
+
+    sb = sub_batch(wb, events)
+    dev = torch.device(device)
+    # the graph is captured on this stream (capture needs a stream other than the legacy default one)
+    s = stream if stream is not None else torch.cuda.Stream(dev)
+    coords = torch.from_numpy(sb.coords).to(dev)
+    ids = torch.from_numpy(sb.ids.view(np.int32)).to(dev)
+    mins = torch.from_numpy(sb.mins).to(dev)
+    maxs = torch.from_numpy(sb.maxs).to(dev)
+    counts = torch.empty(sb.n_queries, dtype=torch.int32, device=dev)
+    digests = torch.empty(sb.n_queries, dtype=torch.int64, device=dev)
+    s.wait_stream(torch.cuda.current_stream(dev))
+    b = _Batch.of(sb, stream=s)
+    try:
+        b.run(coords, ids, mins, maxs, counts, digests)
+        ms = 0.0
+        for _ in range(reps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            b.run(coords, ids, mins, maxs, counts, digests)
+            e1.record(s)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1)
+    finally:
+        b.close()
+    return counts, digests, box_index(wb, events), ms

@@ -25,11 +25,19 @@
 //     build, like FKDTree_OpenCL (FKDTree_opencl.h:194-206);
 //   * failures throw std::runtime_error carrying fkd_last_error(); the
 //     reference aborts or prints instead.
+// Threads: as with the reference, once build() has returned any number of
+// threads may search one tree at the same time (main.cpp:351-359 runs
+// search_in_the_box from a TBB parallel_for); every search call leases its own
+// scratch and stream inside the library.  build() must not overlap any other
+// call on the same tree.  A single-box search is a host round trip to the GPU
+// (tens of microseconds); callers with many boxes should use
+// search_in_the_box_batch, one launch for all of them.
 #ifndef FKDTREE_CUDA_H_
 #define FKDTREE_CUDA_H_
 
 #include <algorithm>  // FKDTree.h uses std::find without including it
 #include <iostream>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <type_traits>
@@ -62,6 +70,7 @@ class FKDTree_CUDA : public FKDTree<TYPE, numberOfDimensions> {
 
   void build() override {
     check(fkd_build_points(h_, points_.data(), n_, FKD_MEM_HOST));
+    std::lock_guard<std::mutex> g(tables_mu_);
     synced_ = false;
   }
 
@@ -70,13 +79,16 @@ class FKDTree_CUDA : public FKDTree<TYPE, numberOfDimensions> {
   std::vector<unsigned int> search_in_the_ball(const Point& centre, float radius) {
     float c[numberOfDimensions];
     for (unsigned int d = 0; d < numberOfDimensions; ++d) c[d] = centre[d];
-    unsigned int count = 0;
-    check(fkd_search_radius_count(h_, c, &radius, 1, &count, FKD_MEM_HOST));
-    std::vector<unsigned int> out(count);
+    thread_local std::vector<unsigned int> buf(256);
     uint64_t offsets[2] = {0, 0};
     uint64_t total = 0;
-    check(fkd_search_radius(h_, c, &radius, 1, offsets, out.data(), count, &total, 1, FKD_MEM_HOST));
-    return out;
+    fkd_status s = fkd_search_radius(h_, c, &radius, 1, offsets, buf.data(), buf.size(), &total, 1, FKD_MEM_HOST);
+    if (s == FKD_ERR_CAPACITY && total > buf.size()) {
+      buf.resize(total + total / 2);
+      s = fkd_search_radius(h_, c, &radius, 1, offsets, buf.data(), buf.size(), &total, 1, FKD_MEM_HOST);
+    }
+    check(s);
+    return std::vector<unsigned int>(buf.begin(), buf.begin() + total);
   }
 
   // The k nearest points of `centre`, ascending in (squared distance, id);
@@ -167,22 +179,29 @@ class FKDTree_CUDA : public FKDTree<TYPE, numberOfDimensions> {
       }
   }
 
+  // One box, one library call: the result lands in a per-thread buffer sized
+  // by the largest box this thread has seen; only a box larger than that
+  // takes a second call (fkd_search reports the total with FKD_ERR_CAPACITY).
   std::vector<unsigned int> one(const Point& minPoint, const Point& maxPoint) {
     float lo[numberOfDimensions], hi[numberOfDimensions];
     for (unsigned int c = 0; c < numberOfDimensions; ++c) {
       lo[c] = minPoint[c];
       hi[c] = maxPoint[c];
     }
-    unsigned int count = 0;
-    check(fkd_search_count(h_, lo, hi, 1, &count, FKD_MEM_HOST));
-    std::vector<unsigned int> out(count);
-    uint64_t offsets[2] = {0, count};
+    thread_local std::vector<unsigned int> buf(256);
+    uint64_t offsets[2] = {0, 0};
     uint64_t total = 0;
-    if (count) check(fkd_search(h_, lo, hi, 1, offsets, out.data(), count, &total, 1, FKD_MEM_HOST));
-    return out;
+    fkd_status s = fkd_search(h_, lo, hi, 1, offsets, buf.data(), buf.size(), &total, 1, FKD_MEM_HOST);
+    if (s == FKD_ERR_CAPACITY && total > buf.size()) {
+      buf.resize(total + total / 2);
+      s = fkd_search(h_, lo, hi, 1, offsets, buf.data(), buf.size(), &total, 1, FKD_MEM_HOST);
+    }
+    check(s);
+    return std::vector<unsigned int>(buf.begin(), buf.begin() + total);
   }
 
   void sync_tables() {
+    std::lock_guard<std::mutex> g(tables_mu_);
     if (synced_) return;
     std::vector<float> flat(numberOfDimensions * n_);
     tab_ids_.resize(n_);
@@ -196,6 +215,7 @@ class FKDTree_CUDA : public FKDTree<TYPE, numberOfDimensions> {
   size_t n_;
   std::vector<Point> points_;
   fkd_tree h_ = nullptr;
+  std::mutex tables_mu_;  // the lazy table download (getDimensionVector / getIdVector)
   bool synced_;
   std::vector<std::vector<TYPE>> dims_;
   std::vector<unsigned int> tab_ids_;

@@ -26,8 +26,17 @@
  *    handle's device; the call is stream-ordered on the handle's stream and,
  *    unless the handle was created with FKD_FLAG_ASYNC, synchronises before it
  *    returns so that errors can be reported).
- *  - a handle is bound to one device and one stream; calls on one handle must
- *    not overlap.  Different handles are independent.
+ *  - a handle is bound to one device and one stream.  Once a build has
+ *    returned, searches (fkd_search*, fkd_search_radius*, fkd_search_knn,
+ *    fkd_get_tables) may be called on the handle from any number of host
+ *    threads at once, as the reference's searches are (main.cpp:351-359):
+ *    each call leases its own scratch from the handle.  Host-memory calls run
+ *    on a stream of that scratch (concurrent calls overlap on the GPU, each
+ *    ordered after the last build); device-memory calls run on the handle's
+ *    stream.  A build, fkd_set_param, fkd_set_mlp, fkd_set_stream or
+ *    fkd_sync must not overlap any other call on the same handle, and with
+ *    FKD_FLAG_ASYNC the caller orders its calls.  Different handles are
+ *    independent.
  *  - NaN coordinates are rejected (FKD_ERR_NAN): the reference comparator
  *    (FKDTree_cpu.h:246-252) is not a strict weak order with NaN.  -0.0 and
  *    +0.0 compare equal and tie on id, as in the reference.
@@ -219,8 +228,17 @@ FKD_API fkd_status fkd_sync(fkd_tree h);
  *   "search_pool"   entries of the record pools (0, the default: sized by the
  *                   previous call's demand; boxes that do not fit are traversed
  *                   again, so any size gives the same results)
+ *   "search_bucket" (0..6, default 4): box searches scan the visited subtrees
+ *                   of height <= this many levels (at most 2^(v+1)-1 points)
+ *                   point by point in in-order layout instead of walking them;
+ *                   0 walks every level.  Costs 16 bytes per point of device
+ *                   memory for the in-order copy of the nodes.
+ *   "tie_fix"       (0/1, default 1): when at most 32 points of a segment share
+ *                   its pivot value, the partition orders them by id instead of
+ *                   two more digit passes over the id bits
  *   "kernel_events" (0/1): record CUDA events around the kernels of every
- *                   fkd_build and fkd_search call for fkd_kernel_times.
+ *                   fkd_build and fkd_search call for fkd_kernel_times (only
+ *                   calls on the handle's stream, from one thread).
  * No reference counterpart. */
 FKD_API fkd_status fkd_set_param(fkd_tree h, const char* name, int64_t value);
 /* Device times (ms) of the kernels of the build / search `back` calls ago
@@ -257,6 +275,9 @@ FKD_API fkd_status fkd_batch_destroy(fkd_batch b);
  *                  box in a launch of their own (0: one launch for all)
  *   "subtree"      shared-memory subtree kernel: 0 auto (presorted lists for
  *                  dims 1-3, radix select for dim 4), 1 radix select, 2 lists
+ *   "tie_fix"      (0/1, default 1) as fkd_set_param's
+ * A failed "hist_ctas" re-plan leaves the batch without a plan: builds then
+ * return FKD_ERR_STATE until a re-plan succeeds.
  * No reference counterpart (the reference has one fixed launch shape). */
 FKD_API fkd_status fkd_batch_set_param(fkd_batch b, const char* name, int64_t value);
 /* Builds every event; the tables equal one FKDTree_CPU::build per event. */

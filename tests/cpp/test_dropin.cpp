@@ -3,9 +3,12 @@
 // (target `dropin`, against the reference headers) into oracle/_ref/test_dropin;
 // run on a GPU by tests/test_dropin_gpu.py.  Prints "DROPIN OK" on success.
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cstdio>
 #include <memory>
 #include <random>
+#include <thread>
 #include <vector>
 
 #include "FKDTree_CUDA.h"
@@ -111,11 +114,67 @@ static int run(unsigned n, unsigned seed, float hw) {
   return 0;
 }
 
+// main.cpp:351-359's pattern: one built tree, `threads` host threads each
+// calling search_in_the_box on its own slice of the boxes at the same time,
+// every list compared with the reference's; then the single-box latency of
+// one thread alone and the box rate of all threads.
+static int run_threads(unsigned n, unsigned q, unsigned threads, float hw) {
+  std::mt19937 gen(7);
+  std::uniform_real_distribution<float> u(0.f, 1.f);
+  std::vector<FKDPoint<float, 3>> pts(n), lo(q), hi(q);
+  for (unsigned i = 0; i < n; ++i) {
+    for (unsigned c = 0; c < 3; ++c) pts[i].setDimension(c, u(gen));
+    pts[i].setId(i);
+  }
+  for (unsigned j = 0; j < q; ++j)
+    for (unsigned c = 0; c < 3; ++c) {
+      lo[j].setDimension(c, pts[j % n][c] - hw);
+      hi[j].setDimension(c, pts[j % n][c] + hw);
+    }
+  FKDTree_CPU<float, 3> cpu(pts);
+  cpu.build();
+  std::unique_ptr<FKDTree<float, 3>> gpu(new FKDTree_CUDA<float, 3>(pts));
+  gpu->build();
+  std::vector<std::vector<unsigned>> got(q);
+  std::atomic<int> failures(0);
+  auto t0 = std::chrono::steady_clock::now();
+  std::vector<std::thread> pool;
+  for (unsigned t = 0; t < threads; ++t)
+    pool.emplace_back([&, t]() {
+      try {
+        for (unsigned j = t; j < q; j += threads) got[j] = gpu->search_in_the_box(lo[j], hi[j]);
+      } catch (const std::exception& e) {
+        std::printf("thread %u: %s\n", t, e.what());
+        failures++;
+      }
+    });
+  for (auto& th : pool) th.join();
+  auto t1 = std::chrono::steady_clock::now();
+  if (failures) return 1;
+  for (unsigned j = 0; j < q; ++j)
+    if (got[j] != cpu.search_in_the_box(lo[j], hi[j])) {
+      std::printf("threads: box %u differs\n", j);
+      return 1;
+    }
+  const unsigned q1 = std::min(q, 2000u);
+  auto t2 = std::chrono::steady_clock::now();
+  for (unsigned j = 0; j < q1; ++j)
+    if (gpu->search_in_the_box(lo[j], hi[j]).size() != got[j].size()) return 1;
+  auto t3 = std::chrono::steady_clock::now();
+  const double mt = std::chrono::duration<double>(t1 - t0).count();
+  const double st = std::chrono::duration<double>(t3 - t2).count();
+  std::printf("threads %u: %u boxes identical to FKDTree_CPU\n", threads, q);
+  std::printf("LATENCY {\"single_box_us\": %.2f, \"threads\": %u, \"boxes_per_s_threaded\": %.1f, \"n\": %u}\n",
+              1e6 * st / q1, threads, q / mt, n);
+  return 0;
+}
+
 int main() {
   int rc = 0;
   rc |= run<3>(50000, 1, 0.02f);
   rc |= run<4>(30000, 2, 0.05f);
   rc |= run<2>(7777, 3, 0.01f);
+  rc |= run_threads(100000, 20000, 8, 0.01f);
   if (rc == 0) std::printf("DROPIN OK\n");
   return rc;
 }

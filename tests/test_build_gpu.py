@@ -136,3 +136,24 @@ def test_subtree_kernels_agree(cuda, subtree, dim, kind):
     got = t.tables()
     t.close()
     assert_same(got, O.build(c, ids), f"subtree={subtree} dim={dim} {kind}")
+
+
+@pytest.mark.parametrize("q", [1 << 21, 1 << 18, 1 << 15, 1 << 13, 1 << 11])
+@pytest.mark.parametrize("dim", [2, 3, 4])
+def test_build_pivot_ties_resolved_by_id(cuda, q, dim):
+    """Coordinates on a grid of q steps: the points sharing a level's pivot
+    value number from one to a few hundred, so some segments take the
+    partition's tie resolution (up to 32 tied points, ordered by id) and
+    others the id digit passes; both must give the reference's tables, with
+    the tie resolution on and off."""
+    rng = np.random.default_rng(q + dim)
+    n = 300_000
+    c = (np.floor(rng.random((dim, n)) * q) / q).astype(np.float32)
+    ids = (rng.permutation(n).astype(np.uint64) * 2654435761 % (1 << 32)).astype(np.uint32)
+    want = O.build(c, ids)
+    for tf in (1, 0):
+        t = F.FKDTree(c, ids)
+        t.set_param("tie_fix", tf)
+        t.build()
+        assert_same(t.tables(), want, f"q={q} dim={dim} tie_fix={tf}")
+        t.close()

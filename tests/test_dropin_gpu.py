@@ -15,5 +15,8 @@ pytestmark = pytest.mark.gpu
 
 @pytest.mark.skipif(not BIN.exists(), reason="drop-in test binary not built (needs the reference headers)")
 def test_cpp_dropin_matches_reference_cpu_tree(cuda):
+    """Includes main.cpp's threaded pattern: 8 std::threads searching one
+    built tree at once, every list equal to FKDTree_CPU's."""
     r = subprocess.run([str(BIN)], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0 and "DROPIN OK" in r.stdout, r.stdout + r.stderr
+    assert "threads 8: 20000 boxes identical" in r.stdout

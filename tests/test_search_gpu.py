@@ -183,3 +183,41 @@ def test_search_record_paths(cuda, record, pool):
     offs, got = t.search_boxes(ev.mins, ev.maxs, ordered=True)
     cl, ol, il, _ = O.search(tab, tid, ev.mins, ev.maxs, variant=O.BRUTE)
     assert np.array_equal(offs, ol) and np.array_equal(got, il)
+
+
+@pytest.mark.parametrize("dim", [1, 2, 3, 4])
+@pytest.mark.parametrize("n", [5, 40, 700, 60_001])
+def test_leaf_buckets_equal_walk(cuda, dim, n):
+    """The bottom subtrees scanned in in-order layout ("search_bucket" 1..6)
+    give exactly the walk's results (bucket 0): counts, ordered lists,
+    unordered sets, digests, recorded and traversing write passes."""
+    rng = np.random.default_rng(100 + dim + n)
+    c = rng.random((dim, n), dtype=np.float32)
+    c[-1] = np.round(c[-1] * 16) / 16  # ties on the last coordinate
+    ids = rng.permutation(n).astype(np.uint32) * 3 + 1
+    q = 1500
+    ctr = c[:, rng.integers(0, n, q)]
+    hw = rng.uniform(0.0, 0.15, (dim, q)).astype(np.float32)
+    mins, maxs = (ctr - hw).astype(np.float32), (ctr + hw).astype(np.float32)
+    t = F.FKDTree(c, ids).build()
+    tab, tid = t.tables()
+    wc, wo, wids, _ = O.search(tab, tid, mins, maxs, variant=O.RECURSIVE)
+    wd = O.digest_of(wids, wo)
+    for b in (0, 1, 3, 4, 6):
+        t.set_param("search_bucket", b)
+        assert np.array_equal(t.count_boxes(mins, maxs), wc), f"bucket {b}: counts"
+        offs, got = t.search_boxes(mins, maxs, ordered=False)
+        assert np.array_equal(offs, wo) and np.array_equal(O.digest_of(got, offs), wd), f"bucket {b}: unordered"
+        offs, got = t.search_boxes(mins, maxs, ordered=True)
+        assert np.array_equal(offs, wo)
+        for j in range(q):
+            a = got[int(offs[j]):int(offs[j + 1])]
+            assert np.array_equal(np.sort(a), np.sort(wids[int(wo[j]):int(wo[j + 1])])), f"bucket {b} box {j}"
+        cc, dd = t.digest_boxes(mins, maxs)
+        assert np.array_equal(cc, wc) and np.array_equal(dd, wd), f"bucket {b}: digests"
+        # the traversing write pass alone (fkd_search_write)
+        t.set_param("search_record", 0)
+        offs, got = t.search_boxes(mins, maxs, ordered=False)
+        assert np.array_equal(O.digest_of(got, offs), wd), f"bucket {b}: traversing write"
+        t.set_param("search_record", 1)
+    t.close()
