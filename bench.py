@@ -269,6 +269,9 @@ def _events_run(wb, mlp, dev, steps, plain_single, cpu_sample=0):
     b.build(coords, ids)
     b.search_digest(mins, maxs)
     out["kernels_per_batched_run"] = int(L.fkd_kernel_launches() - launches0)
+    b.learn_stats(reset=True)
+    b.build(coords, ids)
+    plain_passes = b.learn_stats(reset=True)["passes"]
     out["autotune"] = {"hist_ctas": tune["hist_ctas"], "search_lanes": tune["search_lanes"],
                        "search_big_n": tune["search_big_n"], "search_lanes_big": tune["search_lanes_big"],
                        "build_s": tune["build_s"], "search_s": tune["search_s"], "split_s": tune["split_s"]}
@@ -284,12 +287,18 @@ def _events_run(wb, mlp, dev, steps, plain_single, cpu_sample=0):
     out["learned_graph_ms"] = 1e3 * learned_s
     out["learned_build_ms"] = 1e3 * _timed(lambda: b.build(coords, ids), steps)
     b.learn_stats(reset=True)
+    b.build(coords, ids)
+    learned_passes = b.learn_stats(reset=True)["passes"]
     b.set_mlp(None)
     runs = steps + 1
     hit = st["verified"] / st["brackets"] if st["brackets"] else 0.0
     out["learned"] = {"delta": delta, "brackets_per_run": st["brackets"] // runs, "hit_rate": hit,
                       "fallback_rate": 1.0 - hit if st["brackets"] else 0.0,
-                      "fallbacks_per_run": st["fallbacks"] // runs}
+                      "fallbacks_per_run": st["fallbacks"] // runs,
+                      "digit_passes_per_build_plain": plain_passes,
+                      "digit_passes_per_build_learned": learned_passes,
+                      "digit_passes_saved_per_build": plain_passes - learned_passes,
+                      "speedup_build": out["batched_build_ms"] / out["learned_build_ms"]}
     exact = {"learned_tables_equal_plain_batched": bool(torch.equal(tab0.view(torch.int32), tab1.view(torch.int32))
                                                         and torch.equal(tid0, tid1)),
              "learned_counts_digests_equal_plain_batched": bool(torch.equal(lc, bc) and torch.equal(ld, bd))}

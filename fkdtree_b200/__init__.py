@@ -320,7 +320,7 @@ class FKDTree:
     def learn_stats(self, reset: bool = False) -> dict:
         st = np.zeros(4, dtype=np.uint64)
         check(self._lib.fkd_learn_stats(self._h, _ptr(st), int(reset)))
-        return dict(brackets=int(st[0]), verified=int(st[1]), fallbacks=int(st[2]), bits=int(st[3]))
+        return dict(brackets=int(st[0]), verified=int(st[1]), fallbacks=int(st[2]), passes=int(st[3]))
 
     def close(self) -> None:
         if getattr(self, "_h", None):
@@ -406,7 +406,7 @@ class Batch:
     def learn_stats(self, reset: bool = False) -> dict:
         st = np.zeros(4, dtype=np.uint64)
         check(self._lib.fkd_batch_learn_stats(self._h, _ptr(st), int(reset)))
-        return dict(brackets=int(st[0]), verified=int(st[1]), fallbacks=int(st[2]), bits=int(st[3]))
+        return dict(brackets=int(st[0]), verified=int(st[1]), fallbacks=int(st[2]), passes=int(st[3]))
 
     def record(self, coords, ids, cap: int | None = None):
         """Exact build that records (features, target) of every globally split

@@ -113,7 +113,7 @@ struct Part {
   uint64_t npts = 0, nq = 0;
   uint32_t maxn = 0;  // largest event (sizes the search stack)
   PlanDev plan;
-  Buf io, chunks, work0, work1, nodes, ids, sel, ghist, lfeat, lyhat, lrange, sdig, bnd, tiebuf;
+  Buf io, chunks, work0, work1, nodes, ids, sel, ghist, lfeat, lyhat, lrange, sdig, bnd, tiebuf, ipts, dids;
   uint32_t nchunks = 0;
   std::vector<uint32_t> ev_n;  // points of every (local) event
   // digest search split by event size (knob search_big_n): [0] smaller events, [1] the others
@@ -143,7 +143,9 @@ struct fkd_batch_s {
   uint32_t search_lanes_big = 0;  // lanes per box for events of at least search_big_n points (0: search_lanes)
   uint32_t search_big_n = 0;      // 0: one launch for every event
   int subtree = 0;
-  bool tie_fix = true;  // ties on a pivot value resolved in the partition
+  bool small_fix = true;  // selects stop at SMALL_CAP candidates, the partition orders them
+  bool lin_pass = true;   // a segment's first digit pass bins its value range linearly
+  uint32_t search_bucket = 4;  // leaf-bucket height of the warp-per-box digest search (0: walk every level)
   // learned split
   fkd_mlp mlp = nullptr;
   float mlp_delta = 0.f;
@@ -218,7 +220,7 @@ fkd_status batch_plan(fkd_batch b) {
     BCUDA(p.ids.ensure(p.npts * 4));
     BCUDA(p.sel.ensure(sizeof(SegSel) * (size_t)p.plan.maxseg));
     BCUDA(p.bnd.ensure(2 * sizeof(uint2) * (size_t)p.plan.maxseg));
-    BCUDA(p.tiebuf.ensure((size_t)p.plan.maxseg * TIE_CAP * (p.dim + 1) * 4));
+    BCUDA(p.tiebuf.ensure((size_t)p.plan.maxseg * SMALL_CAP * (p.dim + 1) * 4));
     BCUDA(p.ghist.ensure((size_t)p.plan.maxseg * HIST_BINS * 4));
     BCUDA(p.sdig.ensure(p.npts * sizeof(unsigned long long)));
     BCUDA(p.lfeat.ensure((size_t)p.plan.maxseg * FKD_MLP_FEATURES * 4));
@@ -271,10 +273,12 @@ fkd_status enqueue_build(fkd_batch b, const float* coords, const uint32_t* ids) 
     bc.pending = b->passflags.as<uint32_t>();
     bc.bnd = p.bnd.as<uint2>();
     bc.bnd_stride = p.plan.maxseg;
-    bc.tiebuf = b->tie_fix ? p.tiebuf.as<uint32_t>() : nullptr;
+    bc.tiebuf = b->small_fix ? p.tiebuf.as<uint32_t>() : nullptr;
+    bc.lin = b->lin_pass;
     bc.subtree = b->subtree;
     bc.stream = b->stream;
     memset(&bc.learn, 0, sizeof bc.learn);
+    bc.learn.stats = b->lstats.as<unsigned long long>();  // [3] counts the digit passes
     if (b->mlp || b->rec_x) {
       bc.learn.feat = p.lfeat.as<float>();
       bc.learn.yhat = p.lyhat.as<float>();
@@ -332,6 +336,16 @@ fkd_status enqueue_digest(fkd_batch b, const float* mins, const float* maxs, uin
     if (p.nq == 0) continue;
     Table tab{p.nodes.as<uint4>(), p.ids.as<uint32_t>(), p.sdig.as<unsigned long long>()};
     BCUDA(launch_subtree_digests(p.plan.evs, p.plan.nev, p.maxn, tab, b->stream));
+    // leaf buckets: only the warp-per-box search scans them
+    const bool full_warp = b->search_lanes == 0 || b->search_lanes == 32 ||
+                           (b->search_big_n && (b->search_lanes_big == 0 || b->search_lanes_big == 32));
+    if (b->search_bucket && full_warp) {
+      BCUDA(p.ipts.ensure(p.npts * sizeof(uint4)));
+      if (p.dim > 3) BCUDA(p.dids.ensure(p.npts * sizeof(uint32_t)));
+      tab.ipts = p.ipts.as<uint4>();
+      tab.dids = p.dim > 3 ? p.dids.as<uint32_t>() : nullptr;
+      BCUDA(launch_inorder_events(p.plan.evs, p.plan.nev, p.maxn, tab, b->stream));
+    }
     SearchCtx sc;
     memset(&sc, 0, sizeof sc);
     sc.g = make_geom(p.maxn);  // per-box geometry comes from the event; this sizes the stack
@@ -345,6 +359,7 @@ fkd_status enqueue_digest(fkd_batch b, const float* mins, const float* maxs, uin
     sc.err = b->err.as<uint32_t>();
     sc.capacity = ~0ull;
     sc.lanes = b->search_lanes;
+    sc.bucket = tab.ipts ? b->search_bucket : 0u;
     sc.stream = b->stream;
     if (b->search_big_n == 0) {
       BCUDA(launch_search(sc, p.dim, SEARCH_DIGEST));
@@ -463,9 +478,21 @@ fkd_status fkd_batch_set_param(fkd_batch b, const char* name, int64_t value) {
     drop_graph();
     return FKD_OK;
   }
-  if (strcmp(name, "tie_fix") == 0) {
-    if (value != 0 && value != 1) return capi_fail(FKD_ERR_ARG, "tie_fix must be 0 or 1");
-    b->tie_fix = value != 0;
+  if (strcmp(name, "small_fix") == 0) {
+    if (value != 0 && value != 1) return capi_fail(FKD_ERR_ARG, "small_fix must be 0 or 1");
+    b->small_fix = value != 0;
+    drop_graph();
+    return FKD_OK;
+  }
+  if (strcmp(name, "lin_pass") == 0) {
+    if (value != 0 && value != 1) return capi_fail(FKD_ERR_ARG, "lin_pass must be 0 or 1");
+    b->lin_pass = value != 0;
+    drop_graph();
+    return FKD_OK;
+  }
+  if (strcmp(name, "search_bucket") == 0) {
+    if (value < 0 || value > (int64_t)BUCKET_MAX) return capi_fail(FKD_ERR_ARG, "search_bucket must be 0..6");
+    b->search_bucket = (uint32_t)value;
     drop_graph();
     return FKD_OK;
   }

@@ -61,7 +61,10 @@ static_assert(PTILE == (int)PART_TILE, "partition tile");
 constexpr int GWARPS = GT / 32;
 constexpr int RBITS = 11;          // widest digit of the global select (11, 11, 10 per 32-bit word)
 constexpr int RBINS = 1 << RBITS;
-constexpr int RPASSES = 7;         // 11,11,10 | 11,11,10 bits, plus a verifying pass of a predicted block
+// digit passes a level may need: a linear value pass, the value bits the
+// bin left open (at most three 11-bit digits), the id bits (three), plus a
+// verifying pass of a predicted block that missed
+constexpr int RPASSES = 8;
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
   uint32_t m;
@@ -79,9 +82,64 @@ __device__ __forceinline__ void write_node(const Table& tab, uint32_t h, const u
   tab.ids[h] = rec[dim];
 }
 
+// The float whose order bits (mono_bits) are m (+0.0 for the folded zero).
+__device__ __forceinline__ float from_mono(uint32_t m) {
+  return __uint_as_float((m & 0x80000000u) ? (m & 0x7fffffffu) : ~m);
+}
+
+// Bin of value v in the linear binning of [vmin, vmin + 2048 / scale]: every
+// operation rounded on its own (no contraction), so every kernel that bins v
+// gets the same bin; non-decreasing in v, since each step is.
+__device__ __forceinline__ uint32_t lin_bin(float v, float vmin, float scale) {
+  const float x = __fmul_rn(__fsub_rn(v, vmin), scale);
+  return x >= 2047.f ? 2047u : (x > 0.f ? (uint32_t)x : 0u);
+}
+
+// Sets up the linear binning of the value keys [vlo, vhi]; false when their
+// float range is empty or not finite (the passes then bin key bits).
+__device__ __forceinline__ bool lin_setup(uint32_t vlo, uint32_t vhi, float& vmin, float& scale) {
+  if (vlo >= vhi) return false;
+  const float a = from_mono(vlo), b = from_mono(vhi);
+  const float w = __fsub_rn(b, a);
+  if (!(w > 0.f) || !isfinite(w) || !isfinite(a)) return false;
+  const float sc = __fdiv_rn(2048.f, w);
+  if (!(sc > 0.f) || !isfinite(sc)) return false;
+  vmin = a;
+  scale = sc;
+  return true;
+}
+
+// Level 0 has no parent partition to report its segments' value range: one
+// pass over the split coordinate (the first dimension) reduces each
+// segment's min / max order bits into bnd, as (~min, max) from a zeroed array.
+template <int DIM>
+__global__ void __launch_bounds__(GT) k_bounds0(const EvDesc* __restrict__ evs, const uint2* __restrict__ segs,
+                                                const uint2* __restrict__ tiles, CSoA src, uint2* __restrict__ bnd) {
+  const uint2 tl = tiles[blockIdx.x];
+  const uint32_t s = tl.x, t = tl.y;
+  const uint2 sd = segs[s];
+  const Geom eg = evs[sd.x].g;
+  const uint32_t len = seg_len(eg, 0u, sd.y);
+  const uint32_t start = evs[sd.x].base + seg_start(eg, 0u, sd.y);
+  const uint32_t t0 = start + t * PTILE, t1 = min(start + len, t0 + (uint32_t)PTILE);
+  uint32_t nmn = 0u, mx = 0u;  // ~min, max
+  for (uint32_t e = t0 + threadIdx.x; e < t1; e += GT) {
+    const uint32_t m = mono_bits(__ldcs(src.base + e));
+    nmn = max(nmn, ~m);
+    mx = max(mx, m);
+  }
+  nmn = __reduce_max_sync(0xffffffffu, nmn);
+  mx = __reduce_max_sync(0xffffffffu, mx);
+  if ((threadIdx.x & 31u) == 0u && t0 < t1) {
+    atomicMax(&bnd[s].x, nmn);
+    atomicMax(&bnd[s].y, mx);
+  }
+}
+
 __global__ void k_sel_init(uint32_t d, const EvDesc* __restrict__ evs, const uint2* __restrict__ segs, uint32_t nseg,
                            SegSel* __restrict__ sel, uint32_t* __restrict__ pending, const uint2* __restrict__ bnd_in,
-                           uint2* __restrict__ bnd_out, const uint32_t* __restrict__ child) {
+                           bool bnd_inverted_min, uint2* __restrict__ bnd_out, const uint32_t* __restrict__ child,
+                           bool lin) {
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s == 0) {
     // pending[p] != 0: digit pass p has a segment to work on
@@ -95,11 +153,16 @@ __global__ void k_sel_init(uint32_t d, const EvDesc* __restrict__ evs, const uin
   SegSel st;
   st.prefix = 0ull;
   st.bits = 0u;
+  uint32_t vlo = 0u, vhi = 0xffffffffu;
   if (bnd_in) {
-    // every key of the segment shares the common prefix of its smallest and
-    // largest split coordinate: the select starts below it
-    const uint2 b = bnd_in[s];
+    // every key of the segment lies between its smallest and largest split
+    // coordinate: the select starts from that interval (and, in prefix form,
+    // below their common prefix)
+    uint2 b = bnd_in[s];
+    if (bnd_inverted_min) b.x = ~b.x;
     if (b.x <= b.y) {
+      vlo = b.x;
+      vhi = b.y;
       const uint32_t cp = b.x == b.y ? 32u : (uint32_t)__clz(b.x ^ b.y);
       st.bits = cp;
       st.prefix = cp == 0u ? 0ull : (unsigned long long)(b.x >> (32u - cp));
@@ -115,7 +178,16 @@ __global__ void k_sel_init(uint32_t d, const EvDesc* __restrict__ evs, const uin
   st.verify = 0u;
   st.below = 0u;
   st.kfull = st.krem;
-  st.tie = 0u;
+  st.small = 0u;
+  st.klo = st.klo0 = (unsigned long long)vlo << 32;
+  st.khi = st.khi0 = ((unsigned long long)vhi << 32) | 0xffffffffull;
+  st.vmin = st.vmin0 = 0.f;
+  st.scale = st.scale0 = 0.f;
+  st.lin = st.lin0 = (lin && lin_setup(vlo, vhi, st.vmin0, st.scale0)) ? 1u : 0u;
+  st.vmin = st.vmin0;
+  st.scale = st.scale0;
+  st.cmin = 0xffffffffu;
+  st.cmax = 0u;
   sel[s] = st;
   if (bnd_out && child[s] != ~0u) {
     bnd_out[child[s]] = make_uint2(0xffffffffu, 0u);
@@ -124,16 +196,21 @@ __global__ void k_sel_init(uint32_t d, const EvDesc* __restrict__ evs, const uin
 }
 
 // One digit pass of the segmented select for every segment of depth d.  CTA
-// (s, t) counts the digits of tile t of segment s -- tiles are `ts` records
-// long, so that a level is covered by about four CTAs per SM whatever its
-// segment count -- into HCOPIES interleaved shared histograms (lane %
-// HCOPIES picks the copy, so lanes of clustered data do not all hit one
-// counter), then adds them to the segment's global histogram once.  The last
-// CTA of a segment picks the digit holding the pivot rank.
+// (s, t) counts the digits of the candidates of tile t of segment s -- tiles
+// are `ts` records long, so that a level is covered by about four CTAs per SM
+// whatever its segment count -- into HCOPIES interleaved shared histograms
+// (lane % HCOPIES picks the copy, so lanes of clustered data do not all hit
+// one counter), then adds them to the segment's global histogram once.  The
+// last CTA of a segment picks the bin holding the pivot rank and narrows the
+// interval to it.  Bins: linear in the float value (the segment's first pass,
+// `lin`), else the top 11 bits of (value - vlo) while the value is open, else
+// of (id - ilo) among the points holding the value.
 constexpr int HCOPIES = 4;
 #ifndef FKD_HIST_MINB
 #define FKD_HIST_MINB 4
 #endif
+
+__device__ __forceinline__ uint32_t bitlen32(uint32_t x) { return x ? 32u - (uint32_t)__clz(x) : 0u; }
 
 template <int DIM>
 __global__ void __launch_bounds__(GT, FKD_HIST_MINB) k_hist(uint32_t d, const EvDesc* __restrict__ evs,
@@ -141,7 +218,7 @@ __global__ void __launch_bounds__(GT, FKD_HIST_MINB) k_hist(uint32_t d, const Ev
                                                 uint32_t ts, CSoA src, SegSel* __restrict__ sel,
                                                 uint32_t* __restrict__ ghist, const uint32_t* __restrict__ pending_now,
                                                 uint32_t* __restrict__ pending_next, uint32_t* __restrict__ err,
-                                                unsigned long long* __restrict__ lstats, uint32_t ties) {
+                                                unsigned long long* __restrict__ lstats, uint32_t small_ok) {
   __shared__ uint32_t hist[HCOPIES * RBINS];
   __shared__ uint32_t wsum[GWARPS];
   __shared__ uint32_t s_last;
@@ -158,15 +235,17 @@ __global__ void __launch_bounds__(GT, FKD_HIST_MINB) k_hist(uint32_t d, const Ev
   const uint32_t ntiles = (len + ts - 1) / ts;
   if (t >= ntiles) return;
   if (sel[s].done) return;
-  const uint32_t bits = sel[s].bits;
-  const unsigned long long prefix = sel[s].prefix;
-  // digits never straddle the value/id boundary: at most 11 bits, up to the
-  // end of the current 32-bit word (11, 11, 10 from a word start)
-  const uint32_t inword = bits & 31u;
-  const uint32_t w = (32u - inword) < 11u ? (32u - inword) : 11u;
-  const bool verify = sel[s].verify != 0u;  // prefix is a predicted block (value bits only)
-  const uint32_t nb = 1u << w;
-  const bool need_id = bits >= 32u;
+  const unsigned long long klo = sel[s].klo, khi = sel[s].khi;
+  const bool lin = sel[s].lin != 0u;
+  const float vmin = sel[s].vmin, scale = sel[s].scale;
+  const bool verify = sel[s].verify != 0u;  // [klo, khi] is a predicted block of values
+  const uint32_t vlo = (uint32_t)(klo >> 32), vhi = (uint32_t)(khi >> 32);
+  const bool vphase = vlo != vhi;  // the value is still open
+  const uint32_t ilo = (uint32_t)klo, ihi = (uint32_t)khi;
+  const uint32_t span = vphase ? vhi - vlo : ihi - ilo;
+  const uint32_t bl = bitlen32(span);
+  const uint32_t shift = bl > (uint32_t)RBITS ? bl - (uint32_t)RBITS : 0u;
+  const uint32_t nb = lin ? (uint32_t)RBINS : (span >> shift) + 1u;
   const uint32_t c = d % DIM;
   const uint32_t start = ebase + seg_start(eg, d, sd.y);
   const uint32_t tend = min(start + len, start + t * ts + ts);
@@ -174,26 +253,31 @@ __global__ void __launch_bounds__(GT, FKD_HIST_MINB) k_hist(uint32_t d, const Ev
   for (uint32_t i = threadIdx.x; i < HCOPIES * RBINS; i += GT) hist[i] = 0u;
   __syncthreads();
   const uint32_t* X = src.base + (uint64_t)c * src.stride;
-  const uint32_t vpre = (uint32_t)(prefix >> (bits > 32u ? bits - 32u : 0u));  // value part of the prefix
-  const uint32_t vbits = bits < 32u ? bits : 32u;
   uint32_t nbelow = 0u;  // verify pass: points below the predicted block
-  // one value of the tile: the next digit of the points matching the prefix
+  uint32_t cmn = 0xffffffffu, cmx = 0u;  // smallest / largest candidate value key (id in the id phase)
+  // one value of the tile: the bin of a candidate
   auto count = [&](uint32_t raw, uint32_t e) {
     const uint32_t mv = mono_bits(raw);
-    if (verify && vbits != 0u && (mv >> (32u - vbits)) < vpre) ++nbelow;
-    // value bits first; the id is read only by points whose value matches
-    if (vbits == 0u || (mv >> (32u - vbits)) == vpre) {
-      uint32_t dig;
-      if (!need_id) {
-        dig = (mv >> (32u - bits - w)) & (nb - 1u);
-      } else {
-        const uint32_t id = __ldcs(src.ids + e);
-        const uint32_t ib = bits - 32u;  // id bits already fixed
-        if (ib != 0u && (id >> (32u - ib)) != (uint32_t)(prefix & ((1ull << ib) - 1u))) return;
-        dig = (id >> (32u - ib - w)) & (nb - 1u);
-      }
-      atomicAdd(&myhist[dig], 1u);
+    if (verify && mv < vlo) ++nbelow;
+    if (mv < vlo || mv > vhi) return;
+    uint32_t dig;
+    if (lin) {
+      dig = lin_bin(__uint_as_float(raw), vmin, scale);
+      cmn = min(cmn, mv);
+      cmx = max(cmx, mv);
+    } else if (vphase) {
+      dig = (mv - vlo) >> shift;
+      cmn = min(cmn, mv);
+      cmx = max(cmx, mv);
+    } else {
+      // the value is fixed: the id of the points holding it
+      const uint32_t id = __ldcs(src.ids + e);
+      if (id < ilo || id > ihi) return;
+      dig = (id - ilo) >> shift;
+      cmn = min(cmn, id);
+      cmx = max(cmx, id);
     }
+    atomicAdd(&myhist[dig], 1u);
   };
   // the tile [tb, tend): a scalar head up to a 16-byte boundary, 16-byte
   // loads (two per thread in flight), a scalar tail
@@ -231,6 +315,12 @@ __global__ void __launch_bounds__(GT, FKD_HIST_MINB) k_hist(uint32_t d, const Ev
     for (int o = 16; o > 0; o >>= 1) nbelow += __shfl_xor_sync(0xffffffffu, nbelow, o);
     if (lane == 0 && nbelow) atomicAdd(&sel[s].below, nbelow);
   }
+  cmn = __reduce_min_sync(0xffffffffu, cmn);
+  cmx = __reduce_max_sync(0xffffffffu, cmx);
+  if (lane == 0 && cmn <= cmx) {
+    atomicMin(&sel[s].cmin, cmn);
+    atomicMax(&sel[s].cmax, cmx);
+  }
   __syncthreads();
   uint32_t* gh = ghist + (uint64_t)s * RBINS;
   for (uint32_t i = threadIdx.x; i < nb; i += GT) {
@@ -245,7 +335,8 @@ __global__ void __launch_bounds__(GT, FKD_HIST_MINB) k_hist(uint32_t d, const Ev
   __syncthreads();
   if (!s_last) return;
   __threadfence();
-  // Last CTA of segment s: locate the digit holding rank krem.
+  if (threadIdx.x == 0 && lstats) atomicAdd(&lstats[3], 1ull);  // segment digit passes run
+  // Last CTA of segment s: locate the bin holding rank krem.
   uint32_t krem = *(volatile uint32_t*)&sel[s].krem;
   constexpr int BPT = RBINS / GT;  // bins per thread
   uint32_t h[BPT];
@@ -276,18 +367,20 @@ __global__ void __launch_bounds__(GT, FKD_HIST_MINB) k_hist(uint32_t d, const Ev
       krem -= below;
       if (threadIdx.x == 0) {
         sel[s].verify = 0u;
-        if (lstats) {
-          atomicAdd(&lstats[1], 1ull);
-          atomicAdd(&lstats[3], (unsigned long long)bits);  // key bits the prediction resolved
-        }
+        if (lstats) atomicAdd(&lstats[1], 1ull);
       }
     } else {
-      // miss: restart this segment as the plain radix select
+      // miss: restart this segment from its own interval
       for (uint32_t b = threadIdx.x; b < nb; b += GT) gh[b] = 0u;
       if (threadIdx.x == 0) {
         SegSel* p = &sel[s];
-        p->prefix = p->prefix0;
-        p->bits = p->bits0;
+        p->cmin = 0xffffffffu;
+        p->cmax = 0u;
+        p->klo = p->klo0;
+        p->khi = p->khi0;
+        p->lin = p->lin0;
+        p->vmin = p->vmin0;
+        p->scale = p->scale0;
         p->krem = p->kfull;
         p->cnt = len;
         p->verify = 0u;
@@ -298,23 +391,68 @@ __global__ void __launch_bounds__(GT, FKD_HIST_MINB) k_hist(uint32_t d, const Ev
       return;
     }
   }
+  // every candidate lies in [cmin, cmax]: the chosen bin is clipped to it
+  const uint32_t cmin = *(volatile uint32_t*)&sel[s].cmin, cmax = *(volatile uint32_t*)&sel[s].cmax;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    sel[s].cmin = 0xffffffffu;
+    sel[s].cmax = 0u;
+  }
   uint32_t cum = wbase + incl - mine;
 #pragma unroll
   for (int k = 0; k < BPT; ++k) {
     const uint32_t b = threadIdx.x * BPT + k;
     if (b < nb && krem >= cum && krem < cum + h[k]) {
+      unsigned long long nlo, nhi;
+      if (lin) {
+        // the values of bin b form an interval (lin_bin is monotone): find
+        // its ends among the order bits [vlo, vhi] by bisection
+        uint32_t a0 = vlo, a1 = vhi;  // first key with bin >= b
+        while (a0 < a1) {
+          const uint32_t m = a0 + ((a1 - a0) >> 1);
+          if (lin_bin(from_mono(m), vmin, scale) >= b) a1 = m; else a0 = m + 1u;
+        }
+        uint32_t z0 = a0, z1 = vhi;  // last key with bin <= b
+        while (z0 < z1) {
+          const uint32_t m = z0 + (uint32_t)(((unsigned long long)(z1 - z0) + 1ull) >> 1);
+          if (lin_bin(from_mono(m), vmin, scale) <= b) z0 = m; else z1 = m - 1u;
+        }
+        nlo = (unsigned long long)a0 << 32;
+        nhi = ((unsigned long long)z0 << 32) | 0xffffffffull;
+      } else if (vphase) {
+        const unsigned long long a = (unsigned long long)vlo + ((unsigned long long)b << shift);
+        unsigned long long z = a + ((1ull << shift) - 1ull);
+        if (z > vhi) z = vhi;
+        nlo = a << 32;
+        nhi = (z << 32) | 0xffffffffull;
+      } else {
+        const unsigned long long a = (unsigned long long)ilo + ((unsigned long long)b << shift);
+        unsigned long long z = a + ((1ull << shift) - 1ull);
+        if (z > ihi) z = ihi;
+        nlo = ((unsigned long long)vlo << 32) | a;
+        nhi = ((unsigned long long)vlo << 32) | z;
+      }
+      if (cmin <= cmax) {
+        if (lin || vphase) {
+          nlo = max(nlo, (unsigned long long)cmin << 32);
+          nhi = min(nhi, ((unsigned long long)cmax << 32) | 0xffffffffull);
+        } else {
+          nlo = max(nlo, ((unsigned long long)vlo << 32) | cmin);
+          nhi = min(nhi, ((unsigned long long)vlo << 32) | cmax);
+        }
+      }
       SegSel* p = &sel[s];
-      const uint32_t nbits = bits + w;
-      p->prefix = (prefix << w) | (unsigned long long)b;
-      p->bits = nbits;
+      p->klo = nlo;
+      p->khi = nhi;
+      p->lin = 0u;
       p->krem = krem - cum;
       p->cnt = h[k];
-      p->done = (h[k] == 1u || nbits == 64u) ? 1u : 0u;
-      if (!p->done && ties && nbits == 32u && h[k] <= TIE_CAP) {
-        // the pivot value is known and only a few points carry it: the
-        // partition orders them by id (k_tie_fix) instead of id digit passes
+      p->done = (h[k] == 1u || nlo == nhi) ? 1u : 0u;
+      if (!p->done && small_ok && h[k] <= SMALL_CAP) {
+        // few candidates left: the partition parks them and k_small_fix
+        // orders them by key (no further digit passes)
         p->done = 1u;
-        p->tie = 1u;
+        p->small = 1u;
       }
       if (!p->done) *pending_next = 1u;
     }
@@ -322,8 +460,8 @@ __global__ void __launch_bounds__(GT, FKD_HIST_MINB) k_hist(uint32_t d, const Ev
   }
   for (uint32_t b = threadIdx.x; b < nb; b += GT) gh[b] = 0u;
   if (threadIdx.x == 0) sel[s].tiles_done = 0u;
-  // the last thread's inclusive sum is the number of matching records; it
-  // must cover krem, otherwise the select state is inconsistent.
+  // the last thread's inclusive sum is the number of candidates; it must
+  // cover krem, otherwise the select state is inconsistent.
   if (threadIdx.x == GT - 1 && krem >= total) atomicOr(err, ERRB_INTERNAL);
 }
 
@@ -366,10 +504,10 @@ __global__ void __launch_bounds__(GT, FKD_PART_MINB) k_partition(uint32_t d, con
   const uint32_t node = ebase + (1u << d) - 1u + sd.y;  // this segment's node
   const uint32_t t0 = start + t * PTILE;
   const uint32_t t1 = min(start + len, t0 + (uint32_t)PTILE);
-  const uint32_t bits = sel[s].bits;
-  const unsigned long long prefix = sel[s].prefix;
+  const unsigned long long klo = sel[s].klo, khi = sel[s].khi;
   const uint32_t cnt = sel[s].cnt;
-  const bool tie = sel[s].tie != 0u;
+  const bool small = sel[s].small != 0u;
+  if (threadIdx.x == 0 && !sel[s].done) atomicOr(err, ERRB_INTERNAL);  // the select ran out of passes
   const uint32_t c = d % DIM;
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
 
@@ -395,12 +533,7 @@ __global__ void __launch_bounds__(GT, FKD_PART_MINB) k_partition(uint32_t d, con
         for (int w = 0; w < DIM; ++w) nan |= is_nan_bits(rec[k][w]);
       }
       const uint64_t key = order_key(pick_coord<DIM>(rec[k], c), rec[k][DIM]);
-      if (bits == 0u) {
-        cls = 1u;
-      } else {
-        const uint64_t top = bits >= 64u ? key : (key >> (64u - bits));
-        cls = top < prefix ? 0u : (top > prefix ? 2u : 1u);
-      }
+      cls = key < klo ? 0u : (key > khi ? 2u : 1u);
     }
     if (cls == 1u) eqmask |= 1u << k;
     bl[k] = __ballot_sync(0xffffffffu, cls == 0u);
@@ -463,11 +596,11 @@ __global__ void __launch_bounds__(GT, FKD_PART_MINB) k_partition(uint32_t d, con
     } else if ((br[k] >> lane) & 1u) {
       pos = baseR + sR[k * GWARPS + warp] + __popc(br[k] & lt);
       lim = endR;
-    } else if (((eqmask >> k) & 1u) && tie) {
-      // ties on the pivot value: parked for k_tie_fix, which orders them by id
+    } else if (((eqmask >> k) & 1u) && small) {
+      // the select left a few candidates: parked for k_small_fix, which orders them by key
       const uint32_t slot = atomicAdd(&sel[s].curE, 1u);
-      if (slot < TIE_CAP && tiebuf) {
-        uint32_t* tb = tiebuf + ((size_t)s * TIE_CAP + slot) * (DIM + 1);
+      if (slot < SMALL_CAP && tiebuf) {
+        uint32_t* tb = tiebuf + ((size_t)s * SMALL_CAP + slot) * (DIM + 1);
 #pragma unroll
         for (int w = 0; w <= DIM; ++w) tb[w] = rec[k][w];
       } else {
@@ -539,24 +672,23 @@ __global__ void __launch_bounds__(GT, FKD_PART_MINB) k_partition(uint32_t d, con
   }
 }
 
-// Segments whose pivot value is carried by 2..TIE_CAP points (SegSel::tie):
-// the partition parked those records; one warp per segment orders them by id
-// -- the reference comparator's tie-break (FKDTree_cpu.h:248-251) -- writes
-// the one of rank krem to the table and the others to the ends of the
-// children's intervals the partition left free: the krem smaller ones to the
-// last krem slots of the left interval, the larger ones to the last slots of
-// the right interval.  It also widens the children's split-coordinate bounds.
+// Segments whose select left 2..SMALL_CAP candidates (SegSel::small): the
+// partition parked them; one warp per segment orders them by their order key
+// (coordinate, then id: the reference comparator, FKDTree_cpu.h:246-252),
+// writes the one of rank krem to the table and the others to the ends of the
+// children's intervals the partition left free -- the krem smaller ones to
+// the last krem slots of the left interval, the larger ones to the last
+// slots of the right interval -- and widens the children's coordinate bounds.
 template <int DIM>
-__global__ void k_tie_fix(uint32_t d, const EvDesc* __restrict__ evs, const uint2* __restrict__ segs, uint32_t nseg,
-                          const SegSel* __restrict__ sel, const uint32_t* __restrict__ tiebuf, SoA dst, Table tab,
-                          uint32_t* __restrict__ err, uint2* __restrict__ bnd_out, const uint32_t* __restrict__ child) {
+__global__ void k_small_fix(uint32_t d, const EvDesc* __restrict__ evs, const uint2* __restrict__ segs, uint32_t nseg,
+                            const SegSel* __restrict__ sel, const uint32_t* __restrict__ tiebuf, SoA dst, Table tab,
+                            uint32_t* __restrict__ err, uint2* __restrict__ bnd_out, const uint32_t* __restrict__ child) {
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t s = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (s >= nseg) return;
-  const SegSel st = sel[s];
-  if (!st.tie) return;
-  const uint32_t m = st.cnt;
-  if (m > TIE_CAP || st.curE != m) {
+  if (!sel[s].small) return;
+  const uint32_t m = sel[s].cnt;
+  if (m > SMALL_CAP || sel[s].curE != m) {
     if (lane == 0) atomicOr(err, ERRB_INTERNAL);
     return;
   }
@@ -568,18 +700,19 @@ __global__ void k_tie_fix(uint32_t d, const EvDesc* __restrict__ evs, const uint
   const uint32_t rank = seg_rank(eg, d, sd.y);
   const uint32_t node = ebase + (1u << d) - 1u + sd.y;
   const uint32_t endL = start + rank, endR = start + len;
+  const uint32_t c = d % DIM;
   uint32_t rec[DIM + 1];
   const bool have = lane < m;
 #pragma unroll
-  for (int w = 0; w <= DIM; ++w) rec[w] = have ? tiebuf[((size_t)s * TIE_CAP + lane) * (DIM + 1) + w] : 0u;
-  // rank by id (lane order breaks repeated ids, which the reference leaves undefined)
-  const uint32_t myid = rec[DIM];
+  for (int w = 0; w <= DIM; ++w) rec[w] = have ? tiebuf[((size_t)s * SMALL_CAP + lane) * (DIM + 1) + w] : 0u;
+  // rank by key (lane order breaks repeated keys, which the reference leaves undefined)
+  const unsigned long long mykey = order_key(pick_coord<DIM>(rec, c), rec[DIM]);
   uint32_t r = 0u;
   for (uint32_t o = 0; o < m; ++o) {
-    const uint32_t oid = __shfl_sync(0xffffffffu, myid, o);
-    r += (oid < myid || (oid == myid && o < lane)) ? 1u : 0u;
+    const unsigned long long ok = __shfl_sync(0xffffffffu, mykey, o);
+    r += (ok < mykey || (ok == mykey && o < lane)) ? 1u : 0u;
   }
-  const uint32_t krem = st.krem;
+  const uint32_t krem = sel[s].krem;
   const uint32_t cnext = (d + 1u) % DIM;
   const uint32_t ch = bnd_out ? child[s] : ~0u;
   uint32_t pos = 0xffffffffu, lim = 0u;
@@ -719,6 +852,10 @@ __global__ void __launch_bounds__(SELT) k_select_small(uint32_t d, const EvDesc*
     SegSel* p = &sel[s];
     p->prefix = s_prefix;
     p->bits = s_bits;
+    // the prefix as the key interval the partition classifies by
+    const uint32_t b = s_bits;
+    p->klo = b == 0u ? 0ull : (b >= 64u ? s_prefix : s_prefix << (64u - b));
+    p->khi = b == 0u ? ~0ull : (b >= 64u ? s_prefix : (s_prefix << (64u - b)) | (~0ull >> b));
     p->krem = s_krem;
     p->cnt = s_cnt;
     p->done = 1u;
@@ -1166,16 +1303,25 @@ static cudaError_t run_build(BuildCtx& bc) {
   for (uint32_t d = 0; d < bc.nlevels; ++d) {
     const LevelPlan& lp = bc.levels[d];
     if (lp.nseg == 0) continue;
-    // per-segment bounds: written by level d - 1's partition into bnd[d & 1],
-    // by level d's partition into bnd[(d + 1) & 1]
-    const uint2* bnd_in = (bc.bnd && d > 0) ? bc.bnd + (size_t)(d & 1u) * bc.bnd_stride : nullptr;
-    uint2* bnd_out = bc.bnd ? bc.bnd + (size_t)((d + 1u) & 1u) * bc.bnd_stride : nullptr;
-    k_sel_init<<<(lp.nseg + 255) / 256, 256, 0, bc.stream>>>(d, bc.evs, lp.segs, lp.nseg, bc.sel, bc.pending, bnd_in,
-                                                            bnd_out, lp.child);
-    count_launches(1);
-    const LearnCtx& lc = bc.learn;
     // levels of small segments: one CTA selects a whole segment (no learned bracket there)
     const bool small = lp.maxlen <= (uint32_t)SEL_MAX && bc.small_select;
+    // per-segment bounds: written by level d - 1's partition into bnd[d & 1],
+    // by level d's partition into bnd[(d + 1) & 1]; level 0's by k_bounds0
+    const uint2* bnd_in = (bc.bnd && d > 0) ? bc.bnd + (size_t)(d & 1u) * bc.bnd_stride : nullptr;
+    uint2* bnd_out = bc.bnd ? bc.bnd + (size_t)((d + 1u) & 1u) * bc.bnd_stride : nullptr;
+    bool inv = false;
+    if (d == 0 && bc.bnd && bc.lin && !small) {
+      cudaError_t e = cudaMemsetAsync(bc.bnd, 0, sizeof(uint2) * lp.nseg, bc.stream);
+      if (e != cudaSuccess) return e;
+      k_bounds0<DIM><<<lp.nptile, GT, 0, bc.stream>>>(bc.evs, lp.segs, lp.ptiles, src, bc.bnd);
+      count_launches(1);
+      bnd_in = bc.bnd;
+      inv = true;
+    }
+    k_sel_init<<<(lp.nseg + 255) / 256, 256, 0, bc.stream>>>(d, bc.evs, lp.segs, lp.nseg, bc.sel, bc.pending, bnd_in,
+                                                            inv, bnd_out, lp.child, bc.lin && !small);
+    count_launches(1);
+    const LearnCtx& lc = bc.learn;
     if (lc.rec_x || (lc.params && !small)) {
       cudaError_t e = launch_features(d, bc.evs, lp.segs, lp.nseg, src, DIM, lc.feat, lc.range, bc.stream);
       if (e != cudaSuccess) return e;
@@ -1196,8 +1342,8 @@ static cudaError_t run_build(BuildCtx& bc) {
     const int passes = small ? 0 : (lc.params ? RPASSES : RPASSES - 1);
     for (int pass = 0; pass < passes; ++pass) {
       k_hist<DIM><<<lp.nhtile, GT, 0, bc.stream>>>(d, bc.evs, lp.segs, lp.htiles, lp.hts, src, bc.sel, bc.ghist,
-                                                    bc.pending + pass, bc.pending + pass + 1, bc.err,
-                                                    lc.params ? lc.stats : nullptr, bc.tiebuf ? 1u : 0u);
+                                                    bc.pending + pass, bc.pending + pass + 1, bc.err, lc.stats,
+                                                    bc.tiebuf ? 1u : 0u);
       count_launches(1);
     }
     SoA dst = bufs[nb];
@@ -1205,8 +1351,8 @@ static cudaError_t run_build(BuildCtx& bc) {
                                                         bc.err, bnd_out, lp.child, bc.tiebuf);
     count_launches(1);
     if (bc.tiebuf && !small) {
-      k_tie_fix<DIM><<<(lp.nseg + 7) / 8, 256, 0, bc.stream>>>(d, bc.evs, lp.segs, lp.nseg, bc.sel, bc.tiebuf, dst,
-                                                              bc.tab, bc.err, bnd_out, lp.child);
+      k_small_fix<DIM><<<(lp.nseg + 7) / 8, 256, 0, bc.stream>>>(d, bc.evs, lp.segs, lp.nseg, bc.sel, bc.tiebuf, dst,
+                                                                bc.tab, bc.err, bnd_out, lp.child);
       count_launches(1);
     }
     if (lc.rec_x) {

@@ -128,7 +128,8 @@ struct fkd_tree_s {
   fkd_mlp mlp = nullptr;     // learned split (null: plain radix select)
   float mlp_delta = 0.f;
   DevBuf lfeat, lyhat, lrange, lstats, sdig, dids, dnode, ipts, bnd, tiebuf;
-  bool tie_fix = true;          // ties on a pivot value resolved in the partition ("tie_fix")
+  bool small_fix = true;        // selects stop at SMALL_CAP candidates, the partition orders them ("small_fix")
+  bool lin_pass = true;         // a segment's first digit pass bins its value range linearly ("lin_pass")
   uint32_t search_bucket = 4;   // leaf-bucket height of the searches ("search_bucket"; 0: walk every level)
   bool search_record = true;    // fkd_search records runs in the count pass ("search_record")
   uint64_t search_pool = 0;     // fixed pool entries ("search_pool"; 0: sized by demand)
@@ -456,6 +457,8 @@ fkd_status fkd_create(int dim, uint32_t flags, void* stream, fkd_tree* out) {
   if (e == cudaSuccess) e = h->err.ensure(sizeof(uint32_t) * 4);
   if (e == cudaSuccess) e = h->qctr.ensure(sizeof(uint32_t) * 4);
   if (e == cudaSuccess) e = h->passflags.ensure(sizeof(uint32_t) * 64);
+  if (e == cudaSuccess) e = h->lstats.ensure(4 * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->lstats.p, 0, 4 * sizeof(unsigned long long), h->stream);
   if (e == cudaSuccess) e = cudaMallocHost((void**)&h->herr, sizeof(uint32_t) * 16);
   for (cudaEvent_t* ev : {&h->built_ev, &h->inorder_ev, &h->sdig_ev})
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
@@ -541,7 +544,7 @@ fkd_status build_impl(fkd_tree h, const float* coords, const uint32_t* ids, cons
     FKD_CUDA(h->work0.ensure(rec_bytes));
     FKD_CUDA(h->sel.ensure(sizeof(SegSel) * (size_t)h->plan.maxseg));
     FKD_CUDA(h->bnd.ensure(2 * sizeof(uint2) * (size_t)h->plan.maxseg));
-    if (h->tie_fix) FKD_CUDA(h->tiebuf.ensure((size_t)h->plan.maxseg * TIE_CAP * (dim + 1) * sizeof(uint32_t)));
+    if (h->small_fix) FKD_CUDA(h->tiebuf.ensure((size_t)h->plan.maxseg * SMALL_CAP * (dim + 1) * sizeof(uint32_t)));
     const size_t gw = (size_t)h->plan.maxseg * HIST_BINS;
     FKD_CUDA(h->ghist.ensure(gw * sizeof(uint32_t)));
     FKD_CUDA(cudaMemsetAsync(h->ghist.p, 0, gw * sizeof(uint32_t), h->stream));
@@ -583,12 +586,14 @@ fkd_status build_impl(fkd_tree h, const float* coords, const uint32_t* ids, cons
   bc.err = h->err.as<uint32_t>();
   bc.pending = h->passflags.as<uint32_t>();
   bc.bnd = h->plan.levels.empty() ? nullptr : h->bnd.as<uint2>();
-  bc.tiebuf = (h->tie_fix && !h->plan.levels.empty()) ? h->tiebuf.as<uint32_t>() : nullptr;
+  bc.tiebuf = (h->small_fix && !h->plan.levels.empty()) ? h->tiebuf.as<uint32_t>() : nullptr;
+  bc.lin = h->lin_pass;
   bc.bnd_stride = h->plan.maxseg;
   bc.subtree = h->subtree;
   bc.small_select = h->small_select;
   bc.stream = h->stream;
   memset(&bc.learn, 0, sizeof bc.learn);
+  bc.learn.stats = h->lstats.as<unsigned long long>();  // [3] counts the digit passes of every build
   if (h->mlp && !h->plan.levels.empty()) {
     const size_t ms = h->plan.maxseg;
     FKD_CUDA(h->lfeat.ensure(ms * FKD_MLP_FEATURES * sizeof(float)));
@@ -1136,9 +1141,14 @@ fkd_status fkd_set_param(fkd_tree h, const char* name, int64_t value) {
     h->subtree = (int)value;
     return FKD_OK;
   }
-  if (strcmp(name, "tie_fix") == 0) {
-    if (value != 0 && value != 1) return fail(FKD_ERR_ARG, "tie_fix must be 0 or 1");
-    h->tie_fix = value != 0;
+  if (strcmp(name, "small_fix") == 0) {
+    if (value != 0 && value != 1) return fail(FKD_ERR_ARG, "small_fix must be 0 or 1");
+    h->small_fix = value != 0;
+    return FKD_OK;
+  }
+  if (strcmp(name, "lin_pass") == 0) {
+    if (value != 0 && value != 1) return fail(FKD_ERR_ARG, "lin_pass must be 0 or 1");
+    h->lin_pass = value != 0;
     return FKD_OK;
   }
   if (strcmp(name, "search_bucket") == 0) {

@@ -104,10 +104,11 @@ cudaError_t launch_features(uint32_t d, const EvDesc* evs, const uint2* segs, ui
 }
 
 // Turns the prediction of each segment into a predicted block of the select:
-// the common prefix of the order keys of [v - r, v + r], r = delta * range.
-// The digit pass that follows counts the points below the block; if the
-// pivot's rank falls inside it the select continues from there, otherwise
-// the segment restarts as the plain radix select (fkd_build.cu, k_hist).
+// the value keys of [v - r, v + r], r = delta * range, within the segment's
+// own interval, binned linearly by the pass that follows.  That pass counts
+// the points below the block; if the pivot's rank falls inside it the select
+// continues from the block's bin, otherwise the segment restarts from its own
+// interval (fkd_build.cu, k_hist).
 __global__ void k_bracket(uint32_t d, const EvDesc* __restrict__ evs, const uint2* __restrict__ segs, uint32_t nseg,
                           const float* __restrict__ yhat, const float2* __restrict__ range, float delta,
                           SegSel* __restrict__ sel, unsigned long long* __restrict__ stats) {
@@ -121,16 +122,25 @@ __global__ void k_bracket(uint32_t d, const EvDesc* __restrict__ evs, const uint
   const float v = rg.x + y * w, r = delta * w;
   const float lo = v - r, hi = v + r;
   if (!isfinite(lo) || !isfinite(hi)) return;
-  const uint32_t lk = mono_bits(__float_as_uint(lo)), hk = mono_bits(__float_as_uint(hi));
-  if (lk > hk) return;
-  const uint32_t cp = lk == hk ? 32u : (uint32_t)__clz(lk ^ hk);
-  if (cp < 4u) return;  // a block wider than 1/16 of the key space saves nothing
   SegSel* p = &sel[s];
-  // the segment's common prefix may already fix as many bits, or exclude the block
-  if (p->bits >= cp) return;
-  if (p->bits != 0u && (lk >> (32u - p->bits)) != (uint32_t)p->prefix) return;
-  p->prefix = (unsigned long long)(lk >> (32u - cp));
-  p->bits = cp;
+  const uint32_t slo = (uint32_t)(p->klo0 >> 32), shi = (uint32_t)(p->khi0 >> 32);
+  uint32_t lk = mono_bits(__float_as_uint(lo)), hk = mono_bits(__float_as_uint(hi));
+  lk = lk < slo ? slo : lk;
+  hk = hk > shi ? shi : hk;
+  if (lk >= hk) return;
+  // a block wider than half the segment's value range saves nothing
+  const float a = __uint_as_float((lk & 0x80000000u) ? (lk & 0x7fffffffu) : ~lk);
+  const float b = __uint_as_float((hk & 0x80000000u) ? (hk & 0x7fffffffu) : ~hk);
+  const float bw = __fsub_rn(b, a);
+  if (!(bw > 0.f) || !isfinite(bw)) return;
+  if (p->lin0 && __fmul_rn(bw, p->scale0) > 1024.f) return;
+  const float sc = __fdiv_rn(2048.f, bw);
+  if (!(sc > 0.f) || !isfinite(sc)) return;
+  p->klo = (unsigned long long)lk << 32;
+  p->khi = ((unsigned long long)hk << 32) | 0xffffffffull;
+  p->lin = 1u;
+  p->vmin = a;
+  p->scale = sc;
   p->verify = 1u;
   p->below = 0u;
   if (stats) atomicAdd(&stats[0], 1ull);

@@ -14,27 +14,45 @@ uint64_t launches_total();
 // cudaMalloc with the allocation-failure injection of fkd_debug_fail_alloc
 cudaError_t device_alloc(void** p, size_t bytes);
 
-// Per-segment state of the global-level radix select (one per node of the
-// level being split).
+// Per-segment state of the global-level select (one per node of the level
+// being split).  The digit passes (k_hist) narrow an interval [klo, khi] of
+// 64-bit order keys (mono(coordinate) << 32 | id) that holds the pivot: the
+// candidates are the segment's points whose key lies in it, krem the pivot's
+// rank among them and cnt their number.  While the interval spans several
+// coordinate values its id part is the full range and a pass bins the value
+// (linearly in the float value for the first pass of a segment whose value
+// range is known, `lin`; else the key bits); once the value is fixed a pass
+// bins the id.  The select is done when one candidate is left, when the
+// interval is one key (repeated keys), or when at most SMALL_CAP candidates
+// are left (`small`): the partition then parks them and k_small_fix orders
+// them by key.  k_select_small and the learned bracket also keep the prefix
+// form (prefix / bits) of the levels they serve.
 struct SegSel {
-  unsigned long long prefix;  // the known top `bits` bits of the pivot key
+  unsigned long long prefix;  // k_select_small: the known top `bits` bits of the pivot key
   uint32_t bits;              // 0..64
-  uint32_t krem;              // rank of the pivot among keys matching prefix
-  uint32_t cnt;               // number of keys matching prefix
-  uint32_t done;              // the pivot key is determined
+  uint32_t krem;              // rank of the pivot among the candidates
+  uint32_t cnt;               // number of candidates
+  uint32_t done;              // the pivot is determined (or `small`)
   uint32_t tiles_done;        // CTAs of the current pass that finished
   uint32_t curL, curR, curE;  // partition cursors
-  uint32_t verify;            // 1: prefix is a predicted block, the next pass verifies it
+  uint32_t verify;            // 1: [klo, khi] is a predicted block, the next pass verifies it
   uint32_t below;             // verify pass: points whose key lies below the block
   uint32_t kfull;             // the pivot rank within the segment (fallback restart)
-  uint32_t bits0;             // the common prefix every key of the segment shares (restart point)
+  uint32_t bits0;             // the common prefix every key of the segment shares
   unsigned long long prefix0;
-  uint32_t tie;               // 1: the pivot value is known and cnt <= TIE_CAP points carry it; the
-                              //    partition parks them and k_tie_fix orders them by id (no id passes)
+  uint32_t small;             // done with cnt <= SMALL_CAP candidates: the partition parks them
+  uint32_t lin;               // the next pass bins the value linearly: bin = floor((v - vmin) * scale)
+  unsigned long long klo, khi;    // the candidate key interval
+  unsigned long long klo0, khi0;  // the segment's own interval (fallback restart)
+  float vmin, scale;              // linear binning of the next pass
+  float vmin0, scale0;            // ... of the segment's own range (restart)
+  uint32_t lin0;
+  uint32_t cmin, cmax;            // the pass's smallest / largest candidate value key (id once the
+                                  // value is fixed): the next interval is clipped to them
 };
-// Points sharing a level's pivot value that the partition resolves by id
-// itself; more ties than this fall back to digit passes over the id bits.
-constexpr uint32_t TIE_CAP = 32;
+// Candidates a select may leave for the partition to order itself (one warp
+// sorts them); more are narrowed by further digit passes.
+constexpr uint32_t SMALL_CAP = 32;
 
 constexpr int FKD_MLP_FEATURES = 40;  // node summary width (== FKD_MLP_IN of the C ABI)
 
@@ -92,8 +110,8 @@ struct BuildCtx {
   SegSel* sel;    // >= max segments of a level
   uint32_t* ghist;
   uint32_t* pending;  // one word per digit pass (+1): does that pass have work
-  uint32_t* tiebuf = nullptr;  // >= max segments * TIE_CAP * (dim + 1) words: records tying on the pivot
-                               // value (null: ties resolved by id digit passes)
+  uint32_t* tiebuf = nullptr;  // >= max segments * SMALL_CAP * (dim + 1) words: the candidates a select
+                               // leaves to the partition (null: every select narrows to one key)
   uint2* bnd = nullptr;    // 2 x bnd_stride: per-segment (min, max) of the split coordinate's
                            // order bits, written by the previous level's partition (null: unused)
   uint32_t bnd_stride = 0; // >= max segments of a level
@@ -104,6 +122,7 @@ struct BuildCtx {
   cudaEvent_t ev_sub = nullptr;  // optional: recorded right before the subtree kernel
   int subtree = 0;               // shared-memory subtree kernel: 0 auto, 1 radix select, 2 presorted lists
   bool small_select = true;      // levels of small segments select with one CTA per segment
+  bool lin = true;               // a segment's first digit pass bins its value range linearly
 };
 
 // Number of levels split by the global kernels (the first level whose
@@ -191,6 +210,8 @@ cudaError_t launch_expand(const SearchCtx& sc);
 // Fills tab.dids / tab.dnode (in-order tables; required by SEARCH_WRITE) and,
 // when tab.ipts is set, the in-order node copy the leaf-bucket scan reads.
 cudaError_t launch_inorder(const Geom& g, Table tab, cudaStream_t stream);
+// The same for every event of a batch: ipts, and dids where tab.dids is set.
+cudaError_t launch_inorder_events(const EvDesc* evs, uint32_t nev, uint32_t max_n, Table tab, cudaStream_t stream);
 // Largest leaf-bucket height the searches accept (subtrees of up to 2^(h+1)-1 points).
 constexpr uint32_t BUCKET_MAX = 6;
 // Fills tab.sdig (subtree digests) for every event; required by SEARCH_DIGEST.

@@ -1156,6 +1156,32 @@ cudaError_t launch_inorder(const Geom& g, Table tab, cudaStream_t stream) {
   return cudaGetLastError();
 }
 
+// In-order tables of every event of a batch (event x in block x, grid.y
+// blocks striding over its points): ipts always, dids where given (dim 4,
+// whose ids do not ride in the node).  Node i of event e sits at
+// ev.base + i; its in-order position at ev.base + p.
+__global__ void k_inorder_events(const EvDesc* __restrict__ evs, const uint32_t* __restrict__ ids,
+                                 const uint4* __restrict__ nodes, uint32_t* __restrict__ dids,
+                                 uint4* __restrict__ ipts) {
+  const EvDesc ev = evs[blockIdx.x];
+  const Geom g = ev.g;
+  for (uint32_t i = blockIdx.y * blockDim.x + threadIdx.x; i < g.n; i += gridDim.y * blockDim.x) {
+    const uint32_t d = floor_log2_u32(i + 1u);
+    const uint32_t t = i + 1u - (1u << d);
+    const uint32_t p = seg_start(g, d, t) + (d < g.H ? seg_rank(g, d, t) : 0u);
+    ipts[ev.base + p] = nodes[ev.base + i];
+    if (dids) dids[ev.base + p] = ids[ev.base + i];
+  }
+}
+
+cudaError_t launch_inorder_events(const EvDesc* evs, uint32_t nev, uint32_t max_n, Table tab, cudaStream_t stream) {
+  if (nev == 0 || max_n == 0) return cudaSuccess;
+  const uint32_t gy = (max_n + 255u) / 256u < 16u ? (max_n + 255u) / 256u : 16u;
+  k_inorder_events<<<dim3(nev, gy), 256, 0, stream>>>(evs, tab.ids, tab.nodes, tab.dids, tab.ipts);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
 // ---------------------------------------------------------- subtree digests
 //
 // sdig[i] = mix64(id_i) + sdig[2i+1] + sdig[2i+2] (mod 2^64), level by level

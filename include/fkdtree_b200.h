@@ -233,9 +233,13 @@ FKD_API fkd_status fkd_sync(fkd_tree h);
  *                   point by point in in-order layout instead of walking them;
  *                   0 walks every level.  Costs 16 bytes per point of device
  *                   memory for the in-order copy of the nodes.
- *   "tie_fix"       (0/1, default 1): when at most 32 points of a segment share
- *                   its pivot value, the partition orders them by id instead of
- *                   two more digit passes over the id bits
+ *   "small_fix"     (0/1, default 1): a global level's select stops once at
+ *                   most 32 candidates are left; the partition parks them and
+ *                   one warp orders them by (coordinate, id), instead of more
+ *                   digit passes
+ *   "lin_pass"      (0/1, default 1): a segment's first digit pass bins its
+ *                   value range (known from its parent's partition) in 2048
+ *                   equal float intervals rather than by the top key bits
  *   "kernel_events" (0/1): record CUDA events around the kernels of every
  *                   fkd_build and fkd_search call for fkd_kernel_times (only
  *                   calls on the handle's stream, from one thread).
@@ -275,7 +279,7 @@ FKD_API fkd_status fkd_batch_destroy(fkd_batch b);
  *                  box in a launch of their own (0: one launch for all)
  *   "subtree"      shared-memory subtree kernel: 0 auto (presorted lists for
  *                  dims 1-3, radix select for dim 4), 1 radix select, 2 lists
- *   "tie_fix"      (0/1, default 1) as fkd_set_param's
+ *   "small_fix", "lin_pass", "search_bucket"  as fkd_set_param's
  * A failed "hist_ctas" re-plan leaves the batch without a plan: builds then
  * return FKD_ERR_STATE until a re-plan succeeds.
  * No reference counterpart (the reference has one fixed launch shape). */
@@ -330,8 +334,10 @@ FKD_API fkd_status fkd_mlp_train(fkd_mlp m, const float* x, const float* t, uint
 FKD_API fkd_status fkd_set_mlp(fkd_tree h, fkd_mlp m, float delta);
 FKD_API fkd_status fkd_batch_set_mlp(fkd_batch b, fkd_mlp m, float delta);
 /* stats[0] brackets predicted, [1] verified (the select started inside the
- * predicted block), [2] fell back to the plain select, [3] key bits resolved
- * by the verified predictions (sum); cumulative until reset. */
+ * predicted block), [2] fell back to the plain select, [3] digit passes run
+ * over a segment by the global levels' selects (with or without a network:
+ * what a verified bracket saves shows as fewer passes); cumulative until
+ * reset. */
 FKD_API fkd_status fkd_learn_stats(fkd_tree h, uint64_t* stats, int reset);
 FKD_API fkd_status fkd_batch_learn_stats(fkd_batch b, uint64_t* stats, int reset);
 /* Exact (plain) build of a batch that also records, for every node the

@@ -153,7 +153,7 @@ def test_build_pivot_ties_resolved_by_id(cuda, q, dim):
     want = O.build(c, ids)
     for tf in (1, 0):
         t = F.FKDTree(c, ids)
-        t.set_param("tie_fix", tf)
+        t.set_param("small_fix", tf)
         t.build()
-        assert_same(t.tables(), want, f"q={q} dim={dim} tie_fix={tf}")
+        assert_same(t.tables(), want, f"q={q} dim={dim} small_fix={tf}")
         t.close()
