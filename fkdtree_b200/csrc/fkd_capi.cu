@@ -371,6 +371,7 @@ fkd_status count_pass(fkd_tree h, const Lease& L, const Boxes& b, uint32_t* dcou
     sc.brec_cap = rec->brec_cap;
     sc.flags = rec->flags;
     sc.flag_ctr = rec->flag_ctr;
+    sc.rec_ids = rec->rec_ids;
   }
   FKD_CUDA(launch_search(sc, h->dim, SEARCH_COUNT));
   return FKD_OK;
@@ -722,6 +723,7 @@ fkd_status write_pass(fkd_tree h, const Lease& L, const Boxes& b, const uint64_t
     x.brec = rec->brec;
     x.brec_ctr = rec->brec_ctr;
     x.brec_cap = rec->brec_cap;
+    x.rec_ids = rec->rec_ids;
     FKD_CUDA(launch_expand(x));
     sc.order = rec->flags;
     sc.boxes.q = nflag;
@@ -845,6 +847,7 @@ fkd_status fkd_search(fkd_tree h, const float* mins, const float* maxs, uint64_t
       rec.brec_cap = sl->brec.bytes / (2 * sizeof(uint4));
       rec.flags = sl->rflags.as<uint32_t>();
       rec.flag_ctr = (uint32_t*)(ctr + 3);
+      rec.rec_ids = ordered ? 0 : 1;  // unordered: singles carry their ids, the write pass copies them
     }
   }
   if (q && (s = count_pass(h, L, b, sl->counts.as<uint32_t>(), order, rec_on ? &rec : nullptr)) != FKD_OK) return s;

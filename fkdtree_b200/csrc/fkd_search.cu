@@ -440,7 +440,7 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
             jst[warp][jp] = pos;
             jlen[warp][jp] = rl;
           }
-          if (single) jpre[warp][nsing + __popc(bs & lt)] = pos;
+          if (single) jpre[warp][nsing + __popc(bs & lt)] = sc.rec_ids ? (DIM <= 3 ? pt.w : __ldg(tab.dids + pos)) : pos;
           njobs += __popc(br);
           nsing += __popc(bs);
         }
@@ -529,7 +529,7 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
           if (DIM > 3) in &= (x3 <= hi[3] && x3 >= lo[3]);
           emit = in;
         }
-        if (emit && MODE != SEARCH_COUNT) idv = DIM <= 3 ? nd.w : __ldg(tab.ids + i);
+        if (emit && (MODE != SEARCH_COUNT || (record && sc.rec_ids))) idv = DIM <= 3 ? nd.w : __ldg(tab.ids + i);
         const uint32_t l = 2u * i + 1u;
         const bool visitL = !lower && l < n;
         const bool visitR = (lower || inter) && l + 1u < n;
@@ -609,7 +609,7 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
             jst[warp][jp] = s2;
             jlen[warp][jp] = l2;
           }
-          if (single) jpre[warp][nsing + __popc(bs & lt)] = sg;
+          if (single) jpre[warp][nsing + __popc(bs & lt)] = sc.rec_ids ? idv : sg;
           njobs += __popc(b1) + __popc(b2);
           nsing += __popc(bs);
           if (njobs > (uint32_t)(JN - 64) || nsing > (uint32_t)(JN - 32)) {
@@ -762,7 +762,7 @@ __global__ void __launch_bounds__(XT) k_expand(const uint4* __restrict__ brec,
                                                const uint32_t* __restrict__ pool_len,
                                                const uint64_t* __restrict__ offsets,
                                                const uint32_t* __restrict__ srct, uint32_t* __restrict__ out,
-                                               uint64_t capacity, uint32_t* __restrict__ err) {
+                                               uint64_t capacity, uint32_t* __restrict__ err, int singles_ids) {
   __shared__ uint32_t st[XT / 32][JOBS];
   __shared__ uint32_t pre[XT / 32][JOBS];
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
@@ -783,10 +783,12 @@ __global__ void __launch_bounds__(XT) k_expand(const uint4* __restrict__ brec,
         const uint32_t e = e0 + 32u * u + lane;
         v[u] = e < ns ? __ldg(pool_s + R.z + e) : 0u;
       }
+      if (!singles_ids) {
 #pragma unroll
-      for (int u = 0; u < EXU; ++u) {
-        const uint32_t e = e0 + 32u * u + lane;
-        if (e < ns) v[u] = __ldg(srct + v[u]);
+        for (int u = 0; u < EXU; ++u) {
+          const uint32_t e = e0 + 32u * u + lane;
+          if (e < ns) v[u] = __ldg(srct + v[u]);
+        }
       }
 #pragma unroll
       for (int u = 0; u < EXU; ++u) {
@@ -840,7 +842,7 @@ cudaError_t launch_expand(const SearchCtx& sc) {
   k_expand<<<(unsigned)(sms * per), XT, 0, sc.stream>>>(sc.brec, sc.brec_ctr, sc.brec_cap, sc.pool_s, sc.pool_st,
                                                         sc.pool_len,
                                                         sc.offsets, sc.heap_out ? sc.tab.dnode : sc.tab.dids, sc.out,
-                                                        sc.capacity, sc.err);
+                                                        sc.capacity, sc.err, sc.rec_ids);
   count_launches(1);
   return cudaGetLastError();
 }
