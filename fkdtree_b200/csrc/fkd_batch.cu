@@ -143,6 +143,7 @@ struct fkd_batch_s {
   uint32_t search_lanes_big = 0;  // lanes per box for events of at least search_big_n points (0: search_lanes)
   uint32_t search_big_n = 0;      // 0: one launch for every event
   int subtree = 0;
+  int subtree_size = 0;   // presorted subtree size (0: 1,024)
   bool small_fix = true;  // selects stop at SMALL_CAP candidates, the partition orders them
   bool lin_pass = true;   // a segment's first digit pass bins its value range linearly
   uint32_t search_bucket = 4;  // leaf-bucket height of the warp-per-box digest search (0: walk every level)
@@ -195,7 +196,7 @@ fkd_status batch_plan(fkd_batch b) {
     p.npts = base;
     p.ev_n = n_ev;
     PlanHost ph;
-    plan_build(n_ev.data(), base_ev.data(), (uint32_t)n_ev.size(), p.dim, hist_ctas, ph);
+    plan_build(n_ev.data(), base_ev.data(), (uint32_t)n_ev.size(), p.dim, hist_ctas, ph, b->subtree_size);
     for (uint32_t le = 0; le < p.events.size(); ++le) {
       const uint32_t e = p.events[le];
       EvDesc& d = ph.evs[le];
@@ -276,6 +277,7 @@ fkd_status enqueue_build(fkd_batch b, const float* coords, const uint32_t* ids) 
     bc.tiebuf = b->small_fix ? p.tiebuf.as<uint32_t>() : nullptr;
     bc.lin = b->lin_pass;
     bc.subtree = b->subtree;
+    bc.subn = b->subtree_size;
     bc.stream = b->stream;
     memset(&bc.learn, 0, sizeof bc.learn);
     bc.learn.stats = b->lstats.as<unsigned long long>();  // [3] counts the digit passes
@@ -477,6 +479,13 @@ fkd_status fkd_batch_set_param(fkd_batch b, const char* name, int64_t value) {
     b->subtree = (int)value;
     drop_graph();
     return FKD_OK;
+  }
+  if (strcmp(name, "subtree_size") == 0) {
+    if (value != 0 && value != 512 && value != 1024)
+      return capi_fail(FKD_ERR_ARG, "subtree_size must be 0, 512 or 1024");
+    b->subtree_size = (int)value;
+    drop_graph();
+    return batch_plan(b);
   }
   if (strcmp(name, "small_fix") == 0) {
     if (value != 0 && value != 1) return capi_fail(FKD_ERR_ARG, "small_fix must be 0 or 1");

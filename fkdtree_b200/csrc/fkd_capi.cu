@@ -123,6 +123,7 @@ struct fkd_tree_s {
   uint32_t hist_ctas = 0;    // digit-pass CTAs per level (0: four per SM)
   uint32_t search_lanes = 0; // count / digest lanes per box (0: one warp)
   int subtree = 0;           // subtree kernel: 0 auto, 1 radix select, 2 presorted lists
+  int subtree_size = 0;      // presorted subtree size: 0 (1,024), 512 or 1,024 ("subtree_size")
   bool small_select = true;  // one CTA per segment on levels of small segments
   bool box_order = true;     // search boxes in the spatial order of their centres
   fkd_mlp mlp = nullptr;     // learned split (null: plain radix select)
@@ -531,7 +532,7 @@ fkd_status build_impl(fkd_tree h, const float* coords, const uint32_t* ids, cons
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
     PlanHost ph;
     const uint32_t n32 = (uint32_t)n, base0 = 0u;
-    plan_build(&n32, &base0, 1, dim, h->hist_ctas ? h->hist_ctas : 4u * (uint32_t)sms, ph);
+    plan_build(&n32, &base0, 1, dim, h->hist_ctas ? h->hist_ctas : 4u * (uint32_t)sms, ph, h->subtree_size);
     // a failed upload leaves no plan: the next build must plan again
     h->plan_n = ~0ull;
     FKD_CUDA(h->plan.upload(ph, h->stream));
@@ -591,6 +592,7 @@ fkd_status build_impl(fkd_tree h, const float* coords, const uint32_t* ids, cons
   bc.lin = h->lin_pass;
   bc.bnd_stride = h->plan.maxseg;
   bc.subtree = h->subtree;
+  bc.subn = h->subtree_size;
   bc.small_select = h->small_select;
   bc.stream = h->stream;
   memset(&bc.learn, 0, sizeof bc.learn);
@@ -1142,6 +1144,12 @@ fkd_status fkd_set_param(fkd_tree h, const char* name, int64_t value) {
   if (strcmp(name, "subtree") == 0) {
     if (value < 0 || value > 2) return fail(FKD_ERR_ARG, "subtree must be 0, 1 or 2");
     h->subtree = (int)value;
+    return FKD_OK;
+  }
+  if (strcmp(name, "subtree_size") == 0) {
+    if (value != 0 && value != 512 && value != 1024) return fail(FKD_ERR_ARG, "subtree_size must be 0, 512 or 1024");
+    h->subtree_size = (int)value;
+    h->plan_n = ~0ull;  // re-plan at the next build
     return FKD_OK;
   }
   if (strcmp(name, "small_fix") == 0) {

@@ -15,7 +15,7 @@
 namespace fkd {
 
 void plan_build(const uint32_t* n_ev, const uint32_t* base_ev, uint32_t nev, int dim, uint32_t hist_ctas,
-                PlanHost& out) {
+                PlanHost& out, int subn) {
   out.evs.assign(nev, EvDesc{});
   out.levels.clear();
   out.subs.clear();
@@ -25,7 +25,7 @@ void plan_build(const uint32_t* n_ev, const uint32_t* base_ev, uint32_t nev, int
     EvDesc& d = out.evs[e];
     d.g = make_geom(n_ev[e]);
     d.base = base_ev[e];
-    d.d0 = build_global_levels(n_ev[e], dim);
+    d.d0 = build_global_levels(n_ev[e], dim, subn);
     if (n_ev[e] && d.d0 > maxd0) maxd0 = d.d0;
   }
   out.levels.resize(maxd0);

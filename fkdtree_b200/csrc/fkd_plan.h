@@ -44,6 +44,6 @@ struct PlanDev {
 // base_ev[e] of the concatenated arrays; hist_ctas is the number of
 // digit-pass CTAs to aim for per level.
 void plan_build(const uint32_t* n_ev, const uint32_t* base_ev, uint32_t nev, int dim, uint32_t hist_ctas,
-                PlanHost& out);
+                PlanHost& out, int subn = 0);
 
 }  // namespace fkd

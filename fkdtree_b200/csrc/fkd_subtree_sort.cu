@@ -45,18 +45,14 @@ extern "C" __attribute__((visibility("default"))) void fkd_prof_sorted_reset() {
 
 namespace {
 
-#ifndef FKD_SORTED_SUBN
-#define FKD_SORTED_SUBN 1024
-#endif
-constexpr int XN = FKD_SORTED_SUBN;  // slots: the largest subtree (a power of two, 512..4096)
-constexpr int XPPT = 4;              // slots per thread
-constexpr int XST = XN / XPPT;       // threads
-constexpr int XW = XST / 32;         // warps
-static_assert(XN >= 512 && XN <= 4096 && (XN & (XN - 1)) == 0, "sorted subtree size");
+// XN, a template parameter below: the slots of a CTA, the largest subtree it
+// takes (512 or 1,024: a power of two, 512..4096); XN / XPPT threads
+constexpr int XPPT = 4;  // slots per thread
+constexpr int XN_DEFAULT = 1024;
 constexpr uint16_t GAP = 0xffffu;  // a slot outside every segment (a pivot of an earlier level)
 constexpr uint8_t SL = 0, SR = 1, SP = 2;
 
-template <int DIM>
+template <int DIM, int XN>
 struct XCfg {
   // recs | eofr | lists (DIM x 2 buffers) | seg (2 buffers) | side | scratch (sort keys, later scans)
   static constexpr size_t recs = (size_t)(DIM + 1) * XN * 4;
@@ -74,7 +70,9 @@ __device__ __forceinline__ unsigned long long umax64(unsigned long long a, unsig
 // Sorts XN 64-bit keys (ascending) with the whole CTA: bitonic sort of 128
 // keys per warp in registers, then five merge-path rounds through shared
 // memory.  Returns the buffer (a or b) that holds the result.
+template <int XN>
 __device__ unsigned long long* cta_sort(unsigned long long* a, unsigned long long* b) {
+  static_assert(XN >= 512 && XN <= 4096 && (XN & (XN - 1)) == 0, "sorted subtree size");
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   unsigned long long v[4];
   unsigned long long* wbase = a + warp * 128u;
@@ -153,7 +151,9 @@ __device__ unsigned long long* cta_sort(unsigned long long* a, unsigned long lon
 
 // Exclusive scan of XN uint2 values, slots XPPT*tid .. XPPT*tid + XPPT - 1
 // per thread (in: per-slot values; out: written to sc).  Returns the totals.
+template <int XN>
 __device__ uint2 cta_scan2(const uint2 (&val)[XPPT], uint2* sc, uint2* wtot) {
+  constexpr int XW = XN / XPPT / 32;  // warps
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   uint32_t ax = 0u, ay = 0u;
 #pragma unroll
@@ -219,11 +219,12 @@ __device__ __forceinline__ void seg_local(const Geom& g, uint32_t d, uint32_t t,
 
 }  // namespace
 
-template <int DIM>
-__global__ void __launch_bounds__(XST, 4096 / XN) k_subtree_sorted(const EvDesc* __restrict__ evs,
+template <int DIM, int XN>
+__global__ void __launch_bounds__(XN / XPPT, 4096 / XN) k_subtree_sorted(const EvDesc* __restrict__ evs,
                                                            const uint2* __restrict__ subs, CSoA src_in, CSoA src_b0,
                                                            CSoA src_b1, Table tab_all, uint32_t* __restrict__ err) {
-  using Cfg = XCfg<DIM>;
+  constexpr int XST = XN / XPPT;  // threads
+  using Cfg = XCfg<DIM, XN>;
   extern __shared__ __align__(16) unsigned char smem[];
   uint32_t* recs = (uint32_t*)smem;                                 // [DIM + 1][XN], original slot order
   uint16_t* eofr = (uint16_t*)(smem + Cfg::recs);                   // id rank -> slot
@@ -269,7 +270,7 @@ __global__ void __launch_bounds__(XST, 4096 / XN) k_subtree_sorted(const EvDesc*
   __syncthreads();
   XPROF_T(tp0);
   {
-    const unsigned long long* sk = cta_sort(keys, keys + XN);
+    const unsigned long long* sk = cta_sort<XN>(keys, keys + XN);
     for (uint32_t r = threadIdx.x; r < nloc; r += XST) eofr[r] = (uint16_t)(sk[r] & 0xfffu);
     __syncthreads();
   }
@@ -280,7 +281,7 @@ __global__ void __launch_bounds__(XST, 4096 / XN) k_subtree_sorted(const EvDesc*
     for (uint32_t r = threadIdx.x; r < (uint32_t)XN; r += XST)
       keys[r] = r < nloc ? (((unsigned long long)mono_bits(recs[c * XN + eofr[r]]) << 12) | r) : ~0ull;
     __syncthreads();
-    const unsigned long long* sk = cta_sort(keys, keys + XN);
+    const unsigned long long* sk = cta_sort<XN>(keys, keys + XN);
     uint16_t* lc = lists + (size_t)c * 2 * XN;
     for (uint32_t p = threadIdx.x; p < nloc; p += XST) lc[p] = (uint16_t)(sk[p] & 0xfffu);
     __syncthreads();
@@ -360,7 +361,7 @@ __global__ void __launch_bounds__(XST, 4096 / XN) k_subtree_sorted(const EvDesc*
       val[q].x = (s1 == SL ? 1u : 0u) | (s1 == SR ? 0x10000u : 0u);
       val[q].y = (s2 == SL ? 1u : 0u) | (s2 == SR ? 0x10000u : 0u);
     }
-    cta_scan2(val, scan, wtot);
+    cta_scan2<XN>(val, scan, wtot);
     __syncthreads();
     // (c) scatter into the other buffers
     uint16_t* n1 = lists + ((size_t)o1 * 2 + (cur[o1] ^ 1)) * XN;
@@ -409,26 +410,34 @@ __global__ void __launch_bounds__(XST, 4096 / XN) k_subtree_sorted(const EvDesc*
   XPROF_ADD(2, tp2, tp3);
 }
 
-int sorted_sub_capacity() { return XN; }
+int sorted_sub_capacity(int subn) { return subn == 512 ? 512 : XN_DEFAULT; }
 
-template <int DIM>
+template <int DIM, int XN>
 static cudaError_t run_sorted(const EvDesc* evs, const uint2* subs, uint32_t nsub, CSoA in, CSoA b0, CSoA b1,
                               Table tab, uint32_t* err, cudaStream_t stream) {
-  const size_t smem = XCfg<DIM>::smem;
-  cudaError_t e = cudaFuncSetAttribute(k_subtree_sorted<DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const size_t smem = XCfg<DIM, XN>::smem;
+  cudaError_t e =
+      cudaFuncSetAttribute(k_subtree_sorted<DIM, XN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  k_subtree_sorted<DIM><<<nsub, XST, smem, stream>>>(evs, subs, in, b0, b1, tab, err);
+  k_subtree_sorted<DIM, XN><<<nsub, XN / XPPT, smem, stream>>>(evs, subs, in, b0, b1, tab, err);
   count_launches(1);
   return cudaGetLastError();
 }
 
+template <int DIM>
+static cudaError_t run_sorted_n(int subn, const EvDesc* evs, const uint2* subs, uint32_t nsub, CSoA in, CSoA b0,
+                                CSoA b1, Table tab, uint32_t* err, cudaStream_t stream) {
+  if (sorted_sub_capacity(subn) == 512) return run_sorted<DIM, 512>(evs, subs, nsub, in, b0, b1, tab, err, stream);
+  return run_sorted<DIM, XN_DEFAULT>(evs, subs, nsub, in, b0, b1, tab, err, stream);
+}
+
 cudaError_t launch_subtree_sorted(const EvDesc* evs, const uint2* subs, uint32_t nsub, CSoA in, CSoA b0, CSoA b1,
-                                  Table tab, uint32_t* err, int dim, cudaStream_t stream) {
+                                  Table tab, uint32_t* err, int dim, int subn, cudaStream_t stream) {
   if (nsub == 0) return cudaSuccess;
   switch (dim) {
-    case 1: return run_sorted<1>(evs, subs, nsub, in, b0, b1, tab, err, stream);
-    case 2: return run_sorted<2>(evs, subs, nsub, in, b0, b1, tab, err, stream);
-    case 3: return run_sorted<3>(evs, subs, nsub, in, b0, b1, tab, err, stream);
+    case 1: return run_sorted_n<1>(subn, evs, subs, nsub, in, b0, b1, tab, err, stream);
+    case 2: return run_sorted_n<2>(subn, evs, subs, nsub, in, b0, b1, tab, err, stream);
+    case 3: return run_sorted_n<3>(subn, evs, subs, nsub, in, b0, b1, tab, err, stream);
     default: return cudaErrorInvalidValue;
   }
 }

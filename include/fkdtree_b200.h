@@ -237,6 +237,10 @@ FKD_API fkd_status fkd_sync(fkd_tree h);
  *                   most 32 candidates are left; the partition parks them and
  *                   one warp orders them by (coordinate, id), instead of more
  *                   digit passes
+ *   "subtree_size"  (0, 512 or 1024; 0 = 1024): the largest subtree the
+ *                   presorted-list kernel (dims 1-3) finishes in shared memory;
+ *                   smaller subtrees take one more global level.  Re-plans at
+ *                   the next build.
  *   "lin_pass"      (0/1, default 1): a segment's first digit pass bins its
  *                   value range (known from its parent's partition) in 2048
  *                   equal float intervals rather than by the top key bits
@@ -279,7 +283,8 @@ FKD_API fkd_status fkd_batch_destroy(fkd_batch b);
  *                  box in a launch of their own (0: one launch for all)
  *   "subtree"      shared-memory subtree kernel: 0 auto (presorted lists for
  *                  dims 1-3, radix select for dim 4), 1 radix select, 2 lists
- *   "small_fix", "lin_pass", "search_bucket"  as fkd_set_param's
+ *   "small_fix", "lin_pass", "search_bucket", "subtree_size"  as fkd_set_param's
+ *                  ("subtree_size" re-plans the batch)
  * A failed "hist_ctas" re-plan leaves the batch without a plan: builds then
  * return FKD_ERR_STATE until a re-plan succeeds.
  * No reference counterpart (the reference has one fixed launch shape). */

@@ -157,3 +157,20 @@ def test_build_pivot_ties_resolved_by_id(cuda, q, dim):
         t.build()
         assert_same(t.tables(), want, f"q={q} dim={dim} small_fix={tf}")
         t.close()
+
+
+@pytest.mark.parametrize("subn", [512, 1024])
+@pytest.mark.parametrize("dim", [1, 2, 3])
+@pytest.mark.parametrize("n", [511, 512, 513, 1023, 1025, 70_001])
+def test_build_presorted_subtree_sizes(cuda, subn, dim, n):
+    """Both sizes of the presorted-list subtree kernel ("subtree_size") give
+    the reference's tables; 512 takes one more global level."""
+    rng = np.random.default_rng(n + 31 * dim + subn)
+    c = rng.random((dim, n), dtype=np.float32)
+    c[0, : n // 3] = np.round(c[0, : n // 3] * 64) / 64  # ties
+    ids = rng.permutation(n).astype(np.uint32)
+    t = F.FKDTree(c, ids)
+    t.set_param("subtree_size", subn)
+    t.build()
+    assert_same(t.tables(), O.build(c, ids), f"subn={subn} dim={dim} n={n}")
+    t.close()
