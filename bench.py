@@ -272,9 +272,11 @@ def _events_run(wb, mlp, dev, steps, plain_single, cpu_sample=0):
     b.learn_stats(reset=True)
     b.build(coords, ids)
     plain_passes = b.learn_stats(reset=True)["passes"]
-    out["autotune"] = {"hist_ctas": tune["hist_ctas"], "search_lanes": tune["search_lanes"],
+    out["autotune"] = {"hist_ctas": tune["hist_ctas"], "subtree_size": tune["subtree_size"],
+                       "search_lanes": tune["search_lanes"],
                        "search_big_n": tune["search_big_n"], "search_lanes_big": tune["search_lanes_big"],
-                       "build_s": tune["build_s"], "search_s": tune["search_s"], "split_s": tune["split_s"]}
+                       "build_s": tune["build_s"], "subtree_s": tune["subtree_s"], "search_s": tune["search_s"],
+                       "split_s": tune["split_s"]}
     delta = 0.1
     b.set_mlp(mlp, delta=delta)
     lc = torch.empty(nq, dtype=torch.int32, device=dev)

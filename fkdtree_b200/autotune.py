@@ -6,6 +6,9 @@ expose (include/fkdtree_b200.h):
 
 * ``hist_ctas``     CTAs of each global digit pass and partition of the build
                     (the tile count of the segmented radix select);
+* ``subtree_size``  the largest subtree the presorted-list kernel finishes in
+                    shared memory (512 or 1,024 points: one global level more
+                    against a cheaper subtree kernel);
 * ``search_lanes``  lanes that share one box in the count / digest search
                     (32 = a warp per box; 1 = a thread per box).
 * ``search_big_n``, ``search_lanes_big``  a size split of the digest search:
@@ -34,6 +37,7 @@ import numpy as np
 
 SEARCH_LANES = (32, 16, 8, 4, 2, 1)
 HIST_CTAS_PER_SM = (1, 2, 4, 8)
+SUBTREE_SIZES = (1024, 512)
 # size split of the digest search: events of at least big_n points get their
 # own launch with big_lanes lanes per box ((0, 0): no split)
 SPLITS = ((0, 0), (32768, 32), (65536, 32), (131072, 32), (65536, 16))
@@ -126,12 +130,14 @@ def _sms() -> int:
 def tune_batch(batch, coords, ids, mins, maxs, *, device: Optional[str] = None, use_cache: bool = True,
                cache_file: Optional[str] = None, reps: int = 2, lanes: Sequence[int] = SEARCH_LANES,
                splits: Sequence[Tuple[int, int]] = SPLITS,
-               hist_ctas: Optional[Sequence[int]] = None, sync: Optional[Callable[[], None]] = None,
+               hist_ctas: Optional[Sequence[int]] = None, subtree_sizes: Sequence[int] = SUBTREE_SIZES,
+               sync: Optional[Callable[[], None]] = None,
                clock: Callable[[], float] = time.perf_counter) -> dict:
-    """Chooses hist_ctas (build) and search_lanes (digest search) for
-    `batch` (a fkdtree_b200.Batch) on its own inputs, applies them and returns
-    {"hist_ctas", "search_lanes", "search_big_n", "search_lanes_big", "cached",
-    "key", "build_s", "search_s", "split_s"}.
+    """Chooses hist_ctas and subtree_size (build) and search_lanes (digest
+    search) for `batch` (a fkdtree_b200.Batch) on its own inputs, applies them
+    and returns {"hist_ctas", "subtree_size", "search_lanes", "search_big_n",
+    "search_lanes_big", "cached", "key", "build_s", "subtree_s", "search_s",
+    "split_s"}.
     Inputs may be host arrays or CUDA tensors (device tensors keep the copies
     out of the timing)."""
     if sync is None:
@@ -148,6 +154,7 @@ def tune_batch(batch, coords, ids, mins, maxs, *, device: Optional[str] = None, 
     hit = entries.get(key)
     if hit is not None and "hist_ctas" in hit and "search_lanes" in hit:
         batch.set_param("hist_ctas", int(hit["hist_ctas"]))
+        batch.set_param("subtree_size", int(hit.get("subtree_size", 0)))
         batch.set_param("search_lanes", int(hit["search_lanes"]))
         batch.set_param("search_lanes_big", int(hit.get("search_lanes_big", 0)))
         batch.set_param("search_big_n", int(hit.get("search_big_n", 0)))
@@ -157,6 +164,9 @@ def tune_batch(batch, coords, ids, mins, maxs, *, device: Optional[str] = None, 
     hc, build_table = sweep(hist_ctas, lambda v: batch.set_param("hist_ctas", int(v)),
                             lambda: batch.build(coords, ids), sync, reps=reps, clock=clock)
     batch.set_param("hist_ctas", int(hc))
+    ss, subtree_table = sweep(subtree_sizes, lambda v: batch.set_param("subtree_size", int(v)),
+                              lambda: batch.build(coords, ids), sync, reps=reps, clock=clock)
+    batch.set_param("subtree_size", int(ss))
     batch.build(coords, ids)
     ln, search_table = sweep(lanes, lambda v: batch.set_param("search_lanes", int(v)),
                              lambda: batch.search_digest(mins, maxs), sync, reps=reps, clock=clock)
@@ -169,9 +179,10 @@ def tune_batch(batch, coords, ids, mins, maxs, *, device: Optional[str] = None, 
     sp, split_table = sweep(splits, apply_split, lambda: batch.search_digest(mins, maxs), sync, reps=reps,
                             clock=clock)
     apply_split(sp)
-    result = {"hist_ctas": int(hc), "search_lanes": int(ln), "search_big_n": int(sp[0]),
+    result = {"hist_ctas": int(hc), "subtree_size": int(ss), "search_lanes": int(ln), "search_big_n": int(sp[0]),
               "search_lanes_big": int(sp[1]),
               "build_s": {str(k): v for k, v in build_table},
+              "subtree_s": {str(k): v for k, v in subtree_table},
               "search_s": {str(k): v for k, v in search_table},
               "split_s": {f"{k[0]}:{k[1]}": v for k, v in split_table}}
     if use_cache:

@@ -23,13 +23,13 @@ class FakeBatch:
         self.dims = np.array(dims, np.uint32)
         self.pt_off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.uint64)
         self.q_off = self.pt_off.copy()
-        self.params = {"hist_ctas": 0, "search_lanes": 0, "search_lanes_big": 0, "search_big_n": 0}
+        self.params = {"hist_ctas": 0, "subtree_size": 0, "search_lanes": 0, "search_lanes_big": 0, "search_big_n": 0}
 
     def set_param(self, name, value):
         self.params[name] = value
 
     def build(self, coords, ids):
-        self.clock.t += 1.0 + abs(self.params["hist_ctas"] - 296) / 1000.0
+        self.clock.t += 1.0 + abs(self.params["hist_ctas"] - 296) / 1000.0 - (0.1 if self.params["subtree_size"] == 512 else 0.0)
 
     def search_digest(self, mins, maxs):
         split_gain = 0.5 if (self.params["search_big_n"] == 65536 and self.params["search_lanes_big"] == 32) else 0.0
@@ -53,9 +53,10 @@ def test_tune_batch_sweeps_applies_and_caches(tmp_path):
     cache = str(tmp_path / "tune.json")
     r = A.tune_batch(b, None, None, None, None, device="FakeGPU", cache_file=cache, reps=2,
                      hist_ctas=[148, 296, 592], sync=lambda: None, clock=clk)
-    assert r["hist_ctas"] == 296 and r["search_lanes"] == 4 and not r["cached"]
+    assert r["hist_ctas"] == 296 and r["subtree_size"] == 512 and r["search_lanes"] == 4 and not r["cached"]
     assert r["search_big_n"] == 65536 and r["search_lanes_big"] == 32
-    assert b.params == {"hist_ctas": 296, "search_lanes": 4, "search_lanes_big": 32, "search_big_n": 65536}
+    assert b.params == {"hist_ctas": 296, "subtree_size": 512, "search_lanes": 4, "search_lanes_big": 32,
+                        "search_big_n": 65536}
     data = json.load(open(cache))
     assert r["key"] in data and data[r["key"]]["search_lanes"] == 4
     # a second batch of the same shape takes the cached choice without timing anything
@@ -63,7 +64,8 @@ def test_tune_batch_sweeps_applies_and_caches(tmp_path):
     b2 = FakeBatch(clk2)
     r2 = A.tune_batch(b2, None, None, None, None, device="FakeGPU", cache_file=cache, sync=lambda: None, clock=clk2)
     assert r2["cached"] and clk2.t == 0.0
-    assert b2.params == {"hist_ctas": 296, "search_lanes": 4, "search_lanes_big": 32, "search_big_n": 65536}
+    assert b2.params == {"hist_ctas": 296, "subtree_size": 512, "search_lanes": 4, "search_lanes_big": 32,
+                         "search_big_n": 65536}
 
 
 def test_shape_key_buckets():
