@@ -147,6 +147,7 @@ struct fkd_batch_s {
   bool small_fix = true;  // selects stop at SMALL_CAP candidates, the partition orders them
   bool lin_pass = true;   // a segment's first digit pass bins its value range linearly
   uint32_t search_bucket = 4;  // leaf-bucket height of the warp-per-box digest search (0: walk every level)
+  uint32_t search_bucket_grp = 2;  // ... of the digest search with fewer than 32 lanes per box
   // learned split
   fkd_mlp mlp = nullptr;
   float mlp_delta = 0.f;
@@ -338,10 +339,8 @@ fkd_status enqueue_digest(fkd_batch b, const float* mins, const float* maxs, uin
     if (p.nq == 0) continue;
     Table tab{p.nodes.as<uint4>(), p.ids.as<uint32_t>(), p.sdig.as<unsigned long long>()};
     BCUDA(launch_subtree_digests(p.plan.evs, p.plan.nev, p.maxn, tab, b->stream));
-    // leaf buckets: only the warp-per-box search scans them
-    const bool full_warp = b->search_lanes == 0 || b->search_lanes == 32 ||
-                           (b->search_big_n && (b->search_lanes_big == 0 || b->search_lanes_big == 32));
-    if (b->search_bucket && full_warp) {
+    // leaf buckets (in-order node copy per event)
+    if (b->search_bucket || b->search_bucket_grp) {
       BCUDA(p.ipts.ensure(p.npts * sizeof(uint4)));
       if (p.dim > 3) BCUDA(p.dids.ensure(p.npts * sizeof(uint32_t)));
       tab.ipts = p.ipts.as<uint4>();
@@ -362,6 +361,7 @@ fkd_status enqueue_digest(fkd_batch b, const float* mins, const float* maxs, uin
     sc.capacity = ~0ull;
     sc.lanes = b->search_lanes;
     sc.bucket = tab.ipts ? b->search_bucket : 0u;
+    sc.bucket_grp = tab.ipts ? b->search_bucket_grp : 0u;
     sc.stream = b->stream;
     if (b->search_big_n == 0) {
       BCUDA(launch_search(sc, p.dim, SEARCH_DIGEST));
@@ -502,6 +502,12 @@ fkd_status fkd_batch_set_param(fkd_batch b, const char* name, int64_t value) {
   if (strcmp(name, "search_bucket") == 0) {
     if (value < 0 || value > (int64_t)BUCKET_MAX) return capi_fail(FKD_ERR_ARG, "search_bucket must be 0..6");
     b->search_bucket = (uint32_t)value;
+    drop_graph();
+    return FKD_OK;
+  }
+  if (strcmp(name, "search_bucket_lanes") == 0) {
+    if (value < 0 || value > 3) return capi_fail(FKD_ERR_ARG, "search_bucket_lanes must be 0..3");
+    b->search_bucket_grp = (uint32_t)value;
     drop_graph();
     return FKD_OK;
   }

@@ -132,6 +132,7 @@ struct fkd_tree_s {
   bool small_fix = true;        // selects stop at SMALL_CAP candidates, the partition orders them ("small_fix")
   bool lin_pass = true;         // a segment's first digit pass bins its value range linearly ("lin_pass")
   uint32_t search_bucket = 4;   // leaf-bucket height of the searches ("search_bucket"; 0: walk every level)
+  uint32_t search_bucket_grp = 2;  // ... of the searches with fewer than 32 lanes per box ("search_bucket_lanes")
   bool search_record = true;    // fkd_search records runs in the count pass ("search_record")
   uint64_t search_pool = 0;     // fixed pool entries ("search_pool"; 0: sized by demand)
   // tables derived from the tree on first use (in-order ids / heap indices /
@@ -313,11 +314,12 @@ SearchCtx search_ctx(fkd_tree h, const Lease& L, const Boxes& b) {
   memset(&sc, 0, sizeof sc);
   sc.g = make_geom((uint32_t)h->n);
   sc.tab = table_of(h);
-  if (h->search_bucket && h->ipts_valid) {
+  if ((h->search_bucket || h->search_bucket_grp) && h->ipts_valid) {
     sc.tab.ipts = h->ipts.as<uint4>();
     sc.tab.dids = h->dids.as<uint32_t>();
     sc.tab.dnode = h->dnode.as<uint32_t>();
     sc.bucket = h->search_bucket;
+    sc.bucket_grp = h->search_bucket_grp;
   }
   sc.boxes = b;
   sc.qcounter = L.s->qctr.as<uint32_t>();
@@ -385,7 +387,7 @@ fkd_status ensure_inorder(fkd_tree h, cudaStream_t st) {
   if (h->n == 0) return FKD_OK;
   {
     std::lock_guard<std::mutex> g(h->tree_mu);
-    const bool want_ipts = h->search_bucket != 0;
+    const bool want_ipts = h->search_bucket != 0 || h->search_bucket_grp != 0;
     if (!h->inorder_valid || (want_ipts && !h->ipts_valid)) {
       FKD_CUDA(h->dids.ensure(h->n * sizeof(uint32_t)));
       FKD_CUDA(h->dnode.ensure(h->n * sizeof(uint32_t)));
@@ -408,7 +410,7 @@ fkd_status ensure_inorder(fkd_tree h, cudaStream_t st) {
 
 // The leaf-bucket scan's in-order tables, when it is on.
 fkd_status ensure_buckets(fkd_tree h, cudaStream_t st) {
-  return h->search_bucket ? ensure_inorder(h, st) : FKD_OK;
+  return (h->search_bucket || h->search_bucket_grp) ? ensure_inorder(h, st) : FKD_OK;
 }
 
 // Subtree digests of the current tree (digest search), built once per tree.
@@ -1165,6 +1167,11 @@ fkd_status fkd_set_param(fkd_tree h, const char* name, int64_t value) {
   if (strcmp(name, "search_bucket") == 0) {
     if (value < 0 || value > (int64_t)BUCKET_MAX) return fail(FKD_ERR_ARG, "search_bucket must be 0..6");
     h->search_bucket = (uint32_t)value;
+    return FKD_OK;
+  }
+  if (strcmp(name, "search_bucket_lanes") == 0) {
+    if (value < 0 || value > 3) return fail(FKD_ERR_ARG, "search_bucket_lanes must be 0..3");
+    h->search_bucket_grp = (uint32_t)value;
     return FKD_OK;
   }
   if (strcmp(name, "search_record") == 0) {

@@ -204,6 +204,8 @@ struct SearchCtx {
   // leaf buckets (needs tab.ipts): visited subtrees of height <= bucket are
   // scanned in in-order layout instead of walked (0: walk every level)
   uint32_t bucket;
+  uint32_t bucket_grp;           // the same for the searches with fewer than 32 lanes per box (one lane
+                                 // scans a bucket of at most 2^(h+1)-1 points)
   cudaStream_t stream;
 };
 

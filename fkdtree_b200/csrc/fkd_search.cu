@@ -878,6 +878,10 @@ __global__ void __launch_bounds__(QT) k_search_grp(SearchCtx sc, uint32_t cap) {
   Table tab = sc.tab;
   float lo[4] = {0.f, 0.f, 0.f, 0.f}, hi[4] = {0.f, 0.f, 0.f, 0.f};
   unsigned long long acc = 0ull, acc2 = 0ull;
+  // children at depth >= bdep are leaf buckets: pushed with BUCKET_BIT set and,
+  // when popped, their points scanned by the lane that popped them
+  uint32_t bdep = 0xffffffffu;
+  constexpr uint32_t BUCKET_BIT = 0x80000000u;  // node indices stay below 2^31
 
   // the group's result for its current box (group-uniform call)
   auto finish = [&]() {
@@ -926,6 +930,8 @@ __global__ void __launch_bounds__(QT) k_search_grp(SearchCtx sc, uint32_t cap) {
         tab.nodes = sc.tab.nodes + ev.base;
         tab.ids = sc.tab.ids + ev.base;
         tab.sdig = sc.tab.sdig ? sc.tab.sdig + ev.base : nullptr;
+        tab.ipts = sc.tab.ipts ? sc.tab.ipts + ev.base : nullptr;
+        tab.dids = sc.tab.dids ? sc.tab.dids + ev.base : nullptr;
         blo = sc.boxes.lo + ev.qcbase;
         bhi = sc.boxes.hi + ev.qcbase;
         bstride = ev.nq;
@@ -942,6 +948,7 @@ __global__ void __launch_bounds__(QT) k_search_grp(SearchCtx sc, uint32_t cap) {
       }
       acc = 0ull;
       acc2 = 0ull;
+      bdep = (tab.ipts && sc.bucket_grp) ? (g.H > sc.bucket_grp ? g.H - sc.bucket_grp : 0u) : 0xffffffffu;
       if (g.n == 0) {
         finish();
       } else if (mask0 == FULL) {
@@ -976,9 +983,33 @@ __global__ void __launch_bounds__(QT) k_search_grp(SearchCtx sc, uint32_t cap) {
     }
     __syncwarp();
     top = base;
-    bool pushL = false, pushR = false;
+    bool pushL = false, pushR = false, bucket = false;
     uint32_t maskL = 0u, maskR = 0u;
-    if (have) {
+    if (have && (i & BUCKET_BIT)) {
+      // a leaf bucket: its subtree is the in-order range [S, S + len)
+      bucket = true;
+      const uint32_t nb = i & ~BUCKET_BIT;
+      const uint32_t dep = floor_log2_u32(nb + 1u);
+      const uint32_t t = nb + 1u - (1u << dep);
+      const uint32_t S = seg_start(g, dep, t), len = seg_len(g, dep, t);
+      for (uint32_t k = 0; k < len; ++k) {
+        const uint4 pt = __ldg(tab.ipts + S + k);
+        bool in = true;
+        if (DIM > 0) in &= (__uint_as_float(pt.x) <= hi[0] && __uint_as_float(pt.x) >= lo[0]);
+        if (DIM > 1) in &= (__uint_as_float(pt.y) <= hi[1] && __uint_as_float(pt.y) >= lo[1]);
+        if (DIM > 2) in &= (__uint_as_float(pt.z) <= hi[2] && __uint_as_float(pt.z) >= lo[2]);
+        if (DIM > 3) in &= (__uint_as_float(pt.w) <= hi[3] && __uint_as_float(pt.w) >= lo[3]);
+        if (in) {
+          if (MODE == SEARCH_COUNT) {
+            acc += 1u;
+          } else {
+            acc2 += 1u;
+            acc += mix64(DIM <= 3 ? pt.w : __ldg(tab.dids + S + k));
+          }
+        }
+      }
+    }
+    if (have && !bucket) {
       const uint32_t dep = floor_log2_u32(i + 1u);
       const uint32_t c = dep % DIM;
       const uint4 nd = __ldg(tab.nodes + i);
@@ -1025,13 +1056,15 @@ __global__ void __launch_bounds__(QT) k_search_grp(SearchCtx sc, uint32_t cap) {
       top = 0;
     } else {
       uint32_t p = (uint32_t)top + __popc(bpl & glt) + __popc(bpr & glt);
+      // children at the bucket depth go on the stack as buckets
+      const uint32_t btag = (pushL || pushR) && floor_log2_u32(i + 1u) + 1u >= bdep ? BUCKET_BIT : 0u;
       if (pushL) {
-        stk_node[p] = 2u * i + 1u;
+        stk_node[p] = (2u * i + 1u) | btag;
         stk_mask[p] = (uint8_t)maskL;
         ++p;
       }
       if (pushR) {
-        stk_node[p] = 2u * i + 2u;
+        stk_node[p] = (2u * i + 2u) | btag;
         stk_mask[p] = (uint8_t)maskR;
       }
       top += (int)tot;

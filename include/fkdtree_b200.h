@@ -233,6 +233,9 @@ FKD_API fkd_status fkd_sync(fkd_tree h);
  *                   point by point in in-order layout instead of walking them;
  *                   0 walks every level.  Costs 16 bytes per point of device
  *                   memory for the in-order copy of the nodes.
+ *   "search_bucket_lanes" (0..3, default 2): the same for the count / digest
+ *                   searches with fewer than 32 lanes per box ("search_lanes"):
+ *                   one lane scans a visited subtree of at most 2^(v+1)-1 points
  *   "small_fix"     (0/1, default 1): a global level's select stops once at
  *                   most 32 candidates are left; the partition parks them and
  *                   one warp orders them by (coordinate, id), instead of more
@@ -283,7 +286,8 @@ FKD_API fkd_status fkd_batch_destroy(fkd_batch b);
  *                  box in a launch of their own (0: one launch for all)
  *   "subtree"      shared-memory subtree kernel: 0 auto (presorted lists for
  *                  dims 1-3, radix select for dim 4), 1 radix select, 2 lists
- *   "small_fix", "lin_pass", "search_bucket", "subtree_size"  as fkd_set_param's
+ *   "small_fix", "lin_pass", "search_bucket", "search_bucket_lanes",
+ *   "subtree_size"  as fkd_set_param's
  *                  ("subtree_size" re-plans the batch)
  * A failed "hist_ctas" re-plan leaves the batch without a plan: builds then
  * return FKD_ERR_STATE until a re-plan succeeds.

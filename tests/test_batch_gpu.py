@@ -114,3 +114,26 @@ def test_autotuned_batch_graph(cuda, tmp_path):
     b2.run(coords, ids, mins, maxs, counts, dig)
     tab, tid = b2.tables()
     check_batch(wb, tab, tid, counts.cpu().numpy().view(np.uint32), dig.cpu().numpy().view(np.uint64))
+
+
+@pytest.mark.parametrize("lanes", [2, 32])
+def test_batch_leaf_buckets_equal_walk(cuda, lanes):
+    """Batched digest search with and without leaf buckets, against the oracle."""
+    import torch
+    wb = W.event_batch(n_events=40, median=4000, size_lo=1, size_hi=50_000, clusters_lo=3, clusters_hi=40,
+                       half_width=0.01, seed=41, frac_4d=0.3)
+    _, _, oc, od = O.batch(wb)
+    coords = torch.from_numpy(wb.coords).cuda()
+    ids = torch.from_numpy(wb.ids.view(np.int32)).cuda()
+    mins = torch.from_numpy(wb.mins).cuda()
+    maxs = torch.from_numpy(wb.maxs).cuda()
+    b = F.Batch.of(wb)
+    b.set_param("search_lanes", lanes)
+    b.build(coords, ids)
+    for bk, bg in ((0, 0), (4, 2), (6, 3)):
+        b.set_param("search_bucket", bk)
+        b.set_param("search_bucket_lanes", bg)
+        c, d = b.search_digest(mins, maxs)
+        assert np.array_equal(c.cpu().numpy().view(np.uint32), oc), f"bucket {bk}/{bg}"
+        assert np.array_equal(d.cpu().numpy().view(np.uint64), od), f"bucket {bk}/{bg}"
+    b.close()

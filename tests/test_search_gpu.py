@@ -221,3 +221,29 @@ def test_leaf_buckets_equal_walk(cuda, dim, n):
         assert np.array_equal(O.digest_of(got, offs), wd), f"bucket {b}: traversing write"
         t.set_param("search_record", 1)
     t.close()
+
+
+@pytest.mark.parametrize("dim", [2, 3, 4])
+def test_leaf_buckets_with_lanes_per_box_equal_walk(cuda, dim):
+    """Count and digest with 1-16 lanes per box: leaf buckets of height
+    1..3 scanned by one lane ("search_bucket_lanes") give the walk's result."""
+    rng = np.random.default_rng(300 + dim)
+    n = 40_000
+    c = rng.random((dim, n), dtype=np.float32)
+    ids = rng.permutation(n).astype(np.uint32)
+    q = 2000
+    ctr = c[:, rng.integers(0, n, q)]
+    hw = rng.uniform(0.0, 0.08, (dim, q)).astype(np.float32)
+    mins, maxs = (ctr - hw).astype(np.float32), (ctr + hw).astype(np.float32)
+    t = F.FKDTree(c, ids).build()
+    tab, tid = t.tables()
+    wc, wo, wids, _ = O.search(tab, tid, mins, maxs, variant=O.RECURSIVE)
+    wd = O.digest_of(wids, wo)
+    for lanes in (1, 2, 8, 16):
+        t.set_param("search_lanes", lanes)
+        for b in (0, 1, 2, 3):
+            t.set_param("search_bucket_lanes", b)
+            assert np.array_equal(t.count_boxes(mins, maxs), wc), f"lanes {lanes} bucket {b}"
+            cc, dd = t.digest_boxes(mins, maxs)
+            assert np.array_equal(cc, wc) and np.array_equal(dd, wd), f"lanes {lanes} bucket {b}"
+    t.close()
