@@ -73,6 +73,8 @@ def parse_args():
     ap.add_argument("--batched-events", type=int, default=4096)
     ap.add_argument("--level-times", action="store_true",
                     help="print the device time of every kernel of one build (CUDA activity records) and exit")
+    ap.add_argument("--set", action="append", default=[], metavar="NAME=VALUE",
+                    help="a fkd_set_param knob of the bench tree (repeatable); every value gives the same results")
     return ap.parse_args()
 
 
@@ -450,6 +452,7 @@ def run_ours(args):
     _capi.check(L.fkd_create(dim, _capi.FLAG_ASYNC, C.c_void_p(stream.cuda_stream), C.byref(h)))
     # CUDA events around the library's kernels (read back after the timed region)
     _capi.check(L.fkd_set_param(h, b"kernel_events", 1))
+    apply_knobs(L, h, args.set)
     P = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
 
     coords = torch.from_numpy(ev.coords).to(dev)
@@ -558,7 +561,8 @@ def run_ours(args):
     line = {"metric": METRIC, "value": value, "unit": "Mpoints/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator, fkdtree_b200/workloads.py)",
-            "config": dict(cfg, parallelism=f"replicas{world}", results_per_step=results),
+            "config": dict(cfg, parallelism=f"replicas{world}", results_per_step=results,
+                           **({"knobs": args.set} if args.set else {})),
             "build_mpoints_per_s": n / build_ms / 1e3, "search_mboxes_per_s": q / search_ms / 1e3,
             "phases": phases, "kernels": kern, "roofline": roof, "gpu_launches": int(launches)}
     line["clocks"] = clk.summary()
@@ -989,6 +993,13 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def apply_knobs(L, h, items):
+    from fkdtree_b200 import _capi
+    for it in items:
+        name, _, val = it.partition("=")
+        _capi.check(L.fkd_set_param(h, name.encode(), int(val)))
+
+
 def level_times(args):
     """Device time of every kernel launch of one build of the workload, in
     launch order (CUDA activity records through torch.profiler)."""
@@ -1004,6 +1015,7 @@ def level_times(args):
     ids = torch.from_numpy(ev.ids.view(np.int32)).to(dev)
     h = C.c_void_p()
     _capi.check(L.fkd_create(ev.dim, 0, None, C.byref(h)))
+    apply_knobs(L, h, args.set)
     for _ in range(3):
         _capi.check(L.fkd_build(h, P(coords), P(ids), ev.n, _capi.MEM_DEVICE))
     torch.cuda.synchronize()

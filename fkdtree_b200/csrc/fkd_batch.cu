@@ -223,6 +223,10 @@ fkd_status batch_plan(fkd_batch b) {
     BCUDA(p.sel.ensure(sizeof(SegSel) * (size_t)p.plan.maxseg));
     BCUDA(p.bnd.ensure(2 * sizeof(uint2) * (size_t)p.plan.maxseg));
     BCUDA(p.tiebuf.ensure((size_t)p.plan.maxseg * SMALL_CAP * (p.dim + 1) * 4));
+    // leaf-bucket tables (in-order node copy; ids too in 4-D): allocated here,
+    // never while a graph is being captured
+    BCUDA(p.ipts.ensure(p.npts * sizeof(uint4)));
+    if (p.dim > 3) BCUDA(p.dids.ensure(p.npts * sizeof(uint32_t)));
     BCUDA(p.ghist.ensure((size_t)p.plan.maxseg * HIST_BINS * 4));
     BCUDA(p.sdig.ensure(p.npts * sizeof(unsigned long long)));
     BCUDA(p.lfeat.ensure((size_t)p.plan.maxseg * FKD_MLP_FEATURES * 4));
@@ -341,8 +345,6 @@ fkd_status enqueue_digest(fkd_batch b, const float* mins, const float* maxs, uin
     BCUDA(launch_subtree_digests(p.plan.evs, p.plan.nev, p.maxn, tab, b->stream));
     // leaf buckets (in-order node copy per event)
     if (b->search_bucket || b->search_bucket_grp) {
-      BCUDA(p.ipts.ensure(p.npts * sizeof(uint4)));
-      if (p.dim > 3) BCUDA(p.dids.ensure(p.npts * sizeof(uint32_t)));
       tab.ipts = p.ipts.as<uint4>();
       tab.dids = p.dim > 3 ? p.dids.as<uint32_t>() : nullptr;
       BCUDA(launch_inorder_events(p.plan.evs, p.plan.nev, p.maxn, tab, b->stream));

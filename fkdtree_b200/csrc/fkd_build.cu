@@ -111,29 +111,67 @@ __device__ __forceinline__ bool lin_setup(uint32_t vlo, uint32_t vhi, float& vmi
 
 // Level 0 has no parent partition to report its segments' value range: one
 // pass over the split coordinate (the first dimension) reduces each
-// segment's min / max order bits into bnd, as (~min, max) from a zeroed array.
+// segment's min / max order bits into bnd, as (~min, max) from a zeroed
+// array.  A CTA takes B0_TILES consecutive partition tiles (in segment
+// order) and flushes one pair of atomics per segment it saw.
+constexpr uint32_t B0_TILES = 16;
 template <int DIM>
 __global__ void __launch_bounds__(GT) k_bounds0(const EvDesc* __restrict__ evs, const uint2* __restrict__ segs,
-                                                const uint2* __restrict__ tiles, CSoA src, uint2* __restrict__ bnd) {
-  const uint2 tl = tiles[blockIdx.x];
-  const uint32_t s = tl.x, t = tl.y;
-  const uint2 sd = segs[s];
-  const Geom eg = evs[sd.x].g;
-  const uint32_t len = seg_len(eg, 0u, sd.y);
-  const uint32_t start = evs[sd.x].base + seg_start(eg, 0u, sd.y);
-  const uint32_t t0 = start + t * PTILE, t1 = min(start + len, t0 + (uint32_t)PTILE);
+                                                const uint2* __restrict__ tiles, uint32_t ntiles, CSoA src,
+                                                uint2* __restrict__ bnd) {
+  __shared__ uint32_t red[2][GWARPS];
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint32_t q0 = blockIdx.x * B0_TILES;
+  uint32_t cur = ~0u;
   uint32_t nmn = 0u, mx = 0u;  // ~min, max
-  for (uint32_t e = t0 + threadIdx.x; e < t1; e += GT) {
-    const uint32_t m = mono_bits(__ldcs(src.base + e));
-    nmn = max(nmn, ~m);
-    mx = max(mx, m);
+  auto flush = [&]() {  // block-uniform
+    const uint32_t a = __reduce_max_sync(0xffffffffu, nmn), b = __reduce_max_sync(0xffffffffu, mx);
+    if (lane == 0) {
+      red[0][warp] = a;
+      red[1][warp] = b;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t x = 0u, y = 0u;
+      for (int w = 0; w < GWARPS; ++w) {
+        x = max(x, red[0][w]);
+        y = max(y, red[1][w]);
+      }
+      if (x | y) {
+        atomicMax(&bnd[cur].x, x);
+        atomicMax(&bnd[cur].y, y);
+      }
+    }
+    __syncthreads();
+    nmn = mx = 0u;
+  };
+  for (uint32_t q = q0; q < q0 + B0_TILES && q < ntiles; ++q) {
+    const uint2 tl = tiles[q];
+    if (tl.x != cur) {
+      if (cur != ~0u) flush();
+      cur = tl.x;
+    }
+    const uint2 sd = segs[tl.x];
+    const Geom eg = evs[sd.x].g;
+    const uint32_t len = seg_len(eg, 0u, sd.y);
+    const uint32_t start = evs[sd.x].base + seg_start(eg, 0u, sd.y);
+    const uint32_t t0 = start + tl.y * PTILE, t1 = min(start + len, t0 + (uint32_t)PTILE);
+    uint32_t v[PIPT];
+#pragma unroll
+    for (int k = 0; k < PIPT; ++k) {
+      const uint32_t e = t0 + k * GT + threadIdx.x;
+      v[k] = e < t1 ? __ldcs(src.base + e) : 0u;
+    }
+#pragma unroll
+    for (int k = 0; k < PIPT; ++k) {
+      if (t0 + k * GT + threadIdx.x < t1) {
+        const uint32_t m = mono_bits(v[k]);
+        nmn = max(nmn, ~m);
+        mx = max(mx, m);
+      }
+    }
   }
-  nmn = __reduce_max_sync(0xffffffffu, nmn);
-  mx = __reduce_max_sync(0xffffffffu, mx);
-  if ((threadIdx.x & 31u) == 0u && t0 < t1) {
-    atomicMax(&bnd[s].x, nmn);
-    atomicMax(&bnd[s].y, mx);
-  }
+  if (cur != ~0u) flush();
 }
 
 __global__ void k_sel_init(uint32_t d, const EvDesc* __restrict__ evs, const uint2* __restrict__ segs, uint32_t nseg,
@@ -206,6 +244,10 @@ __global__ void k_sel_init(uint32_t d, const EvDesc* __restrict__ evs, const uin
 // `lin`), else the top 11 bits of (value - vlo) while the value is open, else
 // of (id - ilo) among the points holding the value.
 constexpr int HCOPIES = 4;
+#ifndef FKD_HLOADS
+#define FKD_HLOADS 4
+#endif
+constexpr int HLOADS = FKD_HLOADS;  // 16-byte loads per thread in flight
 #ifndef FKD_HIST_MINB
 #define FKD_HIST_MINB 4
 #endif
@@ -280,7 +322,7 @@ __global__ void __launch_bounds__(GT, FKD_HIST_MINB) k_hist(uint32_t d, const Ev
     atomicAdd(&myhist[dig], 1u);
   };
   // the tile [tb, tend): a scalar head up to a 16-byte boundary, 16-byte
-  // loads (two per thread in flight), a scalar tail
+  // loads (HLOADS per thread in flight), a scalar tail
   const uint32_t tb = start + t * ts;
   const uint32_t tlen = tend > tb ? tend - tb : 0u;
   uint32_t head = (uint32_t)(((16u - ((uint32_t)(uintptr_t)(X + tb) & 15u)) & 15u) >> 2);
@@ -289,24 +331,23 @@ __global__ void __launch_bounds__(GT, FKD_HIST_MINB) k_hist(uint32_t d, const Ev
   const uint32_t vb0 = tb + head;
   const uint32_t nv = (tlen - head) >> 2;
   const uint4* X4 = reinterpret_cast<const uint4*>(X + vb0);
-  for (uint32_t v0 = 0; v0 < nv; v0 += 2u * GT) {
-    const uint32_t va = v0 + threadIdx.x, vb = va + GT;
-    uint4 qa = make_uint4(0u, 0u, 0u, 0u), qb = qa;
-    if (va < nv) qa = __ldcs(X4 + va);
-    if (vb < nv) qb = __ldcs(X4 + vb);
-    if (va < nv) {
-      const uint32_t e = vb0 + 4u * va;
-      count(qa.x, e);
-      count(qa.y, e + 1u);
-      count(qa.z, e + 2u);
-      count(qa.w, e + 3u);
+  for (uint32_t v0 = 0; v0 < nv; v0 += (uint32_t)HLOADS * GT) {
+    uint4 q[HLOADS];
+#pragma unroll
+    for (int u = 0; u < HLOADS; ++u) {
+      const uint32_t va = v0 + u * GT + threadIdx.x;
+      q[u] = va < nv ? __ldcs(X4 + va) : make_uint4(0u, 0u, 0u, 0u);
     }
-    if (vb < nv) {
-      const uint32_t e = vb0 + 4u * vb;
-      count(qb.x, e);
-      count(qb.y, e + 1u);
-      count(qb.z, e + 2u);
-      count(qb.w, e + 3u);
+#pragma unroll
+    for (int u = 0; u < HLOADS; ++u) {
+      const uint32_t va = v0 + u * GT + threadIdx.x;
+      if (va < nv) {
+        const uint32_t e = vb0 + 4u * va;
+        count(q[u].x, e);
+        count(q[u].y, e + 1u);
+        count(q[u].z, e + 2u);
+        count(q[u].w, e + 3u);
+      }
     }
   }
   const uint32_t tail0 = vb0 + 4u * nv;
@@ -1313,7 +1354,8 @@ static cudaError_t run_build(BuildCtx& bc) {
     if (d == 0 && bc.bnd && bc.lin && !small) {
       cudaError_t e = cudaMemsetAsync(bc.bnd, 0, sizeof(uint2) * lp.nseg, bc.stream);
       if (e != cudaSuccess) return e;
-      k_bounds0<DIM><<<lp.nptile, GT, 0, bc.stream>>>(bc.evs, lp.segs, lp.ptiles, src, bc.bnd);
+      k_bounds0<DIM><<<(lp.nptile + B0_TILES - 1) / B0_TILES, GT, 0, bc.stream>>>(bc.evs, lp.segs, lp.ptiles,
+                                                                                lp.nptile, src, bc.bnd);
       count_launches(1);
       bnd_in = bc.bnd;
       inv = true;

@@ -84,7 +84,7 @@ def test_learned_builds_are_bit_identical_and_save_passes(cuda):
     tab0, tid0 = eb.tables()
     assert np.array_equal(tab0.view(np.uint32), otab.view(np.uint32)) and np.array_equal(tid0, otid)
     assert plain["brackets"] == 0 and plain["passes"] > 0
-    eb.set_mlp(m, delta=0.05)
+    eb.set_mlp(m, delta=0.1)
     eb.build(ev.coords, ev.ids)
     tab1, tid1 = eb.tables()
     st = eb.learn_stats(reset=True)
@@ -97,32 +97,44 @@ def test_learned_builds_are_bit_identical_and_save_passes(cuda):
     # (around a guess near the middle of the node's range) mostly miss and
     # cost a pass each
     untrained = F.MLP(seed=99)
-    eb.set_mlp(untrained, delta=0.05)
+    eb.set_mlp(untrained, delta=0.1)
     eb.build(ev.coords, ev.ids)
     su = eb.learn_stats(reset=True)
     tab2, tid2 = eb.tables()
     assert np.array_equal(tab2.view(np.uint32), otab.view(np.uint32)) and np.array_equal(tid2, otid)
-    assert st["verified"] >= 0.8 * st["brackets"]
+    assert st["verified"] >= 0.6 * st["brackets"], st
     assert st["verified"] > su["verified"]
     assert st["passes"] < plain["passes"], (st, plain)
     assert st["passes"] < su["passes"], (st, su)
 
 
 def test_wrong_predictions_fall_back_exactly(cuda):
-    """A network that predicts far outside every node (b3 = 50) makes every
-    bracket fail; the plain select must take over and give the same tree."""
+    """A network that predicts the top of every node's sample range (b3 = 1,
+    every other parameter 0) brackets a value far above nearly every split;
+    those brackets fail and the plain select takes over: the same tree.  A
+    prediction outside the node's value range makes no bracket at all
+    (b3 = 50)."""
     ev = _batch(24, 30)
     otab, otid, _, _ = O.batch(ev)
     m = F.MLP(seed=1)
     p = np.zeros(m.n_params, dtype=np.float32)
-    p[R.OFF_B3] = 50.0
+    p[R.OFF_B3] = 1.0
     m.params = p
     eb = F.Batch.of(ev).set_mlp(m, delta=0.01)
     eb.build(ev.coords, ev.ids)
     tab, tid = eb.tables()
-    st = eb.learn_stats()
+    st = eb.learn_stats(reset=True)
     assert np.array_equal(tab.view(np.uint32), otab.view(np.uint32)) and np.array_equal(tid, otid)
-    assert st["brackets"] > 0 and st["fallbacks"] == st["brackets"]
+    assert st["brackets"] > 0 and st["verified"] + st["fallbacks"] == st["brackets"]
+    assert st["fallbacks"] >= 0.9 * st["brackets"], st
+    p[R.OFF_B3] = 50.0
+    m.params = p
+    eb.set_mlp(m, delta=0.01)
+    eb.build(ev.coords, ev.ids)
+    tab, tid = eb.tables()
+    st = eb.learn_stats(reset=True)
+    assert np.array_equal(tab.view(np.uint32), otab.view(np.uint32)) and np.array_equal(tid, otid)
+    assert st["brackets"] == 0
 
 
 def test_learned_single_event_build(cuda):
