@@ -133,6 +133,7 @@ struct fkd_tree_s {
   bool lin_pass = true;         // a segment's first digit pass bins its value range linearly ("lin_pass")
   uint32_t search_bucket = 4;   // leaf-bucket height of the searches ("search_bucket"; 0: walk every level)
   uint32_t search_bucket_grp = 2;  // ... of the searches with fewer than 32 lanes per box ("search_bucket_lanes")
+  bool bucket_runs = false;     // unordered recorded searches merge consecutive bucket hits into runs ("bucket_runs")
   bool search_record = true;    // fkd_search records runs in the count pass ("search_record")
   uint64_t search_pool = 0;     // fixed pool entries ("search_pool"; 0: sized by demand)
   // tables derived from the tree on first use (in-order ids / heap indices /
@@ -375,6 +376,7 @@ fkd_status count_pass(fkd_tree h, const Lease& L, const Boxes& b, uint32_t* dcou
     sc.flags = rec->flags;
     sc.flag_ctr = rec->flag_ctr;
     sc.rec_ids = rec->rec_ids;
+    sc.bucket_runs = rec->bucket_runs;
   }
   FKD_CUDA(launch_search(sc, h->dim, SEARCH_COUNT));
   return FKD_OK;
@@ -852,6 +854,7 @@ fkd_status fkd_search(fkd_tree h, const float* mins, const float* maxs, uint64_t
       rec.flags = sl->rflags.as<uint32_t>();
       rec.flag_ctr = (uint32_t*)(ctr + 3);
       rec.rec_ids = ordered ? 0 : 1;  // unordered: singles carry their ids, the write pass copies them
+      rec.bucket_runs = h->bucket_runs ? 1 : 0;
     }
   }
   if (q && (s = count_pass(h, L, b, sl->counts.as<uint32_t>(), order, rec_on ? &rec : nullptr)) != FKD_OK) return s;
@@ -1167,6 +1170,11 @@ fkd_status fkd_set_param(fkd_tree h, const char* name, int64_t value) {
   if (strcmp(name, "search_bucket") == 0) {
     if (value < 0 || value > (int64_t)BUCKET_MAX) return fail(FKD_ERR_ARG, "search_bucket must be 0..6");
     h->search_bucket = (uint32_t)value;
+    return FKD_OK;
+  }
+  if (strcmp(name, "bucket_runs") == 0) {
+    if (value != 0 && value != 1) return fail(FKD_ERR_ARG, "bucket_runs must be 0 or 1");
+    h->bucket_runs = value != 0;
     return FKD_OK;
   }
   if (strcmp(name, "search_bucket_lanes") == 0) {

@@ -201,6 +201,7 @@ struct SearchCtx {
   uint32_t* flags;               // boxes whose runs did not fit (the write pass traverses them)
   uint32_t* flag_ctr;            // (zeroed by the caller)
   int rec_ids;                   // the singles pool holds ids, not in-order positions (unordered writes)
+  int bucket_runs;               // recording with ids: leaf-bucket hits at consecutive positions still become runs
   // leaf buckets (needs tab.ipts): visited subtrees of height <= bucket are
   // scanned in in-order layout instead of walked (0: walk every level)
   uint32_t bucket;

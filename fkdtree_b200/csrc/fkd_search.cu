@@ -425,9 +425,12 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
             flush_runs(njobs);
             njobs = 0;
           }
+          // singles that carry ids cost the write pass one copy each: with
+          // them every hit stays a single, unless runs are asked for
+          const bool mk_runs = !sc.rec_ids || sc.bucket_runs;
           const uint32_t hb = __ballot_sync(0xffffffffu, hit);
           const uint32_t ppos = __shfl_up_sync(0xffffffffu, pos, 1);
-          const bool cont = hit && lane > 0u && ((hb >> (lane - 1u)) & 1u) && ppos + 1u == pos;
+          const bool cont = mk_runs && hit && lane > 0u && ((hb >> (lane - 1u)) & 1u) && ppos + 1u == pos;
           const uint32_t cb = __ballot_sync(0xffffffffu, cont);
           const bool start = hit && !cont;
           const uint32_t after = lane < 31u ? (cb >> (lane + 1u)) : 0u;

@@ -233,6 +233,9 @@ FKD_API fkd_status fkd_sync(fkd_tree h);
  *                   point by point in in-order layout instead of walking them;
  *                   0 walks every level.  Costs 16 bytes per point of device
  *                   memory for the in-order copy of the nodes.
+ *   "bucket_runs"   (0/1, default 0): unordered fkd_search records the leaf
+ *                   buckets' hits at consecutive in-order positions as runs
+ *                   instead of single ids
  *   "search_bucket_lanes" (0..3, default 2): the same for the count / digest
  *                   searches with fewer than 32 lanes per box ("search_lanes"):
  *                   one lane scans a visited subtree of at most 2^(v+1)-1 points

@@ -203,8 +203,9 @@ def test_leaf_buckets_equal_walk(cuda, dim, n):
     tab, tid = t.tables()
     wc, wo, wids, _ = O.search(tab, tid, mins, maxs, variant=O.RECURSIVE)
     wd = O.digest_of(wids, wo)
-    for b in (0, 1, 3, 4, 6):
+    for b, runs in ((0, 0), (1, 0), (3, 1), (4, 0), (4, 1), (6, 0)):
         t.set_param("search_bucket", b)
+        t.set_param("bucket_runs", runs)
         assert np.array_equal(t.count_boxes(mins, maxs), wc), f"bucket {b}: counts"
         offs, got = t.search_boxes(mins, maxs, ordered=False)
         assert np.array_equal(offs, wo) and np.array_equal(O.digest_of(got, offs), wd), f"bucket {b}: unordered"
