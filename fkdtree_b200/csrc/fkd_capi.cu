@@ -730,6 +730,7 @@ fkd_status write_pass(fkd_tree h, const Lease& L, const Boxes& b, const uint64_t
     x.brec_ctr = rec->brec_ctr;
     x.brec_cap = rec->brec_cap;
     x.rec_ids = rec->rec_ids;
+    x.work_ctr = rec->work_ctr;
     FKD_CUDA(launch_expand(x));
     sc.order = rec->flags;
     sc.boxes.q = nflag;
@@ -827,7 +828,7 @@ fkd_status fkd_search(fkd_tree h, const float* mins, const float* maxs, uint64_t
     if (ae == cudaSuccess) ae = sl->pool_s.ensure(sw * sizeof(uint32_t));
     if (ae == cudaSuccess) ae = sl->brec.ensure(2 * bw * sizeof(uint4));
     if (ae == cudaSuccess) ae = sl->rflags.ensure(q * sizeof(uint32_t));
-    if (ae == cudaSuccess) ae = sl->jctr.ensure(4 * sizeof(unsigned long long));
+    if (ae == cudaSuccess) ae = sl->jctr.ensure(8 * sizeof(unsigned long long));
     if (ae != cudaSuccess) {
       // no room for the pool: traverse twice
       (void)cudaGetLastError();
@@ -838,7 +839,7 @@ fkd_status fkd_search(fkd_tree h, const float* mins, const float* maxs, uint64_t
       sl->pool_want = sl->pool_s_want = sl->brec_want = 0;
       rec_on = false;
     } else {
-      FKD_CUDA(cudaMemsetAsync(sl->jctr.p, 0, 4 * sizeof(unsigned long long), st));
+      FKD_CUDA(cudaMemsetAsync(sl->jctr.p, 0, 8 * sizeof(unsigned long long), st));
       // chunk records are reserved in blocks; the unused tail of a block must read as empty
       FKD_CUDA(cudaMemsetAsync(sl->brec.p, 0, sl->brec.bytes, st));
       unsigned long long* ctr = sl->jctr.as<unsigned long long>();
@@ -853,6 +854,7 @@ fkd_status fkd_search(fkd_tree h, const float* mins, const float* maxs, uint64_t
       rec.brec_cap = sl->brec.bytes / (2 * sizeof(uint4));
       rec.flags = sl->rflags.as<uint32_t>();
       rec.flag_ctr = (uint32_t*)(ctr + 3);
+      rec.work_ctr = ctr + 4;  // the write pass's record counter
       rec.rec_ids = ordered ? 0 : 1;  // unordered: singles carry their ids, the write pass copies them
       rec.bucket_runs = h->bucket_runs ? 1 : 0;
     }

@@ -202,6 +202,7 @@ struct SearchCtx {
   uint32_t* flag_ctr;            // (zeroed by the caller)
   int rec_ids;                   // the singles pool holds ids, not in-order positions (unordered writes)
   int bucket_runs;               // recording with ids: leaf-bucket hits at consecutive positions still become runs
+  unsigned long long* work_ctr;  // k_expand: records handed out (zeroed by the caller)
   // leaf buckets (needs tab.ipts): visited subtrees of height <= bucket are
   // scanned in in-order layout instead of walked (0: walk every level)
   uint32_t bucket;

@@ -758,6 +758,7 @@ constexpr int XT = 256;  // threads of k_expand
 #define FKD_EXU 8
 #endif
 constexpr int EXU = FKD_EXU;  // k_expand: single ids with loads in flight per lane
+constexpr uint32_t XREC = 4;  // k_expand: chunk records a warp takes from the counter at a time
 __global__ void __launch_bounds__(XT) k_expand(const uint4* __restrict__ brec,
                                                const unsigned long long* __restrict__ brec_ctr, uint64_t brec_cap,
                                                const uint32_t* __restrict__ pool_s,
@@ -765,13 +766,24 @@ __global__ void __launch_bounds__(XT) k_expand(const uint4* __restrict__ brec,
                                                const uint32_t* __restrict__ pool_len,
                                                const uint64_t* __restrict__ offsets,
                                                const uint32_t* __restrict__ srct, uint32_t* __restrict__ out,
-                                               uint64_t capacity, uint32_t* __restrict__ err, int singles_ids) {
+                                               uint64_t capacity, uint32_t* __restrict__ err, int singles_ids,
+                                               unsigned long long* __restrict__ work) {
   __shared__ uint32_t st[XT / 32][JOBS];
   __shared__ uint32_t pre[XT / 32][JOBS];
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   const uint64_t nrec = *brec_ctr < brec_cap ? *brec_ctr : brec_cap;
   bool failed = false;
-  for (uint64_t r = (uint64_t)blockIdx.x * (XT / 32) + warp; r < nrec; r += (uint64_t)gridDim.x * (XT / 32)) {
+  // records are handed out XREC at a time from a counter (their sizes vary
+  // from one id to RCAP), the next block taken before the current one is copied
+  auto grab = [&]() {
+    unsigned long long v = 0ull;
+    if (lane == 0) v = atomicAdd(work, (unsigned long long)XREC);
+    return (uint64_t)__shfl_sync(0xffffffffu, v, 0);
+  };
+  uint64_t r0 = grab();
+  while (r0 < nrec) {
+    const uint64_t rnext = grab();
+  for (uint64_t r = r0; r < r0 + XREC && r < nrec; ++r) {
     const uint4 R = brec[2 * r], R2 = brec[2 * r + 1];
     const uint32_t ns = R.w, nj = R2.y;
     if (ns == 0u && nj == 0u) continue;
@@ -831,11 +843,13 @@ __global__ void __launch_bounds__(XT) k_expand(const uint4* __restrict__ brec,
       __syncwarp();
     }
   }
+    r0 = rnext;
+  }
   if (__any_sync(0xffffffffu, failed) && lane == 0) atomicOr(err, ERRB_CAPACITY);
 }
 
 cudaError_t launch_expand(const SearchCtx& sc) {
-  if (!sc.pool_st) return cudaSuccess;
+  if (!sc.pool_st || !sc.work_ctr) return cudaSuccess;
   int dev = 0, sms = 148, per = 1;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -845,7 +859,7 @@ cudaError_t launch_expand(const SearchCtx& sc) {
   k_expand<<<(unsigned)(sms * per), XT, 0, sc.stream>>>(sc.brec, sc.brec_ctr, sc.brec_cap, sc.pool_s, sc.pool_st,
                                                         sc.pool_len,
                                                         sc.offsets, sc.heap_out ? sc.tab.dnode : sc.tab.dids, sc.out,
-                                                        sc.capacity, sc.err, sc.rec_ids);
+                                                        sc.capacity, sc.err, sc.rec_ids, sc.work_ctr);
   count_launches(1);
   return cudaGetLastError();
 }

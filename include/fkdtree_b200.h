@@ -68,7 +68,8 @@ typedef enum fkd_status {
   FKD_ERR_STATE = 5,     /* e.g. search before build */
   FKD_ERR_CAPACITY = 6,  /* a result or frontier bound was exceeded; nothing was silently dropped */
   FKD_ERR_INTERNAL = 7,  /* a device-side consistency check failed */
-  FKD_ERR_TIMEOUT = 8    /* a bounded device-side wait gave up */
+  FKD_ERR_TIMEOUT = 8    /* reserved for a bounded device-side wait that gives up; no kernel of
+                            this version waits on another, so no call returns it today */
 } fkd_status;
 
 enum { FKD_MEM_HOST = 0, FKD_MEM_DEVICE = 1 };
