@@ -531,6 +531,7 @@ __global__ void __launch_bounds__(GT, FKD_PART_MINB) k_partition(uint32_t d, con
                                                      const uint32_t* __restrict__ child,
                                                      uint32_t* __restrict__ tiebuf) {
   __shared__ uint32_t sL[PIPT * GWARPS], sR[PIPT * GWARPS];
+  __shared__ uint32_t sBL[PIPT * GWARPS], sBR[PIPT * GWARPS];  // the warps' left / right ballots
   __shared__ uint32_t s_base[2];
   const uint2 tl = tiles[blockIdx.x];
   const uint32_t s = tl.x, t = tl.y;
@@ -561,8 +562,7 @@ __global__ void __launch_bounds__(GT, FKD_PART_MINB) k_partition(uint32_t d, con
     for (int w = 0; w < DIM; ++w) rec[k][w] = v ? __ldcs(src.base + (uint64_t)w * src.stride + e) : 0u;
     rec[k][DIM] = v ? __ldcs(src.ids + e) : 0u;
   }
-  uint32_t bl[PIPT], br[PIPT];
-  uint32_t eqmask = 0u;  // bit k: record k matches the pivot prefix
+  uint32_t eqmask = 0u;  // bit k: record k is a candidate of the select (inside [klo, khi])
   bool nan = false;
 #pragma unroll
   for (int k = 0; k < PIPT; ++k) {
@@ -577,11 +577,13 @@ __global__ void __launch_bounds__(GT, FKD_PART_MINB) k_partition(uint32_t d, con
       cls = key < klo ? 0u : (key > khi ? 2u : 1u);
     }
     if (cls == 1u) eqmask |= 1u << k;
-    bl[k] = __ballot_sync(0xffffffffu, cls == 0u);
-    br[k] = __ballot_sync(0xffffffffu, cls == 2u);
+    const uint32_t bl = __ballot_sync(0xffffffffu, cls == 0u);
+    const uint32_t br = __ballot_sync(0xffffffffu, cls == 2u);
     if (lane == 0) {
-      sL[k * GWARPS + warp] = __popc(bl[k]);
-      sR[k * GWARPS + warp] = __popc(br[k]);
+      sL[k * GWARPS + warp] = __popc(bl);
+      sR[k * GWARPS + warp] = __popc(br);
+      sBL[k * GWARPS + warp] = bl;
+      sBR[k * GWARPS + warp] = br;
     }
   }
   if (nan) atomicOr(err, ERRB_NAN);
@@ -631,11 +633,12 @@ __global__ void __launch_bounds__(GT, FKD_PART_MINB) k_partition(uint32_t d, con
 #pragma unroll
   for (int k = 0; k < PIPT; ++k) {
     uint32_t pos = 0xffffffffu, lim = 0u;
-    if ((bl[k] >> lane) & 1u) {
-      pos = baseL + sL[k * GWARPS + warp] + __popc(bl[k] & lt);
+    const uint32_t bl = sBL[k * GWARPS + warp], br = sBR[k * GWARPS + warp];
+    if ((bl >> lane) & 1u) {
+      pos = baseL + sL[k * GWARPS + warp] + __popc(bl & lt);
       lim = endL;
-    } else if ((br[k] >> lane) & 1u) {
-      pos = baseR + sR[k * GWARPS + warp] + __popc(br[k] & lt);
+    } else if ((br >> lane) & 1u) {
+      pos = baseR + sR[k * GWARPS + warp] + __popc(br & lt);
       lim = endR;
     } else if (((eqmask >> k) & 1u) && small) {
       // the select left a few candidates: parked for k_small_fix, which orders them by key
@@ -680,34 +683,20 @@ __global__ void __launch_bounds__(GT, FKD_PART_MINB) k_partition(uint32_t d, con
     }
   }
   if (ch != ~0u) {  // CTA-uniform
-    // warp, then CTA reduction; one global atomic per bound per CTA
+    // warp reduction, then one global atomic (no return value: nothing
+    // waits on it) per bound per warp -- no CTA barrier
     mnL = __reduce_min_sync(0xffffffffu, mnL);
     mxL = __reduce_max_sync(0xffffffffu, mxL);
     mnR = __reduce_min_sync(0xffffffffu, mnR);
     mxR = __reduce_max_sync(0xffffffffu, mxR);
-    __shared__ uint32_t sb[4];
-    if (threadIdx.x == 0) {
-      sb[0] = 0xffffffffu;
-      sb[1] = 0u;
-      sb[2] = 0xffffffffu;
-      sb[3] = 0u;
-    }
-    __syncthreads();
     if (lane == 0u) {
-      atomicMin(&sb[0], mnL);
-      atomicMax(&sb[1], mxL);
-      atomicMin(&sb[2], mnR);
-      atomicMax(&sb[3], mxR);
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      if (sb[0] <= sb[1]) {
-        atomicMin(&bnd_out[ch].x, sb[0]);
-        atomicMax(&bnd_out[ch].y, sb[1]);
+      if (mnL <= mxL) {
+        atomicMin(&bnd_out[ch].x, mnL);
+        atomicMax(&bnd_out[ch].y, mxL);
       }
-      if (sb[2] <= sb[3]) {
-        atomicMin(&bnd_out[ch + 1u].x, sb[2]);
-        atomicMax(&bnd_out[ch + 1u].y, sb[3]);
+      if (mnR <= mxR) {
+        atomicMin(&bnd_out[ch + 1u].x, mnR);
+        atomicMax(&bnd_out[ch + 1u].y, mxR);
       }
     }
   }
