@@ -483,11 +483,40 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
           __syncwarp();
         }
       } else {
-        if (lane == 0) {
-          stk_node[0] = 0u;
-          stk_mask[0] = (uint8_t)mask0;
+        // descend, all lanes alike, while the box lies on one side of the
+        // node's split: such a node is outside the box and the walk would
+        // visit only that one child; the walk starts at the first node the
+        // box straddles (its cell's mask is still mask0)
+        uint32_t r = 0u, dep = 0u;
+        bool empty = false;
+        while (dep + 1u < bdep) {
+          const uint32_t c = dep % (uint32_t)DIM;
+          const uint4 nd = __ldg(tab.nodes + r);
+          const float v = sel4(c, __uint_as_float(nd.x), __uint_as_float(nd.y), __uint_as_float(nd.z),
+                               __uint_as_float(nd.w));
+          const float loc = sel4(c, lo[0], lo[1], lo[2], lo[3]);
+          const float hic = sel4(c, hi[0], hi[1], hi[2], hi[3]);
+          uint32_t nx;
+          if (v < loc)
+            nx = 2u * r + 2u;  // the walk visits the right child only
+          else if (v > hic)
+            nx = 2u * r + 1u;  // the left child only
+          else
+            break;
+          if (nx >= n) {  // that child does not exist: nothing is inside
+            empty = true;
+            break;
+          }
+          r = nx;
+          ++dep;
         }
-        top = 1;
+        if (!empty) {
+          if (lane == 0) {
+            stk_node[0] = r;
+            stk_mask[0] = (uint8_t)(mask0 | (DIM == 3 ? ((dep % 3u) << 6) : 0u));
+          }
+          top = 1;
+        }
       }
     }
     __syncwarp();
@@ -979,12 +1008,40 @@ __global__ void __launch_bounds__(QT) k_search_grp(SearchCtx sc, uint32_t cap) {
         }
         finish();
       } else {
-        if (gl == 0) {
-          stk_node[0] = 0u;
-          stk_mask[0] = (uint8_t)mask0;
+        // descend while the box lies on one side of the split (see k_search)
+        uint32_t r = 0u, dep = 0u;
+        bool empty = false;
+        while (dep + 1u < bdep) {
+          const uint32_t c = dep % (uint32_t)DIM;
+          const uint4 nd = __ldg(tab.nodes + r);
+          const float v = sel4(c, __uint_as_float(nd.x), __uint_as_float(nd.y), __uint_as_float(nd.z),
+                               __uint_as_float(nd.w));
+          const float loc = sel4(c, lo[0], lo[1], lo[2], lo[3]);
+          const float hic = sel4(c, hi[0], hi[1], hi[2], hi[3]);
+          uint32_t nx;
+          if (v < loc)
+            nx = 2u * r + 2u;
+          else if (v > hic)
+            nx = 2u * r + 1u;
+          else
+            break;
+          if (nx >= g.n) {
+            empty = true;
+            break;
+          }
+          r = nx;
+          ++dep;
         }
-        top = 1;
-        active = true;
+        if (empty) {
+          finish();
+        } else {
+          if (gl == 0) {
+            stk_node[0] = r;
+            stk_mask[0] = (uint8_t)mask0;
+          }
+          top = 1;
+          active = true;
+        }
       }
     }
     if (!__any_sync(0xffffffffu, active)) break;
