@@ -40,6 +40,25 @@
 
 namespace fkd {
 
+#ifdef FKD_PROF
+// Cycle counters of the warp-per-box search (profiling builds only):
+// [0] whole boxes, [1] leaf-bucket scans, [2] boxes, [3] walk steps, [4] scan windows.
+__device__ unsigned long long g_prof_search[8];
+extern "C" __attribute__((visibility("default"))) void fkd_prof_search_read(unsigned long long* out) {
+  cudaMemcpyFromSymbol(out, g_prof_search, sizeof(g_prof_search));
+}
+extern "C" __attribute__((visibility("default"))) void fkd_prof_search_reset() {
+  unsigned long long z[8] = {0};
+  cudaMemcpyToSymbol(g_prof_search, z, sizeof(z));
+}
+#define SPROF_T(v) const unsigned long long v = clock64()
+#define SPROF_ADD(slot, x) \
+  if (lane == 0) atomicAdd(&g_prof_search[slot], (unsigned long long)(x))
+#else
+#define SPROF_T(v)
+#define SPROF_ADD(slot, x)
+#endif
+
 constexpr int QT = 128;  // threads per CTA
 constexpr int QW = QT / 32;
 constexpr int JOBS = 256;      // contained-subtree jobs buffered per warp
@@ -194,6 +213,7 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
       bj = qj - ev.qbase;
       oj = ev.qout + bj;
     }
+    SPROF_T(tb0);
     const uint32_t n = g.n;
     // children at depth >= bdep are leaf buckets: subtrees of height <= sc.bucket, scanned in in-order layout
     const uint32_t bdep = (tab.ipts && sc.bucket) ? (g.H > sc.bucket ? g.H - sc.bucket : 0u) : 0xffffffffu;
@@ -359,6 +379,7 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
     // run, isolated ones singles.
     uint32_t nb = 0;  // queued buckets (warp-uniform)
     auto scan_buckets = [&](uint32_t nbk) {
+      SPROF_T(ts0);
       uint32_t carry = 0u;
       for (uint32_t e0 = 0; e0 < nbk; e0 += 32u) {
         const uint32_t e = e0 + lane;
@@ -454,6 +475,9 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
         njobs = 0;
       }
       __syncwarp();
+      SPROF_T(ts1);
+      SPROF_ADD(1, ts1 - ts0);
+      SPROF_ADD(4, (total + 31u) / 32u);
     };
 
     int top = 0;
@@ -522,6 +546,7 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
     __syncwarp();
 
     while (top > 0) {
+      SPROF_ADD(3, 1);
       const int gcount = top < 32 ? top : 32;
       const int base = top - gcount;
       const bool have = (int)lane < gcount;
@@ -774,6 +799,9 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
     }
     if (anyfail && lane == 0) atomicOr(sc.err, ERRB_CAPACITY);
     __syncwarp();
+    SPROF_T(tb1);
+    SPROF_ADD(0, tb1 - tb0);
+    SPROF_ADD(2, 1);
   }
 }
 
