@@ -683,20 +683,36 @@ __global__ void __launch_bounds__(GT, FKD_PART_MINB) k_partition(uint32_t d, con
     }
   }
   if (ch != ~0u) {  // CTA-uniform
-    // warp reduction, then one global atomic (no return value: nothing
-    // waits on it) per bound per warp -- no CTA barrier
+    // warp, then CTA reduction; one global atomic per bound per CTA (every
+    // CTA of a segment hits the same two words: per-warp atomics would
+    // multiply that contention by eight)
     mnL = __reduce_min_sync(0xffffffffu, mnL);
     mxL = __reduce_max_sync(0xffffffffu, mxL);
     mnR = __reduce_min_sync(0xffffffffu, mnR);
     mxR = __reduce_max_sync(0xffffffffu, mxR);
+    __shared__ uint32_t sb[4];
+    if (threadIdx.x == 0) {
+      sb[0] = 0xffffffffu;
+      sb[1] = 0u;
+      sb[2] = 0xffffffffu;
+      sb[3] = 0u;
+    }
+    __syncthreads();
     if (lane == 0u) {
-      if (mnL <= mxL) {
-        atomicMin(&bnd_out[ch].x, mnL);
-        atomicMax(&bnd_out[ch].y, mxL);
+      atomicMin(&sb[0], mnL);
+      atomicMax(&sb[1], mxL);
+      atomicMin(&sb[2], mnR);
+      atomicMax(&sb[3], mxR);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      if (sb[0] <= sb[1]) {
+        atomicMin(&bnd_out[ch].x, sb[0]);
+        atomicMax(&bnd_out[ch].y, sb[1]);
       }
-      if (mnR <= mxR) {
-        atomicMin(&bnd_out[ch + 1u].x, mnR);
-        atomicMax(&bnd_out[ch + 1u].y, mxR);
+      if (sb[2] <= sb[3]) {
+        atomicMin(&bnd_out[ch + 1u].x, sb[2]);
+        atomicMax(&bnd_out[ch + 1u].y, sb[3]);
       }
     }
   }

@@ -234,10 +234,10 @@ FKD_API fkd_status fkd_sync(fkd_tree h);
  *                   point by point in in-order layout instead of walking them;
  *                   0 walks every level.  Costs 16 bytes per point of device
  *                   memory for the in-order copy of the nodes.
- *   "bucket_runs"   (0/1, default 0): unordered fkd_search records the leaf
+ *   "bucket_runs"   (0/1, default 1): unordered fkd_search records the leaf
  *                   buckets' hits at consecutive in-order positions as runs
- *                   instead of single ids
- *   "search_bucket_lanes" (0..3, default 2): the same for the count / digest
+ *                   (0: every hit as a single id)
+ *   "search_bucket_lanes" (0..3, default 0): the same for the count / digest
  *                   searches with fewer than 32 lanes per box ("search_lanes"):
  *                   one lane scans a visited subtree of at most 2^(v+1)-1 points
  *   "small_fix"     (0/1, default 1): a global level's select stops once at
