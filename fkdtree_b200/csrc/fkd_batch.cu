@@ -146,7 +146,7 @@ struct fkd_batch_s {
   int subtree_size = 0;   // presorted subtree size (0: 1,024)
   bool small_fix = true;  // selects stop at SMALL_CAP candidates, the partition orders them
   bool lin_pass = true;   // a segment's first digit pass bins its value range linearly
-  uint32_t search_bucket = 4;  // leaf-bucket height of the warp-per-box digest search (0: walk every level)
+  uint32_t search_bucket = 5;  // leaf-bucket height of the warp-per-box digest search (0: walk every level)
   uint32_t search_bucket_grp = 0;  // ... of the digest search with fewer than 32 lanes per box
   // learned split
   fkd_mlp mlp = nullptr;

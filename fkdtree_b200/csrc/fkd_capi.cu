@@ -131,7 +131,7 @@ struct fkd_tree_s {
   DevBuf lfeat, lyhat, lrange, lstats, sdig, dids, dnode, ipts, bnd, tiebuf;
   bool small_fix = true;        // selects stop at SMALL_CAP candidates, the partition orders them ("small_fix")
   bool lin_pass = true;         // a segment's first digit pass bins its value range linearly ("lin_pass")
-  uint32_t search_bucket = 4;   // leaf-bucket height of the searches ("search_bucket"; 0: walk every level)
+  uint32_t search_bucket = 5;   // leaf-bucket height of the searches ("search_bucket"; 0: walk every level)
   uint32_t search_bucket_grp = 0;  // ... of the searches with fewer than 32 lanes per box ("search_bucket_lanes")
   bool bucket_runs = true;      // unordered recorded searches merge consecutive bucket hits into runs ("bucket_runs")
   bool search_record = true;    // fkd_search records runs in the count pass ("search_record")

@@ -72,6 +72,10 @@ constexpr uint32_t RBLK = 2048;  // runs reserved per warp at a time
 constexpr uint32_t CBLK = 64;    // chunk records reserved per warp at a time
 constexpr uint32_t RCAP = 4096;  // results per chunk record before a new one starts
 constexpr int BQ = 128;          // leaf buckets queued per warp (one step adds at most 64)
+#ifndef FKD_SU
+#define FKD_SU 2
+#endif
+constexpr int SU = FKD_SU;       // leaf-bucket scan: windows of 32 points with loads in flight
 
 __device__ __forceinline__ uint32_t lanemask_lt_s() {
   uint32_t m;
@@ -395,27 +399,10 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
       }
       __syncwarp();
       const uint32_t total = carry;
-      uint32_t jb = 0u;  // the bucket holding slot w0 (warp-uniform)
-      for (uint32_t w0 = 0; w0 < total; w0 += 32u) {
-        const uint32_t k = jb + lane;
-        const bool kv = k < nbk;
-        const uint32_t pk = kv ? bq_len[warp][k] : total;
-        const uint32_t sk = kv ? bq_st[warp][k] : 0u;
-        // buckets after jb start after w0 (every bucket holds at least one point)
-        const uint32_t B =
-            __reduce_or_sync(0xffffffffu, (lane > 0u && kv && pk < w0 + 32u) ? (1u << (pk - w0)) : 0u);
-        const uint32_t jl = __popc(B & (0xffffffffu >> (31u - lane)));
-        const uint32_t mp = __shfl_sync(0xffffffffu, pk, jl);
-        const uint32_t ms = __shfl_sync(0xffffffffu, sk, jl);
-        uint32_t nbn = jb + __popc(B);
-        if (nbn + 1u < nbk && bq_len[warp][nbn + 1u] == w0 + 32u) ++nbn;
-        jb = nbn;
-        const bool ok = w0 + lane < total;
-        const uint32_t pos = ms + (w0 + lane - mp);
+      // one window's points: the in-box test and what the mode does with a hit
+      auto take = [&](bool ok, uint32_t pos, const uint4& pt) {
         bool hit = false;
-        uint4 pt = make_uint4(0u, 0u, 0u, 0u);
         if (ok) {
-          pt = __ldg(tab.ipts + pos);
           bool in = true;
           if (DIM > 0) in &= (__uint_as_float(pt.x) <= hi[0] && __uint_as_float(pt.x) >= lo[0]);
           if (DIM > 1) in &= (__uint_as_float(pt.y) <= hi[1] && __uint_as_float(pt.y) >= lo[1]);
@@ -468,6 +455,36 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
           njobs += __popc(br);
           nsing += __popc(bs);
         }
+      };
+      uint32_t jb = 0u;  // the bucket holding slot w0 (warp-uniform)
+      for (uint32_t w0 = 0; w0 < total; w0 += 32u * SU) {
+        // SU windows: their positions first, then all their loads, then the tests
+        uint32_t pos[SU];
+        bool ok[SU];
+#pragma unroll
+        for (int u = 0; u < SU; ++u) {
+          const uint32_t ww = w0 + 32u * u;
+          const uint32_t k = jb + lane;
+          const bool kv = k < nbk;
+          const uint32_t pk = kv ? bq_len[warp][k] : total;
+          const uint32_t sk = kv ? bq_st[warp][k] : 0u;
+          // buckets after jb start after ww (every bucket holds at least one point)
+          const uint32_t B =
+              __reduce_or_sync(0xffffffffu, (lane > 0u && kv && pk < ww + 32u) ? (1u << (pk - ww)) : 0u);
+          const uint32_t jl = __popc(B & (0xffffffffu >> (31u - lane)));
+          const uint32_t mp = __shfl_sync(0xffffffffu, pk, jl);
+          const uint32_t ms = __shfl_sync(0xffffffffu, sk, jl);
+          uint32_t nbn = jb + __popc(B);
+          if (nbn + 1u < nbk && bq_len[warp][nbn + 1u] == ww + 32u) ++nbn;
+          ok[u] = ww + lane < total;
+          pos[u] = ms + (ww + lane - mp);
+          if (ww < total) jb = nbn;
+        }
+        uint4 pt[SU];
+#pragma unroll
+        for (int u = 0; u < SU; ++u) pt[u] = ok[u] ? __ldg(tab.ipts + pos[u]) : make_uint4(0u, 0u, 0u, 0u);
+#pragma unroll
+        for (int u = 0; u < SU; ++u) take(ok[u], pos[u], pt[u]);
       }
       if (record && (njobs > (uint32_t)(JN - 64) || nsing > (uint32_t)(JN - 32))) {
         __syncwarp();
@@ -1036,40 +1053,14 @@ __global__ void __launch_bounds__(QT) k_search_grp(SearchCtx sc, uint32_t cap) {
         }
         finish();
       } else {
-        // descend while the box lies on one side of the split (see k_search)
-        uint32_t r = 0u, dep = 0u;
-        bool empty = false;
-        while (dep + 1u < bdep) {
-          const uint32_t c = dep % (uint32_t)DIM;
-          const uint4 nd = __ldg(tab.nodes + r);
-          const float v = sel4(c, __uint_as_float(nd.x), __uint_as_float(nd.y), __uint_as_float(nd.z),
-                               __uint_as_float(nd.w));
-          const float loc = sel4(c, lo[0], lo[1], lo[2], lo[3]);
-          const float hic = sel4(c, hi[0], hi[1], hi[2], hi[3]);
-          uint32_t nx;
-          if (v < loc)
-            nx = 2u * r + 2u;
-          else if (v > hic)
-            nx = 2u * r + 1u;
-          else
-            break;
-          if (nx >= g.n) {
-            empty = true;
-            break;
-          }
-          r = nx;
-          ++dep;
+        // (no descent here: a group taking a box would hold up the other
+        // groups of its warp for a chain of dependent loads)
+        if (gl == 0) {
+          stk_node[0] = 0u;
+          stk_mask[0] = (uint8_t)mask0;
         }
-        if (empty) {
-          finish();
-        } else {
-          if (gl == 0) {
-            stk_node[0] = r;
-            stk_mask[0] = (uint8_t)mask0;
-          }
-          top = 1;
-          active = true;
-        }
+        top = 1;
+        active = true;
       }
     }
     if (!__any_sync(0xffffffffu, active)) break;

@@ -229,7 +229,7 @@ FKD_API fkd_status fkd_sync(fkd_tree h);
  *   "search_pool"   entries of the record pools (0, the default: sized by the
  *                   previous call's demand; boxes that do not fit are traversed
  *                   again, so any size gives the same results)
- *   "search_bucket" (0..6, default 4): box searches scan the visited subtrees
+ *   "search_bucket" (0..6, default 5): box searches scan the visited subtrees
  *                   of height <= this many levels (at most 2^(v+1)-1 points)
  *                   point by point in in-order layout instead of walking them;
  *                   0 walks every level.  Costs 16 bytes per point of device
