@@ -343,8 +343,10 @@ fkd_status enqueue_digest(fkd_batch b, const float* mins, const float* maxs, uin
     if (p.nq == 0) continue;
     Table tab{p.nodes.as<uint4>(), p.ids.as<uint32_t>(), p.sdig.as<unsigned long long>()};
     BCUDA(launch_subtree_digests(p.plan.evs, p.plan.nev, p.maxn, tab, b->stream));
-    // leaf buckets (in-order node copy per event)
-    if (b->search_bucket || b->search_bucket_grp) {
+    // leaf buckets (in-order node copy per event), when a search that scans them runs
+    const bool full_warp = b->search_lanes == 0 || b->search_lanes == 32 ||
+                           (b->search_big_n && (b->search_lanes_big == 0 || b->search_lanes_big == 32));
+    if ((b->search_bucket && full_warp) || b->search_bucket_grp) {
       tab.ipts = p.ipts.as<uint4>();
       tab.dids = p.dim > 3 ? p.dids.as<uint32_t>() : nullptr;
       BCUDA(launch_inorder_events(p.plan.evs, p.plan.nev, p.maxn, tab, b->stream));

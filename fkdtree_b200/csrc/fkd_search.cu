@@ -73,7 +73,7 @@ constexpr uint32_t CBLK = 64;    // chunk records reserved per warp at a time
 constexpr uint32_t RCAP = 4096;  // results per chunk record before a new one starts
 constexpr int BQ = 128;          // leaf buckets queued per warp (one step adds at most 64)
 #ifndef FKD_SU
-#define FKD_SU 2
+#define FKD_SU 1
 #endif
 constexpr int SU = FKD_SU;       // leaf-bucket scan: windows of 32 points with loads in flight
 
@@ -946,7 +946,7 @@ cudaError_t launch_expand(const SearchCtx& sc) {
 // those steps leave idle.  Same node tests and accumulation as k_search.
 __host__ __device__ inline uint32_t stack_cap_lanes(const Geom& g, uint32_t G) { return 2u * G * (g.H + 1u) + 1u; }
 
-template <int DIM, int MODE, int G>
+template <int DIM, int MODE, int G, bool BKT>
 __global__ void __launch_bounds__(QT) k_search_grp(SearchCtx sc, uint32_t cap) {
   static_assert(G == 1 || G == 2 || G == 4 || G == 8 || G == 16, "group width");
   constexpr int NG = QT / G;
@@ -1039,7 +1039,7 @@ __global__ void __launch_bounds__(QT) k_search_grp(SearchCtx sc, uint32_t cap) {
       }
       acc = 0ull;
       acc2 = 0ull;
-      bdep = (tab.ipts && sc.bucket_grp) ? (g.H > sc.bucket_grp ? g.H - sc.bucket_grp : 0u) : 0xffffffffu;
+      if (BKT) bdep = (tab.ipts && sc.bucket_grp) ? (g.H > sc.bucket_grp ? g.H - sc.bucket_grp : 0u) : 0xffffffffu;
       if (g.n == 0) {
         finish();
       } else if (mask0 == FULL) {
@@ -1078,7 +1078,7 @@ __global__ void __launch_bounds__(QT) k_search_grp(SearchCtx sc, uint32_t cap) {
     top = base;
     bool pushL = false, pushR = false, bucket = false;
     uint32_t maskL = 0u, maskR = 0u;
-    if (have && (i & BUCKET_BIT)) {
+    if (BKT && have && (i & BUCKET_BIT)) {
       // a leaf bucket: its subtree is the in-order range [S, S + len)
       bucket = true;
       const uint32_t nb = i & ~BUCKET_BIT;
@@ -1150,7 +1150,7 @@ __global__ void __launch_bounds__(QT) k_search_grp(SearchCtx sc, uint32_t cap) {
     } else {
       uint32_t p = (uint32_t)top + __popc(bpl & glt) + __popc(bpr & glt);
       // children at the bucket depth go on the stack as buckets
-      const uint32_t btag = (pushL || pushR) && floor_log2_u32(i + 1u) + 1u >= bdep ? BUCKET_BIT : 0u;
+      const uint32_t btag = (BKT && (pushL || pushR) && floor_log2_u32(i + 1u) + 1u >= bdep) ? BUCKET_BIT : 0u;
       if (pushL) {
         stk_node[p] = (2u * i + 1u) | btag;
         stk_mask[p] = (uint8_t)maskL;
@@ -1167,16 +1167,17 @@ __global__ void __launch_bounds__(QT) k_search_grp(SearchCtx sc, uint32_t cap) {
   }
 }
 
-template <int DIM, int MODE, int G>
-static cudaError_t run_search_grp(SearchCtx& sc) {
+template <int DIM, int MODE, int G, bool BKT>
+static cudaError_t run_search_grp_b(SearchCtx& sc) {
   const uint32_t cap = stack_cap_lanes(sc.g, G);
   const size_t smem = (size_t)(QT / G) * cap * 5u;
-  cudaError_t e = cudaFuncSetAttribute(k_search_grp<DIM, MODE, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e =
+      cudaFuncSetAttribute(k_search_grp<DIM, MODE, G, BKT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int dev = 0, sms = 0, per = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_search_grp<DIM, MODE, G>, QT, smem);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_search_grp<DIM, MODE, G, BKT>, QT, smem);
   if (e != cudaSuccess) return e;
   if (per < 1) per = 1;
   uint64_t blocks = (uint64_t)sms * per;
@@ -1184,9 +1185,17 @@ static cudaError_t run_search_grp(SearchCtx& sc) {
   if (blocks > need) blocks = need ? need : 1;
   e = cudaMemsetAsync(sc.qcounter, 0, sizeof(uint32_t), sc.stream);
   if (e != cudaSuccess) return e;
-  k_search_grp<DIM, MODE, G><<<(unsigned)blocks, QT, smem, sc.stream>>>(sc, cap);
+  k_search_grp<DIM, MODE, G, BKT><<<(unsigned)blocks, QT, smem, sc.stream>>>(sc, cap);
   count_launches(1);
   return cudaGetLastError();
+}
+
+// The leaf-bucket variant only when buckets are asked for: the plain kernel
+// stays free of the bucket branch.
+template <int DIM, int MODE, int G>
+static cudaError_t run_search_grp(SearchCtx& sc) {
+  if (sc.tab.ipts && sc.bucket_grp) return run_search_grp_b<DIM, MODE, G, true>(sc);
+  return run_search_grp_b<DIM, MODE, G, false>(sc);
 }
 
 template <int DIM, int MODE, bool REC = false>
