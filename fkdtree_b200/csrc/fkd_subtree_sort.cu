@@ -6,10 +6,14 @@
 // of a radix select per level, the CTA sorts its points once per dimension
 // and then walks the levels with lists:
 //
-//   1. rank the points by id (a sort of (id, slot) keys): element r is the
-//      point with the r-th smallest id, so (coordinate, r) orders exactly as
-//      the reference comparator's (coordinate, id) (FKDTree_cpu.h:246-252);
-//   2. sort (order bits of coordinate c, r) for every dimension c: list_c;
+//   1-2. for every dimension c, list_c: the slots of the points in the order
+//      of the reference comparator (coordinate c, then id: FKDTree_cpu.h:
+//      246-252).  Usually (a subtree is a small cell) the order bits of c span
+//      less than 2^22 and a sort of 32-bit keys ((bits - min) << 10 | slot)
+//      orders the points by coordinate, then each run of equal coordinates is
+//      re-ordered by id; otherwise (or for runs longer than 32) the points are
+//      ranked by id first (a sort of (id, slot) keys) and sorted by 64-bit
+//      (bits, id rank) keys;
 //   3. level d, split dimension c = d % dim: every segment [ls, ls + m) of
 //      every list holds the same elements, and list_c holds them in split
 //      order, so the pivot is list_c[ls + rank] -- no select at all; the
@@ -64,18 +68,16 @@ struct XCfg {
   static constexpr size_t smem = recs + eofr + lists + seg + side + scratch;
 };
 
-__device__ __forceinline__ unsigned long long umin64(unsigned long long a, unsigned long long b) { return a < b ? a : b; }
-__device__ __forceinline__ unsigned long long umax64(unsigned long long a, unsigned long long b) { return a < b ? b : a; }
 
-// Sorts XN 64-bit keys (ascending) with the whole CTA: bitonic sort of 128
-// keys per warp in registers, then five merge-path rounds through shared
+// Sorts XN keys (32- or 64-bit, ascending) with the whole CTA: bitonic sort
+// of 128 keys per warp in registers, then merge-path rounds through shared
 // memory.  Returns the buffer (a or b) that holds the result.
-template <int XN>
-__device__ unsigned long long* cta_sort(unsigned long long* a, unsigned long long* b) {
+template <int XN, class K>
+__device__ K* cta_sort(K* a, K* b) {
   static_assert(XN >= 512 && XN <= 4096 && (XN & (XN - 1)) == 0, "sorted subtree size");
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-  unsigned long long v[4];
-  unsigned long long* wbase = a + warp * 128u;
+  K v[4];
+  K* wbase = a + warp * 128u;
 #pragma unroll
   for (int i = 0; i < 4; ++i) v[i] = wbase[lane * 4u + i];
 #pragma unroll
@@ -87,10 +89,10 @@ __device__ unsigned long long* cta_sort(unsigned long long* a, unsigned long lon
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
           const uint32_t idx = lane * 4u + i;
-          const unsigned long long o = __shfl_xor_sync(0xffffffffu, v[i], lm);
+          const K o = __shfl_xor_sync(0xffffffffu, v[i], lm);
           const bool lower = (idx & j) == 0u;
           const bool asc = (idx & k) == 0u;
-          v[i] = (lower == asc) ? umin64(v[i], o) : umax64(v[i], o);
+          v[i] = (lower == asc) ? (v[i] < o ? v[i] : o) : (v[i] < o ? o : v[i]);
         }
       } else {
 #pragma unroll
@@ -98,7 +100,7 @@ __device__ unsigned long long* cta_sort(unsigned long long* a, unsigned long lon
           if ((i & (int)j) == 0) {
             const uint32_t idx = lane * 4u + i;
             const bool asc = (idx & k) == 0u;
-            const unsigned long long x = v[i], y = v[i ^ (int)j];
+            const K x = v[i], y = v[i ^ (int)j];
             if ((x > y) == asc) {
               v[i] = y;
               v[i ^ (int)j] = x;
@@ -110,15 +112,15 @@ __device__ unsigned long long* cta_sort(unsigned long long* a, unsigned long lon
   }
 #pragma unroll
   for (int i = 0; i < 4; ++i) wbase[lane * 4u + i] = v[i];
-  unsigned long long* src = a;
-  unsigned long long* dst = b;
+  K* src = a;
+  K* dst = b;
   for (uint32_t s = 128; s < (uint32_t)XN; s <<= 1) {
     __syncthreads();
     const uint32_t og = threadIdx.x * XPPT;  // first of this thread's outputs
     const uint32_t pair = og / (2u * s);
     const uint32_t o = og - pair * 2u * s;
-    const unsigned long long* A = src + pair * 2u * s;
-    const unsigned long long* B = A + s;
+    const K* A = src + pair * 2u * s;
+    const K* B = A + s;
     uint32_t lo = o > s ? o - s : 0u, hi = o < s ? o : s;
     while (lo < hi) {
       const uint32_t mid = (lo + hi) >> 1;
@@ -128,12 +130,12 @@ __device__ unsigned long long* cta_sort(unsigned long long* a, unsigned long lon
         hi = mid;
     }
     uint32_t i = lo, jb = o - lo;
-    unsigned long long* D = dst + pair * 2u * s + o;
+    K* D = dst + pair * 2u * s + o;
 #pragma unroll
     for (int q = 0; q < XPPT; ++q) {
       // an exhausted run reads as the padding key ~0 (never past its end)
-      const unsigned long long va = i < s ? A[i] : ~0ull;
-      const unsigned long long vb = jb < s ? B[jb] : ~0ull;
+      const K va = i < s ? A[i] : (K)~(K)0;
+      const K vb = jb < s ? B[jb] : (K)~(K)0;
       const bool takeA = va < vb || (va == vb && i < s);
       D[q] = takeA ? va : vb;
       if (takeA)
@@ -141,7 +143,7 @@ __device__ unsigned long long* cta_sort(unsigned long long* a, unsigned long lon
       else
         ++jb;
     }
-    unsigned long long* t = src;
+    K* t = src;
     src = dst;
     dst = t;
   }
@@ -228,7 +230,7 @@ __global__ void __launch_bounds__(XN / XPPT, 4096 / XN) k_subtree_sorted(const E
   extern __shared__ __align__(16) unsigned char smem[];
   uint32_t* recs = (uint32_t*)smem;                                 // [DIM + 1][XN], original slot order
   uint16_t* eofr = (uint16_t*)(smem + Cfg::recs);                   // id rank -> slot
-  uint16_t* lists = (uint16_t*)(smem + Cfg::recs + Cfg::eofr);      // [DIM][2][XN] id ranks
+  uint16_t* lists = (uint16_t*)(smem + Cfg::recs + Cfg::eofr);      // [DIM][2][XN] slots
   uint16_t* segb = (uint16_t*)(smem + Cfg::recs + Cfg::eofr + Cfg::lists);  // [2][XN]
   uint8_t* side = smem + Cfg::recs + Cfg::eofr + Cfg::lists + Cfg::seg;
   unsigned long long* keys = (unsigned long long*)(smem + Cfg::recs + Cfg::eofr + Cfg::lists + Cfg::seg + Cfg::side);
@@ -249,42 +251,117 @@ __global__ void __launch_bounds__(XN / XPPT, 4096 / XN) k_subtree_sorted(const E
     if (threadIdx.x == 0) atomicOr(err, ERRB_INTERNAL);
     return;
   }
-  // 1. records, and the id keys
+  // 1. records, and the range of each dimension's order bits
+  __shared__ uint32_t s_mn[4], s_mx[4], s_slow;
+  if (threadIdx.x < 4u) {
+    s_mn[threadIdx.x] = 0xffffffffu;
+    s_mx[threadIdx.x] = 0u;
+  }
+  if (threadIdx.x == 0) s_slow = 0u;
+  __syncthreads();
   bool nan = false;
-  for (uint32_t p = threadIdx.x; p < (uint32_t)XN; p += XST) {
-    if (p < nloc) {
+  uint32_t mn[DIM], mx[DIM];
 #pragma unroll
-      for (int w = 0; w < DIM; ++w) {
-        const uint32_t v = __ldcs(src.base + (uint64_t)w * src.stride + base + p);
-        nan |= is_nan_bits(v);
-        recs[w * XN + p] = v;
-      }
-      const uint32_t id = __ldcs(src.ids + base + p);
-      recs[DIM * XN + p] = id;
-      keys[p] = ((unsigned long long)id << 12) | p;
-    } else {
-      keys[p] = ~0ull;
+  for (int w = 0; w < DIM; ++w) {
+    mn[w] = 0xffffffffu;
+    mx[w] = 0u;
+  }
+  for (uint32_t p = threadIdx.x; p < nloc; p += XST) {
+#pragma unroll
+    for (int w = 0; w < DIM; ++w) {
+      const uint32_t v = __ldcs(src.base + (uint64_t)w * src.stride + base + p);
+      nan |= is_nan_bits(v);
+      recs[w * XN + p] = v;
+      const uint32_t m = mono_bits(v);
+      mn[w] = min(mn[w], m);
+      mx[w] = max(mx[w], m);
     }
+    recs[DIM * XN + p] = __ldcs(src.ids + base + p);
   }
   if (nan) atomicOr(err, ERRB_NAN);
+#pragma unroll
+  for (int w = 0; w < DIM; ++w) {
+    const uint32_t a = __reduce_min_sync(0xffffffffu, mn[w]), b = __reduce_max_sync(0xffffffffu, mx[w]);
+    if ((threadIdx.x & 31u) == 0u) {
+      atomicMin(&s_mn[w], a);
+      atomicMax(&s_mx[w], b);
+    }
+  }
   __syncthreads();
   XPROF_T(tp0);
-  {
-    const unsigned long long* sk = cta_sort<XN>(keys, keys + XN);
-    for (uint32_t r = threadIdx.x; r < nloc; r += XST) eofr[r] = (uint16_t)(sk[r] & 0xfffu);
-    __syncthreads();
+  // 2. one list of slots per dimension, in the reference's order (coordinate,
+  // then id: FKDTree_cpu.h:246-252).  Fast path, when every dimension's order
+  // bits span less than 2^22 - 1 (a subtree is a small cell): 32-bit keys
+  // (bits - min) << 10 | slot, then the runs of equal coordinates -- sorted
+  // by slot -- are re-ordered by id, one thread per run.  A run longer than
+  // TIE_RUN, or a wider range, takes the exact path: a sort by id gives each
+  // point its id rank r, then 64-bit keys (bits << 12 | r).
+  constexpr uint32_t TIE_RUN = 32;
+  static_assert(XN <= 1024, "the 32-bit keys carry a 10-bit slot");
+  bool fast = true;
+#pragma unroll
+  for (int w = 0; w < DIM; ++w) fast &= (s_mx[w] - s_mn[w]) < (1u << 22) - 1u || s_mn[w] > s_mx[w];
+  if (fast) {
+    uint32_t* k32 = (uint32_t*)keys;
+#pragma unroll 1
+    for (int c = 0; c < DIM; ++c) {
+      const uint32_t m0 = s_mn[c];
+      for (uint32_t r = threadIdx.x; r < (uint32_t)XN; r += XST)
+        k32[r] = r < nloc ? (((mono_bits(recs[c * XN + r]) - m0) << 10) | r) : 0xffffffffu;
+      __syncthreads();
+      const uint32_t* sk = cta_sort<XN, uint32_t>(k32, k32 + XN);
+      uint16_t* lc = lists + (size_t)c * 2 * XN;
+      for (uint32_t q = threadIdx.x; q < nloc; q += XST) lc[q] = (uint16_t)(sk[q] & 0x3ffu);
+      __syncthreads();
+      // runs of equal coordinates: each run's first position re-orders it by id
+      // (the others of a run hold the same coordinate, whatever their order)
+      const uint32_t* cx = recs + (size_t)c * XN;
+      const uint32_t* idv = recs + (size_t)DIM * XN;
+      for (uint32_t q = threadIdx.x; q < nloc; q += XST) {
+        const uint32_t mq = mono_bits(cx[lc[q]]);
+        if (q > 0u && mono_bits(cx[lc[q - 1u]]) == mq) continue;  // not the start of a run
+        uint32_t e = q + 1u;
+        while (e < nloc && e - q <= TIE_RUN && mono_bits(cx[lc[e]]) == mq) ++e;
+        if (e - q > TIE_RUN) {
+          s_slow = 1u;
+          continue;
+        }
+        for (uint32_t x = q + 1u; x < e; ++x) {  // insertion sort of [q, e) by id
+          const uint16_t sv = lc[x];
+          const uint32_t key = idv[sv];
+          uint32_t y = x;
+          while (y > q && idv[lc[y - 1u]] > key) {
+            lc[y] = lc[y - 1u];
+            --y;
+          }
+          lc[y] = sv;
+        }
+      }
+      __syncthreads();
+    }
+    fast = s_slow == 0u;
   }
   XPROF_T(tp1);
-  // 2. one sorted list per dimension: keys (order bits, id rank)
+  if (!fast) {
+    // exact path: id ranks (eofr[r] = slot of the r-th smallest id)
+    for (uint32_t p = threadIdx.x; p < (uint32_t)XN; p += XST)
+      keys[p] = p < nloc ? (((unsigned long long)recs[DIM * XN + p] << 12) | p) : ~0ull;
+    __syncthreads();
+    {
+      const unsigned long long* sk = cta_sort<XN, unsigned long long>(keys, keys + XN);
+      for (uint32_t r = threadIdx.x; r < nloc; r += XST) eofr[r] = (uint16_t)(sk[r] & 0xfffu);
+      __syncthreads();
+    }
 #pragma unroll 1
-  for (int c = 0; c < DIM; ++c) {
-    for (uint32_t r = threadIdx.x; r < (uint32_t)XN; r += XST)
-      keys[r] = r < nloc ? (((unsigned long long)mono_bits(recs[c * XN + eofr[r]]) << 12) | r) : ~0ull;
-    __syncthreads();
-    const unsigned long long* sk = cta_sort<XN>(keys, keys + XN);
-    uint16_t* lc = lists + (size_t)c * 2 * XN;
-    for (uint32_t p = threadIdx.x; p < nloc; p += XST) lc[p] = (uint16_t)(sk[p] & 0xfffu);
-    __syncthreads();
+    for (int c = 0; c < DIM; ++c) {
+      for (uint32_t r = threadIdx.x; r < (uint32_t)XN; r += XST)
+        keys[r] = r < nloc ? (((unsigned long long)mono_bits(recs[c * XN + eofr[r]]) << 12) | r) : ~0ull;
+      __syncthreads();
+      const unsigned long long* sk = cta_sort<XN, unsigned long long>(keys, keys + XN);
+      uint16_t* lc = lists + (size_t)c * 2 * XN;
+      for (uint32_t q = threadIdx.x; q < nloc; q += XST) lc[q] = eofr[sk[q] & 0xfffu];  // id rank -> slot
+      __syncthreads();
+    }
   }
   XPROF_T(tp2);
   // 3. levels
@@ -320,7 +397,7 @@ __global__ void __launch_bounds__(XN / XPPT, 4096 / XN) k_subtree_sorted(const E
       if (p == pv) {
         side[r] = SP;
         sgn[p] = GAP;
-        const uint32_t e = eofr[r];
+        const uint32_t e = r;  // the lists hold slots
         uint32_t rec[DIM + 1];
 #pragma unroll
         for (int w = 0; w <= DIM; ++w) rec[w] = recs[w * XN + e];
