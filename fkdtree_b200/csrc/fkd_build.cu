@@ -796,10 +796,12 @@ __global__ void k_small_fix(uint32_t d, const EvDesc* __restrict__ evs, const ui
 //
 // For levels whose segments all hold at most SEL_MAX points, one CTA selects
 // a whole segment: its split coordinate is loaded into shared memory once and
-// every digit pass (value bits, then id bits for points that tie on the
-// value) runs there -- one launch per level instead of a digit pass launch
-// per 11 bits with a global histogram flush each.  Same digits and the same
-// final SegSel as the k_hist passes, so k_partition is unchanged.
+// every pass runs there -- one launch per level instead of a digit pass
+// launch per 11 bits with a global histogram flush each.  With parking on
+// (the partition may leave up to SMALL_CAP candidates to k_small_fix), the
+// passes narrow a value interval until it holds at most SMALL_CAP points,
+// usually after one pass; otherwise (or for a value held by more points) the
+// digit passes of the k_hist select fix the pivot key exactly.
 constexpr int SEL_MAX = 32768;
 constexpr int SELT = 512;  // threads
 constexpr int SELB = 4;    // bins per thread (2,048 bins)
@@ -807,12 +809,13 @@ constexpr int SELB = 4;    // bins per thread (2,048 bins)
 template <int DIM>
 __global__ void __launch_bounds__(SELT) k_select_small(uint32_t d, const EvDesc* __restrict__ evs,
                                                        const uint2* __restrict__ segs, CSoA src,
-                                                       SegSel* __restrict__ sel, uint32_t* __restrict__ err) {
+                                                       SegSel* __restrict__ sel, uint32_t* __restrict__ err,
+                                                       bool park) {
   extern __shared__ uint32_t vals[];  // mono bits of the segment's split coordinate
   __shared__ uint32_t hist[SELT * SELB];
   __shared__ uint32_t wsum[SELT / 32];
   __shared__ unsigned long long s_prefix;
-  __shared__ uint32_t s_bits, s_krem, s_cnt;
+  __shared__ uint32_t s_bits, s_krem, s_cnt, s_lo, s_hi, s_park;
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   const uint32_t s = blockIdx.x;
   if (sel[s].done) return;
@@ -826,14 +829,110 @@ __global__ void __launch_bounds__(SELT) k_select_small(uint32_t d, const EvDesc*
   }
   const uint32_t c = d % DIM;
   const uint32_t* X = src.base + (uint64_t)c * src.stride + start;
-  for (uint32_t p = threadIdx.x; p < len; p += SELT) vals[p] = mono_bits(__ldcs(X + p));
+  uint32_t vmn = 0xffffffffu, vmx = 0u;
+  for (uint32_t p = threadIdx.x; p < len; p += SELT) {
+    const uint32_t v = mono_bits(__ldcs(X + p));
+    vals[p] = v;
+    vmn = min(vmn, v);
+    vmx = max(vmx, v);
+  }
   if (threadIdx.x == 0) {
     s_prefix = sel[s].prefix;
     s_bits = sel[s].bits;
     s_krem = sel[s].krem;
     s_cnt = sel[s].cnt;
+    s_lo = 0xffffffffu;
+    s_hi = 0u;
+    s_park = 0u;
   }
   __syncthreads();
+  vmn = __reduce_min_sync(0xffffffffu, vmn);
+  vmx = __reduce_max_sync(0xffffffffu, vmx);
+  if (lane == 0u) {
+    atomicMin(&s_lo, vmn);
+    atomicMax(&s_hi, vmx);
+  }
+  __syncthreads();
+  // interval passes (when the partition may park candidates): bins of
+  // 2^sh values of the order bits over [lo, hi], sh the smallest shift that
+  // leaves at most 2,048 bins; the bin holding rank krem becomes the interval
+  // (clipped to hi).  Usually one pass leaves at most SMALL_CAP candidates:
+  // the partition parks them and k_small_fix orders them by the full key.
+  // A single value held by more than SMALL_CAP points continues below with
+  // the id digits.
+  if (park && s_bits < 32u) {
+    for (int guard = 0; guard < 4; ++guard) {
+      const uint32_t lo = s_lo, hi = s_hi, cnt = s_cnt, krem = s_krem;
+      if (cnt <= SMALL_CAP || lo >= hi) break;
+      const uint32_t rb = 32u - (uint32_t)__clz(hi - lo);
+      const uint32_t sh = rb > 11u ? rb - 11u : 0u;
+      const uint32_t nb = ((hi - lo) >> sh) + 1u;
+      for (uint32_t i = threadIdx.x; i < nb; i += SELT) hist[i] = 0u;
+      __syncthreads();
+      for (uint32_t p = threadIdx.x; p < len; p += SELT) {
+        const uint32_t v = vals[p];
+        if (v >= lo && v <= hi) atomicAdd(&hist[(v - lo) >> sh], 1u);
+      }
+      __syncthreads();
+      uint32_t h[SELB], mine = 0u;
+#pragma unroll
+      for (int k = 0; k < SELB; ++k) {
+        const uint32_t b = threadIdx.x * SELB + k;
+        h[k] = b < nb ? hist[b] : 0u;
+        mine += h[k];
+      }
+      uint32_t incl = mine;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (uint32_t)o) incl += y;
+      }
+      if (lane == 31u) wsum[warp] = incl;
+      __syncthreads();
+      uint32_t cum = incl - mine;
+      for (uint32_t k = 0; k < warp; ++k) cum += wsum[k];
+      if (krem >= cum && krem < cum + mine) {
+#pragma unroll
+        for (int k = 0; k < SELB; ++k) {
+          const uint32_t b = threadIdx.x * SELB + k;
+          if (b < nb && krem >= cum && krem < cum + h[k]) {
+            const uint32_t nlo = lo + (b << sh);
+            s_lo = nlo;
+            s_hi = (uint32_t)min((unsigned long long)hi, (unsigned long long)nlo + ((1ull << sh) - 1ull));
+            s_krem = krem - cum;
+            s_cnt = h[k];
+          }
+          cum += h[k];
+        }
+      }
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      if (s_cnt <= SMALL_CAP) {
+        s_park = 1u;
+      } else if (s_lo == s_hi) {  // one value: its id digits next
+        s_bits = 32u;
+        s_prefix = s_lo;
+      } else {  // not reached: four passes of 11 bits fix a 32-bit value
+        atomicOr(err, ERRB_INTERNAL);
+        s_park = 1u;
+      }
+    }
+    __syncthreads();
+    if (s_park) {
+      if (threadIdx.x == 0) {
+        SegSel* p = &sel[s];
+        p->klo = (unsigned long long)s_lo << 32;
+        p->khi = ((unsigned long long)s_hi << 32) | 0xffffffffull;
+        p->krem = s_krem;
+        p->cnt = s_cnt;
+        p->small = s_cnt > 1u ? 1u : 0u;
+        p->done = 1u;
+        if (s_cnt == 0u) atomicOr(err, ERRB_INTERNAL);
+      }
+      return;
+    }
+  }
   for (int guard = 0; guard < 8; ++guard) {
     const uint32_t bits = s_bits, cnt = s_cnt, krem = s_krem;
     const unsigned long long prefix = s_prefix;
@@ -1377,7 +1476,8 @@ static cudaError_t run_build(BuildCtx& bc) {
       const size_t sm = (size_t)lp.maxlen * sizeof(uint32_t);
       cudaError_t e = cudaFuncSetAttribute(k_select_small<DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
       if (e != cudaSuccess) return e;
-      k_select_small<DIM><<<lp.nseg, SELT, sm, bc.stream>>>(d, bc.evs, lp.segs, src, bc.sel, bc.err);
+      k_select_small<DIM><<<lp.nseg, SELT, sm, bc.stream>>>(d, bc.evs, lp.segs, src, bc.sel, bc.err,
+                                                            bc.tiebuf != nullptr);
       count_launches(1);
     } else if (lc.params) {
       cudaError_t e = mlp_infer(lc.params, lc.feat, lp.nseg, lc.yhat, bc.stream);
@@ -1397,7 +1497,7 @@ static cudaError_t run_build(BuildCtx& bc) {
     k_partition<DIM><<<lp.nptile, GT, 0, bc.stream>>>(d, bc.evs, lp.segs, lp.ptiles, src, dst, bc.sel, bc.tab,
                                                         bc.err, bnd_out, lp.child, bc.tiebuf);
     count_launches(1);
-    if (bc.tiebuf && !small) {
+    if (bc.tiebuf) {
       k_small_fix<DIM><<<(lp.nseg + 7) / 8, 256, 0, bc.stream>>>(d, bc.evs, lp.segs, lp.nseg, bc.sel, bc.tiebuf, dst,
                                                                 bc.tab, bc.err, bnd_out, lp.child);
       count_launches(1);

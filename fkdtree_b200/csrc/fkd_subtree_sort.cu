@@ -290,48 +290,52 @@ __global__ void __launch_bounds__(XN / XPPT, 4096 / XN) k_subtree_sorted(const E
   __syncthreads();
   XPROF_T(tp0);
   // 2. one list of slots per dimension, in the reference's order (coordinate,
-  // then id: FKDTree_cpu.h:246-252).  Fast path, when every dimension's order
-  // bits span less than 2^22 - 1 (a subtree is a small cell): 32-bit keys
-  // (bits - min) << 10 | slot, then the runs of equal coordinates -- sorted
-  // by slot -- are re-ordered by id, one thread per run.  A run longer than
-  // TIE_RUN, or a wider range, takes the exact path: a sort by id gives each
-  // point its id rank r, then 64-bit keys (bits << 12 | r).
+  // then id: FKDTree_cpu.h:246-252).  Fast path: 32-bit keys
+  // ((bits - min) >> sh) << 10 | slot, sh the smallest shift that brings the
+  // dimension's range of order bits below 2^21, sort, then each run of equal
+  // shifted keys -- sorted by slot -- is re-ordered by the full (bits, id) key,
+  // one thread per run (a subtree is a small cell: sh is 0 and runs are rare
+  // unless the cell reaches down to zero).  A run longer than TIE_RUN takes
+  // the exact path: a sort by id gives each point its id rank r, then 64-bit
+  // keys (bits << 12 | r).
   constexpr uint32_t TIE_RUN = 32;
   static_assert(XN <= 1024, "the 32-bit keys carry a 10-bit slot");
   bool fast = true;
-#pragma unroll
-  for (int w = 0; w < DIM; ++w) fast &= (s_mx[w] - s_mn[w]) < (1u << 22) - 1u || s_mn[w] > s_mx[w];
-  if (fast) {
+  {
     uint32_t* k32 = (uint32_t*)keys;
+    const uint32_t* idv = recs + (size_t)DIM * XN;
 #pragma unroll 1
     for (int c = 0; c < DIM; ++c) {
       const uint32_t m0 = s_mn[c];
+      const uint32_t rb = nloc ? 32u - (uint32_t)__clz(s_mx[c] - m0) : 0u;  // bit length of the range
+      const uint32_t sh = rb > 21u ? rb - 21u : 0u;
       for (uint32_t r = threadIdx.x; r < (uint32_t)XN; r += XST)
-        k32[r] = r < nloc ? (((mono_bits(recs[c * XN + r]) - m0) << 10) | r) : 0xffffffffu;
+        k32[r] = r < nloc ? ((((mono_bits(recs[c * XN + r]) - m0) >> sh) << 10) | r) : 0xffffffffu;
       __syncthreads();
       const uint32_t* sk = cta_sort<XN, uint32_t>(k32, k32 + XN);
       uint16_t* lc = lists + (size_t)c * 2 * XN;
       for (uint32_t q = threadIdx.x; q < nloc; q += XST) lc[q] = (uint16_t)(sk[q] & 0x3ffu);
       __syncthreads();
-      // runs of equal coordinates: each run's first position re-orders it by id
-      // (the others of a run hold the same coordinate, whatever their order)
+      // runs of equal shifted keys: each run's first position re-orders it by
+      // the full key (the positions of a run are one block of the order)
       const uint32_t* cx = recs + (size_t)c * XN;
-      const uint32_t* idv = recs + (size_t)DIM * XN;
       for (uint32_t q = threadIdx.x; q < nloc; q += XST) {
-        const uint32_t mq = mono_bits(cx[lc[q]]);
-        if (q > 0u && mono_bits(cx[lc[q - 1u]]) == mq) continue;  // not the start of a run
+        const uint32_t mq = (mono_bits(cx[lc[q]]) - m0) >> sh;
+        if (q > 0u && ((mono_bits(cx[lc[q - 1u]]) - m0) >> sh) == mq) continue;  // not the start of a run
         uint32_t e = q + 1u;
-        while (e < nloc && e - q <= TIE_RUN && mono_bits(cx[lc[e]]) == mq) ++e;
+        while (e < nloc && e - q <= TIE_RUN && ((mono_bits(cx[lc[e]]) - m0) >> sh) == mq) ++e;
         if (e - q > TIE_RUN) {
           s_slow = 1u;
           continue;
         }
-        for (uint32_t x = q + 1u; x < e; ++x) {  // insertion sort of [q, e) by id
+        for (uint32_t x = q + 1u; x < e; ++x) {  // insertion sort of [q, e) by (bits, id)
           const uint16_t sv = lc[x];
-          const uint32_t key = idv[sv];
+          const unsigned long long key = ((unsigned long long)mono_bits(cx[sv]) << 32) | idv[sv];
           uint32_t y = x;
-          while (y > q && idv[lc[y - 1u]] > key) {
-            lc[y] = lc[y - 1u];
+          while (y > q) {
+            const uint16_t pw = lc[y - 1u];
+            if ((((unsigned long long)mono_bits(cx[pw]) << 32) | idv[pw]) <= key) break;
+            lc[y] = pw;
             --y;
           }
           lc[y] = sv;
@@ -364,12 +368,14 @@ __global__ void __launch_bounds__(XN / XPPT, 4096 / XN) k_subtree_sorted(const E
     }
   }
   XPROF_T(tp2);
-  // 3. levels
+  // 3. levels: with the whole CTA down to dT, the first level whose segments
+  // all hold at most 31 points; from there a warp per segment (section 4)
+  const uint32_t dT = g.H >= d0 + 4u ? g.H - 4u : d0;
   int cur[4] = {0, 0, 0, 0};  // which buffer of each list is current
   int sbuf = 0;
   for (uint32_t p = threadIdx.x; p < (uint32_t)XN; p += XST) segb[p] = p < nloc ? 0u : GAP;
   __syncthreads();
-  for (uint32_t d = d0; d <= g.H; ++d) {
+  for (uint32_t d = d0; d < dT; ++d) {
     const uint32_t j = d - d0;
     const uint32_t t0 = s0 << j;
     const uint32_t c = d % DIM;
@@ -480,6 +486,97 @@ __global__ void __launch_bounds__(XN / XPPT, 4096 / XN) k_subtree_sorted(const E
     if (DIM > 2) cur[o2] ^= 1;
     sbuf ^= 1;
     __syncthreads();
+  }
+  // 4. the last levels, a warp per segment of level dT (at most 31 points):
+  // lane l holds position ls + l of every list; each level's pivot is the
+  // split list's entry at ls' + k' of its sub-segment, the other lists are
+  // partitioned stably with ballots inside each sub-segment and permuted
+  // through a per-warp staging buffer
+  {
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    constexpr uint32_t XW = (uint32_t)XST / 32u;
+    uint16_t* stg = (uint16_t*)keys + warp * 32u;  // the sort keys are no longer needed
+    const uint32_t lt = (1u << lane) - 1u;
+    const uint32_t tT = s0 << (dT - d0);
+    for (uint32_t u = warp; u < (1u << (dT - d0)); u += XW) {
+      uint32_t ls, m, k;
+      seg_local(g, dT, tT + u, base, ls, m, k);
+      if (m == 0u) continue;
+      if (m > 31u || ls + m > nloc) {
+        if (lane == 0) atomicOr(err, ERRB_INTERNAL);
+        continue;
+      }
+      bool live = lane < m;
+      uint32_t L[DIM];
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) {
+        L[c] = live ? lists[((size_t)c * 2 + cur[c]) * XN + ls + lane] : 0u;
+        if (L[c] >= nloc) {  // not a slot of this subtree: broken invariant
+          atomicOr(err, ERRB_INTERNAL);
+          live = false;
+          L[c] = 0u;
+        }
+      }
+      uint32_t v = 0u;  // the lane's sub-segment, relative to this segment
+      for (uint32_t d = dT; d <= g.H; ++d) {
+        const uint32_t c = d % DIM;
+        const uint32_t t = ((tT + u) << (d - dT)) + v;
+        uint32_t ls2 = 0u, m2 = 0u, k2 = 0u;
+        if (live) seg_local(g, d, t, base, ls2, m2, k2);
+        const uint32_t P = ls + lane, pv = ls2 + k2;
+        if (live && (P < ls2 || P >= ls2 + m2)) {  // a lane outside its sub-segment: broken invariant
+          atomicOr(err, ERRB_INTERNAL);
+          live = false;
+        }
+        // the split list: pivots to the table, every element's side
+#pragma unroll
+        for (int cc = 0; cc < DIM; ++cc) {
+          if (cc != (int)c) continue;
+          if (live) {
+            const uint32_t e = L[cc];
+            side[e] = P < pv ? SL : (P > pv ? SR : SP);
+            if (P == pv) {
+              uint32_t rec[DIM + 1];
+#pragma unroll
+              for (int w = 0; w <= DIM; ++w) rec[w] = recs[w * XN + e];
+              uint4 nv;
+              nv.x = rec[0];
+              nv.y = DIM > 1 ? rec[1] : 0u;
+              nv.z = DIM > 2 ? rec[2] : 0u;
+              nv.w = rec[DIM];
+              const uint32_t node = (1u << d) - 1u + t;
+              tab.nodes[node] = nv;
+              tab.ids[node] = rec[DIM];
+            }
+          }
+        }
+        __syncwarp();
+        // the other lists: stable partition inside each sub-segment
+        const uint32_t sub = live ? (((1u << m2) - 1u) << (ls2 - ls)) : 0u;
+#pragma unroll
+        for (int cc = 0; cc < DIM; ++cc) {
+          if (cc == (int)c || d == g.H) continue;
+          const uint32_t so = live ? side[L[cc]] : (uint32_t)SP;
+          const uint32_t bl = __ballot_sync(0xffffffffu, so == SL), br = __ballot_sync(0xffffffffu, so == SR);
+          uint32_t np = 0xffffffffu;
+          if (so == SL) np = (ls2 - ls) + __popc(bl & sub & lt);
+          else if (so == SR) np = (pv - ls) + 1u + __popc(br & sub & lt);
+          if (np != 0xffffffffu) {
+            if (np < 32u && np + ls < ls2 + m2)
+              stg[np] = (uint16_t)L[cc];
+            else
+              atomicOr(err, ERRB_INTERNAL);
+          }
+          __syncwarp();
+          if (live && P != pv) L[cc] = stg[lane];
+          __syncwarp();
+        }
+        if (live) {
+          if (P == pv) live = false;
+          else v = 2u * v + (P > pv ? 1u : 0u);
+        }
+      }
+    }
   }
   XPROF_T(tp3);
   XPROF_ADD(0, tp0, tp1);

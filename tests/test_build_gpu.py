@@ -174,3 +174,32 @@ def test_build_presorted_subtree_sizes(cuda, subn, dim, n):
     t.build()
     assert_same(t.tables(), O.build(c, ids), f"subn={subn} dim={dim} n={n}")
     t.close()
+
+
+@pytest.mark.parametrize("subn", [512, 1024])
+@pytest.mark.parametrize("dim", [1, 2, 3])
+@pytest.mark.parametrize("kind", ["wide", "near_zero", "long_runs", "short_runs"])
+def test_build_presorted_subtree_key_paths(cuda, subn, dim, kind):
+    """The presorted-list kernel's sort keys: ranges of order bits far wider
+    than a 32-bit key holds ("wide": magnitudes over 2^-40..2^40;
+    "near_zero": cells that reach down to 0), where the keys drop low bits and
+    runs of equal keys are re-ordered by (coordinate, id); runs of more than
+    32 equal coordinates ("long_runs"), which take the exact 64-bit path; and
+    runs of a few ("short_runs")."""
+    rng = np.random.default_rng(7 * dim + subn + len(kind))
+    n = 40_001
+    c = rng.random((dim, n), dtype=np.float32)
+    if kind == "wide":
+        c = (rng.standard_normal((dim, n)) * np.exp2(rng.uniform(-40, 40, (dim, n)))).astype(np.float32)
+    elif kind == "near_zero":
+        c = (rng.random((dim, n)) ** 8).astype(np.float32)
+    elif kind == "long_runs":
+        c[-1] = np.floor(c[-1] * 400) / 400  # about 100 points per value
+    else:
+        c[-1] = np.floor(c[-1] * 8000) / 8000  # about 5 points per value
+    ids = rng.permutation(n).astype(np.uint32)
+    t = F.FKDTree(c, ids)
+    t.set_param("subtree_size", subn)
+    t.build()
+    assert_same(t.tables(), O.build(c, ids), f"subn={subn} dim={dim} {kind}")
+    t.close()
