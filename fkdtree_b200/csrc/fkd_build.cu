@@ -830,7 +830,20 @@ __global__ void __launch_bounds__(SELT) k_select_small(uint32_t d, const EvDesc*
   const uint32_t c = d % DIM;
   const uint32_t* X = src.base + (uint64_t)c * src.stride + start;
   uint32_t vmn = 0xffffffffu, vmx = 0u;
-  for (uint32_t p = threadIdx.x; p < len; p += SELT) {
+  uint32_t p = threadIdx.x;
+  for (; p + 7u * SELT < len; p += 8u * SELT) {  // eight loads in flight
+    uint32_t v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) v[u] = __ldcs(X + p + u * SELT);
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const uint32_t m = mono_bits(v[u]);
+      vals[p + u * SELT] = m;
+      vmn = min(vmn, m);
+      vmx = max(vmx, m);
+    }
+  }
+  for (; p < len; p += SELT) {
     const uint32_t v = mono_bits(__ldcs(X + p));
     vals[p] = v;
     vmn = min(vmn, v);

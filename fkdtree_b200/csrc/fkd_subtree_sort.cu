@@ -219,6 +219,17 @@ __device__ __forceinline__ void seg_local(const Geom& g, uint32_t d, uint32_t t,
   }
 }
 
+// A segment's (start, length, rank) in one word: start and length up to
+// 2,047, rank up to 1,023 (subtrees of at most 1,024 points).
+__device__ __forceinline__ uint32_t seg_pack(uint32_t ls, uint32_t m, uint32_t k) {
+  return ls | (m << 11) | (k << 22);
+}
+__device__ __forceinline__ void seg_unpack(uint32_t w, uint32_t& ls, uint32_t& m, uint32_t& k) {
+  ls = w & 0x7ffu;
+  m = (w >> 11) & 0x7ffu;
+  k = w >> 22;
+}
+
 }  // namespace
 
 template <int DIM, int XN>
@@ -368,20 +379,35 @@ __global__ void __launch_bounds__(XN / XPPT, 4096 / XN) k_subtree_sorted(const E
     }
   }
   XPROF_T(tp2);
-  // 3. levels: with the whole CTA down to dT, the first level whose segments
-  // all hold at most 31 points; from there a warp per segment (section 4)
-  const uint32_t dT = g.H >= d0 + 4u ? g.H - 4u : d0;
+  // 3. levels.  Each level's segments (start, length, pivot rank) sit in a
+  // table of packed words, written during the level before (two buffers in
+  // the sort keys' space past the scan's)
+  uint32_t* segt = (uint32_t*)keys + 2u * XN;
   int cur[4] = {0, 0, 0, 0};  // which buffer of each list is current
   int sbuf = 0;
   for (uint32_t p = threadIdx.x; p < (uint32_t)XN; p += XST) segb[p] = p < nloc ? 0u : GAP;
+  if (threadIdx.x == 0) {
+    uint32_t ls, m, k;
+    seg_local(g, d0, s0, base, ls, m, k);
+    segt[0] = seg_pack(ls, m, k);
+  }
   __syncthreads();
-  for (uint32_t d = d0; d < dT; ++d) {
+  for (uint32_t d = d0; d <= g.H; ++d) {
     const uint32_t j = d - d0;
     const uint32_t t0 = s0 << j;
     const uint32_t c = d % DIM;
     const uint16_t* lc = lists + ((size_t)c * 2 + cur[c]) * XN;
     const uint16_t* sg = segb + (size_t)sbuf * XN;
     uint16_t* sgn = segb + (size_t)(sbuf ^ 1) * XN;
+    const uint32_t* T = segt + (j & 1u) * XN;
+    if (d < g.H) {  // the next level's table: 2^(j+1) <= XN segments
+      uint32_t* Tn = segt + ((j + 1u) & 1u) * XN;
+      for (uint32_t u = threadIdx.x; u < (2u << j); u += XST) {
+        uint32_t ls, m, k;
+        seg_local(g, d + 1u, (t0 << 1) + u, base, ls, m, k);
+        Tn[u] = seg_pack(ls, m, k);
+      }
+    }
     // (a) pivots and sides, from the split dimension's list
 #pragma unroll
     for (int q = 0; q < XPPT; ++q) {
@@ -392,7 +418,7 @@ __global__ void __launch_bounds__(XN / XPPT, 4096 / XN) k_subtree_sorted(const E
         continue;
       }
       uint32_t ls, m, k;
-      seg_local(g, d, t0 + u, base, ls, m, k);
+      seg_unpack(T[u], ls, m, k);
       if (p < ls || p >= ls + m) {  // a slot outside its segment: broken invariant
         atomicOr(err, ERRB_INTERNAL);
         sgn[p] = GAP;
@@ -455,7 +481,7 @@ __global__ void __launch_bounds__(XN / XPPT, 4096 / XN) k_subtree_sorted(const E
       const uint16_t u = sg[p];
       if (u == GAP) continue;
       uint32_t ls, m, k;
-      seg_local(g, d, t0 + u, base, ls, m, k);
+      seg_unpack(T[u], ls, m, k);
       const uint2 at = scan[p], st = scan[ls];
       // destinations stay inside the segment's child; anything else is a broken invariant
       uint32_t q1 = 0xffffffffu, q2 = 0xffffffffu;
@@ -486,97 +512,6 @@ __global__ void __launch_bounds__(XN / XPPT, 4096 / XN) k_subtree_sorted(const E
     if (DIM > 2) cur[o2] ^= 1;
     sbuf ^= 1;
     __syncthreads();
-  }
-  // 4. the last levels, a warp per segment of level dT (at most 31 points):
-  // lane l holds position ls + l of every list; each level's pivot is the
-  // split list's entry at ls' + k' of its sub-segment, the other lists are
-  // partitioned stably with ballots inside each sub-segment and permuted
-  // through a per-warp staging buffer
-  {
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    constexpr uint32_t XW = (uint32_t)XST / 32u;
-    uint16_t* stg = (uint16_t*)keys + warp * 32u;  // the sort keys are no longer needed
-    const uint32_t lt = (1u << lane) - 1u;
-    const uint32_t tT = s0 << (dT - d0);
-    for (uint32_t u = warp; u < (1u << (dT - d0)); u += XW) {
-      uint32_t ls, m, k;
-      seg_local(g, dT, tT + u, base, ls, m, k);
-      if (m == 0u) continue;
-      if (m > 31u || ls + m > nloc) {
-        if (lane == 0) atomicOr(err, ERRB_INTERNAL);
-        continue;
-      }
-      bool live = lane < m;
-      uint32_t L[DIM];
-#pragma unroll
-      for (int c = 0; c < DIM; ++c) {
-        L[c] = live ? lists[((size_t)c * 2 + cur[c]) * XN + ls + lane] : 0u;
-        if (L[c] >= nloc) {  // not a slot of this subtree: broken invariant
-          atomicOr(err, ERRB_INTERNAL);
-          live = false;
-          L[c] = 0u;
-        }
-      }
-      uint32_t v = 0u;  // the lane's sub-segment, relative to this segment
-      for (uint32_t d = dT; d <= g.H; ++d) {
-        const uint32_t c = d % DIM;
-        const uint32_t t = ((tT + u) << (d - dT)) + v;
-        uint32_t ls2 = 0u, m2 = 0u, k2 = 0u;
-        if (live) seg_local(g, d, t, base, ls2, m2, k2);
-        const uint32_t P = ls + lane, pv = ls2 + k2;
-        if (live && (P < ls2 || P >= ls2 + m2)) {  // a lane outside its sub-segment: broken invariant
-          atomicOr(err, ERRB_INTERNAL);
-          live = false;
-        }
-        // the split list: pivots to the table, every element's side
-#pragma unroll
-        for (int cc = 0; cc < DIM; ++cc) {
-          if (cc != (int)c) continue;
-          if (live) {
-            const uint32_t e = L[cc];
-            side[e] = P < pv ? SL : (P > pv ? SR : SP);
-            if (P == pv) {
-              uint32_t rec[DIM + 1];
-#pragma unroll
-              for (int w = 0; w <= DIM; ++w) rec[w] = recs[w * XN + e];
-              uint4 nv;
-              nv.x = rec[0];
-              nv.y = DIM > 1 ? rec[1] : 0u;
-              nv.z = DIM > 2 ? rec[2] : 0u;
-              nv.w = rec[DIM];
-              const uint32_t node = (1u << d) - 1u + t;
-              tab.nodes[node] = nv;
-              tab.ids[node] = rec[DIM];
-            }
-          }
-        }
-        __syncwarp();
-        // the other lists: stable partition inside each sub-segment
-        const uint32_t sub = live ? (((1u << m2) - 1u) << (ls2 - ls)) : 0u;
-#pragma unroll
-        for (int cc = 0; cc < DIM; ++cc) {
-          if (cc == (int)c || d == g.H) continue;
-          const uint32_t so = live ? side[L[cc]] : (uint32_t)SP;
-          const uint32_t bl = __ballot_sync(0xffffffffu, so == SL), br = __ballot_sync(0xffffffffu, so == SR);
-          uint32_t np = 0xffffffffu;
-          if (so == SL) np = (ls2 - ls) + __popc(bl & sub & lt);
-          else if (so == SR) np = (pv - ls) + 1u + __popc(br & sub & lt);
-          if (np != 0xffffffffu) {
-            if (np < 32u && np + ls < ls2 + m2)
-              stg[np] = (uint16_t)L[cc];
-            else
-              atomicOr(err, ERRB_INTERNAL);
-          }
-          __syncwarp();
-          if (live && P != pv) L[cc] = stg[lane];
-          __syncwarp();
-        }
-        if (live) {
-          if (P == pv) live = false;
-          else v = 2u * v + (P > pv ? 1u : 0u);
-        }
-      }
-    }
   }
   XPROF_T(tp3);
   XPROF_ADD(0, tp0, tp1);
