@@ -271,6 +271,11 @@ def _events_run(wb, mlp, dev, steps, plain_single, cpu_sample=0):
     b.build(coords, ids)
     b.search_digest(mins, maxs)
     out["kernels_per_batched_run"] = int(L.fkd_kernel_launches() - launches0)
+    # where one batched build's device time goes, against its CUDA-event time:
+    # the gap is what launching level by level costs
+    kt = _kernel_times(lambda: b.build(coords, ids))
+    out["batched_build_device_ms"] = {"per_kernel": kt, "sum": round(sum(v["ms"] for v in kt.values()), 3),
+                                      "launches": sum(v["launches"] for v in kt.values())}
     b.learn_stats(reset=True)
     b.build(coords, ids)
     plain_passes = b.learn_stats(reset=True)["passes"]
@@ -290,6 +295,8 @@ def _events_run(wb, mlp, dev, steps, plain_single, cpu_sample=0):
     _capi.check(L.fkd_batch_get_tables(b._h, P(tab1), P(tid1), _capi.MEM_DEVICE))
     out["learned_graph_ms"] = 1e3 * learned_s
     out["learned_build_ms"] = 1e3 * _timed(lambda: b.build(coords, ids), steps)
+    kt = _kernel_times(lambda: b.build(coords, ids))
+    out["learned_build_device_ms"] = {"per_kernel": kt, "sum": round(sum(v["ms"] for v in kt.values()), 3)}
     b.learn_stats(reset=True)
     b.build(coords, ids)
     learned_passes = b.learn_stats(reset=True)["passes"]
@@ -998,6 +1005,26 @@ def apply_knobs(L, h, items):
     for it in items:
         name, _, val = it.partition("=")
         _capi.check(L.fkd_set_param(h, name.encode(), int(val)))
+
+
+def _kernel_times(fn):
+    """Device time of every kernel (and memset / copy) one call of fn
+    launches, summed per name in ms (CUDA activity records through
+    torch.profiler; outside every timed region)."""
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+    torch.cuda.synchronize()
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        fn()
+        torch.cuda.synchronize()
+    tot, n = {}, {}
+    for e in prof.events():
+        if e.device_type == torch.autograd.DeviceType.CUDA:
+            k = e.name.split("(")[0].replace("void ", "").split("<")[0].replace("fkd::", "").strip() or "other"
+            us = e.device_time_total if hasattr(e, "device_time_total") else e.cuda_time_total
+            tot[k] = tot.get(k, 0.0) + float(us)
+            n[k] = n.get(k, 0) + 1
+    return {k: {"ms": round(v / 1e3, 3), "launches": n[k]} for k, v in sorted(tot.items(), key=lambda kv: -kv[1])}
 
 
 def level_times(args):

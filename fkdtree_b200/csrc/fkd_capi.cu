@@ -92,18 +92,20 @@ struct DevBuf {
 // host-memory calls -- its own stream; the tree tables are only read.
 struct SearchSlot {
   DevBuf qlo, qhi, counts, offsets, partials, out, tmp, digests, qorder;
-  DevBuf pool_st, pool_len, pool_s, brec, jctr, rflags, err, qctr;
+  DevBuf pool_st, pool_len, pool_s, brec, jctr, rflags, err, qctr, one;
   uint32_t* herr = nullptr;      // pinned: [0] error word, [2..3] total, [4..11] pool demand
+  uint32_t* hone = nullptr;      // pinned: the single-box search's count, flag and first ids
   cudaStream_t own = nullptr;    // stream of host-memory calls
   cudaEvent_t done = nullptr;    // the slot's last work (waited on by its next lease)
   // run pool of fkd_search, sized by the previous call's demand
   uint64_t pool_want = 0, pool_s_want = 0, brec_want = 0;
   ~SearchSlot() {
     DevBuf* all[] = {&qlo, &qhi, &counts, &offsets, &partials, &out, &tmp, &digests, &qorder,
-                     &pool_st, &pool_len, &pool_s, &brec, &jctr, &rflags, &err, &qctr};
+                     &pool_st, &pool_len, &pool_s, &brec, &jctr, &rflags, &err, &qctr, &one};
     if (own) cudaStreamSynchronize(own);
     for (DevBuf* b : all) b->release();
     if (herr) cudaFreeHost(herr);
+    if (hone) cudaFreeHost(hone);
     if (done) cudaEventDestroy(done);
     if (own) cudaStreamDestroy(own);
   }
@@ -135,6 +137,7 @@ struct fkd_tree_s {
   uint32_t search_bucket_grp = 0;  // ... of the searches with fewer than 32 lanes per box ("search_bucket_lanes")
   bool bucket_runs = true;      // unordered recorded searches merge consecutive bucket hits into runs ("bucket_runs")
   bool search_record = true;    // fkd_search records runs in the count pass ("search_record")
+  bool search_one = true;       // fkd_search of one host-memory box: one level-order warp ("search_one")
   uint64_t search_pool = 0;     // fixed pool entries ("search_pool"; 0: sized by demand)
   // tables derived from the tree on first use (in-order ids / heap indices /
   // nodes, subtree digests), built once under tree_mu; the events mark them ready
@@ -784,11 +787,75 @@ fkd_status fkd_search_write(fkd_tree h, const float* mins, const float* maxs, ui
   return finish_search(h, L, "fkd_search_write", mem);
 }
 
+}  // extern "C"
+
+namespace {
+
+// fkd_search of one host-memory box (the drop-in's search_in_the_box): one
+// launch of k_one, one copy back of its count and first ids, one wait -- in
+// place of staging, count pass, scan, write pass and their two waits.  Its
+// list is the level-order one (ascending heap index), which serves ordered
+// and unordered calls alike.  Returns FKD_ERR_STATE, without touching the
+// outputs, when the general path must answer instead: a NaN bound (whose
+// meaning the general path defines), a frontier too wide for the warp, or
+// more results than its buffer holds.
+constexpr uint32_t ONE_CAP = 1u << 16;   // ids k_one writes
+constexpr uint32_t ONE_FIRST = 1024;     // ids copied back with the count
+fkd_status search_one(fkd_tree h, const float* mins, const float* maxs, uint64_t* offsets_out, uint32_t* ids_out,
+                      uint64_t capacity, uint64_t* total) {
+  OneBox bx;
+  for (int c = 0; c < 4; ++c) bx.lo[c] = bx.hi[c] = 0.f;
+  for (int c = 0; c < h->dim; ++c) {
+    if (mins[c] != mins[c] || maxs[c] != maxs[c]) return FKD_ERR_STATE;
+    bx.lo[c] = mins[c];
+    bx.hi[c] = maxs[c];
+  }
+  DeviceScope ds(h->device);
+  Lease L;
+  fkd_status s = lease_slot(h, FKD_MEM_HOST, &L);
+  if (s != FKD_OK) return s;
+  SearchSlot* sl = L.s;
+  FKD_CUDA(sl->one.ensure((4 + ONE_CAP) * sizeof(uint32_t)));
+  if (!sl->hone) FKD_CUDA(cudaMallocHost((void**)&sl->hone, (4 + ONE_FIRST) * sizeof(uint32_t)));
+  const uint32_t cap = (uint32_t)std::min<uint64_t>(capacity, ONE_CAP);
+  const uint32_t first = std::min(cap, ONE_FIRST);
+  FKD_CUDA(launch_one(table_of(h), (uint32_t)h->n, h->dim, bx, sl->one.as<uint32_t>(), cap, L.st));
+  FKD_CUDA(cudaMemcpyAsync(sl->hone, sl->one.p, (4 + first) * sizeof(uint32_t), cudaMemcpyDeviceToHost, L.st));
+  FKD_CUDA(cudaStreamSynchronize(L.st));
+  const uint64_t tot = sl->hone[0];
+  if (sl->hone[1] || (tot > cap && tot <= capacity)) return FKD_ERR_STATE;
+  offsets_out[0] = 0;
+  offsets_out[1] = tot;
+  *total = tot;
+  if (tot > capacity) {
+    char buf[128];
+    snprintf(buf, sizeof buf, "fkd_search: %llu results exceed the capacity of %llu ids", (unsigned long long)tot,
+             (unsigned long long)capacity);
+    return fail(FKD_ERR_CAPACITY, buf);
+  }
+  if (tot && !ids_out) return fail(FKD_ERR_ARG, "null ids_out");
+  memcpy(ids_out, sl->hone + 4, std::min<uint64_t>(tot, first) * sizeof(uint32_t));
+  if (tot > first) {
+    FKD_CUDA(cudaMemcpyAsync(ids_out + first, sl->one.as<uint32_t>() + 4 + first, (tot - first) * sizeof(uint32_t),
+                             cudaMemcpyDeviceToHost, L.st));
+    FKD_CUDA(cudaStreamSynchronize(L.st));
+  }
+  return FKD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 fkd_status fkd_search(fkd_tree h, const float* mins, const float* maxs, uint64_t q, uint64_t* offsets_out,
                       uint32_t* ids_out, uint64_t capacity, uint64_t* total, int ordered, int mem) {
   fkd_status s = check_search_args(h, mins, maxs, q, mem);
   if (s != FKD_OK) return s;
   if (!offsets_out || !total) return fail(FKD_ERR_ARG, "null offsets_out or total");
+  if (q == 1 && mem == FKD_MEM_HOST && h->search_one && h->n <= 0xffffffffull) {
+    s = search_one(h, mins, maxs, offsets_out, ids_out, capacity, total);
+    if (s != FKD_ERR_STATE) return s;
+  }
   DeviceScope ds(h->device);
   Lease L;
   if ((s = lease_slot(h, mem, &L)) != FKD_OK) return s;
@@ -1187,6 +1254,11 @@ fkd_status fkd_set_param(fkd_tree h, const char* name, int64_t value) {
   if (strcmp(name, "search_record") == 0) {
     if (value != 0 && value != 1) return fail(FKD_ERR_ARG, "search_record must be 0 or 1");
     h->search_record = value != 0;
+    return FKD_OK;
+  }
+  if (strcmp(name, "search_one") == 0) {
+    if (value != 0 && value != 1) return fail(FKD_ERR_ARG, "search_one must be 0 or 1");
+    h->search_one = value != 0;
     return FKD_OK;
   }
   if (strcmp(name, "search_pool") == 0) {

@@ -212,6 +212,14 @@ struct SearchCtx {
 };
 
 cudaError_t launch_search(SearchCtx& sc, int dim, int mode);
+// One box searched by one warp, level by level (no count pass): out[0] the
+// result count, out[1] a frontier overflow flag, out[4 ..] the first cap ids
+// in ascending heap order.
+struct OneBox {
+  float lo[4], hi[4];
+};
+cudaError_t launch_one(const Table& tab, uint32_t n, int dim, const OneBox& bx, uint32_t* out, uint32_t cap,
+                       cudaStream_t stream);
 // Writes the results of the runs a recording count pass stored (no-op without a pool).
 cudaError_t launch_expand(const SearchCtx& sc);
 // Fills tab.dids / tab.dnode (in-order tables; required by SEARCH_WRITE) and,

@@ -1647,4 +1647,88 @@ cudaError_t launch_order_results(const Geom& g, const Table& tab, const uint64_t
   return cudaGetLastError();
 }
 
+// One box with a host round trip (a caller that searches box by box, as the
+// reference's driver does from its TBB loop, main.cpp:351-359): a single warp
+// walks the tree level by level like search_in_the_box (FKDTree_cpu.h:
+// 123-169) -- the frontier of each depth in ascending heap order, the left
+// child visited when min <= split value, the right when split value <= max --
+// so the in-box nodes come out in ascending heap order, the reference's list,
+// with no count pass, scan or sort.  out[0] = results (all of them, also past
+// cap), out[1] = 1 when a depth's frontier outgrew ONE_FRONTIER (the caller
+// then takes the general path), out[4 ..] = the first cap ids.
+constexpr uint32_t ONE_FRONTIER = 2048;
+template <int DIM>
+__global__ void __launch_bounds__(32) k_one(Table tab, uint32_t n, OneBox bx, uint32_t* __restrict__ out,
+                                            uint32_t cap) {
+  __shared__ uint32_t fr[2][ONE_FRONTIER];
+  const uint32_t lane = threadIdx.x;
+  const uint32_t lt = (1u << lane) - 1u;
+  uint32_t nf = n ? 1u : 0u, total = 0u, cur = 0u;
+  bool ovf = false;
+  if (lane == 0) fr[0][0] = 0u;
+  __syncwarp();
+  for (uint32_t d = 0; nf > 0u && !ovf; ++d) {
+    const uint32_t c = d % DIM;
+    uint32_t nn = 0u;
+    for (uint32_t b0 = 0; b0 < nf; b0 += 32u) {
+      const uint32_t i = b0 + lane;
+      const bool v = i < nf;
+      const uint32_t node = v ? fr[cur][i] : 0u;
+      uint4 p = make_uint4(0u, 0u, 0u, 0u);
+      if (v) p = __ldg(tab.nodes + node);
+      const float x[4] = {__uint_as_float(p.x), __uint_as_float(p.y), __uint_as_float(p.z), __uint_as_float(p.w)};
+      bool in = v;
+#pragma unroll
+      for (int w = 0; w < DIM; ++w) in &= bx.lo[w] <= x[w] && x[w] <= bx.hi[w];
+      const float sv = sel4(c, x[0], x[1], x[2], x[3]);
+      const float lo = sel4(c, bx.lo[0], bx.lo[1], bx.lo[2], bx.lo[3]);
+      const float hi = sel4(c, bx.hi[0], bx.hi[1], bx.hi[2], bx.hi[3]);
+      const bool l = v && 2ull * node + 1ull < n && lo <= sv;
+      const bool r = v && 2ull * node + 2ull < n && sv <= hi;
+      const uint32_t bin = __ballot_sync(0xffffffffu, in);
+      const uint32_t at = total + __popc(bin & lt);
+      if (in && at < cap) out[4 + at] = __ldg(tab.ids + node);
+      total += __popc(bin);
+      // children in lane order, left before right: ascending heap order
+      const uint32_t k = (l ? 1u : 0u) + (r ? 1u : 0u);
+      uint32_t incl = k;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (uint32_t)o) incl += y;
+      }
+      const uint32_t q0 = nn + incl - k;
+      const uint32_t add = __shfl_sync(0xffffffffu, incl, 31);
+      if (nn + add > ONE_FRONTIER) {
+        ovf = true;  // warp-uniform
+        break;
+      }
+      uint32_t q = q0;
+      if (l) fr[cur ^ 1u][q++] = 2u * node + 1u;
+      if (r) fr[cur ^ 1u][q] = 2u * node + 2u;
+      nn += add;
+    }
+    __syncwarp();
+    cur ^= 1u;
+    nf = nn;
+  }
+  if (lane == 0) {
+    out[0] = total;
+    out[1] = ovf ? 1u : 0u;
+  }
+}
+
+cudaError_t launch_one(const Table& tab, uint32_t n, int dim, const OneBox& bx, uint32_t* out, uint32_t cap,
+                       cudaStream_t stream) {
+  switch (dim) {
+    case 1: k_one<1><<<1, 32, 0, stream>>>(tab, n, bx, out, cap); break;
+    case 2: k_one<2><<<1, 32, 0, stream>>>(tab, n, bx, out, cap); break;
+    case 3: k_one<3><<<1, 32, 0, stream>>>(tab, n, bx, out, cap); break;
+    case 4: k_one<4><<<1, 32, 0, stream>>>(tab, n, bx, out, cap); break;
+    default: return cudaErrorInvalidValue;
+  }
+  count_launches(1);
+  return cudaGetLastError();
+}
+
 }  // namespace fkd

@@ -226,6 +226,11 @@ FKD_API fkd_status fkd_sync(fkd_tree h);
  *                   select each segment with one CTA in shared memory
  *   "search_record" (0/1, default 1): fkd_search's count pass records every
  *                   box's result so that the write needs no second traversal
+ *   "search_one"    (0/1, default 1): fkd_search of a single host-memory box
+ *                   runs one warp over the tree level by level (the level-order
+ *                   list straight away, one launch and one wait); boxes with a
+ *                   NaN bound, very wide frontiers or more than 65,536 results
+ *                   take the general count + write path
  *   "search_pool"   entries of the record pools (0, the default: sized by the
  *                   previous call's demand; boxes that do not fit are traversed
  *                   again, so any size gives the same results)

@@ -248,3 +248,57 @@ def test_leaf_buckets_with_lanes_per_box_equal_walk(cuda, dim):
             cc, dd = t.digest_boxes(mins, maxs)
             assert np.array_equal(cc, wc) and np.array_equal(dd, wd), f"lanes {lanes} bucket {b}"
     t.close()
+
+
+@pytest.mark.parametrize("dim", [1, 2, 3, 4])
+def test_single_box_fast_path(cuda, dim):
+    """fkd_search of one host-memory box (the drop-in's search_in_the_box)
+    runs one warp level by level ("search_one"); its lists equal the
+    reference's level-order lists and the general count + write path's, for
+    empty boxes, boxes past the 1,024 ids copied back with the count, boxes
+    whose frontier outgrows the warp's buffer or whose results outgrow its
+    65,536 ids (both answered by the general path), NaN bounds (general path)
+    and a capacity too small (FKD_ERR_CAPACITY with the true total)."""
+    import ctypes as C
+
+    from fkdtree_b200 import _capi
+    rng = np.random.default_rng(40 + dim)
+    n = 100_000
+    c = rng.random((dim, n), dtype=np.float32)
+    c[-1] = np.round(c[-1] * 64) / 64  # ties
+    ids = rng.permutation(n).astype(np.uint32) * 3 + 1
+    t = F.FKDTree(c, ids).build()
+    tab, tid = t.tables()
+    q = 160
+    ctr = rng.random((dim, q), dtype=np.float32)
+    hw = np.exp(rng.uniform(np.log(0.002), np.log(0.4), (1, q))).astype(np.float32)
+    mins, maxs = ctr - hw, ctr + hw
+    mins[:, 0], maxs[:, 0] = -np.inf, np.inf  # the whole tree: more than 65,536 results
+    mins[:, 1], maxs[:, 1] = 0.0, 1.0
+    maxs[-1, 1] = 0.3  # about 30,000 results, a frontier far wider than 2,048 nodes
+    mins[:, 2], maxs[:, 2] = 0.5, 0.4  # empty (min > max)
+    mins[0, 3] = np.nan  # NaN bound
+    mins, maxs = np.ascontiguousarray(mins), np.ascontiguousarray(maxs)
+    _, wo, wi, _ = O.search(tab, tid, mins, maxs, variant=O.LEVEL_ORDER)
+    want = slices(wo, wi)
+    assert len(want[0]) == n and len(want[1]) > 1024
+    for knob in (1, 0):
+        t.set_param("search_one", knob)
+        for j in range(q):
+            got = t.search_in_the_box(mins[:, j], maxs[:, j])
+            assert np.array_equal(got, want[j]), f"search_one={knob} box {j}"
+            got_u = t._one(mins[:, j], maxs[:, j], ordered=False)
+            assert np.array_equal(np.sort(got_u), np.sort(want[j])), f"unordered search_one={knob} box {j}"
+    t.set_param("search_one", 1)
+    L = _capi.lib()
+    j = int(np.argmax([len(w) for w in want[2:]])) + 2
+    lo = np.ascontiguousarray(mins[:, j])
+    hi = np.ascontiguousarray(maxs[:, j])
+    offs = np.zeros(2, dtype=np.uint64)
+    buf = np.empty(1, dtype=np.uint32)
+    tot = C.c_uint64(0)
+    st = L.fkd_search(t._h, lo.ctypes.data_as(C.c_void_p), hi.ctypes.data_as(C.c_void_p), 1,
+                      offs.ctypes.data_as(C.c_void_p), buf.ctypes.data_as(C.c_void_p), 1, C.byref(tot), 1,
+                      _capi.MEM_HOST)
+    assert st == _capi.ERR_CAPACITY and tot.value == len(want[j]) and offs[1] == len(want[j])
+    t.close()
