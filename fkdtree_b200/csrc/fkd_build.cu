@@ -533,6 +533,7 @@ __global__ void __launch_bounds__(GT, FKD_PART_MINB) k_partition(uint32_t d, con
   __shared__ uint32_t sL[PIPT * GWARPS], sR[PIPT * GWARPS];
   __shared__ uint32_t sBL[PIPT * GWARPS], sBR[PIPT * GWARPS];  // the warps' left / right ballots
   __shared__ uint32_t s_base[2];
+  __shared__ uint32_t sb[4], s_arrive;  // the children's bounds, reduced over the CTA's warps
   const uint2 tl = tiles[blockIdx.x];
   const uint32_t s = tl.x, t = tl.y;
   const uint2 sd = segs[s];
@@ -541,6 +542,13 @@ __global__ void __launch_bounds__(GT, FKD_PART_MINB) k_partition(uint32_t d, con
   const uint32_t len = seg_len(eg, d, sd.y);
   const uint32_t ntiles = (len + PTILE - 1) / PTILE;
   if (t >= ntiles) return;
+  if (threadIdx.x == 0) {  // ordered before their first use by the barrier below
+    sb[0] = 0xffffffffu;
+    sb[1] = 0u;
+    sb[2] = 0xffffffffu;
+    sb[3] = 0u;
+    s_arrive = 0u;
+  }
   const uint32_t start = ebase + seg_start(eg, d, sd.y);
   const uint32_t rank = seg_rank(eg, d, sd.y);
   const uint32_t node = ebase + (1u << d) - 1u + sd.y;  // this segment's node
@@ -685,34 +693,30 @@ __global__ void __launch_bounds__(GT, FKD_PART_MINB) k_partition(uint32_t d, con
   if (ch != ~0u) {  // CTA-uniform
     // warp, then CTA reduction; one global atomic per bound per CTA (every
     // CTA of a segment hits the same two words: per-warp atomics would
-    // multiply that contention by eight)
+    // multiply that contention by eight).  No barrier: the warp that
+    // arrives last (a shared counter) sends the CTA's bounds.
     mnL = __reduce_min_sync(0xffffffffu, mnL);
     mxL = __reduce_max_sync(0xffffffffu, mxL);
     mnR = __reduce_min_sync(0xffffffffu, mnR);
     mxR = __reduce_max_sync(0xffffffffu, mxR);
-    __shared__ uint32_t sb[4];
-    if (threadIdx.x == 0) {
-      sb[0] = 0xffffffffu;
-      sb[1] = 0u;
-      sb[2] = 0xffffffffu;
-      sb[3] = 0u;
-    }
-    __syncthreads();
     if (lane == 0u) {
       atomicMin(&sb[0], mnL);
       atomicMax(&sb[1], mxL);
       atomicMin(&sb[2], mnR);
       atomicMax(&sb[3], mxR);
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      if (sb[0] <= sb[1]) {
-        atomicMin(&bnd_out[ch].x, sb[0]);
-        atomicMax(&bnd_out[ch].y, sb[1]);
-      }
-      if (sb[2] <= sb[3]) {
-        atomicMin(&bnd_out[ch + 1u].x, sb[2]);
-        atomicMax(&bnd_out[ch + 1u].y, sb[3]);
+      __threadfence_block();
+      if (atomicAdd(&s_arrive, 1u) == (uint32_t)GWARPS - 1u) {
+        __threadfence_block();
+        const uint32_t b0 = atomicAdd(&sb[0], 0u), b1 = atomicAdd(&sb[1], 0u);
+        const uint32_t b2 = atomicAdd(&sb[2], 0u), b3 = atomicAdd(&sb[3], 0u);
+        if (b0 <= b1) {
+          atomicMin(&bnd_out[ch].x, b0);
+          atomicMax(&bnd_out[ch].y, b1);
+        }
+        if (b2 <= b3) {
+          atomicMin(&bnd_out[ch + 1u].x, b2);
+          atomicMax(&bnd_out[ch + 1u].y, b3);
+        }
       }
     }
   }
@@ -803,14 +807,17 @@ __global__ void k_small_fix(uint32_t d, const EvDesc* __restrict__ evs, const ui
 // usually after one pass; otherwise (or for a value held by more points) the
 // digit passes of the k_hist select fix the pivot key exactly.
 constexpr int SEL_MAX = 32768;
-constexpr int SELT = 512;  // threads
-constexpr int SELB = 4;    // bins per thread (2,048 bins)
+constexpr int SELBINS = 2048;  // bins of a pass
+// threads: 512 for segments of more than SEL_FEW points, else 128 (short
+// CTAs: cheaper barriers, more of them resident to hide the loads)
+constexpr int SEL_FEW = 4096;
 
-template <int DIM>
+template <int DIM, int SELT>
 __global__ void __launch_bounds__(SELT) k_select_small(uint32_t d, const EvDesc* __restrict__ evs,
                                                        const uint2* __restrict__ segs, CSoA src,
                                                        SegSel* __restrict__ sel, uint32_t* __restrict__ err,
                                                        bool park) {
+  constexpr int SELB = SELBINS / SELT;  // bins per thread
   extern __shared__ uint32_t vals[];  // mono bits of the segment's split coordinate
   __shared__ uint32_t hist[SELT * SELB];
   __shared__ uint32_t wsum[SELT / 32];
@@ -1487,10 +1494,18 @@ static cudaError_t run_build(BuildCtx& bc) {
     }
     if (small) {
       const size_t sm = (size_t)lp.maxlen * sizeof(uint32_t);
-      cudaError_t e = cudaFuncSetAttribute(k_select_small<DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      const bool few = lp.maxlen <= (uint32_t)SEL_FEW;
+      cudaError_t e = few ? cudaFuncSetAttribute(k_select_small<DIM, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)sm)
+                          : cudaFuncSetAttribute(k_select_small<DIM, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)sm);
       if (e != cudaSuccess) return e;
-      k_select_small<DIM><<<lp.nseg, SELT, sm, bc.stream>>>(d, bc.evs, lp.segs, src, bc.sel, bc.err,
-                                                            bc.tiebuf != nullptr);
+      if (few)
+        k_select_small<DIM, 128><<<lp.nseg, 128, sm, bc.stream>>>(d, bc.evs, lp.segs, src, bc.sel, bc.err,
+                                                                  bc.tiebuf != nullptr);
+      else
+        k_select_small<DIM, 512><<<lp.nseg, 512, sm, bc.stream>>>(d, bc.evs, lp.segs, src, bc.sel, bc.err,
+                                                                  bc.tiebuf != nullptr);
       count_launches(1);
     } else if (lc.params) {
       cudaError_t e = mlp_infer(lc.params, lc.feat, lp.nseg, lc.yhat, bc.stream);

@@ -55,6 +55,42 @@ constexpr int XPPT = 4;  // slots per thread
 constexpr int XN_DEFAULT = 1024;
 constexpr uint16_t GAP = 0xffffu;  // a slot outside every segment (a pivot of an earlier level)
 constexpr uint8_t SL = 0, SR = 1, SP = 2;
+static_assert(XPPT == 4, "a thread's slots move as one vector");
+
+// A thread's XPPT consecutive slots move as one vector access (shared memory
+// serves a warp's 8- or 16-byte accesses without bank conflicts; four scalar
+// accesses at a stride of XPPT elements conflict).
+__device__ __forceinline__ void ld4(const uint16_t* p, uint32_t (&o)[4]) {
+  const uint2 v = *reinterpret_cast<const uint2*>(p);
+  o[0] = v.x & 0xffffu;
+  o[1] = v.x >> 16;
+  o[2] = v.y & 0xffffu;
+  o[3] = v.y >> 16;
+}
+__device__ __forceinline__ void st4(uint16_t* p, const uint32_t (&o)[4]) {
+  *reinterpret_cast<uint2*>(p) = make_uint2((o[0] & 0xffffu) | (o[1] << 16), (o[2] & 0xffffu) | (o[3] << 16));
+}
+__device__ __forceinline__ void ld4(const uint32_t* p, uint32_t (&o)[4]) {
+  const uint4 v = *reinterpret_cast<const uint4*>(p);
+  o[0] = v.x;
+  o[1] = v.y;
+  o[2] = v.z;
+  o[3] = v.w;
+}
+__device__ __forceinline__ void st4(uint32_t* p, const uint32_t (&o)[4]) {
+  *reinterpret_cast<uint4*>(p) = make_uint4(o[0], o[1], o[2], o[3]);
+}
+__device__ __forceinline__ void ld4(const unsigned long long* p, unsigned long long (&o)[4]) {
+  const ulonglong2 a = reinterpret_cast<const ulonglong2*>(p)[0], b = reinterpret_cast<const ulonglong2*>(p)[1];
+  o[0] = a.x;
+  o[1] = a.y;
+  o[2] = b.x;
+  o[3] = b.y;
+}
+__device__ __forceinline__ void st4(unsigned long long* p, const unsigned long long (&o)[4]) {
+  reinterpret_cast<ulonglong2*>(p)[0] = make_ulonglong2(o[0], o[1]);
+  reinterpret_cast<ulonglong2*>(p)[1] = make_ulonglong2(o[2], o[3]);
+}
 
 template <int DIM, int XN>
 struct XCfg {
@@ -78,8 +114,7 @@ __device__ K* cta_sort(K* a, K* b) {
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   K v[4];
   K* wbase = a + warp * 128u;
-#pragma unroll
-  for (int i = 0; i < 4; ++i) v[i] = wbase[lane * 4u + i];
+  ld4(wbase + lane * 4u, v);
 #pragma unroll
   for (uint32_t k = 2; k <= 128; k <<= 1) {
 #pragma unroll
@@ -110,8 +145,7 @@ __device__ K* cta_sort(K* a, K* b) {
       }
     }
   }
-#pragma unroll
-  for (int i = 0; i < 4; ++i) wbase[lane * 4u + i] = v[i];
+  st4(wbase + lane * 4u, v);
   K* src = a;
   K* dst = b;
   for (uint32_t s = 128; s < (uint32_t)XN; s <<= 1) {
@@ -130,19 +164,20 @@ __device__ K* cta_sort(K* a, K* b) {
         hi = mid;
     }
     uint32_t i = lo, jb = o - lo;
-    K* D = dst + pair * 2u * s + o;
+    K out[XPPT];
 #pragma unroll
     for (int q = 0; q < XPPT; ++q) {
       // an exhausted run reads as the padding key ~0 (never past its end)
       const K va = i < s ? A[i] : (K)~(K)0;
       const K vb = jb < s ? B[jb] : (K)~(K)0;
       const bool takeA = va < vb || (va == vb && i < s);
-      D[q] = takeA ? va : vb;
+      out[q] = takeA ? va : vb;
       if (takeA)
         ++i;
       else
         ++jb;
     }
+    st4(dst + pair * 2u * s + o, out);
     K* t = src;
     src = dst;
     dst = t;
@@ -193,12 +228,17 @@ __device__ uint2 cta_scan2(const uint2 (&val)[XPPT], uint2* sc, uint2* wtot) {
   __syncthreads();
   const uint2 wb = wtot[warp];
   uint32_t rx = wb.x + ix - ax, ry = wb.y + iy - ay;
+  uint32_t o[2 * XPPT];
 #pragma unroll
   for (int k = 0; k < XPPT; ++k) {
-    sc[threadIdx.x * XPPT + k] = make_uint2(rx, ry);
+    o[2 * k] = rx;
+    o[2 * k + 1] = ry;
     rx += val[k].x;
     ry += val[k].y;
   }
+  uint4* s4 = reinterpret_cast<uint4*>(sc + threadIdx.x * XPPT);
+  s4[0] = make_uint4(o[0], o[1], o[2], o[3]);
+  s4[1] = make_uint4(o[4], o[5], o[6], o[7]);
   const uint2 tot = wtot[32];
   return tot;
 }
@@ -409,26 +449,27 @@ __global__ void __launch_bounds__(XN / XPPT, 4096 / XN) k_subtree_sorted(const E
       }
     }
     // (a) pivots and sides, from the split dimension's list
+    const uint32_t pb = threadIdx.x * XPPT;  // this thread's first slot
+    uint32_t uu[XPPT], rr[XPPT], nsg[XPPT];
+    ld4(sg + pb, uu);
+    ld4(lc + pb, rr);
 #pragma unroll
     for (int q = 0; q < XPPT; ++q) {
-      const uint32_t p = threadIdx.x * XPPT + q;
-      const uint16_t u = sg[p];
-      if (u == GAP) {
-        sgn[p] = GAP;
-        continue;
-      }
+      const uint32_t p = pb + q;
+      const uint32_t u = uu[q];
+      nsg[q] = GAP;
+      if (u == GAP) continue;
       uint32_t ls, m, k;
       seg_unpack(T[u], ls, m, k);
       if (p < ls || p >= ls + m) {  // a slot outside its segment: broken invariant
         atomicOr(err, ERRB_INTERNAL);
-        sgn[p] = GAP;
+        uu[q] = GAP;
         continue;
       }
-      const uint32_t r = lc[p];
+      const uint32_t r = rr[q];
       const uint32_t pv = ls + k;
       if (p == pv) {
         side[r] = SP;
-        sgn[p] = GAP;
         const uint32_t e = r;  // the lists hold slots
         uint32_t rec[DIM + 1];
 #pragma unroll
@@ -443,9 +484,10 @@ __global__ void __launch_bounds__(XN / XPPT, 4096 / XN) k_subtree_sorted(const E
         tab.ids[node] = rec[DIM];
       } else {
         side[r] = p < pv ? SL : SR;
-        sgn[p] = (uint16_t)(2u * u + (p < pv ? 0u : 1u));
+        nsg[q] = 2u * u + (p < pv ? 0u : 1u);
       }
     }
+    st4(sgn + pb, nsg);
     if (d == g.H || DIM == 1) {
       // the last level, or a single list: the split list is the whole partition
       __syncthreads();
@@ -459,12 +501,18 @@ __global__ void __launch_bounds__(XN / XPPT, 4096 / XN) k_subtree_sorted(const E
     const uint32_t o1 = (c + 1u) % DIM, o2 = (c + 2u) % DIM;
     const uint16_t* l1 = lists + ((size_t)o1 * 2 + cur[o1]) * XN;
     const uint16_t* l2 = lists + ((size_t)o2 * 2 + cur[o2]) * XN;
+    ld4(l1 + pb, ra);
+    if (DIM > 2) {
+      ld4(l2 + pb, rb);
+    } else {
+#pragma unroll
+      for (int q = 0; q < XPPT; ++q) rb[q] = 0u;
+    }
 #pragma unroll
     for (int q = 0; q < XPPT; ++q) {
-      const uint32_t p = threadIdx.x * XPPT + q;
-      const bool live = sg[p] != GAP;
-      ra[q] = live ? l1[p] : 0u;
-      rb[q] = (live && DIM > 2) ? l2[p] : 0u;
+      const bool live = uu[q] != GAP;
+      if (!live) ra[q] = 0u;
+      rb[q] = (live && DIM > 2) ? rb[q] : 0u;
       const uint8_t s1 = live ? side[ra[q]] : SP;
       const uint8_t s2 = (live && DIM > 2) ? side[rb[q]] : SP;
       val[q].x = (s1 == SL ? 1u : 0u) | (s1 == SR ? 0x10000u : 0u);
@@ -475,14 +523,21 @@ __global__ void __launch_bounds__(XN / XPPT, 4096 / XN) k_subtree_sorted(const E
     // (c) scatter into the other buffers
     uint16_t* n1 = lists + ((size_t)o1 * 2 + (cur[o1] ^ 1)) * XN;
     uint16_t* n2 = lists + ((size_t)o2 * 2 + (cur[o2] ^ 1)) * XN;
+    uint2 sat[XPPT];
+    {
+      const uint4 a0 = reinterpret_cast<const uint4*>(scan + pb)[0], a1 = reinterpret_cast<const uint4*>(scan + pb)[1];
+      sat[0] = make_uint2(a0.x, a0.y);
+      sat[1] = make_uint2(a0.z, a0.w);
+      sat[2] = make_uint2(a1.x, a1.y);
+      sat[3] = make_uint2(a1.z, a1.w);
+    }
 #pragma unroll
     for (int q = 0; q < XPPT; ++q) {
-      const uint32_t p = threadIdx.x * XPPT + q;
-      const uint16_t u = sg[p];
+      const uint32_t u = uu[q];
       if (u == GAP) continue;
       uint32_t ls, m, k;
       seg_unpack(T[u], ls, m, k);
-      const uint2 at = scan[p], st = scan[ls];
+      const uint2 at = sat[q], st = scan[ls];
       // destinations stay inside the segment's child; anything else is a broken invariant
       uint32_t q1 = 0xffffffffu, q2 = 0xffffffffu;
       if (val[q].x & 0xffffu)
