@@ -68,6 +68,7 @@ def parse_args():
     ap.add_argument("--cpu-queries", type=int, default=8192, help="box sample of the CPU baseline")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched / learned events report")
     ap.add_argument("--no-nn", action="store_true", help="skip the radius / kNN search report")
+    ap.add_argument("--no-c1", action="store_true", help="skip the 100k-point sub-report (profiling runs)")
     ap.add_argument("--queries", type=int, default=0,
                     help="box count of the 16M-point workload (0: 1,048,576; smaller cases are for profiling)")
     ap.add_argument("--batched-events", type=int, default=4096)
@@ -596,7 +597,7 @@ def run_ours(args):
     torch.cuda.empty_cache()
     if world > 1 and not args.no_batched:
         line["sharded_events"] = sharded_events(rank, world, dev, args.batched_events)
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and not args.no_c1:
         line["c1"] = c1_report(dev, cpu=not args.no_cpu)
     if rank == 0 and world == 1 and not args.no_batched:
         line["batched"] = batched_report(dev, n_events=args.batched_events, cpu=not args.no_cpu)

@@ -831,9 +831,14 @@ constexpr int XT = 256;  // threads of k_expand
 #ifndef FKD_EXU
 #define FKD_EXU 8
 #endif
-constexpr int EXU = FKD_EXU;  // k_expand: single ids with loads in flight per lane
+// k_expand: single ids with loads in flight per lane (measured on the 16M /
+// 1M-box search: 4 / 8 / 16 -> 7.95-9.23 / 8.09 / 11.3 ms write pass)
+constexpr int EXU = FKD_EXU;
+#ifndef FKD_XMINB
+#define FKD_XMINB 1  // resident CTAs k_expand is compiled for (6 / 8 measured no better)
+#endif
 constexpr uint32_t XREC = 4;  // k_expand: chunk records a warp takes from the counter at a time
-__global__ void __launch_bounds__(XT) k_expand(const uint4* __restrict__ brec,
+__global__ void __launch_bounds__(XT, FKD_XMINB) k_expand(const uint4* __restrict__ brec,
                                                const unsigned long long* __restrict__ brec_ctr, uint64_t brec_cap,
                                                const uint32_t* __restrict__ pool_s,
                                                const uint32_t* __restrict__ pool_st,
