@@ -46,12 +46,15 @@ sys.path.insert(0, ROOT)
 
 METRIC = "build Mpoints/s + box queries/s, learned/batched vs plain GPU, exact results"
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of the recording
-# count pass + k_expand per result id, from one ncu --set full capture of the
-# same search with 65,536 boxes (2.84e8 results: 2.72 GB), scaled to a full
-# search by its results:
+# count pass + k_expand, from ncu --set full captures of the same search with
+# 65,536 boxes (2.84e8 results): the count pass reads 274.5 MB (the tree and
+# the boxes, 83% L2 hits) and writes 138.9 MB (record pools); k_expand reads
+# 601.2 MB and writes 1,087.4 MB.  A full search is modelled as that fixed
+# read plus the rest per result id:
 #   ncu --set full --clock-control none -k regex:k_expand -s 4 -c 1 python bench.py --steps 1 --warmup 4 \
-#       --queries 65536 --no-e2e --no-cpu --no-batched   (and the same for k_search<3,0,1>)
-SEARCH_DRAM_BYTES_PER_RESULT = 9.57
+#       --queries 65536 --no-e2e --no-cpu --no-batched --no-nn --no-c1   (and the same for k_search<3,0,1>)
+SEARCH_DRAM_FIXED = 274.5e6
+SEARCH_DRAM_BYTES_PER_RESULT = (138.9e6 + 601.2e6 + 1087.4e6) / 283829259
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 
@@ -124,14 +127,32 @@ class ClockSampler:
     def __init__(self, index):
         self.index = index
         self.p = None
+        self.lines = []
 
     def __enter__(self):
+        # the timed region starts only once nvidia-smi has attached and printed
+        # its first sample: a sampler starting up during a short timed step
+        # was seen to stall it (a 7.5 ms step measured 1.1 s and 16 s)
+        import threading
         try:
             self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
                                        "--format=csv,noheader,nounits", "-lms", "100"],
                                       stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.p = None
+            return self
+        first = threading.Event()
+
+        def read():
+            for line in self.p.stdout:
+                self.lines.append(line)
+                first.set()
+            first.set()
+
+        self.reader = threading.Thread(target=read, daemon=True)
+        self.reader.start()
+        first.wait(timeout=10.0)
+        self.skip = len(self.lines)  # samples taken before the timed region
         return self
 
     def __exit__(self, *a):
@@ -140,9 +161,11 @@ class ClockSampler:
             time.sleep(0.25)
             self.p.terminate()
             try:
-                self.out, _ = self.p.communicate(timeout=5)
+                self.p.wait(timeout=5)
             except Exception:
                 self.p.kill()
+            self.reader.join(timeout=5)
+            self.out = "".join(self.lines[self.skip:])
 
     def summary(self):
         rows = [r.split(",") for r in (self.out or "").strip().splitlines() if r.count(",") >= 8]
@@ -559,9 +582,10 @@ def run_ours(args):
               key=lambda k: kern[k]["ms"])
     roof = {"bound": "hbm", "kernel": dom, "achieved": kern[dom]["gbs"], "peak": peak, "unit": "GB/s",
             "frac": kern[dom]["gbs"] / peak, "peak_kind": f"{peak_kind} (copy bandwidth, MEASURED_PEAKS.json)",
-            "traffic": (SEARCH_DRAM_BYTES_PER_RESULT * results
+            "traffic": (SEARCH_DRAM_FIXED + SEARCH_DRAM_BYTES_PER_RESULT * results
                         if dom.startswith("search") and args.workload == "clustered16m" else None),
-            "traffic_note": "ncu DRAM bytes of a 65,536-box capture, scaled by results",
+            "traffic_note": ("ncu DRAM bytes of a 65,536-box capture: the count pass's tree read once plus "
+                             "6.44 B per result id (record pools written and read, ids gathered and written)"),
             "algorithmic_bytes_per_launch": kern[dom]["algorithmic_bytes"],
             "launch_ms": kern[dom]["ms"],
             "build_frac": bb / kms[2] / 1e6 / peak if kms[2] > 0 else None}

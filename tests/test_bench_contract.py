@@ -102,3 +102,23 @@ def test_c1_reference_block():
     r = rep["reference"]
     assert r["kind"] == "reference" and r["value"] > 0 and r["build_ms"] > 0
     assert "gpu" not in rep and "exact" not in rep
+
+
+def test_clock_sampler_waits_for_first_sample(tmp_path, monkeypatch):
+    """The sampler's process is running and has printed before the timed
+    region starts; samples printed before it are not counted (a fake
+    nvidia-smi on PATH stands in for the real one)."""
+    import os
+    import time
+    fake = tmp_path / "nvidia-smi"
+    fake.write_text("#!/bin/sh\nwhile true; do echo '0, 1965, 1965, 700.0, 0x0, Not Active, Not Active, "
+                    "Not Active, Not Active'; sleep 0.05; done\n")
+    fake.chmod(0o755)
+    monkeypatch.setenv("PATH", f"{tmp_path}{os.pathsep}{os.environ['PATH']}")
+    with bench.ClockSampler(0) as s:
+        assert s.lines, "no sample before the timed region"
+        t0 = time.time()
+        time.sleep(0.3)
+    assert time.time() - t0 < 10
+    r = s.summary()
+    assert r["sm_mhz"] == 1965.0 and r["reasons"] == [] and r["samples"] >= 2
