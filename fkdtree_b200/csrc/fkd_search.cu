@@ -428,6 +428,8 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
           emit_ballot(hit, node, idv);
         } else {
           acc += hit ? 1u : 0u;
+          const uint32_t hb = __ballot_sync(0xffffffffu, hit);
+          if (hb == 0u) return;  // nothing to record from this window (warp-uniform)
           if (njobs > (uint32_t)(JN - 16) || nsing > (uint32_t)(JN - 32)) {
             __syncwarp();
             flush_runs(njobs);
@@ -436,7 +438,6 @@ __global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
           // singles that carry ids cost the write pass one copy each: with
           // them every hit stays a single, unless runs are asked for
           const bool mk_runs = !sc.rec_ids || sc.bucket_runs;
-          const uint32_t hb = __ballot_sync(0xffffffffu, hit);
           const uint32_t ppos = __shfl_up_sync(0xffffffffu, pos, 1);
           const bool cont = mk_runs && hit && lane > 0u && ((hb >> (lane - 1u)) & 1u) && ppos + 1u == pos;
           const uint32_t cb = __ballot_sync(0xffffffffu, cont);
