@@ -1552,7 +1552,7 @@ static cudaError_t run_build(BuildCtx& bc) {
     if (e != cudaSuccess) return e;
   }
   if (bc.nsub) {
-    if (DIM <= 4 && bc.subtree != 1)
+    if (DIM <= 3 && bc.subtree != 1)
       return launch_subtree_sorted(bc.evs, bc.subs, bc.nsub, bc.input, b0, b1, bc.tab, bc.err, DIM, bc.subn,
                                    bc.stream);
     k_subtree<DIM><<<bc.nsub, ST, smem, bc.stream>>>(bc.evs, bc.subs, bc.input, b0, b1, bc.tab, bc.err);
@@ -1564,9 +1564,9 @@ static cudaError_t run_build(BuildCtx& bc) {
 uint32_t build_global_levels(uint32_t n, int dim, int subn) {
   if (n == 0) return 0;
   const Geom g = make_geom(n);
-  // the global levels stop where every interval fits the subtree kernel:
-  // the presorted-list kernel's size, which the radix kernel also takes
-  const uint32_t cap = (uint32_t)(dim <= 4 ? sorted_sub_capacity(subn) : sub_capacity(dim));
+  // the global levels stop where every interval fits the subtree kernel
+  // (dims 1-3: the presorted-list kernel's size, which the radix kernel also takes)
+  const uint32_t cap = (uint32_t)(dim <= 3 ? sorted_sub_capacity(subn) : sub_capacity(dim));
   uint32_t d0 = 0;
   while (seg_len(g, d0, 0) > cap) ++d0;
   return d0;

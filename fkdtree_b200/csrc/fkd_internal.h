@@ -131,7 +131,7 @@ struct BuildCtx {
 // subn: the presorted-list kernel's subtree size (512 or 1,024; 0 = 1,024).
 uint32_t build_global_levels(uint32_t n, int dim, int subn = 0);
 int sub_capacity(int dim);
-int sorted_sub_capacity(int subn = 0);  // largest subtree of the presorted-list kernel
+int sorted_sub_capacity(int subn = 0);  // largest subtree of the presorted-list kernel (dims 1-3)
 constexpr uint32_t HIST_BINS = 2048;  // global digit histogram per segment
 #ifndef FKD_PART_PIPT
 #define FKD_PART_PIPT 4
@@ -139,7 +139,7 @@ constexpr uint32_t HIST_BINS = 2048;  // global digit histogram per segment
 constexpr uint32_t PART_TILE = 256 * FKD_PART_PIPT;  // records per partition CTA
 constexpr uint32_t HIST_STEP = 2048;  // digit-pass tile granularity
 cudaError_t launch_build(BuildCtx& bc, int dim);
-// fkd_subtree_sort.cu: the subtree kernel by presorted lists (dims 1-4)
+// fkd_subtree_sort.cu: the subtree kernel by presorted lists (dims 1-3)
 cudaError_t launch_subtree_sorted(const EvDesc* evs, const uint2* subs, uint32_t nsub, CSoA in, CSoA b0, CSoA b1,
                                   Table tab, uint32_t* err, int dim, int subn, cudaStream_t stream);
 // The shared-memory subtree kernel alone, for events whose d0 is 0 (reads

@@ -1,5 +1,5 @@
 // fkd_subtree_sort.cu -- the shared-memory subtree kernel by presorted lists
-// (dims 1-4; in 4D the fourth coordinate rides in the node's w word).
+// (dims 1-3).
 //
 // Same contract as k_subtree (fkd_build.cu): one CTA finishes every level
 // below a subtree root of at most SUBN points and writes its nodes.  Instead
@@ -94,16 +94,13 @@ __device__ __forceinline__ void st4(unsigned long long* p, const unsigned long l
 
 template <int DIM, int XN>
 struct XCfg {
-  // recs | eofr | lists (DIM x 2 buffers) | seg (2 buffers) | side | scratch (sort keys; during the
-  // levels the scan -- SCANW words per slot -- then the two segment tables)
-  static constexpr uint32_t SCANW = DIM == 4 ? 4u : 2u;
+  // recs | eofr | lists (DIM x 2 buffers) | seg (2 buffers) | side | scratch (sort keys, later scans)
   static constexpr size_t recs = (size_t)(DIM + 1) * XN * 4;
   static constexpr size_t eofr = (size_t)XN * 2;
   static constexpr size_t lists = (size_t)DIM * 2 * XN * 2;
   static constexpr size_t seg = 2ull * XN * 2;
   static constexpr size_t side = XN;
-  static constexpr size_t scratch = (size_t)(SCANW + 2) * XN * 4 > 2ull * XN * 8 ? (size_t)(SCANW + 2) * XN * 4
-                                                                                : 2ull * XN * 8;
+  static constexpr size_t scratch = 2ull * XN * 8;
   static constexpr size_t smem = recs + eofr + lists + seg + side + scratch;
 };
 
@@ -246,64 +243,6 @@ __device__ uint2 cta_scan2(const uint2 (&val)[XPPT], uint2* sc, uint2* wtot) {
   return tot;
 }
 
-// The same for XN uint4 values (the three other lists of a 4D subtree).
-template <int XN>
-__device__ uint4 cta_scan4(const uint4 (&val)[XPPT], uint4* sc, uint4* wtot) {
-  constexpr int XW = XN / XPPT / 32;  // warps
-  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-  uint4 a = make_uint4(0u, 0u, 0u, 0u);
-#pragma unroll
-  for (int k = 0; k < XPPT; ++k) {
-    a.x += val[k].x;
-    a.y += val[k].y;
-    a.z += val[k].z;
-    a.w += val[k].w;
-  }
-  uint4 in = a;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const uint32_t yx = __shfl_up_sync(0xffffffffu, in.x, o), yy = __shfl_up_sync(0xffffffffu, in.y, o);
-    const uint32_t yz = __shfl_up_sync(0xffffffffu, in.z, o), yw = __shfl_up_sync(0xffffffffu, in.w, o);
-    if (lane >= (uint32_t)o) {
-      in.x += yx;
-      in.y += yy;
-      in.z += yz;
-      in.w += yw;
-    }
-  }
-  if (lane == 31u) wtot[warp] = in;
-  __syncthreads();
-  if (warp == 0) {
-    const uint4 w = lane < (uint32_t)XW ? wtot[lane] : make_uint4(0u, 0u, 0u, 0u);
-    uint4 t = w;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t yx = __shfl_up_sync(0xffffffffu, t.x, o), yy = __shfl_up_sync(0xffffffffu, t.y, o);
-      const uint32_t yz = __shfl_up_sync(0xffffffffu, t.z, o), yw = __shfl_up_sync(0xffffffffu, t.w, o);
-      if (lane >= (uint32_t)o) {
-        t.x += yx;
-        t.y += yy;
-        t.z += yz;
-        t.w += yw;
-      }
-    }
-    if (lane < (uint32_t)XW) wtot[lane] = make_uint4(t.x - w.x, t.y - w.y, t.z - w.z, t.w - w.w);
-    if (lane == 31u) wtot[32] = t;
-  }
-  __syncthreads();
-  const uint4 wb = wtot[warp];
-  uint4 r = make_uint4(wb.x + in.x - a.x, wb.y + in.y - a.y, wb.z + in.z - a.z, wb.w + in.w - a.w);
-#pragma unroll
-  for (int k = 0; k < XPPT; ++k) {
-    sc[threadIdx.x * XPPT + k] = r;  // 16-byte stores
-    r.x += val[k].x;
-    r.y += val[k].y;
-    r.z += val[k].z;
-    r.w += val[k].w;
-  }
-  return wtot[32];
-}
-
 // Segment (d, t) of the event in subtree-local slots: start, length, rank.
 __device__ __forceinline__ void seg_local(const Geom& g, uint32_t d, uint32_t t, uint32_t base, uint32_t& ls,
                                           uint32_t& m, uint32_t& k) {
@@ -334,7 +273,7 @@ __device__ __forceinline__ void seg_unpack(uint32_t w, uint32_t& ls, uint32_t& m
 }  // namespace
 
 template <int DIM, int XN>
-__global__ void __launch_bounds__(XN / XPPT, (DIM == 4 ? 3 : 4) * 1024 / XN) k_subtree_sorted(const EvDesc* __restrict__ evs,
+__global__ void __launch_bounds__(XN / XPPT, 4096 / XN) k_subtree_sorted(const EvDesc* __restrict__ evs,
                                                            const uint2* __restrict__ subs, CSoA src_in, CSoA src_b0,
                                                            CSoA src_b1, Table tab_all, uint32_t* __restrict__ err) {
   constexpr int XST = XN / XPPT;  // threads
@@ -346,10 +285,8 @@ __global__ void __launch_bounds__(XN / XPPT, (DIM == 4 ? 3 : 4) * 1024 / XN) k_s
   uint16_t* segb = (uint16_t*)(smem + Cfg::recs + Cfg::eofr + Cfg::lists);  // [2][XN]
   uint8_t* side = smem + Cfg::recs + Cfg::eofr + Cfg::lists + Cfg::seg;
   unsigned long long* keys = (unsigned long long*)(smem + Cfg::recs + Cfg::eofr + Cfg::lists + Cfg::seg + Cfg::side);
-  uint2* scan = (uint2*)keys;  // after the sorts (dims 1-3: two lists' flags per slot)
-  uint4* scan4 = (uint4*)keys;  // 4D: three lists' flags per slot
+  uint2* scan = (uint2*)keys;  // after the sorts
   __shared__ uint2 wtot[33];  // per-warp scan totals (XW <= 32)
-  __shared__ uint4 wtot4[DIM == 4 ? 33 : 1];
 
   const uint2 sb = subs[blockIdx.x];
   const EvDesc ev = evs[sb.x];
@@ -485,7 +422,7 @@ __global__ void __launch_bounds__(XN / XPPT, (DIM == 4 ? 3 : 4) * 1024 / XN) k_s
   // 3. levels.  Each level's segments (start, length, pivot rank) sit in a
   // table of packed words, written during the level before (two buffers in
   // the sort keys' space past the scan's)
-  uint32_t* segt = (uint32_t*)keys + Cfg::SCANW * XN;
+  uint32_t* segt = (uint32_t*)keys + 2u * XN;
   int cur[4] = {0, 0, 0, 0};  // which buffer of each list is current
   int sbuf = 0;
   for (uint32_t p = threadIdx.x; p < (uint32_t)XN; p += XST) segb[p] = p < nloc ? 0u : GAP;
@@ -541,7 +478,7 @@ __global__ void __launch_bounds__(XN / XPPT, (DIM == 4 ? 3 : 4) * 1024 / XN) k_s
         v.x = rec[0];
         v.y = DIM > 1 ? rec[1] : 0u;
         v.z = DIM > 2 ? rec[2] : 0u;
-        v.w = DIM > 3 ? rec[3] : rec[DIM];  // 4D: the fourth coordinate rides in w, the id in tab.ids
+        v.w = rec[DIM];
         const uint32_t node = (1u << d) - 1u + t0 + u;
         tab.nodes[node] = v;
         tab.ids[node] = rec[DIM];
@@ -560,8 +497,8 @@ __global__ void __launch_bounds__(XN / XPPT, (DIM == 4 ? 3 : 4) * 1024 / XN) k_s
     __syncthreads();
     // (b) stable partition of the other lists: flags (left | right << 16), scan
     uint2 val[XPPT];
-    uint32_t ra[XPPT], rb[XPPT], rc[XPPT], v3[XPPT];
-    const uint32_t o1 = (c + 1u) % DIM, o2 = (c + 2u) % DIM, o3 = (c + 3u) % DIM;
+    uint32_t ra[XPPT], rb[XPPT];
+    const uint32_t o1 = (c + 1u) % DIM, o2 = (c + 2u) % DIM;
     const uint16_t* l1 = lists + ((size_t)o1 * 2 + cur[o1]) * XN;
     const uint16_t* l2 = lists + ((size_t)o2 * 2 + cur[o2]) * XN;
     ld4(l1 + pb, ra);
@@ -571,40 +508,23 @@ __global__ void __launch_bounds__(XN / XPPT, (DIM == 4 ? 3 : 4) * 1024 / XN) k_s
 #pragma unroll
       for (int q = 0; q < XPPT; ++q) rb[q] = 0u;
     }
-    if constexpr (DIM == 4) {
-      ld4(lists + ((size_t)o3 * 2 + cur[o3]) * XN + pb, rc);
-    } else {
-#pragma unroll
-      for (int q = 0; q < XPPT; ++q) rc[q] = 0u;
-    }
 #pragma unroll
     for (int q = 0; q < XPPT; ++q) {
       const bool live = uu[q] != GAP;
       if (!live) ra[q] = 0u;
       rb[q] = (live && DIM > 2) ? rb[q] : 0u;
-      rc[q] = (live && DIM > 3) ? rc[q] : 0u;
       const uint8_t s1 = live ? side[ra[q]] : SP;
       const uint8_t s2 = (live && DIM > 2) ? side[rb[q]] : SP;
-      const uint8_t s3 = (live && DIM > 3) ? side[rc[q]] : SP;
       val[q].x = (s1 == SL ? 1u : 0u) | (s1 == SR ? 0x10000u : 0u);
       val[q].y = (s2 == SL ? 1u : 0u) | (s2 == SR ? 0x10000u : 0u);
-      v3[q] = (s3 == SL ? 1u : 0u) | (s3 == SR ? 0x10000u : 0u);
     }
-    if constexpr (DIM == 4) {
-      uint4 v4[XPPT];
-#pragma unroll
-      for (int q = 0; q < XPPT; ++q) v4[q] = make_uint4(val[q].x, val[q].y, v3[q], 0u);
-      cta_scan4<XN>(v4, scan4, wtot4);
-    } else {
-      cta_scan2<XN>(val, scan, wtot);
-    }
+    cta_scan2<XN>(val, scan, wtot);
     __syncthreads();
     // (c) scatter into the other buffers
     uint16_t* n1 = lists + ((size_t)o1 * 2 + (cur[o1] ^ 1)) * XN;
     uint16_t* n2 = lists + ((size_t)o2 * 2 + (cur[o2] ^ 1)) * XN;
-    uint16_t* n3 = lists + ((size_t)o3 * 2 + (cur[o3] ^ 1)) * XN;
     uint2 sat[XPPT];
-    if constexpr (DIM != 4) {
+    {
       const uint4 a0 = reinterpret_cast<const uint4*>(scan + pb)[0], a1 = reinterpret_cast<const uint4*>(scan + pb)[1];
       sat[0] = make_uint2(a0.x, a0.y);
       sat[1] = make_uint2(a0.z, a0.w);
@@ -617,32 +537,8 @@ __global__ void __launch_bounds__(XN / XPPT, (DIM == 4 ? 3 : 4) * 1024 / XN) k_s
       if (u == GAP) continue;
       uint32_t ls, m, k;
       seg_unpack(T[u], ls, m, k);
-      uint2 at, st;
-      uint32_t at3 = 0u, st3 = 0u;
-      if constexpr (DIM == 4) {
-        const uint4 a4 = scan4[pb + q], s4 = scan4[ls];
-        at = make_uint2(a4.x, a4.y);
-        st = make_uint2(s4.x, s4.y);
-        at3 = a4.z;
-        st3 = s4.z;
-      } else {
-        at = sat[q];
-        st = scan[ls];
-      }
+      const uint2 at = sat[q], st = scan[ls];
       // destinations stay inside the segment's child; anything else is a broken invariant
-      if constexpr (DIM == 4) {
-        uint32_t q3 = 0xffffffffu;
-        if (v3[q] & 0xffffu)
-          q3 = ls + ((at3 & 0xffffu) - (st3 & 0xffffu));
-        else if (v3[q])
-          q3 = ls + k + 1u + ((at3 >> 16) - (st3 >> 16));
-        if (q3 != 0xffffffffu) {
-          if (q3 < ls + m)
-            n3[q3] = (uint16_t)rc[q];
-          else
-            atomicOr(err, ERRB_INTERNAL);
-        }
-      }
       uint32_t q1 = 0xffffffffu, q2 = 0xffffffffu;
       if (val[q].x & 0xffffu)
         q1 = ls + ((at.x & 0xffffu) - (st.x & 0xffffu));
@@ -669,7 +565,6 @@ __global__ void __launch_bounds__(XN / XPPT, (DIM == 4 ? 3 : 4) * 1024 / XN) k_s
     }
     cur[o1] ^= 1;
     if (DIM > 2) cur[o2] ^= 1;
-    if (DIM > 3) cur[o3] ^= 1;
     sbuf ^= 1;
     __syncthreads();
   }
@@ -707,7 +602,6 @@ cudaError_t launch_subtree_sorted(const EvDesc* evs, const uint2* subs, uint32_t
     case 1: return run_sorted_n<1>(subn, evs, subs, nsub, in, b0, b1, tab, err, stream);
     case 2: return run_sorted_n<2>(subn, evs, subs, nsub, in, b0, b1, tab, err, stream);
     case 3: return run_sorted_n<3>(subn, evs, subs, nsub, in, b0, b1, tab, err, stream);
-    case 4: return run_sorted_n<4>(subn, evs, subs, nsub, in, b0, b1, tab, err, stream);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -250,7 +250,7 @@ FKD_API fkd_status fkd_sync(fkd_tree h);
  *                   one warp orders them by (coordinate, id), instead of more
  *                   digit passes
  *   "subtree_size"  (0, 512 or 1024; 0 = 1024): the largest subtree the
- *                   presorted-list kernel finishes in shared memory;
+ *                   presorted-list kernel (dims 1-3) finishes in shared memory;
  *                   smaller subtrees take one more global level.  Re-plans at
  *                   the next build.
  *   "lin_pass"      (0/1, default 1): a segment's first digit pass bins its
@@ -293,8 +293,8 @@ FKD_API fkd_status fkd_batch_destroy(fkd_batch b);
  *   "search_big_n", "search_lanes_big"  digest search: events of at least
  *                  search_big_n points search with search_lanes_big lanes per
  *                  box in a launch of their own (0: one launch for all)
- *   "subtree"      shared-memory subtree kernel: 0 auto (presorted lists),
- *                  1 radix select, 2 lists (both take the same subtrees)
+ *   "subtree"      shared-memory subtree kernel: 0 auto (presorted lists for
+ *                  dims 1-3, radix select for dim 4), 1 radix select, 2 lists
  *   "small_fix", "lin_pass", "search_bucket", "search_bucket_lanes",
  *   "subtree_size"  as fkd_set_param's
  *                  ("subtree_size" re-plans the batch)

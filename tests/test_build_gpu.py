@@ -118,8 +118,7 @@ def test_large_clustered_build_properties(cuda):
 
 @pytest.mark.parametrize("subtree", [1, 2])
 @pytest.mark.parametrize("dim,kind", [(1, "uniform"), (2, "uniform"), (3, "uniform"), (3, "grid"), (2, "grid"),
-                                      (3, "signed_zero"), (3, "sparse_ids"), (4, "uniform"), (4, "grid"),
-                                      (4, "signed_zero")])
+                                      (3, "signed_zero"), (3, "sparse_ids")])
 def test_subtree_kernels_agree(cuda, subtree, dim, kind):
     """Both shared-memory subtree kernels (radix select, presorted lists) give
     the oracle's tables, on ties, signed zeros, and ids far apart."""
@@ -161,7 +160,7 @@ def test_build_pivot_ties_resolved_by_id(cuda, q, dim):
 
 
 @pytest.mark.parametrize("subn", [512, 1024])
-@pytest.mark.parametrize("dim", [1, 2, 3, 4])
+@pytest.mark.parametrize("dim", [1, 2, 3])
 @pytest.mark.parametrize("n", [511, 512, 513, 1023, 1025, 70_001])
 def test_build_presorted_subtree_sizes(cuda, subn, dim, n):
     """Both sizes of the presorted-list subtree kernel ("subtree_size") give
@@ -178,7 +177,7 @@ def test_build_presorted_subtree_sizes(cuda, subn, dim, n):
 
 
 @pytest.mark.parametrize("subn", [512, 1024])
-@pytest.mark.parametrize("dim", [1, 2, 3, 4])
+@pytest.mark.parametrize("dim", [1, 2, 3])
 @pytest.mark.parametrize("kind", ["wide", "near_zero", "long_runs", "short_runs"])
 def test_build_presorted_subtree_key_paths(cuda, subn, dim, kind):
     """The presorted-list kernel's sort keys: ranges of order bits far wider
