@@ -170,8 +170,14 @@ __device__ __forceinline__ void copy_runs(const uint32_t* st, const uint32_t* pr
   }
 }
 
+// resident CTAs k_search is compiled for: 8 keeps the recording count pass at
+// 64 registers (measured on one B200, 16M / 1M-box search: 1 / 5 / 8 / 10 / 12
+// -> 21.7 / 21.7 / 21.3 / 24.6 / 24.9 ms count pass)
+#ifndef FKD_QMINB
+#define FKD_QMINB 8
+#endif
 template <int DIM, int MODE, bool REC = false>
-__global__ void __launch_bounds__(QT) k_search(SearchCtx sc, uint32_t cap) {
+__global__ void __launch_bounds__(QT, FKD_QMINB) k_search(SearchCtx sc, uint32_t cap) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int JN = REC ? JOBS / 2 : JOBS;  // the recording count pass flushes twice as often (occupancy)
   __shared__ uint32_t jst[QW][JN];   // in-order start of each buffered subtree (write pass, recording count)
