@@ -564,6 +564,8 @@ __global__ void __launch_bounds__(GT, FKD_PART_MINB) k_partition(uint32_t d, con
   const uint32_t t0 = start + t * PTILE;
   const uint32_t t1 = min(start + len, t0 + (uint32_t)PTILE);
   const unsigned long long klo = sel[s].klo, khi = sel[s].khi;
+  const uint32_t vlo = (uint32_t)(klo >> 32), vhi = (uint32_t)(khi >> 32);
+  const bool vonly = (uint32_t)klo == 0u && (uint32_t)khi == 0xffffffffu;
   const uint32_t cnt = sel[s].cnt;
   const bool small = sel[s].small != 0u;
   if (threadIdx.x == 0 && !sel[s].done) atomicOr(err, ERRB_INTERNAL);  // the select ran out of passes
@@ -590,8 +592,13 @@ __global__ void __launch_bounds__(GT, FKD_PART_MINB) k_partition(uint32_t d, con
 #pragma unroll
         for (int w = 0; w < DIM; ++w) nan |= is_nan_bits(rec[k][w]);
       }
-      const uint64_t key = order_key(pick_coord<DIM>(rec[k], c), rec[k][DIM]);
-      cls = key < klo ? 0u : (key > khi ? 2u : 1u);
+      const uint32_t mv = mono_bits(pick_coord<DIM>(rec[k], c));
+      if (vonly) {  // the interval spans every id: the order bits decide
+        cls = mv < vlo ? 0u : (mv > vhi ? 2u : 1u);
+      } else {
+        const uint64_t key = ((uint64_t)mv << 32) | rec[k][DIM];
+        cls = key < klo ? 0u : (key > khi ? 2u : 1u);
+      }
     }
     if (cls == 1u) eqmask |= 1u << k;
     const uint32_t bl = __ballot_sync(0xffffffffu, cls == 0u);
