@@ -367,14 +367,15 @@ __global__ void __launch_bounds__(XN / XPPT, 4096 / XN) k_subtree_sorted(const E
       uint16_t* lc = lists + (size_t)c * 2 * XN;
       for (uint32_t q = threadIdx.x; q < nloc; q += XST) lc[q] = (uint16_t)(sk[q] & 0x3ffu);
       __syncthreads();
-      // runs of equal shifted keys: each run's first position re-orders it by
-      // the full key (the positions of a run are one block of the order)
+      // runs of equal shifted keys (the sorted keys' upper bits, still in sk):
+      // each run's first position re-orders it by the full key (the positions
+      // of a run are one block of the order)
       const uint32_t* cx = recs + (size_t)c * XN;
       for (uint32_t q = threadIdx.x; q < nloc; q += XST) {
-        const uint32_t mq = (mono_bits(cx[lc[q]]) - m0) >> sh;
-        if (q > 0u && ((mono_bits(cx[lc[q - 1u]]) - m0) >> sh) == mq) continue;  // not the start of a run
+        const uint32_t mq = sk[q] >> 10;
+        if (q > 0u && (sk[q - 1u] >> 10) == mq) continue;  // not the start of a run
         uint32_t e = q + 1u;
-        while (e < nloc && e - q <= TIE_RUN && ((mono_bits(cx[lc[e]]) - m0) >> sh) == mq) ++e;
+        while (e < nloc && e - q <= TIE_RUN && (sk[e] >> 10) == mq) ++e;
         if (e - q > TIE_RUN) {
           s_slow = 1u;
           continue;
