@@ -26,6 +26,8 @@
 //    rank counting for segments of at most 16 points -- and writes each node
 //    to the table as it is decided.  One HBM read + one table write for the
 //    bottom ~12 levels.
+#include <type_traits>
+
 #include "fkd_internal.h"
 #include "fkd_mlp.h"
 
@@ -297,17 +299,20 @@ __global__ void __launch_bounds__(GT, FKD_HIST_MINB) k_hist(uint32_t d, const Ev
   const uint32_t* X = src.base + (uint64_t)c * src.stride;
   uint32_t nbelow = 0u;  // verify pass: points below the predicted block
   uint32_t cmn = 0xffffffffu, cmx = 0u;  // smallest / largest candidate value key (id in the id phase)
-  // one value of the tile: the bin of a candidate
-  auto count = [&](uint32_t raw, uint32_t e) {
+  // one value of the tile: the bin of a candidate.  The binning mode (M: 0
+  // linear in the value, 1 key bits of the value, 2 id bits) is a template
+  // argument, so that the tile loop below is compiled once per mode
+  auto count = [&](auto M, uint32_t raw, uint32_t e) {
+    constexpr int mode = decltype(M)::value;
     const uint32_t mv = mono_bits(raw);
     if (verify && mv < vlo) ++nbelow;
     if (mv < vlo || mv > vhi) return;
     uint32_t dig;
-    if (lin) {
+    if constexpr (mode == 0) {
       dig = lin_bin(__uint_as_float(raw), vmin, scale);
       cmn = min(cmn, mv);
       cmx = max(cmx, mv);
-    } else if (vphase) {
+    } else if constexpr (mode == 1) {
       dig = (mv - vlo) >> shift;
       cmn = min(cmn, mv);
       cmx = max(cmx, mv);
@@ -327,7 +332,6 @@ __global__ void __launch_bounds__(GT, FKD_HIST_MINB) k_hist(uint32_t d, const Ev
   const uint32_t tlen = tend > tb ? tend - tb : 0u;
   uint32_t head = (uint32_t)(((16u - ((uint32_t)(uintptr_t)(X + tb) & 15u)) & 15u) >> 2);
   if (head > tlen) head = tlen;
-  if (threadIdx.x < head) count(__ldcs(X + tb + threadIdx.x), tb + threadIdx.x);
   const uint32_t vb0 = tb + head;
   const uint32_t nv = (tlen - head) >> 2;
   const uint4* X4 = reinterpret_cast<const uint4*>(X + vb0);
@@ -338,30 +342,36 @@ __global__ void __launch_bounds__(GT, FKD_HIST_MINB) k_hist(uint32_t d, const Ev
       q[u] = va < nv ? __ldcs(X4 + va) : make_uint4(0u, 0u, 0u, 0u);
     }
   };
-  auto take = [&](const uint4 (&q)[HLOADS], uint32_t v0) {
+  constexpr uint32_t HSTEP = (uint32_t)HLOADS * GT;
+  auto tile = [&](auto M) {
+    if (threadIdx.x < head) count(M, __ldcs(X + tb + threadIdx.x), tb + threadIdx.x);
+    // (two register buffers, the next round's loads in flight while this
+    // round is counted, measured slower: 0.714 vs 0.675 ms of digit passes
+    // per build; eight loads per round: 0.690 ms)
+    for (uint32_t v0 = 0; v0 < nv; v0 += HSTEP) {
+      uint4 q[HLOADS];
+      load(q, v0);
 #pragma unroll
-    for (int u = 0; u < HLOADS; ++u) {
-      const uint32_t va = v0 + u * GT + threadIdx.x;
-      if (va < nv) {
-        const uint32_t e = vb0 + 4u * va;
-        count(q[u].x, e);
-        count(q[u].y, e + 1u);
-        count(q[u].z, e + 2u);
-        count(q[u].w, e + 3u);
+      for (int u = 0; u < HLOADS; ++u) {
+        const uint32_t va = v0 + u * GT + threadIdx.x;
+        if (va < nv) {
+          const uint32_t e = vb0 + 4u * va;
+          count(M, q[u].x, e);
+          count(M, q[u].y, e + 1u);
+          count(M, q[u].z, e + 2u);
+          count(M, q[u].w, e + 3u);
+        }
       }
     }
+    const uint32_t tail0 = vb0 + 4u * nv;
+    if (tail0 + threadIdx.x < tend) count(M, __ldcs(X + tail0 + threadIdx.x), tail0 + threadIdx.x);
   };
-  constexpr uint32_t HSTEP = (uint32_t)HLOADS * GT;
-  // (two register buffers, the next round's loads in flight while this
-  // round is counted, measured slower: 0.714 vs 0.675 ms of digit passes
-  // per build; eight loads per round: 0.690 ms)
-  for (uint32_t v0 = 0; v0 < nv; v0 += HSTEP) {
-    uint4 q[HLOADS];
-    load(q, v0);
-    take(q, v0);
-  }
-  const uint32_t tail0 = vb0 + 4u * nv;
-  if (tail0 + threadIdx.x < tend) count(__ldcs(X + tail0 + threadIdx.x), tail0 + threadIdx.x);
+  if (lin)
+    tile(std::integral_constant<int, 0>{});
+  else if (vphase)
+    tile(std::integral_constant<int, 1>{});
+  else
+    tile(std::integral_constant<int, 2>{});
   if (verify) {
     for (int o = 16; o > 0; o >>= 1) nbelow += __shfl_xor_sync(0xffffffffu, nbelow, o);
     if (lane == 0 && nbelow) atomicAdd(&sel[s].below, nbelow);
