@@ -302,10 +302,12 @@ __global__ void __launch_bounds__(GT, FKD_HIST_MINB) k_hist(uint32_t d, const Ev
   // one value of the tile: the bin of a candidate.  The binning mode (M: 0
   // linear in the value, 1 key bits of the value, 2 id bits) is a template
   // argument, so that the tile loop below is compiled once per mode
-  auto count = [&](auto M, uint32_t raw, uint32_t e) {
+  auto count = [&](auto M, auto V, uint32_t raw, uint32_t e) {
     constexpr int mode = decltype(M)::value;
     const uint32_t mv = mono_bits(raw);
-    if (verify && mv < vlo) ++nbelow;
+    if constexpr (decltype(V)::value) {
+      if (mv < vlo) ++nbelow;
+    }
     if (mv < vlo || mv > vhi) return;
     uint32_t dig;
     if constexpr (mode == 0) {
@@ -343,8 +345,8 @@ __global__ void __launch_bounds__(GT, FKD_HIST_MINB) k_hist(uint32_t d, const Ev
     }
   };
   constexpr uint32_t HSTEP = (uint32_t)HLOADS * GT;
-  auto tile = [&](auto M) {
-    if (threadIdx.x < head) count(M, __ldcs(X + tb + threadIdx.x), tb + threadIdx.x);
+  auto tile = [&](auto M, auto V) {
+    if (threadIdx.x < head) count(M, V, __ldcs(X + tb + threadIdx.x), tb + threadIdx.x);
     // (two register buffers, the next round's loads in flight while this
     // round is counted, measured slower: 0.714 vs 0.675 ms of digit passes
     // per build; eight loads per round: 0.690 ms)
@@ -356,22 +358,30 @@ __global__ void __launch_bounds__(GT, FKD_HIST_MINB) k_hist(uint32_t d, const Ev
         const uint32_t va = v0 + u * GT + threadIdx.x;
         if (va < nv) {
           const uint32_t e = vb0 + 4u * va;
-          count(M, q[u].x, e);
-          count(M, q[u].y, e + 1u);
-          count(M, q[u].z, e + 2u);
-          count(M, q[u].w, e + 3u);
+          count(M, V, q[u].x, e);
+          count(M, V, q[u].y, e + 1u);
+          count(M, V, q[u].z, e + 2u);
+          count(M, V, q[u].w, e + 3u);
         }
       }
     }
     const uint32_t tail0 = vb0 + 4u * nv;
-    if (tail0 + threadIdx.x < tend) count(M, __ldcs(X + tail0 + threadIdx.x), tail0 + threadIdx.x);
+    if (tail0 + threadIdx.x < tend) count(M, V, __ldcs(X + tail0 + threadIdx.x), tail0 + threadIdx.x);
+  };
+  // and once per verify case (a learned bracket's verifying pass also counts
+  // the points below the predicted block)
+  auto tile_v = [&](auto M) {
+    if (verify)
+      tile(M, std::true_type{});
+    else
+      tile(M, std::false_type{});
   };
   if (lin)
-    tile(std::integral_constant<int, 0>{});
+    tile_v(std::integral_constant<int, 0>{});
   else if (vphase)
-    tile(std::integral_constant<int, 1>{});
+    tile_v(std::integral_constant<int, 1>{});
   else
-    tile(std::integral_constant<int, 2>{});
+    tile_v(std::integral_constant<int, 2>{});
   if (verify) {
     for (int o = 16; o > 0; o >>= 1) nbelow += __shfl_xor_sync(0xffffffffu, nbelow, o);
     if (lane == 0 && nbelow) atomicAdd(&sel[s].below, nbelow);
