@@ -210,24 +210,21 @@ __device__ uint2 cta_scan2(const uint2 (&val)[XPPT], uint2* sc, uint2* wtot) {
   }
   if (lane == 31u) wtot[warp] = make_uint2(ix, iy);
   __syncthreads();
-  if (warp == 0) {
-    uint2 w = lane < (uint32_t)XW ? wtot[lane] : make_uint2(0u, 0u);
-    uint32_t sx = w.x, sy = w.y;
+  // every warp scans the XW warp totals itself (one barrier, not two)
+  const uint2 w = lane < (uint32_t)XW ? wtot[lane] : make_uint2(0u, 0u);
+  uint32_t sx = w.x, sy = w.y;
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t yx = __shfl_up_sync(0xffffffffu, sx, o);
-      const uint32_t yy = __shfl_up_sync(0xffffffffu, sy, o);
-      if (lane >= (uint32_t)o) {
-        sx += yx;
-        sy += yy;
-      }
+  for (int o = 1; o < XW; o <<= 1) {
+    const uint32_t yx = __shfl_up_sync(0xffffffffu, sx, o);
+    const uint32_t yy = __shfl_up_sync(0xffffffffu, sy, o);
+    if (lane >= (uint32_t)o) {
+      sx += yx;
+      sy += yy;
     }
-    if (lane < (uint32_t)XW) wtot[lane] = make_uint2(sx - w.x, sy - w.y);  // exclusive warp bases
-    if (lane == 31u) wtot[32] = make_uint2(sx, sy);
   }
-  __syncthreads();
-  const uint2 wb = wtot[warp];
-  uint32_t rx = wb.x + ix - ax, ry = wb.y + iy - ay;
+  const uint32_t bx = __shfl_sync(0xffffffffu, sx - w.x, warp), by = __shfl_sync(0xffffffffu, sy - w.y, warp);
+  const uint2 tot = make_uint2(__shfl_sync(0xffffffffu, sx, XW - 1), __shfl_sync(0xffffffffu, sy, XW - 1));
+  uint32_t rx = bx + ix - ax, ry = by + iy - ay;
   uint32_t o[2 * XPPT];
 #pragma unroll
   for (int k = 0; k < XPPT; ++k) {
@@ -239,7 +236,6 @@ __device__ uint2 cta_scan2(const uint2 (&val)[XPPT], uint2* sc, uint2* wtot) {
   uint4* s4 = reinterpret_cast<uint4*>(sc + threadIdx.x * XPPT);
   s4[0] = make_uint4(o[0], o[1], o[2], o[3]);
   s4[1] = make_uint4(o[4], o[5], o[6], o[7]);
-  const uint2 tot = wtot[32];
   return tot;
 }
 
