@@ -844,6 +844,9 @@ constexpr int SELBINS = 2048;  // bins of a pass
 // threads: 512 for segments of more than SEL_FEW points, else 128 (short
 // CTAs: cheaper barriers, more of them resident to hide the loads)
 constexpr int SEL_FEW = 4096;
+// 1024 threads above SEL_MANY points: such a CTA holds up to 128 KB of values,
+// one per SM, so its own threads carry the loads in flight
+constexpr int SEL_MANY = 16384;
 
 template <int DIM, int SELT>
 __global__ void __launch_bounds__(SELT) k_select_small(uint32_t d, const EvDesc* __restrict__ evs,
@@ -1528,14 +1531,20 @@ static cudaError_t run_build(BuildCtx& bc) {
     if (small) {
       const size_t sm = (size_t)lp.maxlen * sizeof(uint32_t);
       const bool few = lp.maxlen <= (uint32_t)SEL_FEW;
-      cudaError_t e = few ? cudaFuncSetAttribute(k_select_small<DIM, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)sm)
-                          : cudaFuncSetAttribute(k_select_small<DIM, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)sm);
+      const bool many = lp.maxlen > (uint32_t)SEL_MANY;
+      cudaError_t e =
+          few ? cudaFuncSetAttribute(k_select_small<DIM, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)
+              : many ? cudaFuncSetAttribute(k_select_small<DIM, 1024>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)sm)
+                     : cudaFuncSetAttribute(k_select_small<DIM, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)sm);
       if (e != cudaSuccess) return e;
       if (few)
         k_select_small<DIM, 128><<<lp.nseg, 128, sm, bc.stream>>>(d, bc.evs, lp.segs, src, bc.sel, bc.err,
                                                                   bc.tiebuf != nullptr);
+      else if (many)
+        k_select_small<DIM, 1024><<<lp.nseg, 1024, sm, bc.stream>>>(d, bc.evs, lp.segs, src, bc.sel, bc.err,
+                                                                    bc.tiebuf != nullptr);
       else
         k_select_small<DIM, 512><<<lp.nseg, 512, sm, bc.stream>>>(d, bc.evs, lp.segs, src, bc.sel, bc.err,
                                                                   bc.tiebuf != nullptr);
