@@ -841,8 +841,9 @@ __global__ void k_small_fix(uint32_t d, const EvDesc* __restrict__ evs, const ui
 // digit passes of the k_hist select fix the pivot key exactly.
 constexpr int SEL_MAX = 32768;
 constexpr int SELBINS = 2048;  // bins of a pass
-// threads: 512 for segments of more than SEL_FEW points, else 128 (short
-// CTAs: cheaper barriers, more of them resident to hide the loads)
+// threads: 128 for segments of at most SEL_FEW points (short CTAs: cheaper
+// barriers, more of them resident to hide the loads), 512 up to SEL_MANY,
+// 1024 above
 constexpr int SEL_FEW = 4096;
 // 1024 threads above SEL_MANY points: such a CTA holds up to 128 KB of values,
 // one per SM, so its own threads carry the loads in flight
