@@ -94,7 +94,8 @@ __device__ __forceinline__ void st4(unsigned long long* p, const unsigned long l
 
 template <int DIM, int XN>
 struct XCfg {
-  // recs | eofr | lists (DIM x 2 buffers) | seg (2 buffers) | side | scratch (sort keys, later scans)
+  // recs | eofr | lists (DIM x 2 buffers) | seg (2 buffers) | side | scratch (sort keys, later the
+  // list levels' segment tables)
   static constexpr size_t recs = (size_t)(DIM + 1) * XN * 4;
   static constexpr size_t eofr = (size_t)XN * 2;
   static constexpr size_t lists = (size_t)DIM * 2 * XN * 2;
@@ -186,57 +187,67 @@ __device__ K* cta_sort(K* a, K* b) {
   return src;
 }
 
-// Exclusive scan of XN uint2 values, slots XPPT*tid .. XPPT*tid + XPPT - 1
-// per thread (in: per-slot values; out: written to sc).  Returns the totals.
+// Segmented exclusive scan of XN uint2 values (slots XPPT*tid ..
+// XPPT*tid + XPPT - 1 per thread): head[k] marks a slot that starts a new
+// segment; ex[k] is the sum of the values before slot k within its segment.
+// Everything stays in registers but the per-warp totals (one barrier).
 template <int XN>
-__device__ uint2 cta_scan2(const uint2 (&val)[XPPT], uint2* sc, uint2* wtot) {
-  constexpr int XW = XN / XPPT / 32;  // warps
+__device__ void cta_segscan2(const uint2 (&val)[XPPT], const bool (&head)[XPPT], uint2 (&ex)[XPPT],
+                             uint4* wtot) {
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-  uint32_t ax = 0u, ay = 0u;
+  // within the thread: prefixes since its last head
+  uint32_t rx = 0u, ry = 0u;
+  bool th = false;  // the thread holds a head
 #pragma unroll
   for (int k = 0; k < XPPT; ++k) {
-    ax += val[k].x;
-    ay += val[k].y;
-  }
-  uint32_t ix = ax, iy = ay;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const uint32_t yx = __shfl_up_sync(0xffffffffu, ix, o);
-    const uint32_t yy = __shfl_up_sync(0xffffffffu, iy, o);
-    if (lane >= (uint32_t)o) {
-      ix += yx;
-      iy += yy;
+    if (head[k]) {
+      rx = ry = 0u;
+      th = true;
     }
-  }
-  if (lane == 31u) wtot[warp] = make_uint2(ix, iy);
-  __syncthreads();
-  // every warp scans the XW warp totals itself (one barrier, not two)
-  const uint2 w = lane < (uint32_t)XW ? wtot[lane] : make_uint2(0u, 0u);
-  uint32_t sx = w.x, sy = w.y;
-#pragma unroll
-  for (int o = 1; o < XW; o <<= 1) {
-    const uint32_t yx = __shfl_up_sync(0xffffffffu, sx, o);
-    const uint32_t yy = __shfl_up_sync(0xffffffffu, sy, o);
-    if (lane >= (uint32_t)o) {
-      sx += yx;
-      sy += yy;
-    }
-  }
-  const uint32_t bx = __shfl_sync(0xffffffffu, sx - w.x, warp), by = __shfl_sync(0xffffffffu, sy - w.y, warp);
-  const uint2 tot = make_uint2(__shfl_sync(0xffffffffu, sx, XW - 1), __shfl_sync(0xffffffffu, sy, XW - 1));
-  uint32_t rx = bx + ix - ax, ry = by + iy - ay;
-  uint32_t o[2 * XPPT];
-#pragma unroll
-  for (int k = 0; k < XPPT; ++k) {
-    o[2 * k] = rx;
-    o[2 * k + 1] = ry;
+    ex[k] = make_uint2(rx, ry);
     rx += val[k].x;
     ry += val[k].y;
   }
-  uint4* s4 = reinterpret_cast<uint4*>(sc + threadIdx.x * XPPT);
-  s4[0] = make_uint4(o[0], o[1], o[2], o[3]);
-  s4[1] = make_uint4(o[4], o[5], o[6], o[7]);
-  return tot;
+  // across the warp: segmented inclusive scan of (tail sums, holds a head)
+  uint32_t sx = rx, sy = ry;
+  bool f = th;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t yx = __shfl_up_sync(0xffffffffu, sx, o);
+    const uint32_t yy = __shfl_up_sync(0xffffffffu, sy, o);
+    const bool yf = __shfl_up_sync(0xffffffffu, f, o);
+    if (lane >= (uint32_t)o) {
+      if (!f) {
+        sx += yx;
+        sy += yy;
+      }
+      f = f || yf;
+    }
+  }
+  if (lane == 31u) wtot[warp] = make_uint4(sx, sy, f ? 1u : 0u, 0u);
+  // the carry into this thread from the lanes before it (up to their last head)
+  uint32_t cx = __shfl_up_sync(0xffffffffu, sx, 1), cy = __shfl_up_sync(0xffffffffu, sy, 1);
+  bool cf = __shfl_up_sync(0xffffffffu, f, 1);
+  if (lane == 0u) {
+    cx = cy = 0u;
+    cf = false;
+  }
+  __syncthreads();
+  if (!cf) {
+    // no head in the lanes before: add the previous warps' tails back to the last head
+    for (int w = (int)warp - 1; w >= 0; --w) {
+      const uint4 t = wtot[w];
+      cx += t.x;
+      cy += t.y;
+      if (t.z) break;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < XPPT; ++k) {
+    if (head[k]) break;  // from the thread's first head on, the prefixes are its own
+    ex[k].x += cx;
+    ex[k].y += cy;
+  }
 }
 
 // Segment (d, t) of the event in subtree-local slots: start, length, rank.
@@ -281,8 +292,7 @@ __global__ void __launch_bounds__(XN / XPPT, 4096 / XN) k_subtree_sorted(const E
   uint16_t* segb = (uint16_t*)(smem + Cfg::recs + Cfg::eofr + Cfg::lists);  // [2][XN]
   uint8_t* side = smem + Cfg::recs + Cfg::eofr + Cfg::lists + Cfg::seg;
   unsigned long long* keys = (unsigned long long*)(smem + Cfg::recs + Cfg::eofr + Cfg::lists + Cfg::seg + Cfg::side);
-  uint2* scan = (uint2*)keys;  // after the sorts
-  __shared__ uint2 wtot[33];  // per-warp scan totals (XW <= 32)
+  __shared__ uint4 wseg[32];  // per-warp totals of the list levels' segmented scan
 
   const uint2 sb = subs[blockIdx.x];
   const EvDesc ev = evs[sb.x];
@@ -418,7 +428,7 @@ __global__ void __launch_bounds__(XN / XPPT, 4096 / XN) k_subtree_sorted(const E
   XPROF_T(tp2);
   // 3. levels.  Each level's segments (start, length, pivot rank) sit in a
   // table of packed words, written during the level before (two buffers in
-  // the sort keys' space past the scan's)
+  // the sort keys' space)
   uint32_t* segt = (uint32_t*)keys + 2u * XN;
   int cur[4] = {0, 0, 0, 0};  // which buffer of each list is current
   int sbuf = 0;
@@ -515,37 +525,36 @@ __global__ void __launch_bounds__(XN / XPPT, 4096 / XN) k_subtree_sorted(const E
       val[q].x = (s1 == SL ? 1u : 0u) | (s1 == SR ? 0x10000u : 0u);
       val[q].y = (s2 == SL ? 1u : 0u) | (s2 == SR ? 0x10000u : 0u);
     }
-    cta_scan2<XN>(val, scan, wtot);
-    __syncthreads();
-    // (c) scatter into the other buffers
+    // a slot starts a segment where the segment id changes (slot 0 always);
+    // segments are separated by gap slots, which carry no flags
+    bool head[XPPT];
+    head[0] = pb == 0u || (uint32_t)sg[pb - 1u] != uu[0];
+#pragma unroll
+    for (int q = 1; q < XPPT; ++q) head[q] = uu[q - 1] != uu[q];
+    uint2 at4[XPPT];  // flags before the slot within its segment
+    cta_segscan2<XN>(val, head, at4, wseg);
+    // (c) scatter into the other buffers (no barrier: the scan left each
+    // slot's prefix in its own registers)
     uint16_t* n1 = lists + ((size_t)o1 * 2 + (cur[o1] ^ 1)) * XN;
     uint16_t* n2 = lists + ((size_t)o2 * 2 + (cur[o2] ^ 1)) * XN;
-    uint2 sat[XPPT];
-    {
-      const uint4 a0 = reinterpret_cast<const uint4*>(scan + pb)[0], a1 = reinterpret_cast<const uint4*>(scan + pb)[1];
-      sat[0] = make_uint2(a0.x, a0.y);
-      sat[1] = make_uint2(a0.z, a0.w);
-      sat[2] = make_uint2(a1.x, a1.y);
-      sat[3] = make_uint2(a1.z, a1.w);
-    }
 #pragma unroll
     for (int q = 0; q < XPPT; ++q) {
       const uint32_t u = uu[q];
       if (u == GAP) continue;
       uint32_t ls, m, k;
       seg_unpack(T[u], ls, m, k);
-      const uint2 at = sat[q], st = scan[ls];
+      const uint2 at = at4[q];
       // destinations stay inside the segment's child; anything else is a broken invariant
       uint32_t q1 = 0xffffffffu, q2 = 0xffffffffu;
       if (val[q].x & 0xffffu)
-        q1 = ls + ((at.x & 0xffffu) - (st.x & 0xffffu));
+        q1 = ls + (at.x & 0xffffu);
       else if (val[q].x)
-        q1 = ls + k + 1u + ((at.x >> 16) - (st.x >> 16));
+        q1 = ls + k + 1u + (at.x >> 16);
       if (DIM > 2) {
         if (val[q].y & 0xffffu)
-          q2 = ls + ((at.y & 0xffffu) - (st.y & 0xffffu));
+          q2 = ls + (at.y & 0xffffu);
         else if (val[q].y)
-          q2 = ls + k + 1u + ((at.y >> 16) - (st.y >> 16));
+          q2 = ls + k + 1u + (at.y >> 16);
       }
       if (q1 != 0xffffffffu) {
         if (q1 < ls + m)
