@@ -108,14 +108,15 @@ struct XCfg {
 
 // Sorts XN keys (32- or 64-bit, ascending) with the whole CTA: bitonic sort
 // of 128 keys per warp in registers, then merge-path rounds through shared
-// memory.  Returns the buffer (a or b) that holds the result.
+// memory.  Returns the buffer (a or b) that holds the result.  Thread t
+// brings the keys of slots 4t .. 4t + 3 in v (cta_sort below loads them
+// from a; a caller that computes them passes them straight in, with no
+// pass through shared memory and no barrier before the sort).
 template <int XN, class K>
-__device__ K* cta_sort(K* a, K* b) {
+__device__ K* cta_sort_regs(K (&v)[4], K* a, K* b) {
   static_assert(XN >= 512 && XN <= 4096 && (XN & (XN - 1)) == 0, "sorted subtree size");
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-  K v[4];
   K* wbase = a + warp * 128u;
-  ld4(wbase + lane * 4u, v);
 #pragma unroll
   for (uint32_t k = 2; k <= 128; k <<= 1) {
 #pragma unroll
@@ -185,6 +186,14 @@ __device__ K* cta_sort(K* a, K* b) {
   }
   __syncthreads();
   return src;
+}
+
+template <int XN, class K>
+__device__ K* cta_sort(K* a, K* b) {
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  K v[4];
+  ld4(a + warp * 128u + lane * 4u, v);
+  return cta_sort_regs<XN, K>(v, a, b);
 }
 
 // Segmented exclusive scan of XN uint2 values (slots XPPT*tid ..
@@ -366,10 +375,15 @@ __global__ void __launch_bounds__(XN / XPPT, 4096 / XN) k_subtree_sorted(const E
       const uint32_t m0 = s_mn[c];
       const uint32_t rb = nloc ? 32u - (uint32_t)__clz(s_mx[c] - m0) : 0u;  // bit length of the range
       const uint32_t sh = rb > 21u ? rb - 21u : 0u;
-      for (uint32_t r = threadIdx.x; r < (uint32_t)XN; r += XST)
-        k32[r] = r < nloc ? ((((mono_bits(recs[c * XN + r]) - m0) >> sh) << 10) | r) : 0xffffffffu;
-      __syncthreads();
-      const uint32_t* sk = cta_sort<XN, uint32_t>(k32, k32 + XN);
+      // this thread's four slots (the sort's register layout) straight from the records
+      uint32_t kv[4];
+      ld4(recs + (size_t)c * XN + threadIdx.x * 4u, kv);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const uint32_t r = threadIdx.x * 4u + (uint32_t)i;
+        kv[i] = r < nloc ? ((((mono_bits(kv[i]) - m0) >> sh) << 10) | r) : 0xffffffffu;
+      }
+      const uint32_t* sk = cta_sort_regs<XN, uint32_t>(kv, k32, k32 + XN);
       uint16_t* lc = lists + (size_t)c * 2 * XN;
       for (uint32_t q = threadIdx.x; q < nloc; q += XST) lc[q] = (uint16_t)(sk[q] & 0x3ffu);
       __syncthreads();
