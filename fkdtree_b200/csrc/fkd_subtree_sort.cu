@@ -19,7 +19,9 @@
 //      order, so the pivot is list_c[ls + rank] -- no select at all; the
 //      elements before it go left, after it right.  list_c is already
 //      partitioned; each other list is partitioned stably (a block scan of
-//      left / right flags), which keeps it sorted inside the children.
+//      left / right flags, segmented at the segments' first slots so that
+//      every slot gets its rank inside its own segment), which keeps it
+//      sorted inside the children.
 //
 // The children's intervals [ls, ls + rank) and [ls + rank + 1, ls + m) are
 // exactly the heap-tree geometry (fkd_common.cuh), and the pivot slot becomes
