@@ -795,18 +795,22 @@ namespace {
 // launch of k_one, one copy back of its count and first ids, one wait -- in
 // place of staging, count pass, scan, write pass and their two waits.  Its
 // list is the level-order one (ascending heap index), which serves ordered
-// and unordered calls alike.  Returns FKD_ERR_STATE, without touching the
-// outputs, when the general path must answer instead: a NaN bound (whose
+// and unordered calls alike.  Sets *general (returning FKD_OK, outputs
+// untouched) when the general path must answer instead: a NaN bound (whose
 // meaning the general path defines), a frontier too wide for the warp, or
 // more results than its buffer holds.
 constexpr uint32_t ONE_CAP = 1u << 16;   // ids k_one writes
 constexpr uint32_t ONE_FIRST = 1024;     // ids copied back with the count
 fkd_status search_one(fkd_tree h, const float* mins, const float* maxs, uint64_t* offsets_out, uint32_t* ids_out,
-                      uint64_t capacity, uint64_t* total) {
+                      uint64_t capacity, uint64_t* total, bool* general) {
+  *general = false;
   OneBox bx;
   for (int c = 0; c < 4; ++c) bx.lo[c] = bx.hi[c] = 0.f;
   for (int c = 0; c < h->dim; ++c) {
-    if (mins[c] != mins[c] || maxs[c] != maxs[c]) return FKD_ERR_STATE;
+    if (mins[c] != mins[c] || maxs[c] != maxs[c]) {
+      *general = true;
+      return FKD_OK;
+    }
     bx.lo[c] = mins[c];
     bx.hi[c] = maxs[c];
   }
@@ -823,7 +827,10 @@ fkd_status search_one(fkd_tree h, const float* mins, const float* maxs, uint64_t
   FKD_CUDA(cudaMemcpyAsync(sl->hone, sl->one.p, (4 + first) * sizeof(uint32_t), cudaMemcpyDeviceToHost, L.st));
   FKD_CUDA(cudaStreamSynchronize(L.st));
   const uint64_t tot = sl->hone[0];
-  if (sl->hone[1] || (tot > cap && tot <= capacity)) return FKD_ERR_STATE;
+  if (sl->hone[1] || (tot > cap && tot <= capacity)) {
+    *general = true;
+    return FKD_OK;
+  }
   offsets_out[0] = 0;
   offsets_out[1] = tot;
   *total = tot;
@@ -853,8 +860,9 @@ fkd_status fkd_search(fkd_tree h, const float* mins, const float* maxs, uint64_t
   if (s != FKD_OK) return s;
   if (!offsets_out || !total) return fail(FKD_ERR_ARG, "null offsets_out or total");
   if (q == 1 && mem == FKD_MEM_HOST && h->search_one && h->n <= 0xffffffffull) {
-    s = search_one(h, mins, maxs, offsets_out, ids_out, capacity, total);
-    if (s != FKD_ERR_STATE) return s;
+    bool general = false;
+    s = search_one(h, mins, maxs, offsets_out, ids_out, capacity, total, &general);
+    if (s != FKD_OK || !general) return s;
   }
   DeviceScope ds(h->device);
   Lease L;
